@@ -1,0 +1,387 @@
+// extern "C" boundary (include/gpp.h).  Every entry point catches C++
+// exceptions and maps them to the status codes the header documents; the C++
+// API in include/gpu_preprocessor/ maps them back to the reference's
+// exception types.
+#include <chrono>
+#include <cmath>
+#include <memory>
+
+#include "folding.hpp"
+#include "presolve.hpp"
+
+struct gpp_record {
+  gpp::PresolveOutput out;
+  gpp::FoldingResult folding;
+  bool presolve_enabled = true;
+};
+
+namespace gpp {
+const char* last_error();
+}
+
+using gpp::check;
+
+namespace {
+
+template <class F>
+int guarded(F f) {
+  try {
+    int dev = 0;
+    if (cudaGetDeviceCount(&dev) != cudaSuccess || dev == 0) {
+      cudaGetLastError();
+      gpp::set_last_error("no CUDA device is available to the presolve engine");
+      return GPP_ERR_NO_DEVICE;
+    }
+    f();
+    gpp::set_last_error("");
+    return GPP_OK;
+  } catch (const gpp::CudaError& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_CUDA;
+  } catch (const std::length_error& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_LENGTH;
+  } catch (const std::invalid_argument& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_INVALID;
+  } catch (const std::exception& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_RUNTIME;
+  }
+}
+
+void validate_lp(const gpp_lp& lp) {
+  if (lp.A.rows < 0 || lp.A.cols < 0 || lp.A.nnz < 0) throw std::invalid_argument("negative LP dimensions");
+  if (lp.AT.rows != lp.A.cols || lp.AT.cols != lp.A.rows || lp.AT.nnz != lp.A.nnz)
+    throw std::invalid_argument("AT must be the transpose of A (dimension/nnz mismatch)");
+  if ((lp.A.cols && (!lp.c || !lp.l || !lp.u)) || (lp.A.rows && (!lp.AL || !lp.AU)) || !lp.A.rowPtr ||
+      !lp.AT.rowPtr || (lp.A.nnz && (!lp.A.colVal || !lp.A.nzVal || !lp.AT.colVal || !lp.AT.nzVal)))
+    throw std::invalid_argument("LP device pointer missing");
+}
+
+void fill_summary(gpp_summary* s, gpp_record* rec, double preprocessing_seconds) {
+  const gpp::PresolveOutput& o = rec->out;
+  *s = gpp_summary{};
+  s->original_rows = o.original_rows;
+  s->original_cols = o.original_cols;
+  s->reduced_rows = o.reduced_rows;
+  s->reduced_cols = o.reduced_cols;
+  s->reduced_nnz = o.reduced_nnz;
+  s->iterations = o.iterations;
+  s->stopped_at_iteration_limit = o.stopped_at_iteration_limit;
+  s->has_change = o.has_change;
+  s->has_infeasible = o.has_infeasible;
+  s->has_unbounded = o.has_unbounded;
+  s->presolve_enabled = rec->presolve_enabled;
+  s->folding_applied = rec->folding.applied;
+  s->owns_reduced_lp = o.owns_reduced;
+  s->elapsed_seconds = o.elapsed_seconds;
+  s->preprocessing_seconds = preprocessing_seconds;
+  s->obj_constant_delta = o.obj_constant_delta;
+  const gpp::WorkingLp& r = o.reduced;
+  s->reduced_lp = gpp_lp{{r.A.rows, r.A.cols, r.A.nnz, r.A.ptr, r.A.idx, r.A.val},
+                         {r.AT.rows, r.AT.cols, r.AT.nnz, r.AT.ptr, r.AT.idx, r.AT.val},
+                         r.c, r.AL, r.AU, r.l, r.u, r.obj, 0, nullptr};
+  s->record = rec;
+}
+
+void identity_output(const gpp_lp& lp, gpp::PresolveOutput& o) {
+  // run_optional_gpu_presolve with enable_presolve = false (folding.cu:145-170).
+  o.original_rows = o.reduced_rows = lp.A.rows;
+  o.original_cols = o.reduced_cols = lp.A.cols;
+  o.reduced_nnz = lp.A.nnz;
+  gpp::init_record(o.record, lp.A.rows, lp.A.cols);
+  o.reduced.A = gpp::DevCsr{lp.A.rows, lp.A.cols, lp.A.nnz, lp.A.rowPtr, lp.A.colVal, lp.A.nzVal};
+  o.reduced.AT = gpp::DevCsr{lp.AT.rows, lp.AT.cols, lp.AT.nnz, lp.AT.rowPtr, lp.AT.colVal, lp.AT.nzVal};
+  o.reduced.c = lp.c; o.reduced.AL = lp.AL; o.reduced.AU = lp.AU; o.reduced.l = lp.l; o.reduced.u = lp.u;
+  o.reduced.obj = lp.obj_constant;
+  o.owns_reduced = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gpp_default_params(gpp_params* p) {
+  *p = gpp_params{};
+  p->max_iters = 512;
+  p->max_time = HUGE_VAL;
+  p->verbose = 0;
+  p->record_postsolve_tape = 1;
+  p->record_postsolve_tape_cpu = 0;
+  p->enable_presolve = 1;
+  p->enable_folding = 1;
+  p->folding_tolerance = 1.0e-8;
+  p->feasibility_tol = 1.0e-6;
+  p->bound_tol = 1.0e-6;
+  p->zero_tol = 1.0e-10;
+  p->bound_strengthening_upper_relaxation_factor = 1.0;
+  p->bound_strengthening_max_rounds = 64;
+  p->bound_strengthening_max_bound_only_rounds = 64;
+  p->bound_strengthening_preserve_free_zero_cost = 1;
+  p->doubleton_equations_max_fill_in_proxy = 96;
+  p->doubleton_equations_scan = 1;
+  p->doubleton_equations_min_selected_per_batch = 256;
+  p->doubleton_equations_min_selected_ratio = 0.005;
+  p->doubleton_equations_max_batch_rounds = 0;
+  p->doubleton_equations_max_time = 0.0;
+  p->enable_infeasible_and_fixed_variables = 1;
+  p->enable_empty_rows = 1;
+  p->enable_singleton_rows = 1;
+  p->enable_infeasible_and_redundant_rows = 1;
+  p->enable_bound_strengthening = 1;
+  p->enable_parallel_rows = 1;
+  p->enable_empty_columns = 1;
+  p->enable_singleton_columns = 1;
+  p->enable_doubleton_equations = 1;
+  p->enable_dual_fix = 1;
+  p->dual_fix_max_nonzero_cost_col_degree = 128;
+  p->enable_parallel_columns = 1;
+  p->parallel_columns_max_abs_ratio = 2.0;
+  p->parallel_columns_scale_guard_max_group_size = 4;
+  p->parallel_columns_scale_guard_min_groups = 128;
+  p->enable_structure_specific_rules = 1;
+  p->enable_redundant_variable_bounds = 0;
+  p->enable_startup = 1;
+  p->bound_strengthening_bound_only_nnz_round_budget = 8000000;
+}
+
+int gpp_run_presolve(const gpp_lp* lp, const gpp_params* params, int keep_reduced_lp, gpp_summary* out) {
+  return guarded([&] {
+    if (!lp || !params || !out) throw std::invalid_argument("null argument");
+    validate_lp(*lp);
+    auto rec = std::make_unique<gpp_record>();
+    const auto t0 = std::chrono::steady_clock::now();
+    gpp::run_presolve(*lp, *params, rec->out);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (!keep_reduced_lp) {
+      rec->out.reduced.free_owned();
+      rec->out.reduced = gpp::WorkingLp{};
+      rec->out.owns_reduced = false;
+    }
+    fill_summary(out, rec.get(), secs);
+    rec.release();
+  });
+}
+
+int gpp_preprocess(const gpp_lp* lp, const gpp_params* params, gpp_summary* out) {
+  // folding::run_gpu_presolve_with_folding(lp, params, true, true) (folding.cu:172-213).
+  return guarded([&] {
+    if (!lp || !params || !out) throw std::invalid_argument("null argument");
+    validate_lp(*lp);
+    auto rec = std::make_unique<gpp_record>();
+    rec->presolve_enabled = params->enable_presolve != 0;
+    gpp::ctx().sync("before preprocessing timer");
+    check(cudaDeviceSynchronize(), "before preprocessing timer");
+    const auto t0 = std::chrono::steady_clock::now();
+    if (params->enable_folding) gpp::run_folding(*lp, params->folding_tolerance, rec->folding);
+    const gpp_lp& input = rec->folding.applied ? rec->folding.folded : *lp;
+    if (params->enable_presolve) gpp::run_presolve(input, *params, rec->out);
+    else identity_output(input, rec->out);
+    gpp::ctx().sync("preprocessing completion");
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    fill_summary(out, rec.get(), secs);
+    rec.release();
+  });
+}
+
+int gpp_postsolve_device(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
+                         const gpp_lp* original, double* x_org, double* y_org, double* z_org) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp_record* rec = summary->record;
+    if (rec->folding.applied) throw std::invalid_argument("folded summaries postsolve through gpp_postprocess");
+    gpp::run_postsolve(rec->out, x_red, y_red, z_red, original, x_org, y_org, z_org);
+  });
+}
+
+int gpp_postprocess(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
+                    const gpp_lp* original, double* x_out, double* y_out, double* z_out) {
+  // postsolve_and_unfold_to_host (folding.cu:215-261).
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp_record* rec = summary->record;
+    auto s = gpp::ctx().stream;
+    const int n0 = summary->original_cols, m0 = summary->original_rows;
+    if (!rec->presolve_enabled && !rec->folding.applied) {
+      auto copy = [&](double* dst, const double* src, int n) {
+        if (dst && src && n) check(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "copy identity");
+      };
+      copy(x_out, x_red, n0); copy(y_out, y_red, m0); copy(z_out, z_red, n0);
+      gpp::ctx().sync("identity postprocess");
+      return;
+    }
+    const int pn = rec->out.record.n0, pm = rec->out.record.m0;
+    gpp::DBuf<double> x(size_t(std::max(pn, 1)), s), y(size_t(std::max(pm, 1)), s), z(size_t(std::max(pn, 1)), s);
+    if (!rec->presolve_enabled) {
+      if (pn) { check(cudaMemcpyAsync(x.p, x_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "x");
+                check(cudaMemcpyAsync(z.p, z_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "z"); }
+      if (pm) check(cudaMemcpyAsync(y.p, y_red, sizeof(double) * pm, cudaMemcpyDeviceToDevice, s), "y");
+    } else {
+      const gpp_lp* model = rec->folding.applied ? &rec->folding.folded : original;
+      gpp::run_postsolve(rec->out, x_red, y_red, z_red, model, x.p, y.p, z.p);
+    }
+    if (rec->folding.applied) {
+      gpp::unfold_to_host(rec->folding, x.p, y.p, z.p, x_out, y_out, z_out);
+    } else {
+      if (x_out && pn) check(cudaMemcpyAsync(x_out, x.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "x d2h");
+      if (y_out && pm) check(cudaMemcpyAsync(y_out, y.p, sizeof(double) * pm, cudaMemcpyDeviceToHost, s), "y d2h");
+      if (z_out && pn) check(cudaMemcpyAsync(z_out, z.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "z d2h");
+    }
+    gpp::ctx().sync("postprocess");
+  });
+}
+
+void gpp_free_summary(gpp_summary* summary) {
+  if (!summary || !summary->record) {
+    if (summary) *summary = gpp_summary{};
+    return;
+  }
+  gpp_record* rec = summary->record;
+  try {
+    rec->out.reduced.free_owned();
+    gpp::free_folding(rec->folding);
+    delete rec;
+    gpp::ctx().sync("free summary");
+  } catch (...) {
+  }
+  *summary = gpp_summary{};
+}
+
+int gpp_export_maps(const gpp_summary* summary, int32_t* row_red2org, int32_t* col_red2org) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::Record& r = summary->record->out.record;
+    auto s = gpp::ctx().stream;
+    if (row_red2org && r.m) check(cudaMemcpyAsync(row_red2org, r.rows.p, 4 * size_t(r.m), cudaMemcpyDeviceToHost, s), "maps");
+    if (col_red2org && r.n) check(cudaMemcpyAsync(col_red2org, r.cols.p, 4 * size_t(r.n), cudaMemcpyDeviceToHost, s), "maps");
+    gpp::ctx().sync("export maps");
+  });
+}
+
+int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t* indices, int64_t* values, int64_t* fixed) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::Record& r = summary->record->out.record;
+    int64_t f = 0;
+    for (const auto& seg : r.fixed) f += seg.count;
+    if (records) *records = r.records;
+    if (indices) *indices = r.indices;
+    if (values) *values = r.values;
+    if (fixed) *fixed = f;
+  });
+}
+
+int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t* index_starts, int64_t* value_starts,
+                    int32_t* indices, double* vals, int32_t* fixed_idx, double* fixed_val) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::Record& r = summary->record->out.record;
+    int64_t rk = 0, ik = 0, vk = 0;
+    if (index_starts) index_starts[0] = 0;
+    if (value_starts) value_starts[0] = 0;
+    for (const auto& seg : r.segments) {
+      auto t = gpp::to_host(seg.types.p, size_t(seg.count));
+      auto is = gpp::to_host(seg.is.p, size_t(seg.count) + 1);
+      auto vs = gpp::to_host(seg.vs.p, size_t(seg.count) + 1);
+      auto id = gpp::to_host(seg.idx.p, size_t(seg.n_idx));
+      auto v = gpp::to_host(seg.val.p, size_t(seg.n_val));
+      for (int64_t k = 0; k < seg.count; ++k) {
+        if (types) types[rk + k] = t[size_t(k)];
+        if (index_starts) index_starts[rk + k + 1] = ik + is[size_t(k) + 1];
+        if (value_starts) value_starts[rk + k + 1] = vk + vs[size_t(k) + 1];
+      }
+      if (indices) std::copy(id.begin(), id.end(), indices + ik);
+      if (vals) std::copy(v.begin(), v.end(), vals + vk);
+      rk += seg.count; ik += seg.n_idx; vk += seg.n_val;
+    }
+    int64_t fk = 0;
+    for (const auto& seg : r.fixed) {
+      auto a = gpp::to_host(seg.idx.p, size_t(seg.count));
+      auto b = gpp::to_host(seg.val.p, size_t(seg.count));
+      if (fixed_idx) std::copy(a.begin(), a.end(), fixed_idx + fk);
+      if (fixed_val) std::copy(b.begin(), b.end(), fixed_val + fk);
+      fk += seg.count;
+    }
+  });
+}
+
+int gpp_row_activity_summary(const gpp_csr* A, const double* l, const double* u, double zero_tol,
+                             const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_degrees,
+                             double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf) {
+  return guarded([&] {
+    gpp::DevCsr M{A->rows, A->cols, A->nnz, A->rowPtr, A->colVal, A->nzVal};
+    gpp::invalidate_schedules();
+    gpp::row_activity_summary(M, l, u, zero_tol, keep_row, keep_col, live_degrees, min_fin, max_fin, min_inf,
+                              max_inf, gpp::ctx().stream);
+    gpp::ctx().sync("activity summary");
+  });
+}
+
+int gpp_live_stats(const gpp_csr* M, const uint8_t* keep_outer, const uint8_t* keep_inner, int32_t* degree,
+                   uint8_t* empty, uint8_t* singleton, int32_t* support, double* coefficient,
+                   unsigned long long* total) {
+  return guarded([&] {
+    gpp::DevCsr D{M->rows, M->cols, M->nnz, M->rowPtr, M->colVal, M->nzVal};
+    gpp::invalidate_schedules();
+    if (total) check(cudaMemsetAsync(total, 0, sizeof(*total), gpp::ctx().stream), "total");
+    gpp::live_stats_side(D, keep_outer, keep_inner, degree, empty, singleton, support, coefficient, total,
+                         gpp::ctx().stream);
+    gpp::ctx().sync("live stats");
+  });
+}
+
+int gpp_col_max_abs(const gpp_csr* AT, const uint8_t* keep_row, double* out) {
+  return guarded([&] {
+    gpp::DevCsr D{AT->rows, AT->cols, AT->nnz, AT->rowPtr, AT->colVal, AT->nzVal};
+    gpp::invalidate_schedules();
+    gpp::col_max_abs(D, keep_row, out, gpp::ctx().stream);
+    gpp::ctx().sync("col max");
+  });
+}
+
+int gpp_compact_and_transpose(const gpp_csr* A, const uint8_t* keep_row, const uint8_t* keep_col, gpp_csr* A_out,
+                              gpp_csr* AT_out) {
+  return guarded([&] {
+    auto s = gpp::ctx().stream;
+    gpp::DevCsr D{A->rows, A->cols, A->nnz, A->rowPtr, A->colVal, A->nzVal};
+    gpp::invalidate_schedules();
+    gpp::DBuf<int32_t> rmap(size_t(std::max(D.rows, 1)), s), cmap(size_t(std::max(D.cols, 1)), s);
+    const int m_new = gpp::build_old_to_new(keep_row, D.rows, rmap.p, s);
+    const int n_new = gpp::build_old_to_new(keep_col, D.cols, cmap.p, s);
+    gpp::DevCsr C = gpp::compact_csr(D, rmap.p, m_new, cmap.p, n_new, s);
+    gpp::DevCsr T = gpp::transpose_csr(C, s);
+    gpp::ctx().sync("compact and transpose");
+    *A_out = gpp_csr{C.rows, C.cols, C.nnz, C.ptr, C.idx, C.val};
+    *AT_out = gpp_csr{T.rows, T.cols, T.nnz, T.ptr, T.idx, T.val};
+  });
+}
+
+int gpp_parallel_row_hashes(const gpp_csr* A, const uint8_t* keep_row, const uint8_t* keep_col, int mode,
+                            uint64_t* hashes) {
+  return guarded([&] {
+    gpp::DevCsr D{A->rows, A->cols, A->nnz, A->rowPtr, A->colVal, A->nzVal};
+    gpp::invalidate_schedules();
+    gpp::parallel_row_hashes(D, keep_row, keep_col, mode, hashes, gpp::ctx().stream);
+    gpp::ctx().sync("row hashes");
+  });
+}
+
+void gpp_device_free(void* p) {
+  if (!p) return;
+  try {
+    cudaFreeAsync(p, gpp::ctx().stream);
+    gpp::ctx().sync("device free");
+  } catch (...) {
+  }
+}
+
+const char* gpp_last_error(void) { return gpp::last_error(); }
+
+uint64_t gpp_kernel_launches(int reset) {
+  const uint64_t v = gpp::launch_counter();
+  if (reset) gpp::launch_counter() = 0;
+  return v;
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+// Shared device/host plumbing of the B200 presolve engine: error handling,
+// the engine stream, stream-ordered buffers, launch accounting, and the
+// deterministic scan / reduction primitives every kernel family uses.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/gpp.h"
+
+namespace gpp {
+
+using offset_t = gpp_offset;
+constexpr int kThreads = 256;
+constexpr int kShortRow = 8;      // rows of live length <= 8: one thread per row
+constexpr int kLongRow = 1024;    // rows of live length > 1024: one block per row
+constexpr int kNumSMs = 148;      // B200
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct InvalidArgument : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct LengthError : std::length_error {
+  using std::length_error::length_error;
+};
+
+inline void check(cudaError_t e, const char* ctx) {
+  if (e != cudaSuccess) throw CudaError(std::string(ctx) + ": " + cudaGetErrorString(e));
+}
+
+// Kernel launch counter (per host thread) for the benchmark's launch report.
+uint64_t& launch_counter();
+
+#define GPP_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
+  do {                                                                              \
+    if ((grid) > 0) {                                                               \
+      kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                   \
+      ::gpp::check(cudaGetLastError(), #kernel);                                    \
+      ++::gpp::launch_counter();                                                    \
+    }                                                                               \
+  } while (0)
+
+inline int blocks_for(int64_t n, int threads = kThreads) {
+  const int64_t b = (n + threads - 1) / threads;
+  return int(b < 1 ? 0 : (b > 2147483647 ? 2147483647 : b));
+}
+// Grid for grid-stride kernels: enough blocks to fill all 148 SMs several
+// times over without launching more than the work needs.
+inline int grid_stride_blocks(int64_t n, int threads = kThreads, int per_sm = 8) {
+  const int64_t want = (n + threads - 1) / threads;
+  const int64_t cap = int64_t(kNumSMs) * per_sm;
+  return int(want < 1 ? 0 : (want < cap ? want : cap));
+}
+
+// ---------------------------------------------------------------------------
+// Engine context: one stream (blocking w.r.t. the legacy default stream so
+// caller work on stream 0 is ordered before ours), a stream-ordered memory
+// pool that keeps its memory between calls, and a pinned status block.
+struct Context {
+  cudaStream_t stream = nullptr;
+  int device = -1;
+  int32_t* host_status = nullptr;   // pinned, kStatusWords ints
+  static constexpr int kStatusWords = 64;
+  Context();
+  ~Context();
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
+  void sync(const char* ctx) { check(cudaStreamSynchronize(stream), ctx); }
+};
+Context& ctx();
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  DBuf() = default;
+  explicit DBuf(size_t count, cudaStream_t stream = nullptr) { alloc(count, stream); }
+  void alloc(size_t count, cudaStream_t stream = nullptr) {
+    release();
+    s = stream ? stream : ctx().stream;
+    n = count;
+    if (count) check(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s), "cudaMallocAsync");
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  T* release_ownership() {
+    T* q = p;
+    p = nullptr;
+    n = 0;
+    return q;
+  }
+  ~DBuf() { release(); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(std::exchange(o.p, nullptr)), n(std::exchange(o.n, 0)), s(o.s) {}
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = std::exchange(o.p, nullptr);
+      n = std::exchange(o.n, 0);
+      s = o.s;
+    }
+    return *this;
+  }
+  T* get() const { return p; }
+  void zero() {
+    if (n) check(cudaMemsetAsync(p, 0, n * sizeof(T), s), "cudaMemsetAsync");
+  }
+  void copy_from(const T* src, size_t count) {
+    if (count) check(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy d2d");
+  }
+};
+
+template <class T>
+T* dalloc(size_t count) {
+  T* p = nullptr;
+  if (count) check(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().stream), "cudaMallocAsync");
+  return p;
+}
+inline void dfree(void* p) {
+  if (p) cudaFreeAsync(p, ctx().stream);
+}
+
+template <class T>
+std::vector<T> to_host(const T* d, size_t count) {
+  std::vector<T> h(count);
+  if (count) {
+    check(cudaMemcpyAsync(h.data(), d, count * sizeof(T), cudaMemcpyDeviceToHost, ctx().stream), "d2h");
+    ctx().sync("d2h sync");
+  }
+  return h;
+}
+template <class T>
+T read_scalar(const T* d) {
+  T v{};
+  check(cudaMemcpyAsync(&v, d, sizeof(T), cudaMemcpyDeviceToHost, ctx().stream), "d2h scalar");
+  ctx().sync("d2h scalar sync");
+  return v;
+}
+
+// Status block: device ints zeroed per use, read back with one copy.
+struct Status {
+  int32_t* d = nullptr;
+  Status();
+  ~Status();
+  void clear(int words = Context::kStatusWords);
+  const int32_t* read(int words = Context::kStatusWords);
+};
+
+// ---------------------------------------------------------------------------
+// Scans (decoupled into three small kernels; deterministic, any length).
+// exclusive prefix sum of in[0..n) into out[0..n]; out[n] = total.  out may
+// alias in for n+1-sized storage only when in has n+1 slots.
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+
+// Canonical deterministic sum (chunks of 2048, 256-thread halving tree, chunk
+// totals added in order on the host).  Returns the value on the host.
+double det_sum(const double* v, int64_t n, cudaStream_t s);
+
+// Thread-local error message for the C ABI.
+void set_last_error(const std::string& s);
+
+}  // namespace gpp

@@ -1,0 +1,362 @@
+// Stream compaction / re-indexing of the working LP and the general transpose.
+//
+// Reference: apply_plan_to_working_lp / compact_csr_by_masks_gpu
+// (cpp/src/presolve/gpu_presolve.cu:95-436,715-770,1793-1930) and
+// transpose_csr64 (cpp/src/presolve/transpose64.cu:54-117).
+//
+// Materialisation compacts A and A^T with the same row/column maps.  A^T is
+// kept row-sorted, and the old->new maps are monotone, so compacting A^T gives
+// exactly cusparseCsr2cscEx2(compact(A)): the per-apply transpose becomes a
+// second streaming pass.  The general transpose below is only needed for an
+// input A^T that is not row-sorted and for matrices rebuilt by a rule.
+#include "engine.cuh"
+
+#include <algorithm>
+
+namespace gpp {
+
+namespace {
+
+__global__ void mask_to_int(const uint8_t* __restrict__ keep, int32_t n, int32_t* __restrict__ out) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = keep[i] != 0;
+}
+__global__ void prefix_to_map(const uint8_t* __restrict__ keep, const int32_t* __restrict__ prefix, int32_t n,
+                              int32_t* __restrict__ old_to_new) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    old_to_new[i] = keep[i] ? prefix[i] : -1;
+}
+
+// Count kept entries of kept rows: short rows by thread, medium by warp,
+// long by block (roles as in live.cu).
+__global__ void __launch_bounds__(kThreads)
+count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+           const int32_t* __restrict__ outer_map, const int32_t* __restrict__ inner_map,
+           const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
+           const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
+           int32_t* __restrict__ out_counts) {
+  __shared__ int scount[8];
+  const int b = blockIdx.x;
+  if (b < short_blocks) {
+    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
+      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
+      const int nr = outer_map[r];
+      if (nr < 0) continue;
+      int c = 0;
+      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) c += inner_map[idx[p]] >= 0;
+      out_counts[nr] = c;
+    }
+    return;
+  }
+  if (b < short_blocks + medium_blocks) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = medium_blocks * (kThreads / 32);
+    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
+      const int r = medium[q];
+      const int nr = outer_map[r];
+      if (nr < 0) continue;
+      int c = 0;
+      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) c += inner_map[idx[p]] >= 0;
+      for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+      if (lane == 0) out_counts[nr] = c;
+    }
+    return;
+  }
+  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+  for (int q = lb; q < counts[1]; q += nlong) {
+    const int r = longq[q];
+    const int nr = outer_map[r];
+    if (nr < 0) continue;  // block-uniform
+    int c = 0;
+    for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads) c += inner_map[idx[p]] >= 0;
+    for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+    if ((threadIdx.x & 31) == 0) scount[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < 8; ++w) c += scount[w];
+      out_counts[nr] = c;
+    }
+    __syncthreads();
+  }
+}
+
+// Stable copy of kept entries (order preserving), remapping inner indices.
+__global__ void __launch_bounds__(kThreads)
+copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+          const double* __restrict__ val, const int32_t* __restrict__ outer_map,
+          const int32_t* __restrict__ inner_map, const int32_t* __restrict__ medium,
+          const int32_t* __restrict__ longq, const int32_t* __restrict__ counts, int short_blocks,
+          int medium_blocks, const offset_t* __restrict__ out_ptr, int32_t* __restrict__ out_idx,
+          double* __restrict__ out_val) {
+  __shared__ int wcount[8];
+  const int b = blockIdx.x;
+  if (b < short_blocks) {
+    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
+      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
+      const int nr = outer_map[r];
+      if (nr < 0) continue;
+      offset_t w = out_ptr[nr];
+      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) {
+        const int c = inner_map[idx[p]];
+        if (c >= 0) { out_idx[w] = c; out_val[w] = val[p]; ++w; }
+      }
+    }
+    return;
+  }
+  if (b < short_blocks + medium_blocks) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = medium_blocks * (kThreads / 32);
+    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
+      const int r = medium[q];
+      const int nr = outer_map[r];
+      if (nr < 0) continue;
+      offset_t w = out_ptr[nr];
+      for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += 32) {
+        const offset_t p = chunk + lane;
+        const int c = p < ptr[r + 1] ? inner_map[idx[p]] : -1;
+        const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
+        if (c >= 0) {
+          const offset_t o = w + __popc(mask & ((1u << lane) - 1u));
+          out_idx[o] = c;
+          out_val[o] = val[p];
+        }
+        w += __popc(mask);
+      }
+    }
+    return;
+  }
+  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = lb; q < counts[1]; q += nlong) {
+    const int r = longq[q];
+    const int nr = outer_map[r];
+    if (nr < 0) continue;
+    offset_t w = out_ptr[nr];
+    for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += kThreads) {
+      const offset_t p = chunk + threadIdx.x;
+      const int c = p < ptr[r + 1] ? inner_map[idx[p]] : -1;
+      const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
+      if (lane == 0) wcount[warp] = __popc(mask);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int k = 0; k < 8; ++k) { before += k < warp ? wcount[k] : 0; total += wcount[k]; }
+      if (c >= 0) {
+        const offset_t o = w + before + __popc(mask & ((1u << lane) - 1u));
+        out_idx[o] = c;
+        out_val[o] = val[p];
+      }
+      w += total;
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void histogram(const int32_t* __restrict__ idx, offset_t nnz, int32_t* __restrict__ counts) {
+  for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * blockDim.x)
+    atomicAdd(counts + idx[p], 1);
+}
+__global__ void scatter_rows(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                             const double* __restrict__ val, int32_t* __restrict__ cursor,
+                             int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+    for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) {
+      const int q = atomicAdd(cursor + idx[p], 1);
+      out_idx[q] = r;
+      out_val[q] = val[p];
+    }
+}
+// Sort every row of (idx, val) by idx.  Rows of up to 32 entries: insertion
+// sort by one thread; up to 4096: bitonic sort in shared memory by one block;
+// longer: rank by counting (each entry's rank = number of smaller keys).
+__global__ void sort_rows_short(int rows, const offset_t* __restrict__ ptr, int32_t* idx, double* val) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const offset_t a = ptr[r], e = ptr[r + 1];
+    if (e - a > 32) continue;
+    for (offset_t i = a + 1; i < e; ++i) {
+      const int k = idx[i];
+      const double v = val[i];
+      offset_t j = i - 1;
+      while (j >= a && idx[j] > k) { idx[j + 1] = idx[j]; val[j + 1] = val[j]; --j; }
+      idx[j + 1] = k;
+      val[j + 1] = v;
+    }
+  }
+}
+__global__ void sort_rows_long(const int32_t* __restrict__ rows_list, const int32_t* __restrict__ count,
+                               const offset_t* __restrict__ ptr, int32_t* idx, double* val,
+                               int32_t* scratch_idx, double* scratch_val) {
+  __shared__ int skey[4096];
+  __shared__ int spos[4096];
+  for (int q = blockIdx.x; q < *count; q += gridDim.x) {
+    const int r = rows_list[q];
+    const offset_t a = ptr[r], e = ptr[r + 1];
+    const int len = int(e - a);
+    if (len <= 32) continue;
+    if (len <= 4096) {
+      int pow2 = 1;
+      while (pow2 < len) pow2 <<= 1;
+      for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
+        skey[i] = i < len ? idx[a + i] : 0x7fffffff;
+        spos[i] = i;
+      }
+      __syncthreads();
+      for (int k = 2; k <= pow2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
+            const int x = i ^ j;
+            if (x > i) {
+              const bool up = (i & k) == 0;
+              if ((skey[i] > skey[x]) == up) {
+                const int tk = skey[i]; skey[i] = skey[x]; skey[x] = tk;
+                const int tp = spos[i]; spos[i] = spos[x]; spos[x] = tp;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        scratch_idx[a + i] = skey[i];
+        scratch_val[a + i] = val[a + spos[i]];
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        idx[a + i] = scratch_idx[a + i];
+        val[a + i] = scratch_val[a + i];
+      }
+      __syncthreads();
+    } else {
+      for (offset_t i = a + threadIdx.x; i < e; i += blockDim.x) {
+        const int k = idx[i];
+        offset_t rank = 0;
+        for (offset_t j = a; j < e; ++j) rank += idx[j] < k;
+        scratch_idx[a + rank] = k;
+        scratch_val[a + rank] = val[i];
+      }
+      __syncthreads();
+      for (offset_t i = a + threadIdx.x; i < e; i += blockDim.x) {
+        idx[i] = scratch_idx[i];
+        val[i] = scratch_val[i];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void check_sorted(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                             int32_t* bad) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+    for (offset_t p = ptr[r] + 1; p < ptr[r + 1]; ++p)
+      if (idx[p - 1] >= idx[p]) { atomicExch(bad, 1); break; }
+}
+
+__global__ void gather_kernel(double* __restrict__ dst, const double* __restrict__ src,
+                              const int32_t* __restrict__ map, int32_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const int k = map[i];
+    if (k >= 0) dst[k] = src[i];
+  }
+}
+__global__ void compose_kernel(int32_t* __restrict__ next, const int32_t* __restrict__ prev,
+                               const int32_t* __restrict__ map, int32_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const int k = map[i];
+    if (k >= 0) next[k] = prev[i];
+  }
+}
+
+int roles_short(int rows) { return grid_stride_blocks(rows, kThreads, 16); }
+int roles_medium(int rows) { return std::min<int>(kNumSMs * 8, (rows + 7) / 8); }
+int roles_long(int rows) { return std::min<int>(kNumSMs * 4, rows); }
+
+}  // namespace
+
+int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cudaStream_t s) {
+  if (n == 0) return 0;
+  DBuf<int32_t> prefix(size_t(n) + 1, s);
+  GPP_LAUNCH(mask_to_int, grid_stride_blocks(n), kThreads, 0, s, keep, n, prefix.p);
+  exclusive_scan_i32(prefix.p, prefix.p, n, s);
+  GPP_LAUNCH(prefix_to_map, grid_stride_blocks(n), kThreads, 0, s, keep, prefix.p, n, old_to_new);
+  return read_scalar(prefix.p + n);
+}
+
+DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
+                   int32_t inner_new, cudaStream_t s) {
+  DevCsr out;
+  out.rows = outer_new;
+  out.cols = inner_new;
+  out.ptr = dalloc<offset_t>(size_t(outer_new) + 1);
+  if (outer_new == 0 || inner_new == 0 || M.nnz == 0) {
+    check(cudaMemsetAsync(out.ptr, 0, sizeof(offset_t) * (size_t(outer_new) + 1), s), "compact empty ptr");
+    return out;
+  }
+  const RowSchedule& sch = stored_schedule(M);
+  const int sb = roles_short(M.rows), mb = roles_medium(M.rows), lb = roles_long(M.rows);
+  DBuf<int32_t> counts(size_t(outer_new) + 1, s);
+  GPP_LAUNCH(count_kept, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map, sch.medium.p,
+             sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
+  exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
+  out.nnz = read_scalar(out.ptr + outer_new);
+  out.idx = dalloc<int32_t>(size_t(out.nnz));
+  out.val = dalloc<double>(size_t(out.nnz));
+  GPP_LAUNCH(copy_kept, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map, inner_map,
+             sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, out.ptr, out.idx, out.val);
+  return out;
+}
+
+DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
+  DevCsr t;
+  t.rows = M.cols;
+  t.cols = M.rows;
+  t.nnz = M.nnz;
+  t.ptr = dalloc<offset_t>(size_t(t.rows) + 1);
+  if (M.nnz == 0) {
+    check(cudaMemsetAsync(t.ptr, 0, sizeof(offset_t) * (size_t(t.rows) + 1), s), "transpose empty");
+    return t;
+  }
+  t.idx = dalloc<int32_t>(size_t(M.nnz));
+  t.val = dalloc<double>(size_t(M.nnz));
+  DBuf<int32_t> cnt(size_t(t.rows) + 1, s);
+  cnt.zero();
+  GPP_LAUNCH(histogram, grid_stride_blocks(M.nnz), kThreads, 0, s, M.idx, M.nnz, cnt.p);
+  exclusive_scan_i32(cnt.p, t.ptr, t.rows, s);
+  DBuf<int32_t> cursor(size_t(t.rows), s);
+  cursor.copy_from(t.ptr, size_t(t.rows));
+  GPP_LAUNCH(scatter_rows, grid_stride_blocks(M.rows), kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, cursor.p,
+             t.idx, t.val);
+  GPP_LAUNCH(sort_rows_short, grid_stride_blocks(t.rows), kThreads, 0, s, t.rows, t.ptr, t.idx, t.val);
+  RowSchedule sch;
+  build_schedule(sch, t, nullptr, s);
+  DBuf<int32_t> sidx(size_t(M.nnz), s);
+  DBuf<double> sval(size_t(M.nnz), s);
+  // Rows longer than 32 are in the medium or long queue.
+  GPP_LAUNCH(sort_rows_long, roles_medium(t.rows), kThreads, 0, s, sch.medium.p, sch.counts.p, t.ptr, t.idx,
+             t.val, sidx.p, sval.p);
+  GPP_LAUNCH(sort_rows_long, roles_long(t.rows), kThreads, 0, s, sch.long_rows.p, sch.counts.p + 1, t.ptr,
+             t.idx, t.val, sidx.p, sval.p);
+  return t;
+}
+
+bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s) {
+  if (M.rows <= 0 || M.nnz <= 1) return true;
+  DBuf<int32_t> bad(1, s);
+  bad.zero();
+  GPP_LAUNCH(check_sorted, grid_stride_blocks(M.rows), kThreads, 0, s, M.rows, M.ptr, M.idx, bad.p);
+  return read_scalar(bad.p) == 0;
+}
+
+void gather_by_map(double* dst, const double* src, const int32_t* old_to_new, int32_t n_old, cudaStream_t s) {
+  GPP_LAUNCH(gather_kernel, grid_stride_blocks(n_old), kThreads, 0, s, dst, src, old_to_new, n_old);
+}
+
+void compose_map(int32_t* next, const int32_t* prev, const int32_t* old_to_new, int32_t n_old, cudaStream_t s) {
+  GPP_LAUNCH(compose_kernel, grid_stride_blocks(n_old), kThreads, 0, s, next, prev, old_to_new, n_old);
+}
+
+void free_csr(DevCsr& M) {
+  dfree(M.ptr);
+  dfree(M.idx);
+  dfree(M.val);
+  M = DevCsr{};
+}
+
+}  // namespace gpp

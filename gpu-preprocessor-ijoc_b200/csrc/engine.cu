@@ -1,0 +1,345 @@
+// The presolve scheduler: a fixed-point loop of Cleanup, Propagation,
+// Aggregation and Parallel phases over a deferred plan that is materialised
+// (compacted) at phase boundaries.
+//
+// Reference: run_gpu_presolve_impl (cpp/src/presolve/gpu_presolve.cu:2081-2645),
+// apply_plan_to_working_lp (:1953-2072), capture_cleanup_recovery
+// (device_recovery.cu:1011-1027).  The phase machine, the iteration budget,
+// the bound-only round limit and the nnz-progress tests follow the reference
+// step for step; every rule reports through one status readback.
+#include <chrono>
+#include <cmath>
+
+#include "engine.cuh"
+#include "presolve.hpp"
+
+namespace gpp {
+
+void WorkingLp::free_owned() {
+  if (!owns) return;
+  free_csr(A);
+  free_csr(AT);
+  dfree(c); dfree(AL); dfree(AU); dfree(l); dfree(u);
+  c = AL = AU = l = u = nullptr;
+  owns = false;
+}
+
+namespace {
+
+__global__ void any_removed(const uint8_t* __restrict__ rows, int m, const uint8_t* __restrict__ cols, int n,
+                            int32_t* flag) {
+  const int top = m > n ? m : n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < top; i += gridDim.x * blockDim.x)
+    if ((i < m && !rows[i]) || (i < n && !cols[i])) { *flag = 1; return; }
+}
+__global__ void fill_u8(uint8_t* p, int n, uint8_t v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+struct Engine {
+  const gpp_params& p;
+  PresolveOutput& out;
+  WorkingLp cur;
+  bool at_sorted = false;     // rows of cur.AT strictly sorted (checked once for the input)
+  bool at_checked = false;
+  bool terminal = false;
+  bool active = false, pending = false;
+  Plan plan;
+  Stats stats;
+  bool stats_dirty = true;
+  DBuf<uint8_t> entry_cols;
+  DBuf<double> ref_bounds;
+  uint64_t deletion_serial = 0;
+  Status status;
+
+  Engine(const gpp_params& params, PresolveOutput& o) : p(params), out(o) {}
+
+  cudaStream_t s() const { return ctx().stream; }
+
+  void init_plan(Plan& pl) {
+    const int m = cur.m(), n = cur.n();
+    pl.keep_row.alloc(size_t(m), s());
+    pl.keep_col.alloc(size_t(n), s());
+    GPP_LAUNCH(fill_u8, grid_stride_blocks(m), kThreads, 0, s(), pl.keep_row.p, m, uint8_t(1));
+    GPP_LAUNCH(fill_u8, grid_stride_blocks(n), kThreads, 0, s(), pl.keep_col.p, n, uint8_t(1));
+    pl.c.alloc(size_t(n), s()); pl.c.copy_from(cur.c, size_t(n));
+    pl.l.alloc(size_t(n), s()); pl.l.copy_from(cur.l, size_t(n));
+    pl.u.alloc(size_t(n), s()); pl.u.copy_from(cur.u, size_t(n));
+    pl.AL.alloc(size_t(m), s()); pl.AL.copy_from(cur.AL, size_t(m));
+    pl.AU.alloc(size_t(m), s()); pl.AU.copy_from(cur.AU, size_t(m));
+  }
+  void prepare() {
+    if (active) return;
+    plan = Plan{};
+    init_plan(plan);
+    allocate_stats(stats, cur.m(), cur.n());
+    entry_cols.alloc(size_t(cur.n()), s());
+    stats_dirty = true;
+    active = true;
+  }
+  void refresh() {
+    if (stats_dirty) {
+      refresh_stats(stats, cur, plan);
+      stats_dirty = false;
+    }
+  }
+  int64_t live_nnz() {
+    if (!active) return cur.A.nnz;
+    refresh();
+    return int64_t(read_scalar(stats.live_nnz.p));
+  }
+
+  template <class F>
+  bool deferred_rule(bool enabled, const char* name, F rule) {
+    if (!enabled || terminal) return false;
+    prepare();
+    refresh();
+    entry_cols.copy_from(plan.keep_col.p, size_t(cur.n()));
+    plan.rule_entry_keep_col = entry_cols.p;
+    plan.has_change = plan.has_row_action = plan.has_col_action = false;
+    plan.has_redundant_row_deletion = plan.has_row_deletion = false;
+    plan.obj_delta = 0.0;
+    rule();
+    out.has_infeasible = plan.has_infeasible;
+    out.has_unbounded = plan.has_unbounded;
+    terminal = plan.has_infeasible || plan.has_unbounded;
+    const bool changed = plan.has_change && !terminal;
+    if (changed) {
+      if (plan.has_row_deletion || plan.has_col_action) ++deletion_serial;
+      cur.obj += plan.obj_delta;
+      capture_tape(out.record, plan.tape);
+      if (plan.has_col_action)
+        append_fixed(out.record, plan.keep_col.p, entry_cols.p, plan.l.p, plan.u.p, cur.n());
+      pending = true;
+      if (plan.has_row_action || plan.has_col_action) stats_dirty = true;
+    } else {
+      plan.tape.clear();
+    }
+    plan.obj_delta = 0.0;
+    out.trace.push_back(std::string("rule=") + name + " changed=" + (changed ? "1" : "0"));
+    return changed;
+  }
+
+  bool keeps_all(const Plan& pl) {
+    status.clear(1);
+    GPP_LAUNCH(any_removed, grid_stride_blocks(std::max(cur.m(), cur.n())), kThreads, 0, s(), pl.keep_row.p,
+               cur.m(), pl.keep_col.p, cur.n(), status.d);
+    return status.read(1)[0] == 0;
+  }
+
+  // apply_plan_to_working_lp (gpu_presolve.cu:1953-2072).
+  void apply(Plan& pl, bool cleanup_captured) {
+    Record& r = out.record;
+    const int m = cur.m(), n = cur.n();
+    if (cur.owns && !pl.has_new_A && keeps_all(pl)) {
+      capture_tape(r, pl.tape);
+      check(cudaMemcpyAsync(cur.c, pl.c.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s()), "commit c");
+      check(cudaMemcpyAsync(cur.l, pl.l.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s()), "commit l");
+      check(cudaMemcpyAsync(cur.u, pl.u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s()), "commit u");
+      check(cudaMemcpyAsync(cur.AL, pl.AL.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s()), "commit AL");
+      check(cudaMemcpyAsync(cur.AU, pl.AU.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s()), "commit AU");
+      cur.obj += pl.obj_delta;
+      return;
+    }
+    DBuf<int32_t> rmap(size_t(std::max(m, 1)), s()), cmap(size_t(std::max(n, 1)), s());
+    const int m_new = build_old_to_new(pl.keep_row.p, m, rmap.p, s());
+    const int n_new = build_old_to_new(pl.keep_col.p, n, cmap.p, s());
+    WorkingLp next;
+    if (pl.has_new_A) {
+      next.A = compact_csr(pl.new_A, rmap.p, m_new, cmap.p, n_new, s());
+      next.AT = transpose_csr(next.A, s());
+    } else {
+      next.A = compact_csr(cur.A, rmap.p, m_new, cmap.p, n_new, s());
+      if (!at_checked) {
+        at_sorted = rows_strictly_sorted(cur.AT, s());
+        at_checked = true;
+      }
+      next.AT = at_sorted ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s()) : transpose_csr(next.A, s());
+    }
+    at_sorted = at_checked = true;
+    next.c = dalloc<double>(size_t(n_new)); gather_by_map(next.c, pl.c.p, cmap.p, n, s());
+    next.l = dalloc<double>(size_t(n_new)); gather_by_map(next.l, pl.l.p, cmap.p, n, s());
+    next.u = dalloc<double>(size_t(n_new)); gather_by_map(next.u, pl.u.p, cmap.p, n, s());
+    next.AL = dalloc<double>(size_t(m_new)); gather_by_map(next.AL, pl.AL.p, rmap.p, m, s());
+    next.AU = dalloc<double>(size_t(m_new)); gather_by_map(next.AU, pl.AU.p, rmap.p, m, s());
+    next.obj = cur.obj + pl.obj_delta;
+    // update_device_recovery (device_recovery.cu:892-975).
+    capture_tape(r, pl.tape);
+    if (!cleanup_captured && n_new != n) append_fixed(r, pl.keep_col.p, nullptr, pl.l.p, pl.u.p, n);
+    if (m_new != r.m) {
+      DBuf<int32_t> rows(size_t(m_new), s());
+      compose_map(rows.p, r.rows.p, rmap.p, m, s());
+      r.rows = std::move(rows);
+      r.m = m_new;
+    }
+    if (n_new != r.n) {
+      DBuf<int32_t> cols(size_t(n_new), s());
+      compose_map(cols.p, r.cols.p, cmap.p, n, s());
+      r.cols = std::move(cols);
+      r.n = n_new;
+    }
+    cur.free_owned();
+    next.owns = true;
+    cur = next;
+    invalidate_schedules();
+  }
+
+  void materialize(const char* boundary) {
+    if (active && pending) {
+      apply(plan, true);
+      out.trace.push_back(std::string("apply=") + boundary);
+    }
+    active = pending = false;
+    plan = Plan{};
+    stats = Stats{};
+  }
+
+  template <class F>
+  bool materialized_rule(bool enabled, const char* name, F rule) {
+    if (!enabled || terminal) return false;
+    Plan pl;
+    init_plan(pl);
+    rule(pl);
+    out.has_infeasible = pl.has_infeasible;
+    out.has_unbounded = pl.has_unbounded;
+    terminal = pl.has_infeasible || pl.has_unbounded;
+    const bool changed = !terminal && pl.has_change;
+    if (changed) {
+      apply(pl, false);
+      out.trace.push_back(std::string("apply=") + name);
+    }
+    if (pl.has_new_A) free_csr(pl.new_A);
+    return changed;
+  }
+};
+
+bool good_progress(int64_t before, int64_t after, int64_t d) { return before >= d && after <= before - d; }
+
+}  // namespace
+
+void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out) {
+  Engine e(p, out);
+  WorkingLp& cur = e.cur;
+  cur.A = DevCsr{input.A.rows, input.A.cols, input.A.nnz, input.A.rowPtr, input.A.colVal, input.A.nzVal};
+  cur.AT = DevCsr{input.AT.rows, input.AT.cols, input.AT.nnz, input.AT.rowPtr, input.AT.colVal, input.AT.nzVal};
+  cur.c = input.c; cur.AL = input.AL; cur.AU = input.AU; cur.l = input.l; cur.u = input.u;
+  cur.obj = input.obj_constant;
+  cur.owns = false;
+  out.original_rows = cur.m();
+  out.original_cols = cur.n();
+  init_record(out.record, cur.m(), cur.n());
+  invalidate_schedules();
+  ctx().sync("presolve initialization");
+  const auto t0 = std::chrono::steady_clock::now();
+  const bool has_time_limit = p.max_time > 0.0 && std::isfinite(p.max_time);
+  auto time_exceeded = [&]() {
+    return has_time_limit &&
+           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= p.max_time;
+  };
+
+  if (p.enable_startup && p.max_iters > 0 && !time_exceeded()) {
+    // Structure-specific startup detectors are outside this engine's scope;
+    // the Startup phase still consumes its iteration (gpu_presolve.cu:2453).
+    ++out.iterations;
+  }
+  auto deferred = [&](bool enabled, const char* name, auto rule) {
+    return !time_exceeded() && e.deferred_rule(enabled, name, rule);
+  };
+  auto cleanup = [&]() {
+    out.trace.push_back("phase=cleanup");
+    bool ch = deferred(p.enable_infeasible_and_fixed_variables, "infeasible_and_fixed_variables",
+                       [&] { rule_fixed_variables(e.plan, cur, p); });
+    ch = deferred(p.enable_empty_columns, "empty_columns", [&] { rule_empty_columns(e.plan, cur, e.stats, p); }) || ch;
+    ch = deferred(p.enable_empty_rows, "empty_rows", [&] { rule_empty_rows(e.plan, cur, e.stats, p); }) || ch;
+    ch = deferred(p.enable_singleton_rows, "singleton_rows", [&] { rule_singleton_rows(e.plan, cur, e.stats, p); }) || ch;
+    ch = deferred(p.enable_singleton_columns, "singleton_columns",
+                  [&] { rule_singleton_columns(e.plan, cur, e.stats, p); }) || ch;
+    return ch;
+  };
+  auto propagation = [&]() {
+    out.trace.push_back("phase=propagation");
+    bool bounds_changed = false;
+    if (p.enable_bound_strengthening && !e.terminal && !time_exceeded()) {
+      e.prepare();
+      const int n = cur.n();
+      e.ref_bounds.alloc(size_t(2 * std::max(n, 1)), ctx().stream);
+      check(cudaMemcpyAsync(e.ref_bounds.p, e.plan.l.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx().stream), "ref l");
+      check(cudaMemcpyAsync(e.ref_bounds.p + n, e.plan.u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx().stream), "ref u");
+      e.plan.ref_l = e.ref_bounds.p;
+      e.plan.ref_u = e.ref_bounds.p + n;
+      bounds_changed = e.deferred_rule(true, "bound_strengthening",
+                                       [&] { rule_bound_strengthening(e.plan, cur, e.stats, p); });
+    }
+    deferred(p.enable_infeasible_and_redundant_rows, "infeasible_and_redundant_rows",
+             [&] { rule_redundant_rows(e.plan, cur, e.stats, p); });
+    deferred(p.enable_dual_fix, "dual_fix", [&] { rule_dual_fix(e.plan, cur, e.stats, p); });
+    return bounds_changed;
+  };
+
+  enum Phase { Cleanup, Propagation, Aggregation, Parallel } phase = Cleanup;
+  const int64_t min_dec = 100;
+  int bound_only_rounds = 0;
+  const int64_t initial_live = p.max_iters > 0 && !e.terminal && !time_exceeded() ? e.live_nnz() : 0;
+  const int configured = std::max(1, p.bound_strengthening_max_bound_only_rounds);
+  int limit = configured;
+  if (p.bound_strengthening_bound_only_nnz_round_budget > 0 && initial_live > 0)
+    limit = int(std::min<int64_t>(limit, std::max<int64_t>(1, p.bound_strengthening_bound_only_nnz_round_budget / initial_live)));
+  {
+    const int64_t m = cur.m(), n = cur.n();
+    if (m >= 512 && m <= 2048 && n >= 128 * m && n <= 256 * m && initial_live >= 2048 * m && initial_live <= 8192 * m)
+      limit = std::max(limit, std::min(2, configured));
+  }
+  while (p.max_iters > 0 && !e.terminal && !time_exceeded()) {
+    if (phase != Cleanup) {
+      if (out.iterations >= p.max_iters) { out.stopped_at_iteration_limit = true; break; }
+      ++out.iterations;
+    }
+    const int64_t before = e.live_nnz();
+    if (phase == Cleanup) {
+      const uint64_t ser = e.deletion_serial;
+      const bool changed = cleanup();
+      if (e.deletion_serial != ser) bound_only_rounds = 0;
+      phase = changed ? Cleanup : Propagation;
+    } else if (phase == Propagation) {
+      const uint64_t ser = e.deletion_serial;
+      const bool bounds_changed = propagation();
+      bound_only_rounds = e.deletion_serial != ser ? 0 : bound_only_rounds + 1;
+      e.materialize("1");
+      const int64_t after = e.live_nnz();
+      const bool nnz_progress = good_progress(before, after, min_dec);
+      const bool bound_progress = bounds_changed && bound_only_rounds < limit;
+      phase = nnz_progress || bound_progress ? Cleanup : Aggregation;
+      if (phase == Aggregation) bound_only_rounds = 0;
+    } else if (phase == Aggregation) {
+      out.trace.push_back("phase=aggregation");
+      if (!time_exceeded())
+        e.materialized_rule(p.enable_doubleton_equations, "doubleton_equations",
+                            [&](Plan& pl) { rule_doubleton_equations(pl, cur, p); });
+      const int64_t after = e.live_nnz();
+      phase = good_progress(before, after, min_dec) ? Cleanup : Parallel;
+    } else {
+      out.trace.push_back("phase=parallel");
+      bool changed = deferred(p.enable_parallel_rows, "parallel_rows",
+                              [&] { rule_parallel_rows(e.plan, cur, e.stats, p); });
+      changed = deferred(p.enable_parallel_columns, "parallel_columns",
+                         [&] { rule_parallel_columns(e.plan, cur, e.stats, p); }) || changed;
+      e.materialize("2");
+      const int64_t after = e.live_nnz();
+      if (!(changed && good_progress(before, after, min_dec))) break;
+      phase = Cleanup;
+    }
+  }
+  e.materialize("finalize");
+  ctx().sync("presolve finalize");
+  out.reduced_rows = cur.m();
+  out.reduced_cols = cur.n();
+  out.reduced_nnz = cur.A.nnz;
+  out.obj_constant_delta = cur.obj - input.obj_constant;
+  out.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  out.has_change = cur.owns;
+  out.reduced = cur;      // ownership moves to the output when cur.owns
+  out.owns_reduced = cur.owns;
+  cur.owns = false;
+}
+
+}  // namespace gpp

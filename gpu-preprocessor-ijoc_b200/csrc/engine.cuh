@@ -1,0 +1,153 @@
+// Internal engine types: device CSR, working LP, deferred plan, live
+// statistics, recovery record.  All device data is owned through DBuf or
+// explicit ownership flags; everything runs on ctx().stream.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gpp {
+
+struct DevCsr {
+  int32_t rows = 0, cols = 0;
+  offset_t nnz = 0;
+  offset_t* ptr = nullptr;
+  int32_t* idx = nullptr;
+  double* val = nullptr;
+};
+
+// Row-length schedule of one CSR matrix: rows with length <= kShortRow are
+// handled one per thread by a pass over all rows; the medium (<= kLongRow)
+// and long queues list the remaining rows for warp- and block-per-row work.
+struct RowSchedule {
+  DBuf<int32_t> medium, long_rows, counts;  // counts[0] medium, counts[1] long
+  const offset_t* ptr = nullptr;
+  int32_t rows = -1;
+  offset_t nnz = -1;
+  uint64_t epoch = 0;
+};
+
+// Builds the schedule of `M` by stored length (live_degrees == nullptr) or by
+// the given per-row live degree.
+void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees, cudaStream_t st);
+// Cached stored-length schedule (A and AT slots), invalidated per materialisation.
+const RowSchedule& stored_schedule(const DevCsr& M);
+void invalidate_schedules();
+
+struct PostsolveSegment {
+  DBuf<int32_t> types;
+  DBuf<int64_t> is, vs;   // record offsets into idx / val (count+1 each)
+  DBuf<int32_t> idx;
+  DBuf<double> val;
+  int64_t count = 0, n_idx = 0, n_val = 0;
+};
+
+struct FixedSegment {
+  DBuf<int32_t> idx;
+  DBuf<double> val;
+  int64_t count = 0;
+};
+
+struct Record {
+  int32_t m0 = 0, n0 = 0;
+  DBuf<int32_t> rows, cols;   // current index -> original index
+  int32_t m = 0, n = 0;
+  std::vector<PostsolveSegment> segments;
+  std::vector<FixedSegment> fixed;
+  int64_t records = 0, indices = 0, values = 0;
+};
+
+struct Plan {
+  DBuf<uint8_t> keep_row, keep_col;
+  DBuf<double> c, l, u, AL, AU;
+  double obj_delta = 0.0;
+  bool has_change = false, has_row_action = false, has_col_action = false;
+  bool has_redundant_row_deletion = false, has_row_deletion = false;
+  bool has_infeasible = false, has_unbounded = false;
+  const uint8_t* rule_entry_keep_col = nullptr;
+  const double* ref_l = nullptr;
+  const double* ref_u = nullptr;
+  bool has_new_A = false;
+  DevCsr new_A;                  // owned when has_new_A
+  std::vector<PostsolveSegment> tape;   // local indices until captured
+};
+
+struct Stats {
+  DBuf<int32_t> row_nnz, col_nnz, srow_col, scol_row;
+  DBuf<uint8_t> empty_row, singleton_row, empty_col, singleton_col;
+  DBuf<double> srow_val, scol_val;
+  DBuf<unsigned long long> live_nnz;
+};
+
+struct WorkingLp {
+  DevCsr A, AT;
+  double *c = nullptr, *AL = nullptr, *AU = nullptr, *l = nullptr, *u = nullptr;
+  double obj = 0.0;
+  bool owns = false;
+  int32_t m() const { return A.rows; }
+  int32_t n() const { return A.cols; }
+  void free_owned();
+};
+
+// ---- kernel families (host wrappers) ---------------------------------------
+// live.cu
+void live_stats_side(const DevCsr& M, const uint8_t* keep_outer, const uint8_t* keep_inner,
+                     int32_t* degree, uint8_t* empty, uint8_t* singleton, int32_t* support,
+                     double* coefficient, unsigned long long* total, cudaStream_t s);
+void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan);
+void allocate_stats(Stats& st, int32_t m, int32_t n);
+void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,
+                          const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
+                          double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,
+                          cudaStream_t s);
+void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStream_t s);
+
+// compact.cu
+int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cudaStream_t s);
+// Stable compaction of M's kept rows (outer map) and kept entries (inner map).
+DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
+                   const int32_t* inner_map, int32_t inner_new, cudaStream_t s);
+// General transpose (histogram, scan, scatter, per-row sort): rows of the
+// result list source rows in ascending order.
+DevCsr transpose_csr(const DevCsr& M, cudaStream_t s);
+bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s);
+void gather_by_map(double* dst, const double* src, const int32_t* old_to_new, int32_t n_old,
+                   cudaStream_t s);
+void compose_map(int32_t* next, const int32_t* prev, const int32_t* old_to_new, int32_t n_old,
+                 cudaStream_t s);
+void free_csr(DevCsr& M);
+
+// recovery.cu
+void init_record(Record& r, int32_t m, int32_t n);
+void globalize_segment(PostsolveSegment& s, const Record& r, cudaStream_t st);
+void capture_tape(Record& r, std::vector<PostsolveSegment>& tape);
+void append_fixed(Record& r, const uint8_t* keep_col, const uint8_t* prior, const double* l,
+                  const double* u, int32_t n);
+// Builds a device segment from host-side packed arrays (records laid out
+// contiguously); used by rules that pack on the device and know the counts.
+PostsolveSegment make_segment(int64_t count, int64_t n_idx, int64_t n_val);
+
+// rules_*.cu
+void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+void rule_empty_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_empty_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_singleton_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_singleton_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_redundant_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_dual_fix(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_parallel_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_parallel_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+
+// Row-wise shift sum_j a_ij * v_j over kept rows and selected columns, in
+// ascending column order (deterministic replacement of atomicAdd shifts).
+// With `radius`, sums |a_ij| * radius_j over selected columns with radius > 0.
+void row_gather_shift(const DevCsr& A, const uint8_t* keep_row, const uint8_t* selected,
+                      const double* value, const double* radius, double* out, cudaStream_t s);
+// Canonical objective sum of contrib over the rule-entry domain.
+double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_t n, cudaStream_t s);
+
+}  // namespace gpp

@@ -1,0 +1,433 @@
+// Live-structure kernels: row schedules, live statistics, row activity
+// summaries and column max |a|.
+//
+// Reference: cpp/src/presolve/gpu_presolve_kernels.cu:96-517,744-809.
+// Each kernel is ONE launch whose blocks split into three roles: a
+// thread-per-row pass over short rows, warp-per-row over the medium queue and
+// block-per-row over the long queue.  Masked traversals hand every lane the
+// live entries with live rank == lane (mod width), exactly the sequence a
+// physically compacted row would give, so the floating-point association of
+// the activity sums is the reference's:
+//   short  : sequential left-to-right sum,
+//   medium : 32 lane partials, shfl_down tree 16,8,4,2,1 (own + peer),
+//   long   : 256 lane partials, per-warp shfl tree 1,2,4,8,16 then warp
+//            aggregates added in warp order (cub::BlockReduce default).
+#include "engine.cuh"
+
+#include <array>
+
+namespace gpp {
+
+namespace {
+
+__device__ __forceinline__ int row_len(const offset_t* ptr, const int32_t* live_deg, int row) {
+  return live_deg ? live_deg[row] : int(ptr[row + 1] - ptr[row]);
+}
+
+__global__ void classify_rows(const offset_t* __restrict__ ptr, int m, const int32_t* __restrict__ live_deg,
+                              int32_t* __restrict__ medium, int32_t* __restrict__ longq,
+                              int32_t* __restrict__ counts) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int len = row < m ? row_len(ptr, live_deg, row) : 0;
+  for (int g = 0; g < 2; ++g) {
+    const bool sel = row < m && (g == 0 ? (len > kShortRow && len <= kLongRow) : len > kLongRow);
+    const unsigned mask = __ballot_sync(0xffffffffu, sel);
+    if (!mask) continue;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counts + g, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (sel) (g == 0 ? medium : longq)[base + __popc(mask & ((1u << lane) - 1u))] = row;
+  }
+}
+
+// Visit the live entries of [first, last) so that the thread with index
+// `lane` (0..W-1) sees live ranks lane, lane+W, ... in order.  `slots` is W
+// ints of shared memory private to the warp (W=32) or block (W=256).
+template <int W, class Visit>
+__device__ __forceinline__ void live_visit(offset_t first, offset_t last, const int32_t* __restrict__ idx,
+                                           const uint8_t* __restrict__ keep, int* slots,
+                                           int* warp_counts, Visit visit) {
+  const int lane = W == 32 ? (threadIdx.x & 31) : threadIdx.x;
+  if (!keep) {
+    for (offset_t p = first + lane; p < last; p += W) visit(p);
+    return;
+  }
+  int carry = 0;
+  for (offset_t chunk = first; chunk < last; chunk += W) {
+    const offset_t p = chunk + lane;
+    const bool live = p < last && keep[idx[p]];
+    const unsigned mask = __ballot_sync(0xffffffffu, live);
+    int rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+    int c = __popc(mask);
+    if constexpr (W == 256) {
+      const int warp = threadIdx.x >> 5;
+      if ((threadIdx.x & 31) == 0) warp_counts[warp] = c;
+      __syncthreads();
+      int before = 0, total = 0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        const int k = warp_counts[w];
+        before += w < warp ? k : 0;
+        total += k;
+      }
+      rank += before;
+      c = total;
+    }
+    if (live) slots[(carry + rank) & (W - 1)] = int(p - first);
+    if constexpr (W == 32) __syncwarp(); else __syncthreads();
+    if (((lane - carry) & (W - 1)) < c) visit(first + slots[lane]);
+    if constexpr (W == 32) __syncwarp(); else __syncthreads();
+    carry = (carry + c) & (W - 1);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum_down(T v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// cub::BlockReduce<T,256>::Sum order; result valid in thread 0.
+template <class T>
+__device__ __forceinline__ T block_sum_cub_order(T v, T* warp_aggs) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T peer = __shfl_down_sync(0xffffffffu, v, off);
+    if (lane + off <= 31) v = v + peer;
+  }
+  if (lane == 0) warp_aggs[threadIdx.x >> 5] = v;
+  __syncthreads();
+  T total = v;
+  if (threadIdx.x == 0) {
+    total = warp_aggs[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) total = total + warp_aggs[w];
+  }
+  __syncthreads();
+  return total;
+}
+
+struct ActivityTerm {
+  const int32_t* idx;
+  const double* val;
+  const double* l;
+  const double* u;
+  double zero_tol;
+  __device__ __forceinline__ void operator()(offset_t p, double& lo, double& hi, int& ni, int& pi) const {
+    const double a = val[p];
+    if (fabs(a) <= zero_tol) return;
+    const int col = idx[p];
+    const double tlo = a >= 0.0 ? a * l[col] : a * u[col];
+    const double thi = a >= 0.0 ? a * u[col] : a * l[col];
+    if (isfinite(tlo)) lo += tlo; else if (tlo < 0.0) ++ni;
+    if (isfinite(thi)) hi += thi; else if (thi > 0.0) ++pi;
+  }
+};
+
+__global__ void __launch_bounds__(kThreads)
+activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                const double* __restrict__ val, const double* __restrict__ l, const double* __restrict__ u,
+                double zero_tol, const uint8_t* __restrict__ keep_row, const uint8_t* __restrict__ keep_col,
+                const int32_t* __restrict__ live_deg, const int32_t* __restrict__ medium,
+                const int32_t* __restrict__ longq, const int32_t* __restrict__ counts, int short_blocks,
+                int medium_blocks, double* __restrict__ min_fin, double* __restrict__ max_fin,
+                int32_t* __restrict__ min_inf, int32_t* __restrict__ max_inf) {
+  __shared__ int slots[256];
+  __shared__ int warp_counts[8];
+  __shared__ double dagg[8];
+  __shared__ int iagg[8];
+  const ActivityTerm term{idx, val, l, u, zero_tol};
+  const int b = blockIdx.x;
+  if (b < short_blocks) {
+    for (int i = b * blockDim.x + threadIdx.x; i < m; i += short_blocks * blockDim.x) {
+      if (row_len(ptr, live_deg, i) > kShortRow) continue;
+      double lo = 0.0, hi = 0.0;
+      int ni = 0, pi = 0;
+      for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+        if ((keep_row && !keep_row[i]) || (keep_col && !keep_col[idx[p]])) continue;
+        term(p, lo, hi, ni, pi);
+      }
+      min_fin[i] = lo; max_fin[i] = hi; min_inf[i] = ni; max_inf[i] = pi;
+    }
+    return;
+  }
+  if (b < short_blocks + medium_blocks) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = medium_blocks * (kThreads / 32);
+    const int count = counts[0];
+    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < count; q += nwarps) {
+      const int row = medium[q];
+      double lo = 0.0, hi = 0.0;
+      int ni = 0, pi = 0;
+      const offset_t first = ptr[row], last = ptr[row + 1];
+      const uint8_t* mask = live_deg && live_deg[row] == int(last - first) ? nullptr : keep_col;
+      if (!keep_row || keep_row[row])
+        live_visit<32>(first, last, idx, mask, slots + warp * 32, nullptr,
+                       [&](offset_t p) { term(p, lo, hi, ni, pi); });
+      lo = warp_sum_down(lo); hi = warp_sum_down(hi); ni = warp_sum_down(ni); pi = warp_sum_down(pi);
+      if (lane == 0) { min_fin[row] = lo; max_fin[row] = hi; min_inf[row] = ni; max_inf[row] = pi; }
+    }
+    return;
+  }
+  const int lb = b - short_blocks - medium_blocks;
+  const int nlong = gridDim.x - short_blocks - medium_blocks;
+  const int count = counts[1];
+  for (int q = lb; q < count; q += nlong) {
+    const int row = longq[q];
+    double lo = 0.0, hi = 0.0;
+    int ni = 0, pi = 0;
+    const offset_t first = ptr[row], last = ptr[row + 1];
+    const uint8_t* mask = live_deg && live_deg[row] == int(last - first) ? nullptr : keep_col;
+    if (!keep_row || keep_row[row])
+      live_visit<256>(first, last, idx, mask, slots, warp_counts,
+                      [&](offset_t p) { term(p, lo, hi, ni, pi); });
+    lo = block_sum_cub_order(lo, dagg);
+    hi = block_sum_cub_order(hi, dagg);
+    ni = block_sum_cub_order(ni, iagg);
+    pi = block_sum_cub_order(pi, iagg);
+    if (threadIdx.x == 0) { min_fin[row] = lo; max_fin[row] = hi; min_inf[row] = ni; max_inf[row] = pi; }
+    __syncthreads();
+  }
+}
+
+// Live degree / singleton support.  Counts and the max live position are
+// order independent, so the roles follow stored length.
+__device__ __forceinline__ void stats_write(int row, bool active, int count, offset_t position,
+                                            const int32_t* idx, const double* val, int32_t* degree,
+                                            uint8_t* empty, uint8_t* singleton, int32_t* support,
+                                            double* coefficient, unsigned long long* total) {
+  if (degree) degree[row] = count;
+  if (empty) empty[row] = active && count == 0;
+  if (singleton) singleton[row] = active && count == 1;
+  if (support) support[row] = count == 1 ? idx[position] : -1;
+  if (coefficient) coefficient[row] = count == 1 ? val[position] : 0.0;
+  if (total && count) atomicAdd(total, (unsigned long long)count);
+}
+
+__global__ void __launch_bounds__(kThreads)
+live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                  const double* __restrict__ val, const uint8_t* __restrict__ keep_outer,
+                  const uint8_t* __restrict__ keep_inner, const int32_t* __restrict__ medium,
+                  const int32_t* __restrict__ longq, const int32_t* __restrict__ counts, int short_blocks,
+                  int medium_blocks, int32_t* degree, uint8_t* empty, uint8_t* singleton,
+                  int32_t* support, double* coefficient, unsigned long long* total) {
+  __shared__ int scount[8];
+  __shared__ long long spos[8];
+  const int b = blockIdx.x;
+  if (b < short_blocks) {
+    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
+      const offset_t first = ptr[r], last = ptr[r + 1];
+      if (last - first > kShortRow) continue;
+      const bool active = !keep_outer || keep_outer[r];
+      int count = 0;
+      offset_t pos = -1;
+      if (active)
+        for (offset_t p = first; p < last; ++p)
+          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+      stats_write(r, active, count, pos, idx, val, degree, empty, singleton, support, coefficient, total);
+    }
+    return;
+  }
+  if (b < short_blocks + medium_blocks) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = medium_blocks * (kThreads / 32);
+    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
+      const int r = medium[q];
+      const bool active = !keep_outer || keep_outer[r];
+      int count = 0;
+      long long pos = -1;
+      if (active)
+        for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
+          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+      for (int off = 16; off; off >>= 1) {
+        count += __shfl_down_sync(0xffffffffu, count, off);
+        pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
+      }
+      if (lane == 0)
+        stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, total);
+    }
+    return;
+  }
+  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+  for (int q = lb; q < counts[1]; q += nlong) {
+    const int r = longq[q];
+    const bool active = !keep_outer || keep_outer[r];
+    int count = 0;
+    long long pos = -1;
+    if (active)
+      for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads)
+        if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+    for (int off = 16; off; off >>= 1) {
+      count += __shfl_down_sync(0xffffffffu, count, off);
+      pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
+    }
+    if ((threadIdx.x & 31) == 0) { scount[threadIdx.x >> 5] = count; spos[threadIdx.x >> 5] = pos; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < 8; ++w) { count += scount[w]; pos = max(pos, spos[w]); }
+      stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, total);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+col_max_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+               const double* __restrict__ val, const uint8_t* __restrict__ keep_row,
+               const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
+               const int32_t* __restrict__ counts, int short_blocks, int medium_blocks, double* out) {
+  __shared__ double smax[8];
+  const int b = blockIdx.x;
+  if (b < short_blocks) {
+    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
+      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
+      double v = 0.0;
+      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p)
+        if (!keep_row || keep_row[idx[p]]) v = fmax(v, fabs(val[p]));
+      out[r] = v;
+    }
+    return;
+  }
+  if (b < short_blocks + medium_blocks) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = medium_blocks * (kThreads / 32);
+    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
+      const int r = medium[q];
+      double v = 0.0;
+      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
+        if (!keep_row || keep_row[idx[p]]) v = fmax(v, fabs(val[p]));
+      for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+      if (lane == 0) out[r] = v;
+    }
+    return;
+  }
+  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+  for (int q = lb; q < counts[1]; q += nlong) {
+    const int r = longq[q];
+    double v = 0.0;
+    for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads)
+      if (!keep_row || keep_row[idx[p]]) v = fmax(v, fabs(val[p]));
+    for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < 8; ++w) v = fmax(v, smax[w]);
+      out[r] = v;
+    }
+    __syncthreads();
+  }
+}
+
+struct Roles {
+  int short_blocks, medium_blocks, long_blocks;
+};
+Roles roles_for(int rows) {
+  Roles r;
+  r.short_blocks = grid_stride_blocks(rows, kThreads, 16);
+  r.medium_blocks = std::min<int>(kNumSMs * 8, (rows + 7) / 8);
+  r.long_blocks = std::min<int>(kNumSMs * 4, rows);
+  return r;
+}
+
+struct ScheduleCache {
+  std::array<RowSchedule, 2> slots;
+  unsigned next = 0;
+  uint64_t epoch = 1;
+};
+ScheduleCache& schedule_cache() {
+  static thread_local ScheduleCache c;
+  return c;
+}
+
+}  // namespace
+
+void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees, cudaStream_t st) {
+  const size_t rows = size_t(std::max(M.rows, 1));
+  if (s.medium.n < rows) s.medium.alloc(rows, st);
+  if (s.long_rows.n < rows) s.long_rows.alloc(rows, st);
+  if (s.counts.n < 2) s.counts.alloc(2, st);
+  check(cudaMemsetAsync(s.counts.p, 0, 2 * sizeof(int32_t), st), "schedule counts");
+  GPP_LAUNCH(classify_rows, blocks_for(M.rows), kThreads, 0, st, M.ptr, M.rows, live_degrees, s.medium.p,
+             s.long_rows.p, s.counts.p);
+  s.ptr = M.ptr;
+  s.rows = M.rows;
+  s.nnz = M.nnz;
+  s.epoch = live_degrees ? 0 : schedule_cache().epoch;
+}
+
+const RowSchedule& stored_schedule(const DevCsr& M) {
+  auto& c = schedule_cache();
+  for (auto& s : c.slots)
+    if (s.epoch == c.epoch && s.ptr == M.ptr && s.rows == M.rows && s.nnz == M.nnz) return s;
+  auto& s = c.slots[c.next++ % c.slots.size()];
+  build_schedule(s, M, nullptr, ctx().stream);
+  return s;
+}
+
+void invalidate_schedules() { ++schedule_cache().epoch; }
+
+void live_stats_side(const DevCsr& M, const uint8_t* keep_outer, const uint8_t* keep_inner, int32_t* degree,
+                     uint8_t* empty, uint8_t* singleton, int32_t* support, double* coefficient,
+                     unsigned long long* total, cudaStream_t s) {
+  if (!M.rows) return;
+  const RowSchedule& sch = stored_schedule(M);
+  const Roles r = roles_for(M.rows);
+  GPP_LAUNCH(live_stats_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, M.rows,
+             M.ptr, M.idx, M.val, keep_outer, keep_inner, sch.medium.p, sch.long_rows.p, sch.counts.p,
+             r.short_blocks, r.medium_blocks, degree, empty, singleton, support, coefficient, total);
+}
+
+void allocate_stats(Stats& st, int32_t m, int32_t n) {
+  auto s = ctx().stream;
+  st.row_nnz.alloc(size_t(m), s); st.empty_row.alloc(size_t(m), s); st.singleton_row.alloc(size_t(m), s);
+  st.srow_col.alloc(size_t(m), s); st.srow_val.alloc(size_t(m), s);
+  st.col_nnz.alloc(size_t(n), s); st.empty_col.alloc(size_t(n), s); st.singleton_col.alloc(size_t(n), s);
+  st.scol_row.alloc(size_t(n), s); st.scol_val.alloc(size_t(n), s);
+  st.live_nnz.alloc(1, s);
+}
+
+void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
+  // refresh_live_stats (gpu_presolve_kernels.cu:493-517).
+  auto s = ctx().stream;
+  st.live_nnz.zero();
+  live_stats_side(lp.A, plan.keep_row.p, plan.keep_col.p, st.row_nnz.p, st.empty_row.p, st.singleton_row.p,
+                  st.srow_col.p, st.srow_val.p, st.live_nnz.p, s);
+  live_stats_side(lp.AT, plan.keep_col.p, plan.keep_row.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p,
+                  st.scol_row.p, st.scol_val.p, nullptr, s);
+}
+
+void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,
+                          const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
+                          double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,
+                          cudaStream_t s) {
+  // compute_row_activity_summary (gpu_presolve_kernels.cu:744-787).
+  if (!A.rows) return;
+  static thread_local RowSchedule live_schedule;
+  const RowSchedule* sch;
+  if (live_deg) {
+    build_schedule(live_schedule, A, live_deg, s);
+    sch = &live_schedule;
+  } else {
+    sch = &stored_schedule(A);
+  }
+  const Roles r = roles_for(A.rows);
+  GPP_LAUNCH(activity_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
+             A.idx, A.val, l, u, zero_tol, keep_row, keep_col, live_deg, sch->medium.p, sch->long_rows.p,
+             sch->counts.p, r.short_blocks, r.medium_blocks, min_fin, max_fin, min_inf, max_inf);
+}
+
+void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStream_t s) {
+  // compute_col_max_abs (gpu_presolve_kernels.cu:789-809).
+  if (!AT.rows) return;
+  const RowSchedule& sch = stored_schedule(AT);
+  const Roles r = roles_for(AT.rows);
+  GPP_LAUNCH(col_max_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, AT.rows,
+             AT.ptr, AT.idx, AT.val, keep_row, sch.medium.p, sch.long_rows.p, sch.counts.p, r.short_blocks,
+             r.medium_blocks, out);
+}
+
+}  // namespace gpp

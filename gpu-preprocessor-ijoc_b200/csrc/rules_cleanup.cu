@@ -1,0 +1,290 @@
+// Cleanup rules: infeasible/fixed variables, empty columns, empty rows and
+// singleton rows.  Each rule works on the deferred plan (keep masks plus the
+// working copies of c, l, u, AL, AU) over the physical A / A^T, and reports
+// through one status block read back once per rule.
+//
+// Reference: rules/rule_infeasible_and_fixed_variables.cu:65-348,
+// rules/empty_rows_and_columns/columns.cu:64-249, rows.cu:26-121,
+// rules/rule_singleton_rows.cu:76-275.
+#include "engine.cuh"
+
+namespace gpp {
+
+namespace {
+
+__device__ __forceinline__ double atomic_max_d(double* addr, double v) {
+  auto* a = reinterpret_cast<unsigned long long*>(addr);
+  unsigned long long old = *a, assumed;
+  do {
+    assumed = old;
+    if (__longlong_as_double((long long)assumed) >= v) break;
+    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
+  } while (assumed != old);
+  return __longlong_as_double((long long)old);
+}
+__device__ __forceinline__ double atomic_min_d(double* addr, double v) {
+  auto* a = reinterpret_cast<unsigned long long*>(addr);
+  unsigned long long old = *a, assumed;
+  do {
+    assumed = old;
+    if (__longlong_as_double((long long)assumed) <= v) break;
+    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
+  } while (assumed != old);
+  return __longlong_as_double((long long)old);
+}
+
+// Row sums over selected columns in stored (ascending column) order; one
+// thread per row, rows without a selected column cost one pass over their
+// indices.
+__global__ void row_gather_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                  const double* __restrict__ val, const uint8_t* __restrict__ keep_row,
+                                  const uint8_t* __restrict__ selected, const double* __restrict__ value,
+                                  const double* __restrict__ radius, double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    if (keep_row[i])
+      for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+        const int j = idx[p];
+        if (!selected[j]) continue;
+        if (radius) {
+          if (radius[j] > 0.0) acc += fabs(val[p]) * radius[j];
+        } else {
+          acc += val[p] * value[j];
+        }
+      }
+    out[i] = acc;
+  }
+}
+
+__global__ void mask_contrib(int n, const double* __restrict__ contrib, const uint8_t* __restrict__ entry,
+                             double* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    out[j] = entry && !entry[j] ? 0.0 : contrib[j];
+}
+
+// --- infeasible / fixed variables ------------------------------------------
+__global__ void fixed_candidates(int n, const uint8_t* __restrict__ keep_col, const double* __restrict__ l,
+                                 const double* __restrict__ u, const double* __restrict__ c, double bound_tol,
+                                 uint8_t* __restrict__ fixed, double* __restrict__ fval,
+                                 double* __restrict__ contrib, double* __restrict__ radius) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    uint8_t f = 0;
+    double v = 0.0, cb = 0.0, rad = 0.0;
+    if (keep_col[j]) {
+      const double lj = l[j], uj = u[j];
+      if (isfinite(lj) && isfinite(uj) && lj <= uj && uj - lj <= bound_tol) {
+        v = lj + 0.5 * (uj - lj);
+        rad = fmax(v - lj, uj - v);
+        f = 1;
+        cb = c[j] * v;
+      }
+    }
+    fixed[j] = f; fval[j] = v; contrib[j] = cb; radius[j] = rad;
+  }
+}
+__global__ void fixed_filter(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
+                             const uint8_t* __restrict__ keep_row, const double* __restrict__ l,
+                             const double* __restrict__ u, const double* __restrict__ row_error, double budget,
+                             uint8_t* __restrict__ fixed, double* __restrict__ contrib, int32_t* __restrict__ status) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (!fixed[j]) continue;
+    bool keep_fix = true;
+    if (l[j] != u[j])
+      for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) {
+        const int row = at_idx[p];
+        if (keep_row[row] && !(row_error[row] <= budget)) { keep_fix = false; break; }
+      }
+    if (!keep_fix) { fixed[j] = 0; contrib[j] = 0.0; }
+    else atomicAdd(status, 1);
+  }
+}
+__global__ void fixed_apply(int n, int m, const uint8_t* __restrict__ fixed, const double* __restrict__ fval,
+                            const double* __restrict__ shift, uint8_t* __restrict__ keep_col, double* __restrict__ l,
+                            double* __restrict__ u, double* __restrict__ AL, double* __restrict__ AU) {
+  const int top = n > m ? n : m;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < top; j += gridDim.x * blockDim.x) {
+    if (j < n && fixed[j]) { l[j] = fval[j]; u[j] = fval[j]; keep_col[j] = 0; }
+    if (j < m) { AL[j] -= shift[j]; AU[j] -= shift[j]; }
+  }
+}
+
+// --- empty columns -----------------------------------------------------------
+__global__ void empty_columns_classify(int n, const uint8_t* __restrict__ keep_col, const uint8_t* __restrict__ empty,
+                                       const double* __restrict__ c, const double* __restrict__ l,
+                                       const double* __restrict__ u, double bound_tol, double zero_tol,
+                                       uint8_t* __restrict__ fixed, double* __restrict__ fval,
+                                       double* __restrict__ contrib, int32_t* __restrict__ status) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    fixed[j] = 0; fval[j] = 0.0; contrib[j] = 0.0;
+    if (!(keep_col[j] && empty[j])) continue;
+    const double cj = c[j], lj = l[j], uj = u[j];
+    if (lj > uj + bound_tol) { atomicMax(status + 0, 1); continue; }
+    if ((cj > zero_tol && !isfinite(lj)) || (cj < -zero_tol && !isfinite(uj))) { atomicMax(status + 1, 1); continue; }
+    double v = 0.0;
+    if (cj > zero_tol) v = lj;
+    else if (cj < -zero_tol) v = uj;
+    else if (isfinite(lj)) v = lj;
+    else if (isfinite(uj)) v = uj;
+    fixed[j] = 1; fval[j] = v; contrib[j] = cj * v;
+    atomicMax(status + 2, 1);
+  }
+}
+__global__ void fix_columns(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ fval,
+                            uint8_t* __restrict__ keep_col, double* __restrict__ l, double* __restrict__ u) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    if (fixed[j]) { l[j] = fval[j]; u[j] = fval[j]; keep_col[j] = 0; }
+}
+
+// --- empty rows ----------------------------------------------------------------
+__global__ void empty_rows_kernel(int m, uint8_t* __restrict__ keep_row, const int32_t* __restrict__ row_nnz,
+                                  const double* __restrict__ AL, const double* __restrict__ AU, double tol,
+                                  int32_t* __restrict__ status, int apply) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    if (!(keep_row[i] && row_nnz[i] == 0)) continue;
+    const bool feasible = AL[i] <= tol && AU[i] >= -tol;
+    if (!apply) atomicMax(status + (feasible ? 1 : 0), 1);
+    else if (feasible) keep_row[i] = 0;
+  }
+}
+
+// --- singleton rows -----------------------------------------------------------
+__global__ void singleton_row_bounds(int m, int n, const uint8_t* __restrict__ keep_row,
+                                     const uint8_t* __restrict__ singleton, const int32_t* __restrict__ scol,
+                                     const double* __restrict__ sval, const double* __restrict__ AL,
+                                     const double* __restrict__ AU, double zero_tol, double* cand_l, double* cand_u,
+                                     uint8_t* __restrict__ remove) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    remove[i] = 0;
+    if (!(keep_row[i] && singleton[i])) continue;
+    const int col = scol[i];
+    const double a = sval[i];
+    if (!(col >= 0 && col < n && fabs(a) > zero_tol)) continue;
+    const double lo = AL[i], hi = AU[i];
+    atomic_max_d(&cand_l[col], a > 0.0 ? lo / a : hi / a);
+    atomic_min_d(&cand_u[col], a > 0.0 ? hi / a : lo / a);
+    remove[i] = 1;
+  }
+}
+__global__ void singleton_rows_check(int m, int n, const double* __restrict__ cand_l, const double* __restrict__ cand_u,
+                                     const double* __restrict__ l, const double* __restrict__ u,
+                                     const uint8_t* __restrict__ remove, double tol, int32_t* __restrict__ status) {
+  const int top = n > m ? n : m;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < top; j += gridDim.x * blockDim.x) {
+    if (j < n) {
+      if (cand_l[j] > cand_u[j] + tol) atomicMax(status + 0, 1);
+      if (cand_l[j] != l[j] || cand_u[j] != u[j]) atomicMax(status + 2, 1);
+    }
+    if (j < m && remove[j]) atomicMax(status + 1, 1);
+  }
+}
+__global__ void singleton_rows_commit(int m, int n, const uint8_t* __restrict__ remove, uint8_t* __restrict__ keep_row) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    if (remove[i]) keep_row[i] = 0;
+}
+
+}  // namespace
+
+void row_gather_shift(const DevCsr& A, const uint8_t* keep_row, const uint8_t* selected, const double* value,
+                      const double* radius, double* out, cudaStream_t s) {
+  GPP_LAUNCH(row_gather_kernel, grid_stride_blocks(A.rows), kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, keep_row,
+             selected, value, radius, out);
+}
+
+double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_t n, cudaStream_t s) {
+  // sum_cleanup_domain (cleanup_support.cuh:13-31): the sum over the rule's
+  // entry domain, with the canonical deterministic reduction.
+  if (n <= 0) return 0.0;
+  DBuf<double> masked(size_t(n), s);
+  GPP_LAUNCH(mask_contrib, grid_stride_blocks(n), kThreads, 0, s, n, contrib, entry_keep, masked.p);
+  return det_sum(masked.p, n, s);
+}
+
+void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int n = lp.n(), m = lp.m();
+  if (n == 0) return;
+  auto s = ctx().stream;
+  DBuf<uint8_t> fixed(size_t(n), s);
+  DBuf<double> fval(size_t(n), s), contrib(size_t(n), s), radius(size_t(n), s), row_err(size_t(m), s),
+      shift(size_t(m), s);
+  Status st;
+  st.clear(4);
+  GPP_LAUNCH(fixed_candidates, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, plan.l.p, plan.u.p,
+             plan.c.p, p.bound_tol, fixed.p, fval.p, contrib.p, radius.p);
+  row_gather_shift(lp.A, plan.keep_row.p, fixed.p, fval.p, radius.p, row_err.p, s);
+  GPP_LAUNCH(fixed_filter, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, plan.keep_row.p,
+             plan.l.p, plan.u.p, row_err.p, 0.1 * p.feasibility_tol, fixed.p, contrib.p, st.d);
+  if (st.read(1)[0] == 0) return;
+  row_gather_shift(lp.A, plan.keep_row.p, fixed.p, fval.p, nullptr, shift.p, s);
+  GPP_LAUNCH(fixed_apply, grid_stride_blocks(std::max(n, m)), kThreads, 0, s, n, m, fixed.p, fval.p, shift.p,
+             plan.keep_col.p, plan.l.p, plan.u.p, plan.AL.p, plan.AU.p);
+  plan.obj_delta += domain_objective(contrib.p, plan.rule_entry_keep_col, n, s);
+  plan.has_col_action = plan.has_change = true;
+}
+
+void rule_empty_columns(Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int n = lp.n();
+  if (n == 0) return;
+  auto s = ctx().stream;
+  DBuf<uint8_t> fixed(size_t(n), s);
+  DBuf<double> fval(size_t(n), s), contrib(size_t(n), s);
+  Status st;
+  st.clear(3);
+  GPP_LAUNCH(empty_columns_classify, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, stats.empty_col.p,
+             plan.c.p, plan.l.p, plan.u.p, p.bound_tol, p.zero_tol, fixed.p, fval.p, contrib.p, st.d);
+  const int32_t* f = st.read(3);
+  if (f[0]) { plan.has_infeasible = true; return; }
+  if (f[1]) { plan.has_unbounded = true; return; }
+  if (!f[2]) return;
+  GPP_LAUNCH(fix_columns, grid_stride_blocks(n), kThreads, 0, s, n, fixed.p, fval.p, plan.keep_col.p, plan.l.p,
+             plan.u.p);
+  plan.obj_delta += domain_objective(contrib.p, plan.rule_entry_keep_col, n, s);
+  plan.has_col_action = plan.has_change = true;
+}
+
+void rule_empty_rows(Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m();
+  if (m == 0) return;
+  auto s = ctx().stream;
+  Status st;
+  st.clear(2);
+  GPP_LAUNCH(empty_rows_kernel, grid_stride_blocks(m), kThreads, 0, s, m, plan.keep_row.p, stats.row_nnz.p,
+             plan.AL.p, plan.AU.p, p.feasibility_tol, st.d, 0);
+  const int32_t* f = st.read(2);
+  if (f[0]) { plan.has_infeasible = true; return; }
+  if (!f[1]) return;
+  GPP_LAUNCH(empty_rows_kernel, grid_stride_blocks(m), kThreads, 0, s, m, plan.keep_row.p, stats.row_nnz.p,
+             plan.AL.p, plan.AU.p, p.feasibility_tol, st.d, 1);
+  plan.has_row_action = plan.has_row_deletion = plan.has_change = true;
+}
+
+void rule_singleton_rows(Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (m == 0) return;
+  auto s = ctx().stream;
+  DBuf<double> cl(size_t(n), s), cu(size_t(n), s);
+  DBuf<uint8_t> remove(size_t(m), s);
+  cl.copy_from(plan.l.p, size_t(n));
+  cu.copy_from(plan.u.p, size_t(n));
+  Status st;
+  st.clear(3);
+  GPP_LAUNCH(singleton_row_bounds, grid_stride_blocks(m), kThreads, 0, s, m, n, plan.keep_row.p,
+             stats.singleton_row.p, stats.srow_col.p, stats.srow_val.p, plan.AL.p, plan.AU.p, p.zero_tol, cl.p,
+             cu.p, remove.p);
+  GPP_LAUNCH(singleton_rows_check, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, m, n, cl.p, cu.p, plan.l.p,
+             plan.u.p, remove.p, p.bound_tol, st.d);
+  const int32_t* f = st.read(3);
+  if (f[0]) { plan.has_infeasible = true; return; }
+  if (!f[1] && !f[2]) return;
+  const bool removed = f[1] != 0;
+  GPP_LAUNCH(singleton_rows_commit, grid_stride_blocks(m), kThreads, 0, s, m, n, remove.p, plan.keep_row.p);
+  std::swap(plan.l, cl);
+  std::swap(plan.u, cu);
+  plan.has_row_action = plan.has_change = true;
+  plan.has_row_deletion = plan.has_row_deletion || removed;
+}
+
+}  // namespace gpp

@@ -1,0 +1,148 @@
+"""ctypes mirror of include/gpp.h and the loader of the CUDA engine.
+
+The engine is the shared library ``libgpp_b200.so`` built in this directory by
+``build.py`` (sm_100a).  ``load()`` fails loudly when it is missing: there is
+no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpp_b200.so")
+
+u8, i32, i64, f64 = C.c_uint8, C.c_int32, C.c_int64, C.c_double
+P = C.POINTER
+
+
+class Csr(C.Structure):
+    _fields_ = [("rows", i32), ("cols", i32), ("nnz", i32),
+                ("rowPtr", C.c_void_p), ("colVal", C.c_void_p), ("nzVal", C.c_void_p)]
+
+
+class Lp(C.Structure):
+    _fields_ = [("A", Csr), ("AT", Csr), ("c", C.c_void_p), ("AL", C.c_void_p),
+                ("AU", C.c_void_p), ("l", C.c_void_p), ("u", C.c_void_p),
+                ("obj_constant", f64), ("AT_leading_slack", i32), ("AT_slack_after", C.c_void_p)]
+
+
+_PARAM_FIELDS = [
+    ("max_iters", i32, 512), ("max_time", f64, math.inf), ("verbose", u8, 0),
+    ("record_postsolve_tape", u8, 1), ("record_postsolve_tape_cpu", u8, 0),
+    ("enable_presolve", u8, 1), ("enable_folding", u8, 1), ("folding_tolerance", f64, 1e-8),
+    ("feasibility_tol", f64, 1e-6), ("bound_tol", f64, 1e-6), ("zero_tol", f64, 1e-10),
+    ("bound_strengthening_upper_relaxation_factor", f64, 1.0),
+    ("bound_strengthening_max_rounds", i32, 64),
+    ("bound_strengthening_max_bound_only_rounds", i32, 64),
+    ("bound_strengthening_preserve_free_zero_cost", u8, 1),
+    ("doubleton_equations_max_fill_in_proxy", i32, 96), ("doubleton_equations_scan", u8, 1),
+    ("doubleton_equations_min_selected_per_batch", i32, 256),
+    ("doubleton_equations_min_selected_ratio", f64, 0.005),
+    ("doubleton_equations_max_batch_rounds", i32, 0), ("doubleton_equations_max_time", f64, 0.0),
+    ("enable_infeasible_and_fixed_variables", u8, 1), ("enable_empty_rows", u8, 1),
+    ("enable_singleton_rows", u8, 1), ("enable_infeasible_and_redundant_rows", u8, 1),
+    ("enable_bound_strengthening", u8, 1), ("enable_parallel_rows", u8, 1),
+    ("enable_empty_columns", u8, 1), ("enable_singleton_columns", u8, 1),
+    ("enable_doubleton_equations", u8, 1), ("enable_dual_fix", u8, 1),
+    ("dual_fix_max_nonzero_cost_col_degree", i32, 128), ("enable_parallel_columns", u8, 1),
+    ("parallel_columns_max_abs_ratio", f64, 2.0),
+    ("parallel_columns_scale_guard_max_group_size", i32, 4),
+    ("parallel_columns_scale_guard_min_groups", i32, 128),
+    ("enable_structure_specific_rules", u8, 1), ("enable_redundant_variable_bounds", u8, 0),
+    ("enable_startup", u8, 1), ("bound_strengthening_bound_only_nnz_round_budget", i64, 8_000_000),
+]
+
+
+class Params(C.Structure):
+    _fields_ = [(name, typ) for name, typ, _ in _PARAM_FIELDS]
+
+    @classmethod
+    def defaults(cls, **overrides) -> "Params":
+        p = cls()
+        for name, _, value in _PARAM_FIELDS:
+            setattr(p, name, value)
+        for k, v in overrides.items():
+            if not hasattr(p, k):
+                raise AttributeError(k)
+            setattr(p, k, v)
+        return p
+
+
+RULE_FLAGS = ["enable_infeasible_and_fixed_variables", "enable_empty_rows", "enable_singleton_rows",
+              "enable_infeasible_and_redundant_rows", "enable_bound_strengthening",
+              "enable_parallel_rows", "enable_empty_columns", "enable_singleton_columns",
+              "enable_doubleton_equations", "enable_dual_fix", "enable_parallel_columns"]
+
+
+def params_with_rules(rules, **extra) -> Params:
+    """Parameters with exactly the named rules enabled (names without 'enable_')."""
+    kw = {f: 0 for f in RULE_FLAGS}
+    for r in rules:
+        kw["enable_" + r] = 1
+    kw.update(extra)
+    return Params.defaults(**kw)
+
+
+class Summary(C.Structure):
+    _fields_ = [("original_rows", i32), ("original_cols", i32), ("reduced_rows", i32),
+                ("reduced_cols", i32), ("reduced_nnz", i32), ("iterations", i32),
+                ("stopped_at_iteration_limit", u8), ("has_change", u8), ("has_infeasible", u8),
+                ("has_unbounded", u8), ("presolve_enabled", u8), ("folding_applied", u8),
+                ("owns_reduced_lp", u8), ("elapsed_seconds", f64), ("preprocessing_seconds", f64),
+                ("obj_constant_delta", f64), ("reduced_lp", Lp), ("record", C.c_void_p)]
+
+
+_lib = None
+
+
+def load():
+    """Load the engine library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA engine not built: {LIB_PATH} is missing (run build.py)")
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "gpp_default_params": (None, [P(Params)]),
+        "gpp_preprocess": (C.c_int, [P(Lp), P(Params), P(Summary)]),
+        "gpp_run_presolve": (C.c_int, [P(Lp), P(Params), C.c_int, P(Summary)]),
+        "gpp_postprocess": (C.c_int, [vp, vp, vp, P(Summary), P(Lp), vp, vp, vp]),
+        "gpp_postsolve_device": (C.c_int, [vp, vp, vp, P(Summary), P(Lp), vp, vp, vp]),
+        "gpp_free_summary": (None, [P(Summary)]),
+        "gpp_export_maps": (C.c_int, [P(Summary), vp, vp]),
+        "gpp_tape_sizes": (C.c_int, [P(Summary), P(i64), P(i64), P(i64), P(i64)]),
+        "gpp_export_tape": (C.c_int, [P(Summary), vp, vp, vp, vp, vp, vp, vp]),
+        "gpp_row_activity_summary": (C.c_int, [P(Csr), vp, vp, f64, vp, vp, vp, vp, vp, vp, vp]),
+        "gpp_live_stats": (C.c_int, [P(Csr), vp, vp, vp, vp, vp, vp, vp, vp]),
+        "gpp_col_max_abs": (C.c_int, [P(Csr), vp, vp]),
+        "gpp_compact_and_transpose": (C.c_int, [P(Csr), vp, vp, P(Csr), P(Csr)]),
+        "gpp_parallel_row_hashes": (C.c_int, [P(Csr), vp, vp, C.c_int, vp]),
+        "gpp_device_free": (None, [vp]),
+        "gpp_last_error": (C.c_char_p, []),
+        "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+EXPORTED = [
+    "gpp_default_params", "gpp_preprocess", "gpp_run_presolve", "gpp_postprocess",
+    "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
+    "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
+    "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_device_free",
+    "gpp_last_error", "gpp_kernel_launches",
+]
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = load().gpp_last_error().decode(errors="replace")
+        raise RuntimeError(f"gpp error {status}: {msg}")

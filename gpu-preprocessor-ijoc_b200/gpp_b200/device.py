@@ -1,0 +1,174 @@
+"""Host-side mirror of the reference's plain-path API over the C ABI.
+
+``DeviceLp`` uploads a host LP to CUDA memory (torch tensors are used only as
+device allocations) and exposes the ``gpp_lp`` view the engine expects.
+``preprocess`` / ``postprocess`` / ``free_summary`` mirror
+gpu_preprocessor::preprocess/postprocess/free_summary
+(cpp/include/gpu_preprocessor/gpu_preprocessor.hpp:22-39); errors surface as
+the same Python exception families the reference's C++ exceptions map to.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+
+_ERR = {1: RuntimeError, 2: OverflowError, 3: ValueError, 4: RuntimeError, 5: RuntimeError}
+
+
+def _raise(status: int):
+    if status:
+        msg = capi.load().gpp_last_error().decode(errors="replace")
+        raise _ERR.get(status, RuntimeError)(f"gpp status {status}: {msg}")
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("no CUDA device")
+    return torch
+
+
+def to_device(arr, dtype=None):
+    torch = _torch()
+    a = np.ascontiguousarray(arr if dtype is None else np.asarray(arr, dtype=dtype))
+    return torch.from_numpy(a).to("cuda")
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None and t.numel() else C.c_void_p(0)
+
+
+class DeviceLp:
+    """A host LP uploaded to the GPU; keeps the tensors alive."""
+
+    def __init__(self, lp, pinned: bool = False):
+        torch = _torch()
+        lp.ensure_transpose()
+        self.host = lp
+        self.m, self.n, self.nnz = lp.m, lp.n, lp.nnz
+        arrays = {
+            "A_ptr": (lp.row_ptr, np.int32), "A_idx": (lp.col_idx, np.int32), "A_val": (lp.values, np.float64),
+            "AT_ptr": (lp.at_ptr, np.int32), "AT_idx": (lp.at_idx, np.int32), "AT_val": (lp.at_val, np.float64),
+            "c": (lp.c, np.float64), "AL": (lp.AL, np.float64), "AU": (lp.AU, np.float64),
+            "l": (lp.l, np.float64), "u": (lp.u, np.float64),
+        }
+        self.t = {}
+        for k, (a, dt) in arrays.items():
+            h = torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt)))
+            if pinned:
+                h = h.pin_memory()
+            self.t[k] = h.to("cuda", non_blocking=pinned)
+        self.obj_constant = float(lp.obj_constant)
+
+    def struct(self) -> capi.Lp:
+        t = self.t
+        A = capi.Csr(self.m, self.n, self.nnz, ptr(t["A_ptr"]), ptr(t["A_idx"]), ptr(t["A_val"]))
+        AT = capi.Csr(self.n, self.m, self.nnz, ptr(t["AT_ptr"]), ptr(t["AT_idx"]), ptr(t["AT_val"]))
+        return capi.Lp(A, AT, ptr(t["c"]), ptr(t["AL"]), ptr(t["AU"]), ptr(t["l"]), ptr(t["u"]),
+                       self.obj_constant, 0, None)
+
+
+def _d2h(p, count, dtype):
+    """Copy `count` elements of a device pointer into a new numpy array."""
+    torch = _torch()
+    out = np.zeros(count, dtype=dtype)
+    if count and p:
+        torch.cuda.synchronize()
+        cudart = _cudart()
+        st = cudart.cudaMemcpy(C.c_void_p(out.ctypes.data), C.c_void_p(p), C.c_size_t(out.nbytes), 2)
+        if st:
+            raise RuntimeError(f"cudaMemcpy failed ({st})")
+    return out
+
+
+_CUDART = None
+
+
+def _cudart():
+    global _CUDART
+    if _CUDART is None:
+        import glob
+        import os
+        import torch
+        cands = glob.glob(os.path.join(os.path.dirname(torch.__file__), "lib", "libcudart.so*"))
+        cands += glob.glob("/usr/local/cuda/lib64/libcudart.so*")
+        for c in cands:
+            try:
+                _CUDART = C.CDLL(c)
+                break
+            except OSError:
+                continue
+        if _CUDART is None:
+            _CUDART = C.CDLL("libcudart.so")
+        _CUDART.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    return _CUDART
+
+
+class Result:
+    """Host copy of a presolve summary and its reduced LP, maps and tape."""
+
+    def __init__(self, summary: capi.Summary, copy_lp: bool = True, copy_tape: bool = True):
+        lib = capi.load()
+        s = summary
+        self.summary = s
+        m, n, nnz = s.reduced_rows, s.reduced_cols, s.reduced_nnz
+        if copy_lp and s.has_infeasible == 0 and s.has_unbounded == 0:
+            L = s.reduced_lp
+            self.A_ptr = _d2h(L.A.rowPtr, m + 1, np.int32)
+            self.A_idx = _d2h(L.A.colVal, nnz, np.int32)
+            self.A_val = _d2h(L.A.nzVal, nnz, np.float64)
+            self.AT_ptr = _d2h(L.AT.rowPtr, n + 1, np.int32)
+            self.AT_idx = _d2h(L.AT.colVal, nnz, np.int32)
+            self.AT_val = _d2h(L.AT.nzVal, nnz, np.float64)
+            self.c = _d2h(L.c, n, np.float64)
+            self.l = _d2h(L.l, n, np.float64)
+            self.u = _d2h(L.u, n, np.float64)
+            self.AL = _d2h(L.AL, m, np.float64)
+            self.AU = _d2h(L.AU, m, np.float64)
+            self.obj_constant = L.obj_constant
+        self.row_map = np.zeros(m, np.int32)
+        self.col_map = np.zeros(n, np.int32)
+        _raise(lib.gpp_export_maps(C.byref(s), self.row_map.ctypes.data_as(C.c_void_p),
+                                   self.col_map.ctypes.data_as(C.c_void_p)))
+        if copy_tape:
+            r, i, v, f = (C.c_int64() for _ in range(4))
+            _raise(lib.gpp_tape_sizes(C.byref(s), C.byref(r), C.byref(i), C.byref(v), C.byref(f)))
+            self.tape_types = np.zeros(r.value, np.int32)
+            self.tape_is = np.zeros(r.value + 1, np.int64)
+            self.tape_vs = np.zeros(r.value + 1, np.int64)
+            self.tape_idx = np.zeros(i.value, np.int32)
+            self.tape_val = np.zeros(v.value)
+            self.fixed_idx = np.zeros(f.value, np.int32)
+            self.fixed_val = np.zeros(f.value)
+            _raise(lib.gpp_export_tape(C.byref(s), *(a.ctypes.data_as(C.c_void_p) for a in (
+                self.tape_types, self.tape_is, self.tape_vs, self.tape_idx, self.tape_val, self.fixed_idx,
+                self.fixed_val))))
+
+
+def preprocess(dlp: DeviceLp, params=None) -> capi.Summary:
+    lib = capi.load()
+    params = params or capi.Params.defaults()
+    s = capi.Summary()
+    lp = dlp.struct()
+    _raise(lib.gpp_preprocess(C.byref(lp), C.byref(params), C.byref(s)))
+    return s
+
+
+def postprocess(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp):
+    """x/y/z_red: torch CUDA float64 tensors in reduced order; returns host numpy x, y, z."""
+    lib = capi.load()
+    x = np.zeros(summary.original_cols)
+    y = np.zeros(summary.original_rows)
+    z = np.zeros(summary.original_cols)
+    lp = original.struct()
+    _raise(lib.gpp_postprocess(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
+                               x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                               z.ctypes.data_as(C.c_void_p)))
+    return x, y, z
+
+
+def free_summary(summary: capi.Summary) -> None:
+    capi.load().gpp_free_summary(C.byref(summary))

@@ -1,0 +1,319 @@
+"""Seeded synthetic LP generators for the presolve workloads.
+
+The LPs have the form ``min c'x  s.t.  AL <= A x <= AU,  l <= x <= u`` and are
+returned as host CSR arrays (int32 indices, float64 values) plus the CSR of
+A^T, matching the device layout of ``LPInfoGpu`` in the reference
+(cpp/include/gpu_preprocessor/presolve/presolve_structs.hpp:160-180).
+
+Three families are produced:
+
+* ``random_lp(m, n, seed, hub_rows=0)`` -- the "plain presolve" family: per
+  column 1+Poisson(4) nonzeros at uniform rows, values U[-10,10] on a 1e-3 grid,
+  with injected singleton rows (5%), two-entry equality rows (5%), scaled copy
+  rows (3%), scaled copy columns (2%) and empty columns (2%).  Row sides come
+  from a planted point x0 so the LP is feasible.  ``hub_rows`` extra rows get
+  log-uniform lengths in [500, 5000] to skew the row-length distribution.
+  The 2,000 x 5,000 instance is the CPU-runnable case; 2,000,000 x 5,000,000
+  with 2,000 hub rows (~29M nonzeros) is the single-GPU scale case.
+* ``qap_lp(N, seed)`` -- the LP relaxation of a quadratic assignment problem in
+  Adams-Johnson form, laid out row-for-row and column-for-column like the
+  reference's QAP exporter (scripts/generate_qap20.jl:26-112), with flow and
+  distance matrices drawn i.i.d. from {0..9} (zero diagonal).
+
+Nothing here reads a benchmark data set; every instance is synthetic.
+"""
+from __future__ import annotations
+
+import dataclasses
+import struct
+
+import numpy as np
+
+INF = np.inf
+
+
+@dataclasses.dataclass
+class HostLP:
+    m: int
+    n: int
+    row_ptr: np.ndarray   # int32 [m+1]
+    col_idx: np.ndarray   # int32 [nnz]
+    values: np.ndarray    # float64 [nnz]
+    c: np.ndarray
+    AL: np.ndarray
+    AU: np.ndarray
+    l: np.ndarray
+    u: np.ndarray
+    obj_constant: float = 0.0
+    at_ptr: np.ndarray | None = None
+    at_idx: np.ndarray | None = None
+    at_val: np.ndarray | None = None
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_ptr[-1])
+
+    def ensure_transpose(self) -> "HostLP":
+        if self.at_ptr is None:
+            self.at_ptr, self.at_idx, self.at_val = csr_transpose(
+                self.m, self.n, self.row_ptr, self.col_idx, self.values)
+        return self
+
+
+def csr_transpose(m, n, ptr, idx, val):
+    """Stable CSR transpose: rows of A^T list the rows of A in ascending order."""
+    rows = np.repeat(np.arange(m, dtype=np.int32), np.diff(ptr))
+    order = np.argsort(idx, kind="stable")
+    t_idx = rows[order].astype(np.int32)
+    t_val = val[order].astype(np.float64)
+    counts = np.bincount(idx, minlength=n)
+    t_ptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(counts, out=t_ptr[1:])
+    return t_ptr.astype(np.int32), t_idx, t_val
+
+
+def coo_to_csr(m, rows, cols, vals):
+    order = np.lexsort((cols, rows))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    counts = np.bincount(rows, minlength=m)
+    ptr = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(counts, out=ptr[1:])
+    if ptr[-1] > np.iinfo(np.int32).max:
+        raise ValueError("nnz exceeds the int32 offset range")
+    return ptr.astype(np.int32), cols.astype(np.int32), vals.astype(np.float64)
+
+
+def _grid_values(rng, k):
+    v = np.round(rng.uniform(-10.0, 10.0, size=k), 3)
+    bad = v == 0.0
+    while bad.any():
+        v[bad] = np.round(rng.uniform(-10.0, 10.0, size=int(bad.sum())), 3)
+        bad = v == 0.0
+    return v
+
+
+def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
+    """Plain-presolve family (see module docstring)."""
+    rng = np.random.default_rng(seed)
+    n_single = int(round(0.05 * m))
+    n_dton = int(round(0.05 * m))
+    n_copy_rows = int(round(0.03 * m))
+    n_normal = m - n_single - n_dton - n_copy_rows
+    if n_normal < 1:
+        raise ValueError("too few rows")
+    # Row roles are interleaved by a permutation so no rule sees a block layout.
+    role = np.zeros(m, dtype=np.int8)  # 0 normal, 1 singleton, 2 doubleton eq, 3 copy
+    role[n_normal:n_normal + n_single] = 1
+    role[n_normal + n_single:n_normal + n_single + n_dton] = 2
+    role[n_normal + n_single + n_dton:] = 3
+    role = role[rng.permutation(m)]
+    normal_rows = np.flatnonzero(role == 0).astype(np.int64)
+
+    n_empty = int(round(0.02 * n))
+    n_copy_cols = int(round(0.02 * n))
+    crole = np.zeros(n, dtype=np.int8)  # 0 regular, 1 copy, 2 empty
+    crole[:n_copy_cols] = 1
+    crole[n_copy_cols:n_copy_cols + n_empty] = 2
+    crole = crole[rng.permutation(n)]
+    regular_cols = np.flatnonzero(crole == 0).astype(np.int64)
+
+    # Regular columns: 1 + Poisson(4) entries at uniformly drawn normal rows.
+    per_col = 1 + rng.poisson(4.0, size=regular_cols.size)
+    cols = np.repeat(regular_cols, per_col)
+    rows = normal_rows[rng.integers(0, normal_rows.size, size=cols.size)]
+    key = np.unique(cols * m + rows)            # drop repeated (row, col) draws
+    cols, rows = key // m, key % m
+    vals = _grid_values(rng, rows.size)
+
+    # Hub rows: extra long rows over regular columns (log-uniform lengths).
+    if hub_rows > 0:
+        hubs = rng.choice(normal_rows, size=hub_rows, replace=False)
+        lengths = np.exp(rng.uniform(np.log(500.0), np.log(5000.0), size=hub_rows)).astype(np.int64)
+        lengths = np.minimum(lengths, regular_cols.size)
+        h_rows = np.repeat(hubs, lengths)
+        h_cols = regular_cols[rng.integers(0, regular_cols.size, size=h_rows.size)]
+        hkey = np.unique(np.concatenate([cols * m + rows, h_cols * m + h_rows]))
+        new = np.setdiff1d(hkey, cols * m + rows, assume_unique=True)
+        new_cols, new_rows = new // m, new % m
+        cols = np.concatenate([cols, new_cols])
+        rows = np.concatenate([rows, new_rows])
+        vals = np.concatenate([vals, _grid_values(rng, new.size)])
+
+    # Copy columns: a regular column scaled by a factor in [0.5, 4] of random sign.
+    copy_cols = np.flatnonzero(crole == 1)
+    src_cols = regular_cols[rng.integers(0, regular_cols.size, size=copy_cols.size)]
+    col_factor = rng.uniform(0.5, 4.0, size=copy_cols.size) * rng.choice([-1.0, 1.0], size=copy_cols.size)
+    order = np.argsort(cols, kind="stable")
+    cols, rows, vals = cols[order], rows[order], vals[order]
+    cstart = np.searchsorted(cols, src_cols, side="left")
+    cstop = np.searchsorted(cols, src_cols, side="right")
+    lens = cstop - cstart
+    take = np.concatenate([np.arange(a, b) for a, b in zip(cstart, cstop)]) if lens.sum() else np.zeros(0, np.int64)
+    cc_cols = np.repeat(copy_cols, lens)
+    cc_rows = rows[take]
+    cc_vals = vals[take] * np.repeat(col_factor, lens)
+    cols = np.concatenate([cols, cc_cols])
+    rows = np.concatenate([rows, cc_rows])
+    vals = np.concatenate([vals, cc_vals])
+
+    # Copy rows: a normal row scaled by U[0.5, 4].
+    copy_rows = np.flatnonzero(role == 3)
+    src_rows = normal_rows[rng.integers(0, normal_rows.size, size=copy_rows.size)]
+    row_factor = rng.uniform(0.5, 4.0, size=copy_rows.size)
+    order = np.lexsort((cols, rows))
+    cols, rows, vals = cols[order], rows[order], vals[order]
+    rstart = np.searchsorted(rows, src_rows, side="left")
+    rstop = np.searchsorted(rows, src_rows, side="right")
+    rlens = rstop - rstart
+    rtake = np.concatenate([np.arange(a, b) for a, b in zip(rstart, rstop)]) if rlens.sum() else np.zeros(0, np.int64)
+    cr_rows = np.repeat(copy_rows, rlens)
+    cr_cols = cols[rtake]
+    cr_vals = vals[rtake] * np.repeat(row_factor, rlens)
+
+    # Singleton rows and two-entry equality rows over regular columns.
+    s_rows = np.flatnonzero(role == 1)
+    s_cols = regular_cols[rng.integers(0, regular_cols.size, size=s_rows.size)]
+    s_vals = _grid_values(rng, s_rows.size)
+    d_rows = np.flatnonzero(role == 2)
+    d1 = rng.integers(0, regular_cols.size, size=d_rows.size)
+    d2 = (d1 + 1 + rng.integers(0, regular_cols.size - 1, size=d_rows.size)) % regular_cols.size
+    d_cols = np.stack([regular_cols[d1], regular_cols[d2]], axis=1).reshape(-1)
+    d_rows2 = np.repeat(d_rows, 2)
+    d_vals = _grid_values(rng, d_rows2.size)
+
+    rows = np.concatenate([rows, cr_rows, s_rows, d_rows2]).astype(np.int64)
+    cols = np.concatenate([cols, cr_cols, s_cols, d_cols]).astype(np.int64)
+    vals = np.concatenate([vals, cr_vals, s_vals, d_vals]).astype(np.float64)
+    ptr, idx, val = coo_to_csr(m, rows, cols, vals)
+
+    # Bounds, planted point, sides and costs.
+    l = np.zeros(n)
+    u = rng.uniform(1.0, 100.0, size=n)
+    inf_u = rng.random(n) < 0.2
+    u[inf_u] = INF
+    x0 = np.where(inf_u, rng.uniform(0.0, 10.0, size=n), rng.uniform(0.0, 1.0, size=n) * u)
+    x0 = np.where(inf_u, x0, np.minimum(x0, u))
+    act = np.add.reduceat(val * x0[idx], ptr[:-1]) if idx.size else np.zeros(m)
+    act = np.where(np.diff(ptr) > 0, act, 0.0)
+    s_lo = rng.uniform(0.0, 5.0, size=m)
+    s_hi = rng.uniform(0.0, 5.0, size=m)
+    lo_fin = rng.random(m) < 0.5
+    hi_fin = rng.random(m) < 0.5
+    AL = np.where(lo_fin, act - s_lo, -INF)
+    AU = np.where(hi_fin, act + s_hi, INF)
+    eq = role == 2
+    AL[eq] = act[eq]
+    AU[eq] = act[eq]
+    c = rng.standard_normal(n)
+    c[inf_u] = np.abs(c[inf_u])
+    return HostLP(m, n, ptr, idx, val, c, AL, AU, l, u).ensure_transpose()
+
+
+def qap_lp(N: int, seed: int = 0) -> HostLP:
+    """Adams-Johnson QAP relaxation in the reference exporter's row/column order."""
+    rng = np.random.default_rng(seed)
+    flow = rng.integers(0, 10, size=(N, N)).astype(np.float64)
+    dist = rng.integers(0, 10, size=(N, N)).astype(np.float64)
+    np.fill_diagonal(flow, 0.0)
+    np.fill_diagonal(dist, 0.0)
+    n2, n3, n4 = N * N, N ** 3, N ** 4
+    neq = 2 * N + 2 * n3 + n4
+    m = n4 + neq + n2
+    n = n2 + n4
+    eq0 = n4                      # first equality row
+    rng_rows0 = n4 + neq          # first ranged row
+    # Zero-based index helpers matching idx2/idx3/idx4 (column-major, 1-based in the exporter).
+    i, j = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    i, j = i.reshape(-1), j.reshape(-1)
+    xcol = i + N * j
+    R, C, V = [], [], []
+    t = np.arange(N)
+    # x[i,j] column entries.
+    R += [eq0 + i, eq0 + N + j]
+    C += [xcol, xcol]
+    V += [np.ones(n2), np.ones(n2)]
+    for tt in range(N):
+        R.append(eq0 + 2 * N + (tt + N * i + n2 * j))
+        C.append(xcol)
+        V.append(-np.ones(n2))
+        R.append(eq0 + 2 * N + n3 + (tt + N * i + n2 * j))
+        C.append(xcol)
+        V.append(-np.ones(n2))
+    R.append(rng_rows0 + xcol)
+    C.append(xcol)
+    V.append(np.ones(n2))
+    # y[i,j,k,l] column entries.
+    ii, jj, kk, ll = np.meshgrid(t, t, t, t, indexing="ij")
+    ii, jj, kk, ll = (a.reshape(-1) for a in (ii, jj, kk, ll))
+    q = ii + N * jj + n2 * kk + n3 * ll
+    rq = kk + N * ll + n2 * ii + n3 * jj
+    ycol = n2 + q
+    R += [q, eq0 + 2 * N + (jj + N * kk + n2 * ll), eq0 + 2 * N + n3 + (ii + N * kk + n2 * ll)]
+    C += [ycol, ycol, ycol]
+    V += [-np.ones(n4), np.ones(n4), np.ones(n4)]
+    off = q != rq
+    first = np.minimum(q, rq)[off]
+    second = np.maximum(q, rq)[off]
+    sign = np.where(q < rq, 1.0, -1.0)[off]
+    R += [eq0 + 2 * N + 2 * n3 + first, eq0 + 2 * N + 2 * n3 + second]
+    C += [ycol[off], ycol[off]]
+    V += [sign, -sign]
+    rows = np.concatenate(R).astype(np.int64)
+    cols = np.concatenate(C).astype(np.int64)
+    vals = np.concatenate(V).astype(np.float64)
+    ptr, idx, val = coo_to_csr(m, rows, cols, vals)
+    c = np.zeros(n)
+    c[n2 + q] = flow[ii, kk] * dist[jj, ll]
+    AL = np.empty(m)
+    AU = np.empty(m)
+    AL[:n4], AU[:n4] = -INF, 0.0
+    AL[eq0:eq0 + neq] = 0.0
+    AU[eq0:eq0 + neq] = 0.0
+    AL[eq0:eq0 + 2 * N] = 1.0
+    AU[eq0:eq0 + 2 * N] = 1.0
+    AL[rng_rows0:], AU[rng_rows0:] = 0.0, 1.0
+    l = np.full(n, -INF)
+    u = np.full(n, INF)
+    return HostLP(m, n, ptr, idx, val, c, AL, AU, l, u).ensure_transpose()
+
+
+def workload(name: str, seed: int = 0) -> HostLP:
+    """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30'."""
+    if name == "small":
+        return random_lp(2000, 5000, seed)
+    if name == "scale":
+        return random_lp(2_000_000, 5_000_000, seed, hub_rows=2000)
+    if name == "qap30":
+        return qap_lp(30, seed)
+    if name.startswith("random:"):
+        m, n = (int(v) for v in name.split(":")[1].split("x"))
+        return random_lp(m, n, seed)
+    if name.startswith("qap:"):
+        return qap_lp(int(name.split(":")[1]), seed)
+    raise ValueError(f"unknown workload {name!r}")
+
+
+_MAGIC = b"GPPLP001"
+
+
+def save_lp(path: str, lp: HostLP) -> None:
+    """Binary LP file: magic, m, n, nnz, then A (CSR), c, l, u, AL, AU, obj_constant."""
+    with open(path, "wb") as f:
+        f.write(_MAGIC)
+        f.write(struct.pack("<qqqd", lp.m, lp.n, lp.nnz, lp.obj_constant))
+        for arr, dt in ((lp.row_ptr, np.int32), (lp.col_idx, np.int32), (lp.values, np.float64),
+                        (lp.c, np.float64), (lp.l, np.float64), (lp.u, np.float64),
+                        (lp.AL, np.float64), (lp.AU, np.float64)):
+            f.write(np.ascontiguousarray(arr, dtype=dt).tobytes())
+
+
+def load_lp(path: str) -> HostLP:
+    with open(path, "rb") as f:
+        if f.read(8) != _MAGIC:
+            raise ValueError("not an LP file")
+        m, n, nnz, obj = struct.unpack("<qqqd", f.read(32))
+        rd = lambda k, dt: np.frombuffer(f.read(k * np.dtype(dt).itemsize), dtype=dt).copy()
+        ptr, idx, val = rd(m + 1, np.int32), rd(nnz, np.int32), rd(nnz, np.float64)
+        c, l, u, AL, AU = (rd(n, np.float64), rd(n, np.float64), rd(n, np.float64),
+                           rd(m, np.float64), rd(m, np.float64))
+    return HostLP(m, n, ptr, idx, val, c, AL, AU, l, u, obj).ensure_transpose()

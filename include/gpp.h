@@ -1,0 +1,256 @@
+/*
+ * gpp.h -- C ABI of the B200-native LP presolve / postsolve engine.
+ *
+ * This is the drop-in boundary for the plain presolve path of GPU-Preprocessor.
+ * Every entry point takes plain pointers and sizes (device pointers where the
+ * reference takes device pointers), returns an int status (0 = success) and
+ * never throws.  The C++ API of the reference (namespaces gpu_preprocessor,
+ * gpu_preprocessor::presolve, gpu_preprocessor::folding) is provided as a
+ * header-only layer over these functions in include/gpu_preprocessor/.
+ *
+ * Layouts follow the reference's public structs:
+ *   gpp_csr      <-> DeviceCsrMatrix   (cpp/include/gpu_preprocessor/presolve/presolve_structs.hpp:160-167)
+ *   gpp_lp       <-> LPInfoGpu         (presolve_structs.hpp:169-180)
+ *   gpp_params   <-> PresolveParams    (presolve_structs.hpp:28-158)
+ *   gpp_summary  <-> GpuPresolveSummary + FoldingPipelineSummary
+ *                                      (presolve/gpu_presolve.hpp:14-30, folding/folding_structs.hpp:94-109)
+ * Offsets (NnzOffset) are int32, the reference's default ABI
+ * (cpp/include/gpu_preprocessor/offset.hpp:12-19).
+ */
+#ifndef GPP_H_
+#define GPP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GPP_API __attribute__((visibility("default")))
+#else
+#define GPP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gpp_offset;
+
+/* Status codes.  Model status (infeasible / unbounded) is reported in the
+ * summary, not as an error, exactly as the reference does
+ * (presolve/gpu_presolve.hpp:25-26). */
+enum {
+  GPP_OK = 0,
+  GPP_ERR_CUDA = 1,          /* maps to std::runtime_error("context: cudaGetErrorString") */
+  GPP_ERR_LENGTH = 2,        /* maps to std::length_error (offset overflow, offset.hpp:20-30) */
+  GPP_ERR_INVALID = 3,       /* maps to std::invalid_argument (bad CSR / tolerance, folding.cu:79-81) */
+  GPP_ERR_RUNTIME = 4,       /* other std::runtime_error */
+  GPP_ERR_NO_DEVICE = 5      /* the CUDA extension cannot run: no device */
+};
+
+typedef struct gpp_csr {
+  int32_t rows;
+  int32_t cols;
+  gpp_offset nnz;
+  gpp_offset* rowPtr;
+  int32_t* colVal;
+  double* nzVal;
+} gpp_csr;
+
+typedef struct gpp_lp {
+  gpp_csr A;
+  gpp_csr AT;
+  double* c;
+  double* AL;
+  double* AU;
+  double* l;
+  double* u;
+  double obj_constant;
+  gpp_offset AT_leading_slack;
+  gpp_offset* AT_slack_after;
+} gpp_lp;
+
+/* Field order and defaults of PresolveParams (presolve_structs.hpp:28-158).
+ * bools are uint8_t; the residual-bound-mode enum is a uint8_t. */
+typedef struct gpp_params {
+  int32_t max_iters;
+  double max_time;
+  uint8_t verbose;
+  uint8_t record_postsolve_tape;
+  uint8_t record_postsolve_tape_cpu;
+  uint8_t enable_presolve;
+  uint8_t enable_folding;
+  double folding_tolerance;
+  double feasibility_tol;
+  double bound_tol;
+  double zero_tol;
+  double bound_strengthening_upper_relaxation_factor;
+  int32_t bound_strengthening_max_rounds;
+  int32_t bound_strengthening_max_bound_only_rounds;
+  uint8_t bound_strengthening_preserve_free_zero_cost;
+  int32_t doubleton_equations_max_fill_in_proxy;
+  uint8_t doubleton_equations_scan;
+  int32_t doubleton_equations_min_selected_per_batch;
+  double doubleton_equations_min_selected_ratio;
+  int32_t doubleton_equations_max_batch_rounds;
+  double doubleton_equations_max_time;
+  uint8_t enable_infeasible_and_fixed_variables;
+  uint8_t enable_empty_rows;
+  uint8_t enable_singleton_rows;
+  uint8_t enable_infeasible_and_redundant_rows;
+  uint8_t enable_bound_strengthening;
+  uint8_t enable_parallel_rows;
+  uint8_t enable_empty_columns;
+  uint8_t enable_singleton_columns;
+  uint8_t enable_doubleton_equations;
+  uint8_t enable_dual_fix;
+  int32_t dual_fix_max_nonzero_cost_col_degree;
+  uint8_t enable_parallel_columns;
+  double parallel_columns_max_abs_ratio;
+  int32_t parallel_columns_scale_guard_max_group_size;
+  int32_t parallel_columns_scale_guard_min_groups;
+  /* Master switch of the structure-specific startup rules.  They are outside
+   * this engine's scope: a nonzero value is accepted only when the startup
+   * detectors provably cannot fire (see gpp_presolve's documentation). */
+  uint8_t enable_structure_specific_rules;
+  uint8_t enable_redundant_variable_bounds;
+  uint8_t enable_startup;
+  int64_t bound_strengthening_bound_only_nnz_round_budget;
+} gpp_params;
+
+/* Reference defaults (presolve_structs.hpp:28-158). */
+GPP_API void gpp_default_params(gpp_params* params);
+
+/* Opaque GPU-resident postsolve record (PresolveRecordGpu's device state,
+ * presolve_structs.hpp:338-368).  Owned by the summary. */
+typedef struct gpp_record gpp_record;
+
+/* GpuPresolveSummary (presolve/gpu_presolve.hpp:14-30) merged with the
+ * pipeline fields of FoldingPipelineSummary (folding/folding_structs.hpp:94-109). */
+typedef struct gpp_summary {
+  int32_t original_rows;
+  int32_t original_cols;
+  int32_t reduced_rows;
+  int32_t reduced_cols;
+  gpp_offset reduced_nnz;
+  int32_t iterations;
+  uint8_t stopped_at_iteration_limit;
+  uint8_t has_change;
+  uint8_t has_infeasible;
+  uint8_t has_unbounded;
+  uint8_t presolve_enabled;
+  uint8_t folding_applied;
+  uint8_t owns_reduced_lp;
+  double elapsed_seconds;          /* presolve core wall time */
+  double preprocessing_seconds;    /* whole preprocess() wall time */
+  double obj_constant_delta;
+  gpp_lp reduced_lp;               /* device arrays; borrowed from the input when !owns_reduced_lp */
+  gpp_record* record;
+} gpp_summary;
+
+/* ---- Plain pipeline: preprocess / postprocess / free_summary ------------- */
+
+/* gpu_preprocessor::preprocess (cpp/include/gpu_preprocessor/gpu_preprocessor.hpp:22-24),
+ * i.e. folding::run_gpu_presolve_with_folding(lp, params, true, true)
+ * (folding/folding.hpp:48-51).  `lp` is caller-owned device data and is never
+ * written.  The input must provide both A and AT = A^T in CSR form. */
+GPP_API int gpp_preprocess(const gpp_lp* lp, const gpp_params* params, gpp_summary* out);
+
+/* presolve::run_gpu_presolve_with_reduced_lp (presolve/gpu_presolve.hpp:35-36):
+ * presolve only, reduced LP kept.  keep_reduced_lp = 0 gives
+ * run_gpu_presolve_with_record (gpu_presolve.hpp:32-33). */
+GPP_API int gpp_run_presolve(const gpp_lp* lp, const gpp_params* params, int keep_reduced_lp,
+                     gpp_summary* out);
+
+/* gpu_preprocessor::postprocess (gpu_preprocessor.hpp:30-33) /
+ * folding::postsolve_and_unfold_to_host (folding/folding.hpp:53-57).
+ * x_red (reduced_cols), y_red (reduced_rows), z_red (reduced_cols) are
+ * caller-owned device arrays in reduced order; any may be NULL.  x_out (n0),
+ * y_out (m0), z_out (n0) are HOST arrays in original order.  Dual convention
+ * c - A^T y - z = 0.  `original` must be the LP given to preprocess. */
+GPP_API int gpp_postprocess(const double* x_red, const double* y_red, const double* z_red,
+                    const gpp_summary* summary, const gpp_lp* original,
+                    double* x_out, double* y_out, double* z_out);
+
+/* presolve::postsolve_gpu (presolve/gpu_postsolve.hpp:20-31): same as
+ * gpp_postprocess but x_org/y_org/z_org are DEVICE arrays (n0, m0, n0) that
+ * the caller owns.  `original` may be NULL (primal-only recovery, no dual
+ * projection). */
+GPP_API int gpp_postsolve_device(const double* x_red, const double* y_red, const double* z_red,
+                         const gpp_summary* summary, const gpp_lp* original,
+                         double* x_org, double* y_org, double* z_org);
+
+/* gpu_preprocessor::free_summary (gpu_preprocessor.hpp:35-39) /
+ * presolve::free_gpu_presolve_reduced_lp (gpu_presolve.hpp:38).
+ * Idempotent: a second call is a no-op. */
+GPP_API void gpp_free_summary(gpp_summary* summary);
+
+/* Export of the recovery maps (the reference's export_recovery_record,
+ * presolve/device_recovery.hpp:84).  Host arrays of length reduced_rows and
+ * reduced_cols receive the original index of every kept row / column. */
+GPP_API int gpp_export_maps(const gpp_summary* summary, int32_t* row_red2org, int32_t* col_red2org);
+
+/* Size of the postsolve tape held by the record (records, indices, values,
+ * fixed-value entries). */
+GPP_API int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t* indices,
+                   int64_t* values, int64_t* fixed);
+
+/* Copies the tape to host arrays (types[records], index_starts[records+1],
+ * value_starts[records+1], indices[indices], vals[values], fixed_idx[fixed],
+ * fixed_val[fixed]); any pointer may be NULL. */
+GPP_API int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t* index_starts,
+                    int64_t* value_starts, int32_t* indices, double* vals,
+                    int32_t* fixed_idx, double* fixed_val);
+
+/* ---- Kernel-level entry points (rule / kernel parity tests) -------------- */
+
+/* compute_row_activity_summary (presolve/gpu_presolve_kernels.hpp:76-86):
+ * per row finite min/max activity and counts of -inf/+inf contributions,
+ * entries with |a| <= zero_tol skipped, optional keep masks (NULL = all kept)
+ * and optional live degrees used for the short/medium/long row split.  All
+ * pointers are device pointers; runs on the legacy default stream. */
+GPP_API int gpp_row_activity_summary(const gpp_csr* A, const double* l, const double* u,
+                             double zero_tol, const uint8_t* keep_row,
+                             const uint8_t* keep_col, const int32_t* live_degrees,
+                             double* min_fin, double* max_fin,
+                             int32_t* min_inf, int32_t* max_inf);
+
+/* refresh_live_stats (presolve/gpu_presolve_kernels.hpp:45-56) for one side:
+ * live degree, empty / singleton flags, singleton support index and value of
+ * every row of `M` under keep_outer (rows) and keep_inner (columns), plus the
+ * live nonzero total (device u64, may be NULL). */
+GPP_API int gpp_live_stats(const gpp_csr* M, const uint8_t* keep_outer, const uint8_t* keep_inner,
+                   int32_t* degree, uint8_t* empty, uint8_t* singleton,
+                   int32_t* support, double* coefficient, unsigned long long* total);
+
+/* compute_col_max_abs (gpu_presolve_kernels.hpp:88-89): max |a| per row of AT
+ * over kept rows of A. */
+GPP_API int gpp_col_max_abs(const gpp_csr* AT, const uint8_t* keep_row, double* col_max_abs);
+
+/* Stable CSR compaction by row/column keep masks followed by the transpose
+ * (apply_plan_to_working_lp's compact_csr_by_masks_gpu + transpose_csr64,
+ * cpp/src/presolve/gpu_presolve.cu:1793-1930, transpose64.cu:54-117).
+ * Outputs are newly allocated device arrays owned by the caller (free with
+ * gpp_device_free). */
+GPP_API int gpp_compact_and_transpose(const gpp_csr* A, const uint8_t* keep_row, const uint8_t* keep_col,
+                              gpp_csr* A_out, gpp_csr* AT_out);
+
+/* Parallel-row hashes (rule_parallel_rows.cu:132-343): FNV-1a fold of the
+ * pivot-normalised live pattern of every row, mode 0 sequential, 1 XOR
+ * aggregate. */
+GPP_API int gpp_parallel_row_hashes(const gpp_csr* A, const uint8_t* keep_row, const uint8_t* keep_col,
+                            int mode, uint64_t* hashes);
+
+GPP_API void gpp_device_free(void* device_ptr);
+
+/* Last error message of the calling thread ("" when none). */
+GPP_API const char* gpp_last_error(void);
+
+/* Number of CUDA kernels this library launched on the calling thread since
+ * the last reset (used by the benchmark to report its launch count). */
+GPP_API uint64_t gpp_kernel_launches(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPP_H_ */

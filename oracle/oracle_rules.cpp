@@ -1,0 +1,392 @@
+// Oracle presolve rules: CPU restatements of the reference's apply_rule_*
+// functions.  TEST INFRASTRUCTURE ONLY (see oracle.hpp).
+#include "oracle_rules.hpp"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <stdexcept>
+
+namespace oracle {
+
+namespace {
+inline bool fin(double x) { return std::isfinite(x); }
+}
+
+void refresh_stats(Stats& s, const Lp& lp, const Plan& plan) {
+  // refresh_live_stats (gpu_presolve_kernels.cu:493-517): rows over A with
+  // keep_row outer / keep_col inner, columns over AT with the roles swapped.
+  const int m = lp.m(), n = lp.n();
+  s.row_nnz.assign(m, 0); s.empty_row.assign(m, 0); s.singleton_row.assign(m, 0);
+  s.srow_col.assign(m, -1); s.srow_val.assign(m, 0.0);
+  s.col_nnz.assign(n, 0); s.empty_col.assign(n, 0); s.singleton_col.assign(n, 0);
+  s.scol_row.assign(n, -1); s.scol_val.assign(n, 0.0);
+  s.live_nnz = 0;
+  live_stats(lp.A, plan.keep_row.data(), plan.keep_col.data(), s.row_nnz.data(), s.empty_row.data(),
+             s.singleton_row.data(), s.srow_col.data(), s.srow_val.data(), &s.live_nnz);
+  live_stats(lp.AT, plan.keep_col.data(), plan.keep_row.data(), s.col_nnz.data(), s.empty_col.data(),
+             s.singleton_col.data(), s.scol_row.data(), s.scol_val.data(), nullptr);
+}
+
+// Row sums of a_ij * v_j over kept rows and selected columns, in ascending
+// column order (the reference accumulates the same terms with atomicAdd).
+static std::vector<double> row_shift_gather(const Lp& lp, const std::vector<uint8_t>& keep_row,
+                                            const std::vector<uint8_t>& selected,
+                                            const std::vector<double>& value, bool absolute,
+                                            const std::vector<double>* radius = nullptr) {
+  std::vector<double> shift(lp.m(), 0.0);
+  for (int i = 0; i < lp.m(); ++i) {
+    if (!keep_row[i]) continue;
+    double acc = 0.0;
+    for (int p = lp.A.ptr[i]; p < lp.A.ptr[i + 1]; ++p) {
+      const int j = lp.A.idx[p];
+      if (!selected[j]) continue;
+      if (absolute) {
+        if ((*radius)[j] > 0.0) acc += std::fabs(lp.A.val[p]) * (*radius)[j];
+      } else {
+        acc += lp.A.val[p] * value[j];
+      }
+    }
+    shift[i] = acc;
+  }
+  return shift;
+}
+
+static double domain_objective(const std::vector<double>& contrib, const Plan& plan) {
+  // sum_cleanup_domain (cleanup_support.cuh:13-31) restricted to the rule's
+  // entry domain; nonselected entries are zero, so the canonical sum over the
+  // compacted domain equals the sum over the masked full vector.
+  std::vector<double> v(contrib);
+  if (plan.rule_entry_keep_col)
+    for (size_t j = 0; j < v.size(); ++j)
+      if (!(*plan.rule_entry_keep_col)[j]) v[j] = 0.0;
+  return det_sum(v);
+}
+
+void rule_fixed_variables(Plan& plan, const Lp& lp, const gpp_params& p) {
+  // apply_rule_infeasible_and_fixed_variables (rule_infeasible_and_fixed_variables.cu:65-348).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int n = lp.n(), m = lp.m();
+  if (n == 0) return;
+  std::vector<uint8_t> fixed(n, 0);
+  std::vector<double> fval(n, 0.0), contrib(n, 0.0), radius(n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[j]) continue;
+    const double lj = plan.l[j], uj = plan.u[j];
+    if (fin(lj) && fin(uj) && lj <= uj && uj - lj <= p.bound_tol) {
+      const double vj = lj + 0.5 * (uj - lj);
+      radius[j] = std::fmax(vj - lj, uj - vj);
+      fixed[j] = 1;
+      fval[j] = vj;
+      contrib[j] = plan.c[j] * vj;
+    }
+  }
+  // Row error budget (sum of |a| * radius over candidates) and the filter.
+  const std::vector<double> row_error = row_shift_gather(lp, plan.keep_row, fixed, fval, true, &radius);
+  const double budget = 0.1 * p.feasibility_tol;
+  for (int j = 0; j < n; ++j) {
+    if (!fixed[j] || plan.l[j] == plan.u[j]) continue;
+    for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q) {
+      const int row = lp.AT.idx[q];
+      if (plan.keep_row[row] && !(row_error[row] <= budget)) {
+        fixed[j] = 0;
+        contrib[j] = 0.0;
+        break;
+      }
+    }
+  }
+  int count = 0;
+  for (int j = 0; j < n; ++j) count += fixed[j];
+  if (count == 0) return;
+  const std::vector<double> shift = row_shift_gather(lp, plan.keep_row, fixed, fval, false);
+  for (int j = 0; j < n; ++j)
+    if (fixed[j]) { plan.l[j] = fval[j]; plan.u[j] = fval[j]; plan.keep_col[j] = 0; }
+  for (int i = 0; i < m; ++i) { plan.AL[i] -= shift[i]; plan.AU[i] -= shift[i]; }
+  plan.obj_delta += domain_objective(contrib, plan);
+  plan.has_col_action = true;
+  plan.has_change = true;
+}
+
+void rule_empty_columns(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_empty_columns (empty_rows_and_columns/columns.cu:64-249).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int n = lp.n();
+  if (n == 0) return;
+  bool infeasible = false, unbounded = false, any = false;
+  std::vector<uint8_t> fixed(n, 0);
+  std::vector<double> fval(n, 0.0), contrib(n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    if (!(plan.keep_col[j] && s.empty_col[j])) continue;
+    const double cj = plan.c[j], lj = plan.l[j], uj = plan.u[j];
+    if (lj > uj + p.bound_tol) { infeasible = true; continue; }
+    if ((cj > p.zero_tol && !fin(lj)) || (cj < -p.zero_tol && !fin(uj))) { unbounded = true; continue; }
+    double v = 0.0;
+    if (cj > p.zero_tol) v = lj;
+    else if (cj < -p.zero_tol) v = uj;
+    else if (fin(lj)) v = lj;
+    else if (fin(uj)) v = uj;
+    fixed[j] = 1; fval[j] = v; contrib[j] = cj * v; any = true;
+  }
+  if (infeasible) { plan.has_infeasible = true; return; }
+  if (unbounded) { plan.has_unbounded = true; return; }
+  if (!any) return;
+  for (int j = 0; j < n; ++j)
+    if (fixed[j]) { plan.l[j] = fval[j]; plan.u[j] = fval[j]; plan.keep_col[j] = 0; }
+  plan.obj_delta += domain_objective(contrib, plan);
+  plan.has_col_action = true;
+  plan.has_change = true;
+}
+
+void rule_empty_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_empty_rows (empty_rows_and_columns/rows.cu:26-121).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m();
+  if (m == 0) return;
+  bool infeasible = false, any = false;
+  const double tol = p.feasibility_tol;
+  for (int i = 0; i < m; ++i) {
+    if (!(plan.keep_row[i] && s.row_nnz[i] == 0)) continue;
+    if (plan.AL[i] <= tol && plan.AU[i] >= -tol) any = true; else infeasible = true;
+  }
+  if (infeasible) { plan.has_infeasible = true; return; }
+  if (!any) return;
+  for (int i = 0; i < m; ++i)
+    if (plan.keep_row[i] && s.row_nnz[i] == 0 && plan.AL[i] <= tol && plan.AU[i] >= -tol)
+      plan.keep_row[i] = 0;
+  plan.has_row_action = plan.has_row_deletion = plan.has_change = true;
+}
+
+void rule_singleton_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_singleton_rows (rule_singleton_rows.cu:76-275).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (m == 0) return;
+  std::vector<double> cl(plan.l), cu(plan.u);
+  std::vector<uint8_t> remove(m, 0);
+  bool any_remove = false;
+  for (int i = 0; i < m; ++i) {
+    if (!(plan.keep_row[i] && s.singleton_row[i])) continue;
+    const int col = s.srow_col[i];
+    const double a = s.srow_val[i];
+    if (col < 0 || col >= n || !(std::fabs(a) > p.zero_tol)) continue;
+    const double lo = plan.AL[i], hi = plan.AU[i];
+    const double il = a > 0.0 ? lo / a : hi / a;
+    const double iu = a > 0.0 ? hi / a : lo / a;
+    if (!(cl[col] >= il)) cl[col] = il;   // atomic_max_double
+    if (!(cu[col] <= iu)) cu[col] = iu;   // atomic_min_double
+    remove[i] = 1;
+    any_remove = true;
+  }
+  bool infeasible = false, bounds_changed = false;
+  for (int j = 0; j < n; ++j) {
+    if (cl[j] > cu[j] + p.bound_tol) infeasible = true;
+    if (cl[j] != plan.l[j] || cu[j] != plan.u[j]) bounds_changed = true;
+  }
+  if (infeasible) { plan.has_infeasible = true; return; }
+  if (!any_remove && !bounds_changed) return;
+  for (int i = 0; i < m; ++i) if (remove[i]) plan.keep_row[i] = 0;
+  plan.l = cl;
+  plan.u = cu;
+  plan.has_row_action = true;
+  plan.has_row_deletion = plan.has_row_deletion || any_remove;
+  plan.has_change = true;
+}
+
+namespace {
+inline void term_interval(double a, double lj, double uj, double& tmin, double& tmax) {
+  if (a >= 0.0) { tmin = a * lj; tmax = a * uj; } else { tmin = a * uj; tmax = a * lj; }
+}
+inline double residual_min(double fin_sum, int ninf, double t) {
+  if (fin(t)) return ninf == 0 ? fin_sum - t : -INFINITY;
+  if (t < 0.0) return ninf > 1 ? -INFINITY : fin_sum;
+  return fin_sum;
+}
+inline double residual_max(double fin_sum, int pinf, double t) {
+  if (fin(t)) return pinf == 0 ? fin_sum - t : INFINITY;
+  if (t > 0.0) return pinf > 1 ? INFINITY : fin_sum;
+  return fin_sum;
+}
+// Implied bounds of column j from row i (rule_bound_strengthening.cu:349-430).
+inline void implied_bounds(double a, double lj, double uj, double al, double au, double mn, double mx,
+                           int ni, int pi, double& il, double& iu) {
+  double tmin, tmax;
+  term_interval(a, lj, uj, tmin, tmax);
+  const double rmin = residual_min(mn, ni, tmin);
+  const double rmax = residual_max(mx, pi, tmax);
+  il = -INFINITY;
+  iu = INFINITY;
+  if (a > 0.0) {
+    if (fin(al) && fin(rmax)) il = (al - rmax) / a;
+    if (fin(au) && fin(rmin)) iu = (au - rmin) / a;
+  } else {
+    if (fin(au) && fin(rmin)) il = (au - rmin) / a;
+    if (fin(al) && fin(rmax)) iu = (al - rmax) / a;
+  }
+}
+}  // namespace
+
+void rule_bound_strengthening(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_bound_strengthening (rule_bound_strengthening.cu:1176-1557):
+  // one Jacobi round of activity-based implied bounds.
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (m == 0 || n == 0) return;
+  std::vector<double> cl(plan.l), cu(plan.u);
+  std::vector<double> mn(m), mx(m);
+  std::vector<int> ni(m), pi(m);
+  row_activity_summary(lp.A, plan.l, plan.u, p.zero_tol, plan.keep_row.data(), plan.keep_col.data(),
+                       s.row_nnz.data(), mn.data(), mx.data(), ni.data(), pi.data());
+  for (int i = 0; i < m; ++i) {
+    if (!plan.keep_row[i] || s.row_nnz[i] <= 1) continue;
+    for (int q = lp.A.ptr[i]; q < lp.A.ptr[i + 1]; ++q) {
+      const int j = lp.A.idx[q];
+      if (!plan.keep_col[j]) continue;
+      const double a = lp.A.val[q];
+      if (std::fabs(a) <= p.zero_tol) continue;
+      const double ol = plan.l[j], ou = plan.u[j];
+      double il, iu;
+      implied_bounds(a, ol, ou, plan.AL[i], plan.AU[i], mn[i], mx[i], ni[i], pi[i], il, iu);
+      double nl = ol, nu = ou;
+      if (fin(il)) nl = std::fmax(nl, il);
+      if (fin(iu)) nu = std::fmin(nu, iu);
+      if (nl > ol && !(cl[j] >= nl)) cl[j] = nl;
+      if (nu < ou && !(cu[j] <= nu)) cu[j] = nu;
+    }
+  }
+  std::vector<double> cmax(n);
+  col_max_abs(lp.AT, plan.keep_row.data(), cmax.data());
+  const std::vector<double>& refl = plan.ref_l ? *plan.ref_l : plan.l;
+  const std::vector<double>& refu = plan.ref_u ? *plan.ref_u : plan.u;
+  const double ft = p.feasibility_tol;
+  std::vector<double> fl(n), fu(n), fixv(n, 0.0);
+  std::vector<uint8_t> lch(n, 0), uch(n, 0), fx(n, 0);
+  bool f_infeasible = false, f_changed = false, f_fixed = false;
+  // _kernel_finalize_bound_strengthening (rule_bound_strengthening.cu:646-796).
+  for (int j = 0; j < n; ++j) {
+    const double lj = plan.l[j], uj = plan.u[j];
+    if (!plan.keep_col[j]) { fl[j] = lj; fu[j] = uj; continue; }
+    double cand_l = cl[j], cand_u = cu[j];
+    const double vmax = cmax[j];
+    double nl = lj, nu = uj;
+    uint8_t lc = 0, uc = 0, fj = 0;
+    double fat = 0.0;
+    double el = lj, eu = uj;
+    if (fin(cand_l)) el = std::fmax(el, cand_l);
+    if (fin(cand_u)) eu = std::fmin(eu, cand_u);
+    if (el > eu + ft) { f_infeasible = true; continue; }
+    const bool was_free = !fin(refl[j]) && !fin(refu[j]);
+    const bool box = fin(cand_l) && fin(cand_u);
+    const bool zero_cost = std::fabs(plan.c[j]) <= p.zero_tol;
+    const bool nearly_fixed = box && (cand_u <= cand_l || (cand_u - cand_l) * vmax <= ft);
+    if (p.bound_strengthening_preserve_free_zero_cost && was_free && box && zero_cost && !nearly_fixed) {
+      cand_l = lj;
+      cand_u = uj;
+    }
+    if (fin(cand_l) && cand_l > lj && fin(uj)) {
+      if (cand_l >= uj + ft) { f_infeasible = true; continue; }
+      if (cand_l >= uj || (uj - cand_l) * vmax <= ft) { fj = 1; fat = uj; nl = uj; nu = uj; }
+    }
+    if (!fj && fin(cand_l) && cand_l > lj) {
+      const bool tighten = !fin(lj) || ((cand_l - lj > ft * 1.0e4) && (cand_l - lj > 1.0e-2 * std::fabs(lj)));
+      if (tighten) {
+        if (cand_l != std::nearbyint(cand_l)) cand_l -= 0.5 * ft * std::fabs(cand_l);
+        nl = cand_l;
+        lc = 1;
+      }
+    }
+    if (!fj && fin(cand_u) && cand_u < uj && fin(nl)) {
+      if (cand_u <= nl - ft) { f_infeasible = true; continue; }
+      if (cand_u <= nl || (cand_u - nl) * vmax <= ft) { fj = 1; fat = nl; nu = nl; }
+    }
+    if (!fj && fin(cand_u) && cand_u < uj) {
+      const bool tighten = !fin(uj) || ((uj - cand_u > ft * 1.0e4) && (uj - cand_u > 1.0e-2 * std::fabs(uj)));
+      if (tighten) {
+        if (cand_u != std::nearbyint(cand_u))
+          cand_u += p.bound_strengthening_upper_relaxation_factor * ft * std::fabs(cand_u);
+        nu = cand_u;
+        uc = 1;
+      }
+    }
+    if (fj) { lc = uc = 0; f_fixed = true; }
+    if (lc || uc) f_changed = true;
+    fl[j] = nl; fu[j] = nu; lch[j] = lc; uch[j] = uc; fx[j] = fj; fixv[j] = fat;
+  }
+  if (f_infeasible) { plan.has_infeasible = true; return; }
+  if (!f_changed && !f_fixed) return;
+  if (p.record_postsolve_tape && f_changed) {
+    // Support rows (rule_bound_strengthening.cu:815-960): the smallest live row
+    // whose implied bound reproduces the finalized bound within support_tol.
+    const double support_tol = std::fmax(10.0 * p.bound_tol, 1.0e-10);
+    Tape seg;
+    for (int j = 0; j < n; ++j) {
+      if (!lch[j] && !uch[j]) continue;
+      int sl = INT_MAX, su = INT_MAX;
+      for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q) {
+        const int i = lp.AT.idx[q];
+        if (!plan.keep_row[i] || s.row_nnz[i] <= 1) continue;
+        const double a = lp.AT.val[q];
+        if (std::fabs(a) <= p.zero_tol) continue;
+        double il, iu;
+        implied_bounds(a, plan.l[j], plan.u[j], plan.AL[i], plan.AU[i], mn[i], mx[i], ni[i], pi[i], il, iu);
+        if (lch[j] && fl[j] > plan.l[j] + p.bound_tol && fin(il) && std::fabs(il - fl[j]) <= support_tol)
+          sl = std::min(sl, i);
+        if (uch[j] && fu[j] < plan.u[j] - p.bound_tol && fin(iu) && std::fabs(iu - fu[j]) <= support_tol)
+          su = std::min(su, i);
+      }
+      double cur_l = plan.l[j];
+      const double cur_u = plan.u[j];
+      if (lch[j]) {
+        if (sl != INT_MAX) seg.add(RowImpliedBoundChange, {j, sl}, {cur_l, cur_u, fl[j], cur_u});
+        else seg.add(VariableBoundChange, {j}, {cur_l, cur_u, fl[j], cur_u});
+        cur_l = fl[j];
+      }
+      if (uch[j]) {
+        if (su != INT_MAX) seg.add(RowImpliedBoundChange, {j, su}, {cur_l, cur_u, cur_l, fu[j]});
+        else seg.add(VariableBoundChange, {j}, {cur_l, cur_u, cur_l, fu[j]});
+      }
+    }
+    plan.tape.append(seg);
+  }
+  for (int j = 0; j < n; ++j) {
+    plan.l[j] = fl[j];
+    plan.u[j] = fu[j];
+    if (fx[j]) plan.keep_col[j] = 0;
+  }
+  bool empty_infeasible = false;
+  if (f_fixed) {
+    const std::vector<double> shift = row_shift_gather(lp, plan.keep_row, fx, fixv, false);
+    for (int i = 0; i < m; ++i) { plan.AL[i] -= shift[i]; plan.AU[i] -= shift[i]; }
+    for (int i = 0; i < m; ++i) {
+      if (!plan.keep_row[i]) continue;
+      int cnt = 0;
+      for (int q = lp.A.ptr[i]; q < lp.A.ptr[i + 1]; ++q) cnt += plan.keep_col[lp.A.idx[q]] != 0;
+      if (cnt != 0) continue;
+      if (plan.AL[i] <= ft && plan.AU[i] >= -ft) plan.keep_row[i] = 0; else empty_infeasible = true;
+    }
+  }
+  if (empty_infeasible) { plan.has_infeasible = true; return; }
+  double obj_delta = 0.0;
+  if (f_fixed) {
+    // append_compact_fixed_variable_tape_from_device (fixed_variable_tape.cu:141-327).
+    long double acc = 0.0L;
+    Tape seg;
+    for (int j = 0; j < n; ++j) {
+      if (!fx[j]) continue;
+      acc += (long double)plan.c[j] * (long double)fixv[j];
+      if (!p.record_postsolve_tape) continue;
+      std::vector<int> ii{j};
+      std::vector<double> vv{fixv[j], plan.c[j]};
+      for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q)
+        if (plan.keep_row[lp.AT.idx[q]]) { ii.push_back(lp.AT.idx[q]); vv.push_back(lp.AT.val[q]); }
+      seg.add(FixedVariable, ii, vv);
+    }
+    plan.tape.append(seg);
+    obj_delta = double(acc);
+  }
+  plan.obj_delta += obj_delta;
+  plan.has_row_action = plan.has_row_action || f_fixed;
+  plan.has_col_action = plan.has_col_action || f_fixed;
+  plan.has_change = true;
+}
+
+}  // namespace oracle

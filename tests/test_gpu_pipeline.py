@@ -1,0 +1,91 @@
+"""End-to-end parity on the GPU through the C ABI: preprocess -> reduced LP,
+maps, tape and fixed values against the oracle (bitwise), then postprocess
+against the oracle's postsolve and the unreduced LP's optimum (HiGHS)."""
+import numpy as np
+import pytest
+
+import lpsolve
+import pyoracle
+from gpp_b200 import device, lpgen
+from gpp_b200.capi import params_with_rules
+
+pytestmark = pytest.mark.gpu
+
+CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
+BUILT = CLEANUP + ["bound_strengthening"]
+
+
+def bits(a):
+    a = np.asarray(a)
+    return a.view(np.uint64) if a.dtype == np.float64 else a
+
+
+def assert_same(gpu, orc):
+    s, o = gpu.summary, orc.summary
+    for f in ("reduced_rows", "reduced_cols", "reduced_nnz", "iterations", "has_infeasible", "has_unbounded",
+              "has_change", "stopped_at_iteration_limit"):
+        assert getattr(s, f) == getattr(o, f), f
+    for f in ("A_ptr", "A_idx", "A_val", "AT_ptr", "AT_idx", "AT_val", "c", "l", "u", "AL", "AU", "row_map",
+              "col_map", "tape_types", "tape_is", "tape_vs", "tape_idx", "tape_val", "fixed_idx", "fixed_val"):
+        assert np.array_equal(bits(getattr(gpu, f)), bits(getattr(orc, f))), f
+    assert s.obj_constant_delta == o.obj_constant_delta
+
+
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT])
+@pytest.mark.parametrize("workload", ["random:400x1000", "small"])
+def test_presolve_bitwise_vs_oracle(rules, workload):
+    lp = lpgen.workload(workload, seed=0)
+    params = params_with_rules(rules, enable_folding=0)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params)
+    try:
+        gpu = device.Result(s)
+        orc = pyoracle.presolve(lp, params)
+        assert_same(gpu, orc)
+    finally:
+        device.free_summary(s)
+        device.free_summary(s)  # idempotent
+
+
+@pytest.mark.parametrize("seed", [0, 3])
+def test_postprocess_vs_oracle_and_highs(seed):
+    import torch
+    lp = lpgen.random_lp(400, 1000, seed=seed)
+    params = params_with_rules(BUILT, enable_folding=0)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params)
+    try:
+        gpu = device.Result(s)
+        res0, _, _ = lpsolve.solve(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values, lp.c, lp.AL, lp.AU, lp.l, lp.u)
+        rr, yr, zr = lpsolve.solve(s.reduced_rows, s.reduced_cols, gpu.A_ptr, gpu.A_idx, gpu.A_val, gpu.c, gpu.AL,
+                                   gpu.AU, gpu.l, gpu.u)
+        xd = torch.from_numpy(rr.x).cuda()
+        yd = torch.from_numpy(yr).cuda()
+        zd = torch.from_numpy(zr).cuda()
+        x, y, z = device.postprocess(xd, yd, zd, s, dlp)
+        orc = pyoracle.presolve(lp, params)
+        xo, yo, zo = orc.postsolve(rr.x, yr, zr)
+        assert np.array_equal(bits(x), bits(xo))
+        assert np.array_equal(bits(y), bits(yo))
+        assert np.array_equal(bits(z), bits(zo))
+        assert abs(lp.c @ x - res0.fun) <= 1e-9 * max(1.0, abs(res0.fun))
+    finally:
+        device.free_summary(s)
+
+
+def test_identity_when_presolve_disabled():
+    lp = lpgen.random_lp(200, 500, seed=1)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params_with_rules(BUILT, enable_folding=0, enable_presolve=0))
+    try:
+        assert s.owns_reduced_lp == 0 and s.reduced_rows == lp.m and s.reduced_cols == lp.n
+        assert s.reduced_lp.A.rowPtr == dlp.t["A_ptr"].data_ptr()
+    finally:
+        device.free_summary(s)
+
+
+def test_folding_request_fails_loudly_until_built():
+    lp = lpgen.random_lp(200, 500, seed=1)
+    dlp = device.DeviceLp(lp)
+    with pytest.raises(RuntimeError):
+        device.preprocess(dlp, params_with_rules(BUILT, enable_folding=1))
