@@ -1,0 +1,277 @@
+"""Benchmark: plain presolve + postsolve of the 25M-nnz synthetic LP on B200.
+
+One step = gpu_preprocessor::preprocess (presolve) + postprocess (postsolve
+of a fixed reduced solution) of the single-GPU scale LP: the seeded random
+family at m = 2,000,000, n = 5,000,000 with 2,000 hub rows (~29.8M nnz).  The
+inputs stay resident in HBM for `value`; `e2e` repeats the step through the
+C ABI with the LP uploaded from pinned host memory and the solution read back
+every step.  The LP (~1 GB of arrays) is larger than the 126 MB L2, so no
+flush is needed between steps.
+
+--impl reference times the reference's own CPU implementation of the path,
+its bundled PSLP presolver (built from the reference sources into
+oracle/_ref/pslp_driver), on the same workload.
+
+Multi-GPU: the plain path does not shard (every presolve round couples all
+rows and columns), so --gpus N runs N independent replicas, one per rank;
+the value is the max-over-ranks step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-preprocessor-ijoc_b200"))
+
+WORKLOAD = "scale"
+WORKLOAD_DESC = "random LP m=2,000,000 n=5,000,000 + 2,000 hub rows (500-5000 nnz), seed 0"
+METRIC = "presolve ms, HBM GB/s @25M nnz (presolve+postsolve ms per LP)"
+RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows",
+         "bound_strengthening"]
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], None, set()
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                 parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU path (bundled PSLP) on rank 0 only."""
+    if rank != 0:
+        return
+    from gpp_b200 import lpgen
+    driver = os.path.join(ROOT, "oracle", "_ref", "pslp_driver")
+    if not os.path.exists(driver):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pslp_driver was not built "
+                          "(needs the reference sources at build time)"}))
+        return
+    lp = lpgen.workload(WORKLOAD, seed=0)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "lp.bin")
+        lpgen.save_lp(path, lp)
+        runs = min(args.steps, 5)
+        warm = min(args.warmup, 1)
+        out = subprocess.run([driver, path, str(warm + runs)], capture_output=True, text=True, check=True).stdout
+    lines = [l for l in out.splitlines() if l.startswith("pslp run=")]
+    wall = [float(l.split("wall_s=")[1].split()[0]) for l in lines][warm:]
+    core = [float(l.split("presolve_s=")[1].split()[0]) for l in lines][warm:]
+    ms = 1e3 * statistics.mean(wall)
+    sample = (f"PSLP 0.0.11 (reference third_party/pslp, gcc -O3) default settings, full {WORKLOAD_DESC}, "
+              f"{len(wall)} timed runs after {warm} warm-up; presolve only (PSLP core {1e3*statistics.mean(core):.0f} ms)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+        "steps": len(wall), "warmup": warm, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "nnz": lp.nnz, "parallelism": "cpu, 1 thread"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import ctypes as C
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from gpp_b200 import capi, device, lpgen
+    from gpp_b200.capi import params_with_rules
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = capi.load()
+    lp = lpgen.workload(args.workload, seed=0)
+    params = params_with_rules(RULES, enable_folding=0)
+    dlp = device.DeviceLp(lp)
+    stream = torch.cuda.current_stream()
+
+    # Warm-up: also fixes the reduced solution the postsolve step replays.
+    red = None
+    for _ in range(max(args.warmup, 3)):
+        s = device.preprocess(dlp, params)
+        if red is None:
+            res = device.Result(s, copy_lp=True, copy_tape=False)
+            x0 = np.clip(np.zeros(s.reduced_cols), res.l, res.u)
+            red = (torch.from_numpy(x0).cuda(), torch.zeros(s.reduced_rows, dtype=torch.float64, device="cuda"),
+                   torch.zeros(s.reduced_cols, dtype=torch.float64, device="cuda"))
+            reduced = (s.reduced_rows, s.reduced_cols, s.reduced_nnz, s.iterations)
+        device.postprocess(*red, s, dlp)
+        device.free_summary(s)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # Device-resident timed region (kernels timed per launch by CUDA events).
+    clocks = Clocks(local)
+    lib.gpp_kernel_launches(1)
+    lib.gpp_profile_enable(1)
+    barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pre_ms = []
+    out = (torch.empty(lp.n, dtype=torch.float64, device="cuda"), torch.empty(lp.m, dtype=torch.float64, device="cuda"),
+           torch.empty(lp.n, dtype=torch.float64, device="cuda"))
+    t0.record(stream)
+    for _ in range(args.steps):
+        s = device.preprocess(dlp, params)
+        pre_ms.append(1e3 * s.elapsed_seconds)
+        device.postsolve_device(*red, s, dlp, out)
+        device.free_summary(s)
+    t1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    step_ms = t0.elapsed_time(t1) / args.steps
+    launches = int(lib.gpp_kernel_launches(0)) // args.steps
+    prof = capi.profile_read()
+    lib.gpp_profile_enable(0)
+
+    # End to end through the C ABI from pinned host memory.
+    host = {k: v.cpu().pin_memory() for k, v in dlp.t.items()}
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    d2h = 8 * (lp.n + lp.m + lp.n)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for k, v in host.items():
+            dlp.t[k].copy_(v, non_blocking=True)
+        s = device.preprocess(dlp, params)
+        device.postprocess(*red, s, dlp)
+        device.free_summary(s)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    if world > 1:
+        t = torch.tensor([step_ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, e2e_ms = float(t[0]), float(t[1])
+
+    peak, peak_kind = peaks()
+    top = max(prof, key=lambda r: r[2]) if prof else None
+    roofline = None
+    if top:
+        name, nl, ms, by = top
+        bytes_top = [r for r in prof if r[3] > 0]
+        best = max(bytes_top, key=lambda r: r[2]) if bytes_top else None
+        if best:
+            name, nl, ms, by = best
+            achieved = (by / 1e9) / (ms / 1e3)
+            roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                        "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                        "launches_per_step": nl // args.steps, "avg_launch_us": round(1e3 * ms / nl, 2),
+                        "bytes_per_launch": int(by / nl), "traffic": None}
+    kernels = sorted(prof, key=lambda r: -r[2])[:8]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        driver = os.path.join(ROOT, "oracle", "_ref", "pslp_driver")
+        if os.path.exists(driver):
+            with tempfile.TemporaryDirectory() as d:
+                path = os.path.join(d, "lp.bin")
+                lpgen.save_lp(path, lp)
+                out = subprocess.run([driver, path, "1"], capture_output=True, text=True).stdout
+            wall = [float(l.split("wall_s=")[1].split()[0]) for l in out.splitlines() if l.startswith("pslp run=")]
+            if wall:
+                cpu = {"value": round(1e3 * wall[0], 1), "unit": "ms", "cores": 1, "kind": "reference",
+                       "sample": f"one PSLP 0.0.11 presolve of the full workload ({WORKLOAD_DESC}) on 1 host core"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round(step_ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC, "rows": lp.m, "cols": lp.n, "nnz": lp.nnz,
+                       "rules": RULES, "folding": False,
+                       "reduced": {"rows": reduced[0], "cols": reduced[1], "nnz": reduced[2], "iterations": reduced[3]},
+                       "presolve_ms": round(statistics.mean(pre_ms), 3),
+                       "l2": "inputs (~1 GB) larger than L2; no flush",
+                       "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "gpu_launches": launches,
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roofline,
+            "kernels": [{"name": n, "launches_per_step": l // args.steps, "ms_per_step": round(m / args.steps, 3)}
+                        for n, l, m, b in kernels],
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -3,6 +3,7 @@
 // API in include/gpu_preprocessor/ maps them back to the reference's
 // exception types.
 #include <chrono>
+#include <cstring>
 #include <cmath>
 #include <memory>
 
@@ -377,6 +378,29 @@ void gpp_device_free(void* p) {
 }
 
 const char* gpp_last_error(void) { return gpp::last_error(); }
+
+void gpp_profile_enable(int enable) { gpp::profile_enable(enable != 0); }
+
+int gpp_profile_read(int index, char* name, size_t name_len, int64_t* launches, double* ms, double* bytes) {
+  try {
+    static thread_local std::vector<gpp::ProfileSummary> cache;
+    if (index == 0) cache = gpp::profile_summary();
+    if (index >= 0 && size_t(index) < cache.size()) {
+      const auto& e = cache[size_t(index)];
+      if (name && name_len) {
+        std::strncpy(name, e.name.c_str(), name_len - 1);
+        name[name_len - 1] = 0;
+      }
+      if (launches) *launches = e.launches;
+      if (ms) *ms = e.ms;
+      if (bytes) *bytes = e.bytes;
+    }
+    return int(cache.size());
+  } catch (const std::exception& e) {
+    gpp::set_last_error(e.what());
+    return -1;
+  }
+}
 
 uint64_t gpp_kernel_launches(int reset) {
   const uint64_t v = gpp::launch_counter();

@@ -32,12 +32,15 @@ Context::~Context() {
 Context& ctx() {
   // One context per host thread and device (the reference's contract is one
   // presolve per host thread on the current device).
-  static thread_local std::vector<std::unique_ptr<Context>> per_device;
+  // Never destroyed: the stream and pinned block stay valid until process
+  // exit, so buffers released during thread-exit destruction can still be
+  // returned to the stream-ordered pool.
+  static thread_local std::vector<Context*>* per_device = new std::vector<Context*>();
   int dev = 0;
   check(cudaGetDevice(&dev), "cudaGetDevice");
-  if (size_t(dev) >= per_device.size()) per_device.resize(size_t(dev) + 1);
-  if (!per_device[size_t(dev)]) per_device[size_t(dev)] = std::make_unique<Context>();
-  return *per_device[size_t(dev)];
+  if (size_t(dev) >= per_device->size()) per_device->resize(size_t(dev) + 1, nullptr);
+  if (!(*per_device)[size_t(dev)]) (*per_device)[size_t(dev)] = new Context();
+  return *(*per_device)[size_t(dev)];
 }
 
 Status::Status() { check(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().stream), "status alloc"); }
@@ -182,6 +185,63 @@ double det_sum(const double* v, int64_t n, cudaStream_t s) {
 
 namespace {
 thread_local std::string g_last_error;
+
+struct ProfileRecord {
+  const char* name;
+  double bytes;
+  cudaEvent_t begin, end;
+};
+struct ProfileState {
+  bool on = false;
+  std::vector<ProfileRecord> records;
+  std::vector<cudaEvent_t> pool;
+  size_t next = 0;
+};
+ProfileState& profile_state() {
+  static thread_local ProfileState* p = new ProfileState;  // never destroyed (see ctx())
+  return *p;
+}
+}  // namespace
+
+bool profiling() { return profile_state().on; }
+cudaEvent_t profile_event() {
+  auto& p = profile_state();
+  if (p.next == p.pool.size()) {
+    cudaEvent_t e;
+    check(cudaEventCreate(&e), "cudaEventCreate");
+    p.pool.push_back(e);
+  }
+  return p.pool[p.next++];
+}
+void profile_record(const char* name, double bytes, cudaEvent_t begin, cudaEvent_t end) {
+  profile_state().records.push_back({name, bytes, begin, end});
+}
+void profile_enable(bool on) {
+  auto& p = profile_state();
+  p.on = on;
+  p.records.clear();
+  p.next = 0;
+}
+// Aggregates recorded launches by kernel name: launches, total ms, total bytes.
+std::vector<ProfileSummary> profile_summary() {
+  auto& p = profile_state();
+  check(cudaDeviceSynchronize(), "profile sync");
+  std::vector<ProfileSummary> out;
+  for (const auto& r : p.records) {
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, r.begin, r.end), "cudaEventElapsedTime");
+    ProfileSummary* s = nullptr;
+    for (auto& o : out)
+      if (o.name == r.name) s = &o;
+    if (!s) {
+      out.push_back({r.name, 0, 0.0, 0.0});
+      s = &out.back();
+    }
+    s->launches += 1;
+    s->ms += ms;
+    s->bytes += r.bytes;
+  }
+  return out;
 }
 void set_last_error(const std::string& s) { g_last_error = s; }
 const char* last_error() { return g_last_error.c_str(); }

@@ -39,14 +39,32 @@ inline void check(cudaError_t e, const char* ctx) {
 // Kernel launch counter (per host thread) for the benchmark's launch report.
 uint64_t& launch_counter();
 
-#define GPP_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
+// Optional per-launch timing (CUDA events on the launching stream) used by
+// the benchmark's roofline report; off unless gpp_profile_enable(1).
+bool profiling();
+void profile_record(const char* name, double bytes, cudaEvent_t begin, cudaEvent_t end);
+cudaEvent_t profile_event();
+
+#define GPP_LAUNCH_BYTES(kernel, bytes, grid, block, smem, stream, ...)             \
   do {                                                                              \
     if ((grid) > 0) {                                                               \
+      cudaEvent_t gpp_ev0 = nullptr, gpp_ev1 = nullptr;                             \
+      if (::gpp::profiling()) {                                                     \
+        gpp_ev0 = ::gpp::profile_event();                                           \
+        gpp_ev1 = ::gpp::profile_event();                                           \
+        cudaEventRecord(gpp_ev0, (stream));                                         \
+      }                                                                             \
       kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                   \
       ::gpp::check(cudaGetLastError(), #kernel);                                    \
       ++::gpp::launch_counter();                                                    \
+      if (gpp_ev1) {                                                                \
+        cudaEventRecord(gpp_ev1, (stream));                                         \
+        ::gpp::profile_record(#kernel, double(bytes), gpp_ev0, gpp_ev1);            \
+      }                                                                             \
     }                                                                               \
   } while (0)
+#define GPP_LAUNCH(kernel, grid, block, smem, stream, ...) \
+  GPP_LAUNCH_BYTES(kernel, 0.0, grid, block, smem, stream, __VA_ARGS__)
 
 inline int blocks_for(int64_t n, int threads = kThreads) {
   const int64_t b = (n + threads - 1) / threads;
@@ -169,6 +187,15 @@ void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t
 // Canonical deterministic sum (chunks of 2048, 256-thread halving tree, chunk
 // totals added in order on the host).  Returns the value on the host.
 double det_sum(const double* v, int64_t n, cudaStream_t s);
+
+struct ProfileSummary {
+  std::string name;
+  int64_t launches;
+  double ms;
+  double bytes;
+};
+void profile_enable(bool on);
+std::vector<ProfileSummary> profile_summary();
 
 // Thread-local error message for the C ABI.
 void set_last_error(const std::string& s);

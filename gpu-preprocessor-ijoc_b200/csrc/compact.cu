@@ -292,13 +292,16 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
   const RowSchedule& sch = stored_schedule(M);
   const int sb = roles_short(M.rows), mb = roles_medium(M.rows), lb = roles_long(M.rows);
   DBuf<int32_t> counts(size_t(outer_new) + 1, s);
-  GPP_LAUNCH(count_kept, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map, sch.medium.p,
+  const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * outer_new;
+  GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map, sch.medium.p,
              sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
   exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
   out.nnz = read_scalar(out.ptr + outer_new);
   out.idx = dalloc<int32_t>(size_t(out.nnz));
   out.val = dalloc<double>(size_t(out.nnz));
-  GPP_LAUNCH(copy_kept, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map, inner_map,
+  const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +
+                            4.0 * (outer_new + 1) + 12.0 * out.nnz;
+  GPP_LAUNCH_BYTES(copy_kept, copy_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map, inner_map,
              sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, out.ptr, out.idx, out.val);
   return out;
 }

@@ -338,9 +338,16 @@ struct ScheduleCache {
   unsigned next = 0;
   uint64_t epoch = 1;
 };
+// Thread-lifetime caches are deliberately never destroyed: their device
+// buffers live until process exit, when the driver reclaims them, so no CUDA
+// call runs during thread-exit destruction (whose order relative to the
+// engine stream is unspecified).
 ScheduleCache& schedule_cache() {
-  static thread_local ScheduleCache c;
-  return c;
+  static thread_local ScheduleCache* c = [] {
+    ctx();
+    return new ScheduleCache;
+  }();
+  return *c;
 }
 
 }  // namespace
@@ -376,7 +383,11 @@ void live_stats_side(const DevCsr& M, const uint8_t* keep_outer, const uint8_t* 
   if (!M.rows) return;
   const RowSchedule& sch = stored_schedule(M);
   const Roles r = roles_for(M.rows);
-  GPP_LAUNCH(live_stats_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, M.rows,
+  // Algorithmic bytes: row pointers, inner indices, both masks, five outputs.
+  const double bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + (keep_outer ? M.rows : 0) + (keep_inner ? M.cols : 0) +
+                       double(M.rows) * ((degree ? 4 : 0) + (empty ? 1 : 0) + (singleton ? 1 : 0) +
+                                         (support ? 4 : 0) + (coefficient ? 8 : 0));
+  GPP_LAUNCH_BYTES(live_stats_kernel, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, M.rows,
              M.ptr, M.idx, M.val, keep_outer, keep_inner, sch.medium.p, sch.long_rows.p, sch.counts.p,
              r.short_blocks, r.medium_blocks, degree, empty, singleton, support, coefficient, total);
 }
@@ -406,16 +417,20 @@ void row_activity_summary(const DevCsr& A, const double* l, const double* u, dou
                           cudaStream_t s) {
   // compute_row_activity_summary (gpu_presolve_kernels.cu:744-787).
   if (!A.rows) return;
-  static thread_local RowSchedule live_schedule;
+  static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
   const RowSchedule* sch;
   if (live_deg) {
-    build_schedule(live_schedule, A, live_deg, s);
-    sch = &live_schedule;
+    build_schedule(*live_schedule, A, live_deg, s);
+    sch = live_schedule;
   } else {
     sch = &stored_schedule(A);
   }
   const Roles r = roles_for(A.rows);
-  GPP_LAUNCH(activity_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
+  // Algorithmic bytes (each array charged once): row pointers, column indices
+  // and values, column bounds, masks, live degrees, four outputs.
+  const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
+                       (keep_col ? A.cols : 0) + (live_deg ? 4.0 * A.rows : 0) + 24.0 * A.rows;
+  GPP_LAUNCH_BYTES(activity_kernel, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
              A.idx, A.val, l, u, zero_tol, keep_row, keep_col, live_deg, sch->medium.p, sch->long_rows.p,
              sch->counts.p, r.short_blocks, r.medium_blocks, min_fin, max_fin, min_inf, max_inf);
 }
@@ -425,7 +440,8 @@ void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStr
   if (!AT.rows) return;
   const RowSchedule& sch = stored_schedule(AT);
   const Roles r = roles_for(AT.rows);
-  GPP_LAUNCH(col_max_kernel, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, AT.rows,
+  const double bytes = 4.0 * (AT.rows + 1) + 12.0 * AT.nnz + (keep_row ? AT.cols : 0) + 8.0 * AT.rows;
+  GPP_LAUNCH_BYTES(col_max_kernel, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, AT.rows,
              AT.ptr, AT.idx, AT.val, keep_row, sch.medium.p, sch.long_rows.p, sch.counts.p, r.short_blocks,
              r.medium_blocks, out);
 }

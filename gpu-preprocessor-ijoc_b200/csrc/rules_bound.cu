@@ -335,7 +335,9 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
               lb = std::min<int>(kNumSMs * 4, m);
     CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, plan.keep_col.p, stats.row_nnz.p, plan.AL.p,
                plan.AU.p, plan.l.p, plan.u.p, rs, p.zero_tol, cl.p, cu.p};
-    GPP_LAUNCH(candidates_kernel, sb + mb + lb, kThreads, 0, s, m, g, sch.medium.p, sch.long_rows.p, sch.counts.p,
+    const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + double(n) + 4.0 * m + 16.0 * m + 24.0 * m +
+                         16.0 * n + 16.0 * n;
+    GPP_LAUNCH_BYTES(candidates_kernel, bytes, sb + mb + lb, kThreads, 0, s, m, g, sch.medium.p, sch.long_rows.p, sch.counts.p,
                sb, mb);
   }
   col_max_abs(lp.AT, plan.keep_row.p, vmax.p, s);

@@ -124,6 +124,8 @@ def load():
         "gpp_device_free": (None, [vp]),
         "gpp_last_error": (C.c_char_p, []),
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
+        "gpp_profile_enable": (None, [C.c_int]),
+        "gpp_profile_read": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(i64), P(f64), P(f64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -138,7 +140,7 @@ EXPORTED = [
     "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
     "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_device_free",
-    "gpp_last_error", "gpp_kernel_launches",
+    "gpp_last_error", "gpp_kernel_launches", "gpp_profile_enable", "gpp_profile_read",
 ]
 
 
@@ -146,3 +148,16 @@ def check(status: int) -> None:
     if status != 0:
         msg = load().gpp_last_error().decode(errors="replace")
         raise RuntimeError(f"gpp error {status}: {msg}")
+
+
+def profile_read():
+    """Per-kernel (name, launches, ms, bytes) recorded since gpp_profile_enable(1)."""
+    lib = load()
+    out = []
+    count = lib.gpp_profile_read(0, None, 0, None, None, None)
+    for k in range(max(count, 0)):
+        name = C.create_string_buffer(128)
+        launches, ms, by = i64(), f64(), f64()
+        lib.gpp_profile_read(k, name, 128, C.byref(launches), C.byref(ms), C.byref(by))
+        out.append((name.value.decode(), launches.value, ms.value, by.value))
+    return out

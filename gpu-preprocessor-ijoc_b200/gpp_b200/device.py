@@ -172,3 +172,16 @@ def postprocess(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp):
 
 def free_summary(summary: capi.Summary) -> None:
     capi.load().gpp_free_summary(C.byref(summary))
+
+
+def postsolve_device(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp, out=None):
+    """presolve::postsolve_gpu: original-space x, y, z as CUDA tensors."""
+    torch = _torch()
+    if out is None:
+        out = (torch.empty(summary.original_cols, dtype=torch.float64, device="cuda"),
+               torch.empty(summary.original_rows, dtype=torch.float64, device="cuda"),
+               torch.empty(summary.original_cols, dtype=torch.float64, device="cuda"))
+    lp = original.struct()
+    _raise(capi.load().gpp_postsolve_device(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
+                                            *(ptr(t) for t in out)))
+    return out

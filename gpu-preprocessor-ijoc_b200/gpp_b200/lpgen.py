@@ -72,8 +72,20 @@ def csr_transpose(m, n, ptr, idx, val):
     return t_ptr.astype(np.int32), t_idx, t_val
 
 
+def _sorted_unique(keys):
+    keys = np.sort(keys)
+    if keys.size:
+        keys = keys[np.concatenate(([True], keys[1:] != keys[:-1]))]
+    return keys
+
+
+def _row_major_order(rows, cols):
+    span = int(cols.max()) + 1 if cols.size else 1
+    return np.argsort(rows.astype(np.int64) * span + cols, kind="stable")
+
+
 def coo_to_csr(m, rows, cols, vals):
-    order = np.lexsort((cols, rows))
+    order = _row_major_order(rows, cols)
     rows, cols, vals = rows[order], cols[order], vals[order]
     counts = np.bincount(rows, minlength=m)
     ptr = np.zeros(m + 1, dtype=np.int64)
@@ -121,7 +133,7 @@ def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
     per_col = 1 + rng.poisson(4.0, size=regular_cols.size)
     cols = np.repeat(regular_cols, per_col)
     rows = normal_rows[rng.integers(0, normal_rows.size, size=cols.size)]
-    key = np.unique(cols * m + rows)            # drop repeated (row, col) draws
+    key = _sorted_unique(cols * m + rows)       # drop repeated (row, col) draws
     cols, rows = key // m, key % m
     vals = _grid_values(rng, rows.size)
 
@@ -132,8 +144,9 @@ def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
         lengths = np.minimum(lengths, regular_cols.size)
         h_rows = np.repeat(hubs, lengths)
         h_cols = regular_cols[rng.integers(0, regular_cols.size, size=h_rows.size)]
-        hkey = np.unique(np.concatenate([cols * m + rows, h_cols * m + h_rows]))
-        new = np.setdiff1d(hkey, cols * m + rows, assume_unique=True)
+        base = cols * m + rows
+        hkey = _sorted_unique(h_cols * m + h_rows)
+        new = hkey[~np.isin(hkey, base, assume_unique=True)]
         new_cols, new_rows = new // m, new % m
         cols = np.concatenate([cols, new_cols])
         rows = np.concatenate([rows, new_rows])
@@ -160,7 +173,7 @@ def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
     copy_rows = np.flatnonzero(role == 3)
     src_rows = normal_rows[rng.integers(0, normal_rows.size, size=copy_rows.size)]
     row_factor = rng.uniform(0.5, 4.0, size=copy_rows.size)
-    order = np.lexsort((cols, rows))
+    order = _row_major_order(rows, cols)
     cols, rows, vals = cols[order], rows[order], vals[order]
     rstart = np.searchsorted(rows, src_rows, side="left")
     rstop = np.searchsorted(rows, src_rows, side="right")

@@ -245,6 +245,15 @@ GPP_API void gpp_device_free(void* device_ptr);
 /* Last error message of the calling thread ("" when none). */
 GPP_API const char* gpp_last_error(void);
 
+/* Per-kernel timing for the benchmark's roofline report.  While enabled,
+ * every launch on the calling thread is bracketed by CUDA events on its
+ * stream; gpp_profile_read aggregates by kernel name (launches, total ms,
+ * algorithmic bytes the launch was charged) and returns the number of kernel
+ * names, filling entry `index` when it exists.  Enabling clears old records. */
+GPP_API void gpp_profile_enable(int enable);
+GPP_API int gpp_profile_read(int index, char* name, size_t name_len, int64_t* launches, double* ms,
+                             double* bytes);
+
 /* Number of CUDA kernels this library launched on the calling thread since
  * the last reset (used by the benchmark to report its launch count). */
 GPP_API uint64_t gpp_kernel_launches(int reset);

@@ -93,7 +93,8 @@ def test_live_stats_and_col_max_vs_oracle():
         assert ref[5] == int(tot.item())
     AT, keep = dev_csr(lp.n, lp.m, lp.at_ptr, lp.at_idx, lp.at_val)
     out = torch.zeros(lp.n, dtype=torch.float64, device="cuda")
-    _raise(capi.load().gpp_col_max_abs(C.byref(AT), ptr(to_device(keep_r, np.uint8)), ptr(out)))
+    dkr = to_device(keep_r, np.uint8)
+    _raise(capi.load().gpp_col_max_abs(C.byref(AT), ptr(dkr), ptr(out)))
     assert np.array_equal(out.cpu().numpy(), pyoracle.col_max_abs(lp.n, lp.m, lp.at_ptr, lp.at_idx, lp.at_val, keep_r))
 
 
@@ -104,8 +105,8 @@ def test_compaction_and_transpose_vs_numpy():
     keep_c = (rng.random(lp.n) < 0.6).astype(np.uint8)
     A, keep = dev_csr(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values)
     Ao, ATo = capi.Csr(), capi.Csr()
-    _raise(capi.load().gpp_compact_and_transpose(C.byref(A), ptr(to_device(keep_r, np.uint8)),
-                                                 ptr(to_device(keep_c, np.uint8)), C.byref(Ao), C.byref(ATo)))
+    dkr, dkc = to_device(keep_r, np.uint8), to_device(keep_c, np.uint8)   # kept alive across the call
+    _raise(capi.load().gpp_compact_and_transpose(C.byref(A), ptr(dkr), ptr(dkc), C.byref(Ao), C.byref(ATo)))
     rmap = np.cumsum(keep_r) - 1
     cmap = np.cumsum(keep_c) - 1
     rows = np.repeat(np.arange(lp.m), np.diff(lp.row_ptr))

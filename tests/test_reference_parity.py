@@ -1,0 +1,93 @@
+"""Parity with the REFERENCE implementation itself, run on the same GPU.
+
+oracle/_ref/ref_driver is the reference GPU-Preprocessor library, compiled from
+its own sources by oracle/ref.mk, behind a small exporter (oracle/ref_driver.cpp).
+The test runs it and the CUDA engine on identical synthetic LPs with the same
+rule set and requires what the north star asks: the removed rows and columns,
+the row/column maps and the sparsity pattern bit-exact; coefficients, bounds
+and sides within 1e-12 relative.  Skipped when the reference build is absent
+(it needs the reference sources at build time).
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import pyoracle
+from gpp_b200 import device, lpgen
+from gpp_b200.capi import RULE_FLAGS, params_with_rules
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
+BUILT = CLEANUP + ["bound_strengthening"]
+
+
+def run_reference(lp, rules, extra=None):
+    d = tempfile.mkdtemp()
+    path = os.path.join(d, "lp.bin")
+    lpgen.save_lp(path, lp)
+    args = [DRIVER, path, d, "enable_folding=0", "enable_structure_specific_rules=0"]
+    for f in RULE_FLAGS:
+        args.append(f"{f}={1 if f[len('enable_'):] in rules else 0}")
+    args += extra or []
+    r = subprocess.run(args, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    meta = {}
+    for line in open(os.path.join(d, "meta.txt")):
+        k, *v = line.split()
+        meta[k] = v[0] if len(v) == 1 else v
+    out = {"meta": meta}
+    spec = {"A_ptr": np.int32, "A_idx": np.int32, "A_val": np.float64, "AT_ptr": np.int32, "AT_idx": np.int32,
+            "AT_val": np.float64, "c": np.float64, "l": np.float64, "u": np.float64, "AL": np.float64,
+            "AU": np.float64, "row_map": np.int32, "col_map": np.int32, "fixed_idx": np.int32,
+            "fixed_val": np.float64, "tape_types": np.int32, "tape_is": np.int32, "tape_vs": np.int32,
+            "tape_idx": np.int32, "tape_val": np.float64}
+    for k, dt in spec.items():
+        p = os.path.join(d, k)
+        out[k] = np.fromfile(p, dtype=dt) if os.path.exists(p) else None
+    return out
+
+
+def close(a, b, rel=1e-12):
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    both_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    ok = both_inf | (np.abs(a - b) <= rel * np.maximum(1.0, np.maximum(np.abs(a), np.abs(b))))
+    return bool(np.all(ok))
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT])
+@pytest.mark.parametrize("workload", ["random:400x1000", "small"])
+def test_structure_matches_reference(rules, workload):
+    lp = lpgen.workload(workload, seed=0)
+    ref = run_reference(lp, rules)
+    params = params_with_rules(rules, enable_folding=0)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params)
+    try:
+        got = device.Result(s)
+        m = ref["meta"]
+        assert (s.reduced_rows, s.reduced_cols, s.reduced_nnz) == (
+            int(m["reduced_rows"]), int(m["reduced_cols"]), int(m["reduced_nnz"]))
+        assert s.iterations == int(m["iterations"])
+        assert np.array_equal(got.row_map, ref["row_map"]) and np.array_equal(got.col_map, ref["col_map"])
+        for k in ("A_ptr", "A_idx", "AT_ptr", "AT_idx"):
+            assert np.array_equal(getattr(got, k), ref[k]), k
+        for k in ("A_val", "AT_val", "c", "l", "u", "AL", "AU"):
+            assert close(getattr(got, k), ref[k]), k
+        assert np.array_equal(np.sort(got.fixed_idx), np.sort(ref["fixed_idx"]))
+        assert np.array_equal(got.tape_types, ref["tape_types"])
+        assert np.array_equal(got.tape_idx, ref["tape_idx"])
+        assert close(got.tape_val, ref["tape_val"], 1e-9)
+        # The oracle agrees with both.
+        orc = pyoracle.presolve(lp, params)
+        assert np.array_equal(orc.row_map, ref["row_map"]) and np.array_equal(orc.col_map, ref["col_map"])
+    finally:
+        device.free_summary(s)
