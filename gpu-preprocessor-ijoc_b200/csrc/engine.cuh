@@ -102,6 +102,9 @@ void row_activity_summary(const DevCsr& A, const double* l, const double* u, dou
                           const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
                           double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,
                           cudaStream_t s);
+void row_plain_minmax(const DevCsr& A, const double* l, const double* u, const uint8_t* keep_row,
+                      const uint8_t* keep_col, const int32_t* live_deg, double* row_min, double* row_max,
+                      cudaStream_t s);
 void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStream_t s);
 
 // compact.cu
@@ -145,7 +148,7 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
 // Row-wise shift sum_j a_ij * v_j over kept rows and selected columns, in
 // ascending column order (deterministic replacement of atomicAdd shifts).
 // With `radius`, sums |a_ij| * radius_j over selected columns with radius > 0.
-void row_gather_shift(const DevCsr& A, const uint8_t* keep_row, const uint8_t* selected,
+void row_gather_shift(const DevCsr& A, const DevCsr& AT, const uint8_t* keep_row, const uint8_t* selected,
                       const double* value, const double* radius, double* out, cudaStream_t s);
 // Canonical objective sum of contrib over the rule-entry domain.
 double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_t n, cudaStream_t s);

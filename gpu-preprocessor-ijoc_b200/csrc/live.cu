@@ -111,6 +111,7 @@ __device__ __forceinline__ T block_sum_cub_order(T v, T* warp_aggs) {
   return total;
 }
 
+template <bool Plain>
 struct ActivityTerm {
   const int32_t* idx;
   const double* val;
@@ -119,6 +120,13 @@ struct ActivityTerm {
   double zero_tol;
   __device__ __forceinline__ void operator()(offset_t p, double& lo, double& hi, int& ni, int& pi) const {
     const double a = val[p];
+    if constexpr (Plain) {
+      // Plain sums of the redundant-row test: infinities propagate.
+      const int col = idx[p];
+      lo += a >= 0.0 ? a * l[col] : a * u[col];
+      hi += a >= 0.0 ? a * u[col] : a * l[col];
+      return;
+    }
     if (fabs(a) <= zero_tol) return;
     const int col = idx[p];
     const double tlo = a >= 0.0 ? a * l[col] : a * u[col];
@@ -128,6 +136,7 @@ struct ActivityTerm {
   }
 };
 
+template <bool Plain>
 __global__ void __launch_bounds__(kThreads)
 activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                 const double* __restrict__ val, const double* __restrict__ l, const double* __restrict__ u,
@@ -140,7 +149,7 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   __shared__ int warp_counts[8];
   __shared__ double dagg[8];
   __shared__ int iagg[8];
-  const ActivityTerm term{idx, val, l, u, zero_tol};
+  const ActivityTerm<Plain> term{idx, val, l, u, zero_tol};
   const int b = blockIdx.x;
   if (b < short_blocks) {
     for (int i = b * blockDim.x + threadIdx.x; i < m; i += short_blocks * blockDim.x) {
@@ -151,7 +160,8 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
         if ((keep_row && !keep_row[i]) || (keep_col && !keep_col[idx[p]])) continue;
         term(p, lo, hi, ni, pi);
       }
-      min_fin[i] = lo; max_fin[i] = hi; min_inf[i] = ni; max_inf[i] = pi;
+      min_fin[i] = lo; max_fin[i] = hi;
+      if (min_inf) { min_inf[i] = ni; max_inf[i] = pi; }
     }
     return;
   }
@@ -169,7 +179,10 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
         live_visit<32>(first, last, idx, mask, slots + warp * 32, nullptr,
                        [&](offset_t p) { term(p, lo, hi, ni, pi); });
       lo = warp_sum_down(lo); hi = warp_sum_down(hi); ni = warp_sum_down(ni); pi = warp_sum_down(pi);
-      if (lane == 0) { min_fin[row] = lo; max_fin[row] = hi; min_inf[row] = ni; max_inf[row] = pi; }
+      if (lane == 0) {
+        min_fin[row] = lo; max_fin[row] = hi;
+        if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
+      }
     }
     return;
   }
@@ -189,7 +202,10 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
     hi = block_sum_cub_order(hi, dagg);
     ni = block_sum_cub_order(ni, iagg);
     pi = block_sum_cub_order(pi, iagg);
-    if (threadIdx.x == 0) { min_fin[row] = lo; max_fin[row] = hi; min_inf[row] = ni; max_inf[row] = pi; }
+    if (threadIdx.x == 0) {
+      min_fin[row] = lo; max_fin[row] = hi;
+      if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
+    }
     __syncthreads();
   }
 }
@@ -217,7 +233,9 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
                   int32_t* support, double* coefficient, unsigned long long* total) {
   __shared__ int scount[8];
   __shared__ long long spos[8];
+  __shared__ unsigned long long stotal[8];
   const int b = blockIdx.x;
+  unsigned long long acc = 0;  // live entries seen by this thread, added once per block
   if (b < short_blocks) {
     for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
       const offset_t first = ptr[r], last = ptr[r + 1];
@@ -228,11 +246,10 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
       if (active)
         for (offset_t p = first; p < last; ++p)
           if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
-      stats_write(r, active, count, pos, idx, val, degree, empty, singleton, support, coefficient, total);
+      stats_write(r, active, count, pos, idx, val, degree, empty, singleton, support, coefficient, nullptr);
+      acc += unsigned(count);
     }
-    return;
-  }
-  if (b < short_blocks + medium_blocks) {
+  } else if (b < short_blocks + medium_blocks) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = medium_blocks * (kThreads / 32);
     for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
@@ -247,31 +264,43 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
         count += __shfl_down_sync(0xffffffffu, count, off);
         pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
       }
-      if (lane == 0)
-        stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, total);
+      if (lane == 0) {
+        stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, nullptr);
+        acc += unsigned(count);
+      }
     }
-    return;
+  } else {
+    const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+    for (int q = lb; q < counts[1]; q += nlong) {
+      const int r = longq[q];
+      const bool active = !keep_outer || keep_outer[r];
+      int count = 0;
+      long long pos = -1;
+      if (active)
+        for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads)
+          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+      for (int off = 16; off; off >>= 1) {
+        count += __shfl_down_sync(0xffffffffu, count, off);
+        pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
+      }
+      if ((threadIdx.x & 31) == 0) { scount[threadIdx.x >> 5] = count; spos[threadIdx.x >> 5] = pos; }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) { count += scount[w]; pos = max(pos, spos[w]); }
+        stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, nullptr);
+        acc += unsigned(count);
+      }
+      __syncthreads();
+    }
   }
-  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
-  for (int q = lb; q < counts[1]; q += nlong) {
-    const int r = longq[q];
-    const bool active = !keep_outer || keep_outer[r];
-    int count = 0;
-    long long pos = -1;
-    if (active)
-      for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads)
-        if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
-    for (int off = 16; off; off >>= 1) {
-      count += __shfl_down_sync(0xffffffffu, count, off);
-      pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
-    }
-    if ((threadIdx.x & 31) == 0) { scount[threadIdx.x >> 5] = count; spos[threadIdx.x >> 5] = pos; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 1; w < 8; ++w) { count += scount[w]; pos = max(pos, spos[w]); }
-      stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, total);
-    }
-    __syncthreads();
+  if (!total) return;
+  for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) stotal[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < 8; ++w) t += stotal[w];
+    if (t) atomicAdd(total, t);
   }
 }
 
@@ -430,9 +459,31 @@ void row_activity_summary(const DevCsr& A, const double* l, const double* u, dou
   // and values, column bounds, masks, live degrees, four outputs.
   const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
                        (keep_col ? A.cols : 0) + (live_deg ? 4.0 * A.rows : 0) + 24.0 * A.rows;
-  GPP_LAUNCH_BYTES(activity_kernel, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
+  GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
              A.idx, A.val, l, u, zero_tol, keep_row, keep_col, live_deg, sch->medium.p, sch->long_rows.p,
              sch->counts.p, r.short_blocks, r.medium_blocks, min_fin, max_fin, min_inf, max_inf);
+}
+
+void row_plain_minmax(const DevCsr& A, const double* l, const double* u, const uint8_t* keep_row,
+                      const uint8_t* keep_col, const int32_t* live_deg, double* row_min, double* row_max,
+                      cudaStream_t s) {
+  // Row sums of the redundant-row rule (rule_infeasible_and_redundant_rows.cu:46-156).
+  if (!A.rows) return;
+  static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
+  const RowSchedule* sch;
+  if (live_deg) {
+    build_schedule(*live_schedule, A, live_deg, s);
+    sch = live_schedule;
+  } else {
+    sch = &stored_schedule(A);
+  }
+  const Roles r = roles_for(A.rows);
+  const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
+                       (keep_col ? A.cols : 0) + (live_deg ? 4.0 * A.rows : 0) + 16.0 * A.rows;
+  GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s,
+                   A.rows, A.ptr, A.idx, A.val, l, u, 0.0, keep_row, keep_col, live_deg, sch->medium.p,
+                   sch->long_rows.p, sch->counts.p, r.short_blocks, r.medium_blocks, row_min, row_max,
+                   (int32_t*)nullptr, (int32_t*)nullptr);
 }
 
 void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStream_t s) {

@@ -375,7 +375,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
   double obj_delta = 0.0;
   if (fixed) {
     DBuf<double> shift(size_t(m), s);
-    row_gather_shift(lp.A, plan.keep_row.p, fx.p, fixv.p, nullptr, shift.p, s);
+    row_gather_shift(lp.A, lp.AT, plan.keep_row.p, fx.p, fixv.p, nullptr, shift.p, s);
     GPP_LAUNCH(shift_and_empty_rows, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, shift.p,
                plan.keep_col.p, plan.keep_row.p, plan.AL.p, plan.AU.p, p.feasibility_tol, st.d);
     const int32_t* g = st.read(5);

@@ -33,16 +33,26 @@ __device__ __forceinline__ double atomic_min_d(double* addr, double v) {
   return __longlong_as_double((long long)old);
 }
 
+// Rows touched by a selected column (with positive radius in radius mode).
+__global__ void mark_touched_rows(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
+                                  const uint8_t* __restrict__ selected, const double* __restrict__ radius,
+                                  uint8_t* __restrict__ touched) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (!selected[j] || (radius && !(radius[j] > 0.0))) continue;
+    for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) touched[at_idx[p]] = 1;
+  }
+}
+
 // Row sums over selected columns in stored (ascending column) order; one
-// thread per row, rows without a selected column cost one pass over their
-// indices.
+// thread per touched row, every other row gets 0.
 __global__ void row_gather_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                   const double* __restrict__ val, const uint8_t* __restrict__ keep_row,
-                                  const uint8_t* __restrict__ selected, const double* __restrict__ value,
-                                  const double* __restrict__ radius, double* __restrict__ out) {
+                                  const uint8_t* __restrict__ touched, const uint8_t* __restrict__ selected,
+                                  const double* __restrict__ value, const double* __restrict__ radius,
+                                  double* __restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     double acc = 0.0;
-    if (keep_row[i])
+    if (keep_row[i] && touched[i])
       for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
         const int j = idx[p];
         if (!selected[j]) continue;
@@ -66,7 +76,7 @@ __global__ void mask_contrib(int n, const double* __restrict__ contrib, const ui
 __global__ void fixed_candidates(int n, const uint8_t* __restrict__ keep_col, const double* __restrict__ l,
                                  const double* __restrict__ u, const double* __restrict__ c, double bound_tol,
                                  uint8_t* __restrict__ fixed, double* __restrict__ fval,
-                                 double* __restrict__ contrib, double* __restrict__ radius) {
+                                 double* __restrict__ contrib, double* __restrict__ radius, int32_t* __restrict__ any) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     uint8_t f = 0;
     double v = 0.0, cb = 0.0, rad = 0.0;
@@ -80,6 +90,7 @@ __global__ void fixed_candidates(int n, const uint8_t* __restrict__ keep_col, co
       }
     }
     fixed[j] = f; fval[j] = v; contrib[j] = cb; radius[j] = rad;
+    if (f) *any = 1;
   }
 }
 __global__ void fixed_filter(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
@@ -184,10 +195,14 @@ __global__ void singleton_rows_commit(int m, int n, const uint8_t* __restrict__ 
 
 }  // namespace
 
-void row_gather_shift(const DevCsr& A, const uint8_t* keep_row, const uint8_t* selected, const double* value,
-                      const double* radius, double* out, cudaStream_t s) {
+void row_gather_shift(const DevCsr& A, const DevCsr& AT, const uint8_t* keep_row, const uint8_t* selected,
+                      const double* value, const double* radius, double* out, cudaStream_t s) {
+  DBuf<uint8_t> touched(size_t(std::max(A.rows, 1)), s);
+  touched.zero();
+  GPP_LAUNCH(mark_touched_rows, grid_stride_blocks(AT.rows), kThreads, 0, s, AT.rows, AT.ptr, AT.idx, selected, radius,
+             touched.p);
   GPP_LAUNCH(row_gather_kernel, grid_stride_blocks(A.rows), kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, keep_row,
-             selected, value, radius, out);
+             touched.p, selected, value, radius, out);
 }
 
 double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_t n, cudaStream_t s) {
@@ -210,12 +225,13 @@ void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p) 
   Status st;
   st.clear(4);
   GPP_LAUNCH(fixed_candidates, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, plan.l.p, plan.u.p,
-             plan.c.p, p.bound_tol, fixed.p, fval.p, contrib.p, radius.p);
-  row_gather_shift(lp.A, plan.keep_row.p, fixed.p, fval.p, radius.p, row_err.p, s);
+             plan.c.p, p.bound_tol, fixed.p, fval.p, contrib.p, radius.p, st.d + 1);
+  if (st.read(2)[1] == 0) return;
+  row_gather_shift(lp.A, lp.AT, plan.keep_row.p, fixed.p, fval.p, radius.p, row_err.p, s);
   GPP_LAUNCH(fixed_filter, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, plan.keep_row.p,
              plan.l.p, plan.u.p, row_err.p, 0.1 * p.feasibility_tol, fixed.p, contrib.p, st.d);
   if (st.read(1)[0] == 0) return;
-  row_gather_shift(lp.A, plan.keep_row.p, fixed.p, fval.p, nullptr, shift.p, s);
+  row_gather_shift(lp.A, lp.AT, plan.keep_row.p, fixed.p, fval.p, nullptr, shift.p, s);
   GPP_LAUNCH(fixed_apply, grid_stride_blocks(std::max(n, m)), kThreads, 0, s, n, m, fixed.p, fval.p, shift.p,
              plan.keep_col.p, plan.l.p, plan.u.p, plan.AL.p, plan.AU.p);
   plan.obj_delta += domain_objective(contrib.p, plan.rule_entry_keep_col, n, s);

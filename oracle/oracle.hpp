@@ -104,6 +104,13 @@ void row_activity_summary(const Csr& A, const std::vector<double>& l, const std:
                           double zero_tol, const uint8_t* keep_row, const uint8_t* keep_col,
                           const int* live_degrees, double* min_fin, double* max_fin,
                           int* min_inf, int* max_inf);
+void row_activity_impl(const Csr& A, const std::vector<double>& l, const std::vector<double>& u,
+                       double zero_tol, const uint8_t* keep_row, const uint8_t* keep_col,
+                       const int* live_degrees, double* min_fin, double* max_fin, int* min_inf, int* max_inf,
+                       bool plain);
+void row_plain_minmax(const Csr& A, const std::vector<double>& l, const std::vector<double>& u,
+                      const uint8_t* keep_row, const uint8_t* keep_col, const int* live_degrees,
+                      double* row_min, double* row_max);
 void live_stats(const Csr& M, const uint8_t* keep_outer, const uint8_t* keep_inner, int* degree,
                 uint8_t* empty, uint8_t* singleton, int* support, double* coefficient,
                 int64_t* total);

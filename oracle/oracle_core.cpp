@@ -104,6 +104,23 @@ void row_activity_summary(const Csr& A, const std::vector<double>& l, const std:
                           double zero_tol, const uint8_t* keep_row, const uint8_t* keep_col,
                           const int* live_degrees, double* min_fin, double* max_fin,
                           int* min_inf, int* max_inf) {
+  row_activity_impl(A, l, u, zero_tol, keep_row, keep_col, live_degrees, min_fin, max_fin, min_inf, max_inf, false);
+}
+
+void row_plain_minmax(const Csr& A, const std::vector<double>& l, const std::vector<double>& u,
+                      const uint8_t* keep_row, const uint8_t* keep_col, const int* live_degrees,
+                      double* row_min, double* row_max) {
+  // The redundant-row sums (rule_infeasible_and_redundant_rows.cu:46-156):
+  // plain sums of a*l / a*u over live entries, infinities propagate, same
+  // bucket association as the activity summary.
+  std::vector<int> ni(static_cast<size_t>(A.rows)), pi(static_cast<size_t>(A.rows));
+  row_activity_impl(A, l, u, 0.0, keep_row, keep_col, live_degrees, row_min, row_max, ni.data(), pi.data(), true);
+}
+
+void row_activity_impl(const Csr& A, const std::vector<double>& l, const std::vector<double>& u,
+                       double zero_tol, const uint8_t* keep_row, const uint8_t* keep_col,
+                       const int* live_degrees, double* min_fin, double* max_fin,
+                       int* min_inf, int* max_inf, bool plain) {
   // compute_row_activity_summary (gpu_presolve_kernels.cu:96-148,194-245,744-787):
   // rows of (live) length <= 8 sum sequentially; 9..1024 use 32 lane-strided
   // partials and a shfl_down tree; > 1024 use 256 partials and cub BlockReduce.
@@ -114,6 +131,12 @@ void row_activity_summary(const Csr& A, const std::vector<double>& l, const std:
     if (active) live_positions(A, i, keep_col, pos); else pos.clear();
     auto term = [&](int p, double& lo, double& hi, int& ni, int& pi) {
       const double a = A.val[p];
+      if (plain) {
+        const int col = A.idx[p];
+        lo += a >= 0.0 ? a * l[col] : a * u[col];
+        hi += a >= 0.0 ? a * u[col] : a * l[col];
+        return;
+      }
       if (std::fabs(a) <= zero_tol) return;
       const int col = A.idx[p];
       const double tlo = a >= 0.0 ? a * l[col] : a * u[col];

@@ -389,4 +389,137 @@ void rule_bound_strengthening(Plan& plan, const Lp& lp, const Stats& s, const gp
   plan.has_change = true;
 }
 
+void rule_redundant_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_infeasible_and_redundant_rows (rule_infeasible_and_redundant_rows.cu:178-331).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m();
+  if (m == 0) return;
+  std::vector<double> mn(static_cast<size_t>(m)), mx(static_cast<size_t>(m));
+  row_plain_minmax(lp.A, plan.l, plan.u, plan.keep_row.data(), plan.keep_col.data(), s.row_nnz.data(), mn.data(),
+                   mx.data());
+  const double tol = p.bound_tol;
+  std::vector<uint8_t> full(size_t(m), 0), dl(size_t(m), 0), du(size_t(m), 0);
+  bool infeasible = false, any = false, any_full = false;
+  for (int i = 0; i < m; ++i) {
+    if (!plan.keep_row[i] || s.row_nnz[i] <= 1) continue;
+    const double al = plan.AL[i], au = plan.AU[i];
+    const bool lf = fin(al), uf = fin(au);
+    if (lf && uf && std::fabs(au - al) <= tol) continue;
+    const double lo = mn[i], hi = mx[i];
+    if ((lf && hi < al - tol) || (uf && lo > au + tol)) { infeasible = true; continue; }
+    const bool li = !lf || lo >= al - tol, ui = !uf || hi <= au + tol;
+    if (li && ui) { full[i] = 1; any = any_full = true; }
+    else if (lf && li) { dl[i] = 1; any = true; }
+    else if (uf && ui) { du[i] = 1; any = true; }
+  }
+  if (infeasible) { plan.has_infeasible = true; return; }
+  if (!any) return;
+  for (int i = 0; i < m; ++i) {
+    if (full[i]) plan.keep_row[i] = 0;
+    if (dl[i]) plan.AL[i] = -INFINITY;
+    if (du[i]) plan.AU[i] = INFINITY;
+  }
+  plan.has_row_action = true;
+  plan.has_redundant_row_deletion = plan.has_redundant_row_deletion || any_full;
+  plan.has_row_deletion = plan.has_row_deletion || any_full;
+  plan.has_change = true;
+}
+
+void rule_dual_fix(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_dual_fix (rule_dual_fix.cu:203-645) on the deferred plan.
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int n = lp.n(), m = lp.m();
+  if (n == 0) return;
+  std::vector<uint8_t> fixed(size_t(n), 0), inf(size_t(n), 0);
+  std::vector<double> fval(size_t(n), 0.0), contrib(size_t(n), 0.0);
+  int status0 = 0;
+  bool any = false, any_inf = false;
+  const double zt = p.zero_tol;
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[j]) continue;
+    const double lj = plan.l[j], uj = plan.u[j];
+    if (lj > uj + p.bound_tol) { status0 = std::max(status0, 1); continue; }
+    const double cj = plan.c[j];
+    if (std::fabs(cj) > zt && s.col_nnz[j] > p.dual_fix_max_nonzero_cost_col_degree) continue;
+    bool down = false, up = false;
+    for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q) {
+      const int row = lp.AT.idx[q];
+      if (!plan.keep_row[row]) continue;
+      const double a = lp.AT.val[q];
+      if (a > zt) { down = down || fin(plan.AL[row]); up = up || fin(plan.AU[row]); }
+      else if (a < -zt) { down = down || fin(plan.AU[row]); up = up || fin(plan.AL[row]); }
+      if (down && up) break;
+    }
+    bool f = false, fi = false;
+    double v = 0.0;
+    if (cj > zt) {
+      if (!down) { if (fin(lj)) { v = lj; f = true; } else { status0 = std::max(status0, 2); continue; } }
+    } else if (cj < -zt) {
+      if (!up) { if (fin(uj)) { v = uj; f = true; } else { status0 = std::max(status0, 2); continue; } }
+    } else if (std::fabs(cj) <= zt) {
+      if (!down) { f = true; if (fin(lj)) v = lj; else { v = -INFINITY; fi = true; } }
+      else if (!up) { f = true; if (fin(uj)) v = uj; else { v = INFINITY; fi = true; } }
+    }
+    if (f) {
+      fixed[j] = 1; inf[j] = fi; fval[j] = v; contrib[j] = fi ? 0.0 : cj * v;
+      any = true;
+      any_inf = any_inf || fi;
+    }
+  }
+  if (status0 == 1) { plan.has_infeasible = true; return; }
+  if (status0 == 2) { plan.has_unbounded = true; return; }
+  if (!any) return;
+  std::vector<uint8_t> finite_fixed(size_t(n), 0);
+  for (int j = 0; j < n; ++j) finite_fixed[size_t(j)] = fixed[size_t(j)] && !inf[size_t(j)];
+  const std::vector<double> shift = row_shift_gather(lp, plan.keep_row, finite_fixed, fval, false);
+  std::vector<uint8_t> remove(size_t(m), 0);
+  bool row_changed = false;
+  for (int j = 0; j < n; ++j) {
+    if (!(fixed[j] && inf[j])) continue;
+    for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q)
+      if (plan.keep_row[lp.AT.idx[q]]) { remove[size_t(lp.AT.idx[q])] = 1; row_changed = true; }
+  }
+  if (p.record_postsolve_tape && any_inf) {
+    // infinite_counts / infinite_pack (device_recovery.cu:350-412): rows of the
+    // column with their entries restricted to the rule-entry column domain.
+    const std::vector<uint8_t>& entry = *plan.rule_entry_keep_col;
+    Tape seg;
+    for (int j = 0; j < n; ++j) {
+      if (!(fixed[j] && inf[j])) continue;
+      const bool pos = fval[j] > 0;
+      std::vector<int> ii{pos ? 1 : -1, j, 0};
+      std::vector<double> vv{pos ? plan.l[j] : plan.u[j]};
+      int active = 0;
+      for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q) {
+        const int row = lp.AT.idx[q];
+        if (!plan.keep_row[row]) continue;
+        ++active;
+        const size_t header = ii.size();
+        ii.push_back(0);
+        vv.push_back(fin(plan.AL[row]) ? plan.AL[row] : plan.AU[row]);
+        for (int t = lp.A.ptr[row]; t < lp.A.ptr[row + 1]; ++t) {
+          if (!entry[size_t(lp.A.idx[t])]) continue;
+          ++ii[header];
+          ii.push_back(lp.A.idx[t]);
+          vv.push_back(lp.A.val[t]);
+        }
+      }
+      ii[2] = active;
+      seg.add(InfiniteBoundDualFix, ii, vv);
+    }
+    plan.tape.append(seg);
+  }
+  for (int j = 0; j < n; ++j)
+    if (fixed[j]) { plan.l[j] = fval[j]; plan.u[j] = fval[j]; plan.keep_col[j] = 0; }
+  for (int i = 0; i < m; ++i) {
+    plan.AL[i] -= shift[i];
+    plan.AU[i] -= shift[i];
+    if (remove[i]) plan.keep_row[i] = 0;
+  }
+  plan.obj_delta += domain_objective(contrib, plan);
+  plan.has_row_action = plan.has_row_action || row_changed;
+  plan.has_col_action = true;
+  plan.has_change = true;
+}
+
 }  // namespace oracle

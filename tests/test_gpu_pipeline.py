@@ -13,6 +13,7 @@ pytestmark = pytest.mark.gpu
 
 CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
 BUILT = CLEANUP + ["bound_strengthening"]
+PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 
 
 def bits(a):
@@ -31,7 +32,7 @@ def assert_same(gpu, orc):
     assert s.obj_constant_delta == o.obj_constant_delta
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION])
 @pytest.mark.parametrize("workload", ["random:400x1000", "small"])
 def test_presolve_bitwise_vs_oracle(rules, workload):
     lp = lpgen.workload(workload, seed=0)
@@ -51,7 +52,7 @@ def test_presolve_bitwise_vs_oracle(rules, workload):
 def test_postprocess_vs_oracle_and_highs(seed):
     import torch
     lp = lpgen.random_lp(400, 1000, seed=seed)
-    params = params_with_rules(BUILT, enable_folding=0)
+    params = params_with_rules(PROPAGATION, enable_folding=0)
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
     try:

@@ -11,6 +11,7 @@ from gpp_b200.capi import params_with_rules
 
 CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
 BUILT = CLEANUP + ["bound_strengthening"]
+PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 
 
 def test_dyadic_activity_matches_reference_fixture():
@@ -67,7 +68,7 @@ def test_det_sum_tree():
     assert pyoracle.det_sum(v) == total
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION])
 @pytest.mark.parametrize("seed", [0, 1])
 def test_postsolved_objective_matches_unreduced(rules, seed):
     lp = lpgen.random_lp(400, 1000, seed=seed)
