@@ -9,6 +9,7 @@
 
 #include "folding.hpp"
 #include "presolve.hpp"
+#include "sort.hpp"
 
 struct gpp_record {
   gpp::PresolveOutput out;
@@ -365,6 +366,13 @@ int gpp_parallel_row_hashes(const gpp_csr* A, const uint8_t* keep_row, const uin
     gpp::invalidate_schedules();
     gpp::parallel_row_hashes(D, keep_row, keep_col, mode, hashes, gpp::ctx().stream);
     gpp::ctx().sync("row hashes");
+  });
+}
+
+int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n) {
+  return guarded([&] {
+    gpp::radix_sort_pairs(keys, values, n, gpp::ctx().stream);
+    gpp::ctx().sync("sort pairs");
   });
 }
 

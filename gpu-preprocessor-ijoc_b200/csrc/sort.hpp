@@ -1,0 +1,9 @@
+// Device sort primitive shared by the duplicate-detection rules.
+#pragma once
+
+#include "common.cuh"
+
+namespace gpp {
+// Stable sort of n (key, value) pairs by key, in place.
+void radix_sort_pairs(uint64_t* keys, int32_t* vals, int64_t n, cudaStream_t s);
+}  // namespace gpp

@@ -240,6 +240,11 @@ GPP_API int gpp_compact_and_transpose(const gpp_csr* A, const uint8_t* keep_row,
 GPP_API int gpp_parallel_row_hashes(const gpp_csr* A, const uint8_t* keep_row, const uint8_t* keep_col,
                             int mode, uint64_t* hashes);
 
+/* Stable sort of n (uint64 key, int32 value) device pairs by key, in place:
+ * the engine's radix sort that replaces the reference's thrust::sort of
+ * (hash, id) tuples (rule_parallel_rows.cu:742-770). */
+GPP_API int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n);
+
 GPP_API void gpp_device_free(void* device_ptr);
 
 /* Last error message of the calling thread ("" when none). */

@@ -116,6 +116,8 @@ void live_stats(const Csr& M, const uint8_t* keep_outer, const uint8_t* keep_inn
                 int64_t* total);
 void col_max_abs(const Csr& AT, const uint8_t* keep_row, double* out);
 uint64_t row_hash(const Csr& A, int row, const uint8_t* keep_col, int mode);
+uint64_t row_hash_tol(const Csr& A, int row, const uint8_t* keep_col, int mode, double tol);
+uint64_t col_hash(const Csr& AT, int col, const uint8_t* keep_row, double tol);
 
 // --- pipeline -------------------------------------------------------------
 Result presolve(const Lp& lp, const gpp_params& params);

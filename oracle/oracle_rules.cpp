@@ -522,4 +522,288 @@ void rule_dual_fix(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p
   plan.has_change = true;
 }
 
+namespace {
+// (hash, index) pairs of live rows / columns sorted ascending.
+std::vector<std::pair<uint64_t, int>> sorted_groups(std::vector<uint64_t> h, const std::vector<uint8_t>& keep) {
+  std::vector<std::pair<uint64_t, int>> v;
+  for (size_t i = 0; i < keep.size(); ++i)
+    if (keep[i]) v.push_back({h[i], int(i)});
+  std::sort(v.begin(), v.end());
+  return v;
+}
+
+// _parallel_row_ratio (rule_parallel_rows.cu:346-377).
+bool row_ratio(const Csr& A, int i, int k, double tol, const std::vector<uint8_t>& keep_col, double* out) {
+  std::vector<int> L, R;
+  for (int p = A.ptr[i]; p < A.ptr[i + 1]; ++p) if (keep_col[A.idx[p]]) L.push_back(p);
+  for (int p = A.ptr[k]; p < A.ptr[k + 1]; ++p) if (keep_col[A.idx[p]]) R.push_back(p);
+  if (L.empty() && R.empty()) { *out = 1.0; return true; }
+  double ratio = 0.0;
+  bool set = false;
+  size_t a = 0;
+  for (; a < L.size() && a < R.size(); ++a) {
+    if (A.idx[L[a]] != A.idx[R[a]]) return false;
+    const double ai = A.val[L[a]], ak = A.val[R[a]];
+    if (!set) {
+      if (std::fabs(ak) <= tol) return false;
+      ratio = ai / ak;
+      set = true;
+    }
+    if (std::fabs(ai - ratio * ak) > tol) return false;
+  }
+  *out = ratio;
+  return set && a == L.size() && a == R.size();
+}
+
+// _parallel_column_ratio (rule_parallel_columns.cu:262-321).
+bool col_ratio(const Csr& AT, int j, int k, const std::vector<uint8_t>& keep_row, double zt, double ct, double* out) {
+  auto live = [&](int c) {
+    std::vector<int> v;
+    for (int p = AT.ptr[c]; p < AT.ptr[c + 1]; ++p)
+      if (keep_row[AT.idx[p]] && std::fabs(AT.val[p]) > zt) v.push_back(p);
+    return v;
+  };
+  const auto J = live(j), K = live(k);
+  double ratio = 0.0;
+  bool set = false;
+  size_t a = 0;
+  for (; a < J.size() && a < K.size(); ++a) {
+    if (AT.idx[J[a]] != AT.idx[K[a]]) return false;
+    const double aj = AT.val[J[a]], ak = AT.val[K[a]];
+    if (!set) {
+      if (std::fabs(aj) <= zt) return false;
+      ratio = ak / aj;
+      if (std::fabs(ratio) <= zt || !fin(ratio)) return false;
+      set = true;
+    }
+    const double expected = ratio * aj;
+    const double scale = std::fmax(std::fabs(ak), std::fabs(expected));
+    if (!fin(expected) || std::fabs(ak - expected) > ct * scale) return false;
+  }
+  if (a < J.size() || a < K.size() || !set) return false;
+  *out = ratio;
+  return true;
+}
+
+void scaled(double lo, double hi, double r, double& sl, double& su) {
+  const double a = lo * r, b = hi * r;
+  if (r >= 0.0) { sl = a; su = b; } else { sl = b; su = a; }
+}
+}  // namespace
+
+void rule_parallel_rows(Plan& plan, const Lp& lp, const Stats&, const gpp_params& p) {
+  // apply_rule_parallel_rows (rule_parallel_rows.cu:643-888).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m();
+  if (m <= 1) return;
+  const int mode = int64_t(lp.A.nnz()) > 32LL * m ? 1 : 0;
+  std::vector<uint64_t> h(static_cast<size_t>(m));
+  for (int i = 0; i < m; ++i)
+    h[size_t(i)] = plan.keep_row[i] ? row_hash_tol(lp.A, i, plan.keep_col.data(), mode, p.zero_tol) : uint64_t(i);
+  const auto g = sorted_groups(h, plan.keep_row);
+  const double ct = p.zero_tol, it = p.feasibility_tol;
+  struct Rec { int step, kept, del; double v[5]; };
+  std::vector<Rec> recs;
+  std::vector<uint8_t> del(size_t(m), 0);
+  for (size_t s = 0; s < g.size();) {
+    size_t e = s;
+    while (e + 1 < g.size() && g[e + 1].first == g[s].first) ++e;
+    const size_t s0 = s;
+    s = e + 1;
+    if (e == s0) continue;
+    int seed = -1;
+    bool seed_eq = false;
+    for (size_t a = s0; a <= e; ++a) {
+      const int row = g[a].second;
+      if (!plan.keep_row[row]) continue;
+      const bool eq = fin(plan.AL[row]) && fin(plan.AU[row]) && std::fabs(plan.AL[row] - plan.AU[row]) <= it;
+      if (seed < 0 || (eq && !seed_eq)) { seed = row; seed_eq = eq; }
+    }
+    if (seed < 0) continue;
+    int rep = seed;
+    double rsl = plan.AL[seed], rsu = plan.AU[seed];
+    for (size_t a = s0; a <= e; ++a) {
+      const int row = g[a].second;
+      if (row == seed || !plan.keep_row[row]) continue;
+      double r;
+      if (!row_ratio(lp.A, seed, row, ct, plan.keep_col, &r)) continue;
+      double sl, su;
+      scaled(plan.AL[row], plan.AU[row], r, sl, su);
+      if (rsl <= sl + it && su <= rsu + it) { rep = row; rsl = sl; rsu = su; }
+    }
+    double rl = plan.AL[rep], ru = plan.AU[rep];
+    bool found = false;
+    int step = 0;
+    for (size_t a = s0; a <= e; ++a) {
+      const int row = g[a].second;
+      if (row == rep || !plan.keep_row[row]) continue;
+      double r;
+      if (!row_ratio(lp.A, rep, row, ct, plan.keep_col, &r)) continue;
+      found = true;
+      double sl, su;
+      scaled(plan.AL[row], plan.AU[row], r, sl, su);
+      if (std::fmax(rl, sl) > std::fmin(ru, su) + it) { plan.has_infeasible = true; return; }
+      ++step;
+      recs.push_back({step, rep, row, {r, rl, ru, plan.AL[row], plan.AU[row]}});
+      rl = std::fmax(rl, sl);
+      ru = std::fmin(ru, su);
+      del[size_t(row)] = 1;
+    }
+    if (found) { plan.AL[rep] = rl; plan.AU[rep] = ru; }
+  }
+  if (recs.empty()) return;
+  for (int i = 0; i < m; ++i) if (del[size_t(i)]) plan.keep_row[i] = 0;
+  if (p.record_postsolve_tape) {
+    std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
+      return a.step != b.step ? a.step < b.step : a.del < b.del;
+    });
+    Tape seg;
+    for (const auto& r : recs)
+      seg.add(ParallelRow, {r.kept, r.del}, {r.v[0], r.v[1], r.v[2], r.v[3], r.v[4]});
+    plan.tape.append(seg);
+  }
+  plan.has_row_action = plan.has_change = true;
+}
+
+void rule_parallel_columns(Plan& plan, const Lp& lp, const Stats&, const gpp_params& p) {
+  // apply_rule_parallel_columns (rule_parallel_columns.cu:725-1127).
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (n <= 1) return;
+  std::vector<uint64_t> h(static_cast<size_t>(n));
+  for (int j = 0; j < n; ++j)
+    h[size_t(j)] = plan.keep_col[j] ? col_hash(lp.AT, j, plan.keep_row.data(), p.zero_tol) : uint64_t(j);
+  const auto g = sorted_groups(h, plan.keep_col);
+  const double zt = p.zero_tol, ct = std::fmax(p.zero_tol, p.bound_tol), ot = ct;
+  const double max_abs = p.parallel_columns_max_abs_ratio;
+  const bool guard = fin(max_abs) && p.parallel_columns_scale_guard_min_groups > 1;
+  auto guarded = [](double r, double mx) {
+    const double a = std::fabs(r);
+    return fin(mx) && (mx < 1.0 || a > mx || a * mx < 1.0);
+  };
+  int guard_count = 0;
+  if (guard) {
+    for (size_t s = 0; s < g.size();) {
+      size_t e = s;
+      while (e + 1 < g.size() && g[e + 1].first == g[s].first) ++e;
+      const size_t s0 = s;
+      s = e + 1;
+      const int size = int(e - s0 + 1);
+      if (size < 2 || size > p.parallel_columns_scale_guard_max_group_size) continue;
+      bool hit = false;
+      for (size_t a = s0; a < e && !hit; ++a) {
+        const int j = g[a].second;
+        for (size_t b = a + 1; b <= e; ++b) {
+          const int k = g[b].second;
+          double r;
+          if (!col_ratio(lp.AT, j, k, plan.keep_row, zt, ct, &r)) continue;
+          if (std::fabs(plan.c[k] - r * plan.c[j]) > ot) continue;
+          if (max_abs < 1.0 || std::fabs(r) > max_abs || std::fabs(r) * max_abs < 1.0) { hit = true; break; }
+        }
+      }
+      if (hit) ++guard_count;
+    }
+  }
+  const double active_max = guard && guard_count < p.parallel_columns_scale_guard_min_groups ? INFINITY : max_abs;
+  std::vector<uint8_t> del(size_t(n), 0), fixed(size_t(n), 0);
+  std::vector<double> fval(size_t(n), 0.0);
+  struct Rec { int del, kept; double v[5]; };
+  std::vector<Rec> recs;
+  bool any_fixed = false;
+  for (size_t s = 0; s < g.size();) {
+    size_t e = s;
+    while (e + 1 < g.size() && g[e + 1].first == g[s].first) ++e;
+    const size_t s0 = s;
+    s = e + 1;
+    if (e == s0) continue;
+    for (size_t a = s0; a < e; ++a) {
+      const int j = g[a].second;
+      if (!plan.keep_col[j] || del[size_t(j)] || fixed[size_t(j)]) continue;
+      for (size_t b = a + 1; b <= e; ++b) {
+        const int k = g[b].second;
+        if (!plan.keep_col[k] || del[size_t(k)] || fixed[size_t(k)]) continue;
+        double r;
+        if (!col_ratio(lp.AT, j, k, plan.keep_row, zt, ct, &r)) continue;
+        if (guarded(r, active_max)) continue;
+        const double gap = plan.c[k] - r * plan.c[j];
+        const double tl = plan.l[j], tu = plan.u[j], sl = plan.l[k], su = plan.u[k];
+        if (std::fabs(gap) <= ot) {
+          recs.push_back({k, j, {r, sl, su, tl, tu}});
+          double nl = -INFINITY, nu = INFINITY;
+          if (r > 0.0) { if (fin(tl) && fin(sl)) nl = tl + r * sl; }
+          else if (fin(tl) && fin(su)) nl = tl + r * su;
+          if (r > 0.0) { if (fin(tu) && fin(su)) nu = tu + r * su; }
+          else if (fin(tu) && fin(sl)) nu = tu + r * sl;
+          plan.l[j] = nl;
+          plan.u[j] = nu;
+          del[size_t(k)] = 1;
+          continue;
+        }
+        bool k_lo = false, k_hi = false, j_lo = false, j_hi = false;
+        if (gap > ot) {
+          if (r > 0.0) { k_lo = !fin(tu); j_hi = !fin(sl); } else { k_lo = !fin(tl); j_lo = !fin(sl); }
+        } else {
+          if (r > 0.0) { k_hi = !fin(tl); j_lo = !fin(su); } else { k_hi = !fin(tu); j_hi = !fin(su); }
+        }
+        if (k_lo) {
+          if (!fin(sl)) { plan.has_unbounded = true; return; }
+          fixed[size_t(k)] = 1; fval[size_t(k)] = sl; any_fixed = true;
+          continue;
+        } else if (k_hi) {
+          if (!fin(su)) { plan.has_unbounded = true; return; }
+          fixed[size_t(k)] = 1; fval[size_t(k)] = su; any_fixed = true;
+          continue;
+        }
+        if (j_lo) {
+          if (!fin(tl)) { plan.has_unbounded = true; return; }
+          fixed[size_t(j)] = 1; fval[size_t(j)] = tl; any_fixed = true;
+          break;
+        } else if (j_hi) {
+          if (!fin(tu)) { plan.has_unbounded = true; return; }
+          fixed[size_t(j)] = 1; fval[size_t(j)] = tu; any_fixed = true;
+          break;
+        }
+      }
+    }
+  }
+  if (recs.empty() && !any_fixed) return;
+  if (!recs.empty() && p.record_postsolve_tape) {
+    std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) { return a.del < b.del; });
+    Tape seg;
+    for (const auto& r : recs) seg.add(ParallelColumn, {r.del, r.kept}, {r.v[0], r.v[1], r.v[2], r.v[3], r.v[4]});
+    plan.tape.append(seg);
+  }
+  std::vector<double> shift(size_t(m), 0.0);
+  if (any_fixed) {
+    if (p.record_postsolve_tape) {
+      Tape seg;
+      for (int j = 0; j < n; ++j) {
+        if (!fixed[size_t(j)]) continue;
+        std::vector<int> ii{j};
+        std::vector<double> vv{fval[size_t(j)], plan.c[j]};
+        for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q)
+          if (plan.keep_row[lp.AT.idx[q]]) { ii.push_back(lp.AT.idx[q]); vv.push_back(lp.AT.val[q]); }
+        seg.add(FixedVariable, ii, vv);
+      }
+      plan.tape.append(seg);
+    }
+    shift = row_shift_gather(lp, plan.keep_row, fixed, fval, false);
+    plan.has_row_action = true;
+  }
+  std::vector<double> contrib(size_t(n), 0.0);
+  for (int q = 0; q < n; ++q) {
+    if (!(del[size_t(q)] || fixed[size_t(q)])) continue;
+    plan.keep_col[q] = 0;
+    if (fixed[size_t(q)]) {
+      plan.l[q] = fval[size_t(q)];
+      plan.u[q] = fval[size_t(q)];
+      contrib[size_t(q)] = plan.c[q] * fval[size_t(q)];
+    }
+  }
+  if (any_fixed)
+    for (int i = 0; i < m; ++i) { plan.AL[i] -= shift[size_t(i)]; plan.AU[i] -= shift[size_t(i)]; }
+  plan.obj_delta += any_fixed ? det_sum(contrib) : 0.0;
+  plan.has_col_action = plan.has_change = true;
+}
+
 }  // namespace oracle

@@ -124,3 +124,14 @@ def test_compaction_and_transpose_vs_numpy():
     lib = capi.load()
     for p_ in (Ao.rowPtr, Ao.colVal, Ao.nzVal, ATo.rowPtr, ATo.colVal, ATo.nzVal):
         lib.gpp_device_free(p_)
+
+
+@pytest.mark.parametrize("rows", [10, 2100])
+def test_row_hash_fixture_on_gpu(rows):
+    import torch
+    f = fixtures.hash_fixture(rows)
+    A, keep = dev_csr(rows, f["cols"], f["ptr"], f["idx"], f["val"])
+    dk = to_device(f["keep"], np.uint8)
+    out = torch.zeros(rows, dtype=torch.int64, device="cuda")
+    _raise(capi.load().gpp_parallel_row_hashes(C.byref(A), ptr(dk), None, -1, ptr(out)))
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), f["expected"])

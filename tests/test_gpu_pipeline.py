@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
+PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 
 
 def bits(a):
@@ -32,7 +33,7 @@ def assert_same(gpu, orc):
     assert s.obj_constant_delta == o.obj_constant_delta
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
 @pytest.mark.parametrize("workload", ["random:400x1000", "small"])
 def test_presolve_bitwise_vs_oracle(rules, workload):
     lp = lpgen.workload(workload, seed=0)

@@ -12,6 +12,7 @@ from gpp_b200.capi import params_with_rules
 CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
+PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 
 
 def test_dyadic_activity_matches_reference_fixture():
@@ -68,7 +69,7 @@ def test_det_sum_tree():
     assert pyoracle.det_sum(v) == total
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
 @pytest.mark.parametrize("seed", [0, 1])
 def test_postsolved_objective_matches_unreduced(rules, seed):
     lp = lpgen.random_lp(400, 1000, seed=seed)
@@ -115,3 +116,26 @@ def test_schedule_trace_phase_order():
         if a == "phase=propagation":
             assert b in ("phase=cleanup", "phase=aggregation")
     assert r.summary.iterations >= 1
+
+
+@pytest.mark.parametrize("rows", [10, 2100])
+def test_row_hash_matches_reference_fixture(rows):
+    f = fixtures.hash_fixture(rows)
+    for i in range(rows):
+        if not f["keep"][i]:
+            continue
+        h = pyoracle.lib().orc_row_hash(rows, f["cols"], pyoracle.ptr(f["ptr"]), pyoracle.ptr(f["idx"]),
+                                        pyoracle.ptr(f["val"]), i, None, f["mode"])
+        assert h == int(f["expected"][i]), i
+
+
+def test_parallel_rules_postsolve_objective():
+    lp = lpgen.random_lp(600, 1500, seed=4)
+    rules = BUILT + ["infeasible_and_redundant_rows", "dual_fix", "parallel_rows", "parallel_columns"]
+    res0, _, _ = lpsolve.solve(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values, lp.c, lp.AL, lp.AU, lp.l, lp.u)
+    r = pyoracle.presolve(lp, params_with_rules(rules))
+    s = r.summary
+    rr, yr, zr = lpsolve.solve(s.reduced_rows, s.reduced_cols, r.A_ptr, r.A_idx, r.A_val, r.c, r.AL, r.AU, r.l, r.u)
+    x, _, _ = r.postsolve(rr.x, yr, zr)
+    assert abs(lp.c @ x - res0.fun) <= 1e-9 * max(1.0, abs(res0.fun))
+    assert lpsolve.primal_violation(lp, x) <= 1e-6

@@ -26,6 +26,7 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows"]
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
+PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 
 
 def run_reference(lp, rules, extra=None):
@@ -64,7 +65,7 @@ def close(a, b, rel=1e-12):
 
 
 @pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
 @pytest.mark.parametrize("workload", ["random:400x1000", "small"])
 def test_structure_matches_reference(rules, workload):
     lp = lpgen.workload(workload, seed=0)
