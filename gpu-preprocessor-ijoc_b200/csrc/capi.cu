@@ -376,6 +376,10 @@ int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n) {
   });
 }
 
+int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, void* stream) {
+  return guarded([&] { gpp::radix_sort_pairs_static(keys, values, n, static_cast<cudaStream_t>(stream)); });
+}
+
 void gpp_device_free(void* p) {
   if (!p) return;
   try {

@@ -122,6 +122,7 @@ def load():
         "gpp_compact_and_transpose": (C.c_int, [P(Csr), vp, vp, P(Csr), P(Csr)]),
         "gpp_parallel_row_hashes": (C.c_int, [P(Csr), vp, vp, C.c_int, vp]),
         "gpp_sort_pairs": (C.c_int, [vp, vp, i64]),
+        "gpp_sort_pairs_static": (C.c_int, [vp, vp, i64, vp]),
         "gpp_device_free": (None, [vp]),
         "gpp_last_error": (C.c_char_p, []),
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
@@ -140,7 +141,7 @@ EXPORTED = [
     "gpp_default_params", "gpp_preprocess", "gpp_run_presolve", "gpp_postprocess",
     "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
-    "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_device_free",
+    "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_free",
     "gpp_last_error", "gpp_kernel_launches", "gpp_profile_enable", "gpp_profile_read",
 ]
 

@@ -245,6 +245,26 @@ GPP_API int gpp_parallel_row_hashes(const gpp_csr* A, const uint8_t* keep_row, c
  * (hash, id) tuples (rule_parallel_rows.cu:742-770). */
 GPP_API int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n);
 
+/* The same stable sort of n (uint64 key, int32 value) device pairs, for
+ * callers that cannot allocate device memory when they call it: an LP solver
+ * that hands the whole device to its own arena allocator, or a host
+ * application that was promised a fixed device footprint, cannot let this
+ * library call cudaMalloc or grow a memory pool on its behalf.  This entry
+ * point has no counterpart in the reference.
+ *
+ * Its scratch is one fixed device array inside the library, sized for
+ * GPP_SORT_STATIC_MAX_PAIRS pairs (about 12.5 MiB); a larger n returns
+ * GPP_ERR_LENGTH without touching the data.  A call launches kernels on
+ * `stream` (a cudaStream_t; NULL for the legacy default stream) and returns
+ * without synchronizing; it calls no cudaMalloc, cudaFree or allocating
+ * library routine.  The first call on each device looks up the array's
+ * device address with that device current; make that first call before any
+ * stream capture.  Every call shares the one array, so calls whose work
+ * overlaps on the GPU race and give wrong results: order them on one stream
+ * or synchronize between them.  Output equals gpp_sort_pairs'. */
+#define GPP_SORT_STATIC_MAX_PAIRS (1 << 20)
+GPP_API int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, void* stream);
+
 GPP_API void gpp_device_free(void* device_ptr);
 
 /* Last error message of the calling thread ("" when none). */
