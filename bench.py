@@ -34,7 +34,8 @@ WORKLOAD = "scale"
 WORKLOAD_DESC = "random LP m=2,000,000 n=5,000,000 + 2,000 hub rows (500-5000 nnz), seed 0"
 METRIC = "presolve ms, HBM GB/s @25M nnz (presolve+postsolve ms per LP)"
 RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows",
-         "bound_strengthening"]
+         "singleton_columns", "bound_strengthening", "infeasible_and_redundant_rows", "dual_fix",
+         "parallel_rows", "parallel_columns"]
 
 
 def peaks():

@@ -1,6 +1,7 @@
 // Engine context, status block, scans and the canonical deterministic sum.
 #include "common.cuh"
 
+#include <algorithm>
 #include <memory>
 #include <mutex>
 
@@ -180,6 +181,23 @@ double det_sum(const double* v, int64_t n, cudaStream_t s) {
   check(cudaStreamSynchronize(s), "det_sum sync");
   double total = 0.0;
   for (double x : h) total += x;
+  return total;
+}
+
+double det_sum_sparse(std::vector<std::pair<int64_t, double>> entries) {
+  std::sort(entries.begin(), entries.end(),
+            [](const std::pair<int64_t, double>& a, const std::pair<int64_t, double>& b) { return a.first < b.first; });
+  double total = 0.0;
+  size_t k = 0;
+  while (k < entries.size()) {
+    const int64_t chunk = entries[k].first / 2048;
+    double slot[kThreads] = {};
+    for (; k < entries.size() && entries[k].first / 2048 == chunk; ++k)
+      slot[entries[k].first % kThreads] += entries[k].second;
+    for (int h = kThreads / 2; h > 0; h >>= 1)
+      for (int t = 0; t < h; ++t) slot[t] = slot[t] + slot[t + h];
+    total += slot[0];
+  }
   return total;
 }
 

@@ -187,6 +187,10 @@ void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t
 // Canonical deterministic sum (chunks of 2048, 256-thread halving tree, chunk
 // totals added in order on the host).  Returns the value on the host.
 double det_sum(const double* v, int64_t n, cudaStream_t s);
+// det_sum of a length-n vector that is zero except at the given (index,
+// value) entries, evaluated on the host in the same association: the +0.0
+// terms of the dense form are identities, so only the entries are needed.
+double det_sum_sparse(std::vector<std::pair<int64_t, double>> entries);
 
 struct ProfileSummary {
   std::string name;

@@ -13,6 +13,7 @@
 //   long   : 256 lane partials, per-warp shfl tree 1,2,4,8,16 then warp
 //            aggregates added in warp order (cub::BlockReduce default).
 #include "engine.cuh"
+#include "live_visit.cuh"
 
 #include <array>
 
@@ -39,47 +40,6 @@ __global__ void classify_rows(const offset_t* __restrict__ ptr, int m, const int
     if (lane == leader) base = atomicAdd(counts + g, __popc(mask));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (sel) (g == 0 ? medium : longq)[base + __popc(mask & ((1u << lane) - 1u))] = row;
-  }
-}
-
-// Visit the live entries of [first, last) so that the thread with index
-// `lane` (0..W-1) sees live ranks lane, lane+W, ... in order.  `slots` is W
-// ints of shared memory private to the warp (W=32) or block (W=256).
-template <int W, class Visit>
-__device__ __forceinline__ void live_visit(offset_t first, offset_t last, const int32_t* __restrict__ idx,
-                                           const uint8_t* __restrict__ keep, int* slots,
-                                           int* warp_counts, Visit visit) {
-  const int lane = W == 32 ? (threadIdx.x & 31) : threadIdx.x;
-  if (!keep) {
-    for (offset_t p = first + lane; p < last; p += W) visit(p);
-    return;
-  }
-  int carry = 0;
-  for (offset_t chunk = first; chunk < last; chunk += W) {
-    const offset_t p = chunk + lane;
-    const bool live = p < last && keep[idx[p]];
-    const unsigned mask = __ballot_sync(0xffffffffu, live);
-    int rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
-    int c = __popc(mask);
-    if constexpr (W == 256) {
-      const int warp = threadIdx.x >> 5;
-      if ((threadIdx.x & 31) == 0) warp_counts[warp] = c;
-      __syncthreads();
-      int before = 0, total = 0;
-#pragma unroll
-      for (int w = 0; w < 8; ++w) {
-        const int k = warp_counts[w];
-        before += w < warp ? k : 0;
-        total += k;
-      }
-      rank += before;
-      c = total;
-    }
-    if (live) slots[(carry + rank) & (W - 1)] = int(p - first);
-    if constexpr (W == 32) __syncwarp(); else __syncthreads();
-    if (((lane - carry) & (W - 1)) < c) visit(first + slots[lane]);
-    if constexpr (W == 32) __syncwarp(); else __syncthreads();
-    carry = (carry + c) & (W - 1);
   }
 }
 

@@ -6,7 +6,6 @@ namespace gpp {
 
 #define GPP_PENDING(name, ...) \
   void name(__VA_ARGS__) { throw std::runtime_error(#name " is not available in this build; disable it in gpp_params"); }
-GPP_PENDING(rule_singleton_columns, Plan&, const WorkingLp&, const Stats&, const gpp_params&)
 GPP_PENDING(rule_doubleton_equations, Plan&, const WorkingLp&, const gpp_params&)
 
 }  // namespace gpp

@@ -104,8 +104,9 @@ def _grid_values(rng, k):
     return v
 
 
-def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
-    """Plain-presolve family (see module docstring)."""
+def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0, slack_frac: float = 0.0) -> HostLP:
+    """Plain-presolve family (see module docstring).  ``slack_frac`` > 0 appends
+    one singleton column to that fraction of the rows (see _add_slacks)."""
     rng = np.random.default_rng(seed)
     n_single = int(round(0.05 * m))
     n_dton = int(round(0.05 * m))
@@ -219,7 +220,55 @@ def random_lp(m: int, n: int, seed: int = 0, hub_rows: int = 0) -> HostLP:
     AU[eq] = act[eq]
     c = rng.standard_normal(n)
     c[inf_u] = np.abs(c[inf_u])
-    return HostLP(m, n, ptr, idx, val, c, AL, AU, l, u).ensure_transpose()
+    lp = HostLP(m, n, ptr, idx, val, c, AL, AU, l, u)
+    if slack_frac > 0.0:
+        lp = _add_slacks(lp, act, slack_frac, seed)
+    return lp.ensure_transpose()
+
+
+def _add_slacks(lp: HostLP, act, frac: float, seed: int) -> HostLP:
+    """Append one singleton column to a fraction of the rows: nonnegative
+    columns, free columns and boxed columns (kinds 0/3, 1, 2).  Half of those
+    rows become equalities.  The planted point is extended so the LP stays
+    feasible, and the costs of the whole LP are redrawn from a planted dual
+    point so it stays bounded."""
+    rng = np.random.default_rng(seed + 7919)
+    m, n = lp.m, lp.n
+    rows = np.flatnonzero(rng.random(m) < frac)
+    k = rows.size
+    kind = rng.integers(0, 4, size=k)
+    coef = _grid_values(rng, k)
+    sl = np.where(kind == 1, -INF, 0.0)
+    su = np.where(kind == 2, rng.uniform(1.0, 20.0, size=k), INF)
+    xs = np.where(kind == 2, rng.uniform(0.0, 1.0, size=k) * su, rng.uniform(0.0, 5.0, size=k))
+    shift = coef * xs
+    AL, AU = lp.AL.copy(), lp.AU.copy()
+    eq = rng.random(k) < 0.5
+    eq |= ~np.isfinite(AL[rows]) & ~np.isfinite(AU[rows])   # no slack in a free row
+    base = act[rows] + shift
+    AL[rows] = np.where(eq, base, AL[rows] + shift)
+    AU[rows] = np.where(eq, base, AU[rows] + shift)
+    counts = np.diff(lp.row_ptr).astype(np.int64)
+    r_all = np.repeat(np.arange(m, dtype=np.int64), counts)
+    rows_c = np.concatenate([r_all, rows.astype(np.int64)])
+    cols_c = np.concatenate([lp.col_idx.astype(np.int64), n + np.arange(k, dtype=np.int64)])
+    vals_c = np.concatenate([lp.values, coef])
+    ptr, idx, val = coo_to_csr(m, rows_c, cols_c, vals_c)
+    l = np.concatenate([lp.l, sl])
+    u = np.concatenate([lp.u, su])
+    # Costs from a planted dual point (c = A'y + z with signs that fit the
+    # finite sides and bounds), so the LP has a finite optimum even with free
+    # columns in it.
+    y = np.abs(rng.standard_normal(m)) * (rng.random(m) < 0.5)
+    lo_f, hi_f = np.isfinite(AL), np.isfinite(AU)
+    y = np.where(lo_f & hi_f, y * rng.choice([-1.0, 1.0], size=m), np.where(lo_f, y, np.where(hi_f, -y, 0.0)))
+    zmag = np.abs(rng.standard_normal(n + k)) * (rng.random(n + k) < 0.5)
+    l_f, u_f = np.isfinite(l), np.isfinite(u)
+    z = np.where(l_f & u_f, zmag * rng.choice([-1.0, 1.0], size=n + k), np.where(l_f, zmag, np.where(u_f, -zmag, 0.0)))
+    c = np.zeros(n + k)
+    np.add.at(c, idx, val * np.repeat(y, np.diff(ptr)))
+    c += z
+    return HostLP(m, n + k, ptr, idx, val, c, AL, AU, l, u)
 
 
 def qap_lp(N: int, seed: int = 0) -> HostLP:
@@ -291,7 +340,8 @@ def qap_lp(N: int, seed: int = 0) -> HostLP:
 
 
 def workload(name: str, seed: int = 0) -> HostLP:
-    """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30'."""
+    """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
+    'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows), 'qap:N'."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -301,6 +351,9 @@ def workload(name: str, seed: int = 0) -> HostLP:
     if name.startswith("random:"):
         m, n = (int(v) for v in name.split(":")[1].split("x"))
         return random_lp(m, n, seed)
+    if name.startswith("slack:"):
+        m, n = (int(v) for v in name.split(":")[1].split("x"))
+        return random_lp(m, n, seed, slack_frac=0.3)
     if name.startswith("qap:"):
         return qap_lp(int(name.split(":")[1]), seed)
     raise ValueError(f"unknown workload {name!r}")

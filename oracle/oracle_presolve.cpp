@@ -685,7 +685,5 @@ void postsolve(const Result& r, const Lp& M, const double* x_red, const double* 
 // Rules not restated yet fail loudly so a parity run can never silently skip them.
 #define ORACLE_TODO(name, ...) \
   void name(__VA_ARGS__) { throw std::runtime_error("oracle: " #name " is not restated"); }
-ORACLE_TODO(rule_singleton_columns, Plan&, const Lp&, const Stats&, const gpp_params&)
-ORACLE_TODO(rule_doubleton_equations, Plan&, const Lp&, const gpp_params&)
 
 }  // namespace oracle

@@ -192,6 +192,526 @@ void rule_singleton_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_par
   plan.has_change = true;
 }
 
+// ---- doubleton equations ----------------------------------------------------
+
+namespace {
+constexpr int kDoubletonRounds = 8;          // DOUBLETON_EQUATION_BATCH_MATCHING_ROUNDS
+constexpr double kDoubletonMaxPivotRatio = 1.0e3;
+
+bool integral_ratio(double num, double den, double tol) {
+  // _is_integral_ratio_doubleton_equations (rule_doubleton_equations.cu:150-159).
+  if (std::fabs(den) <= tol) return false;
+  const double r = std::fabs(num / den);
+  if (!std::isfinite(r)) return false;
+  return std::fabs(r - std::nearbyint(r)) <= tol;
+}
+
+bool strictly_sorted(const Csr& M) {
+  for (int r = 0; r < M.rows; ++r)
+    for (int p = M.ptr[r] + 1; p < M.ptr[r + 1]; ++p)
+      if (M.idx[p - 1] >= M.idx[p]) return false;
+  return true;
+}
+
+// _doubleton_equations_fill_in_proxy_device_live (rule_doubleton_equations.cu:843-890).
+int fill_in_proxy(const Csr& AT, const std::vector<uint8_t>& keep_row, double zt, int keep, int elim) {
+  int fill = -1;
+  int jj = AT.ptr[keep], kk = AT.ptr[elim];
+  const int js = AT.ptr[keep + 1], ks = AT.ptr[elim + 1];
+  if (js <= jj || ks <= kk) return fill;
+  auto next_live = [&](int col, int& pos) {
+    while (pos < AT.ptr[col + 1]) {
+      const int r = AT.idx[pos];
+      if (keep_row[r] && std::fabs(AT.val[pos]) > zt) return r;
+      ++pos;
+    }
+    return INT_MAX;
+  };
+  while (jj < js && kk < ks) {
+    int jl = jj, kl = kk;
+    const int rj = next_live(keep, jl), rk = next_live(elim, kl);
+    if (rj == INT_MAX || rk == INT_MAX) break;
+    if (rj == rk) { jj = jl + 1; kk = kl + 1; }
+    else if (rk < rj) { kk = kl + 1; ++fill; }
+    else jj = jl + 1;
+  }
+  while (kk < ks) {
+    int kl = kk;
+    if (next_live(elim, kl) == INT_MAX) break;
+    ++fill;
+    kk = kl + 1;
+  }
+  return fill;
+}
+}  // namespace
+
+void rule_doubleton_equations(Plan& plan, const Lp& lp, const gpp_params& p) {
+  // apply_rule_doubleton_equations -> _batch -> _batch_once
+  // (rule_doubleton_equations.cu:1512-1812, 1948-1957): one batch of
+  // non-overlapping doubleton equalities per call.
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  if (!p.doubleton_equations_scan)
+    throw std::runtime_error("oracle: doubleton_equations_scan = 0 (single-row mode) is not restated");
+  const int m = lp.m(), n = lp.n();
+  if (m == 0 || n == 0) return;
+  const Csr& A = lp.A;
+  const Csr ATs = strictly_sorted(lp.AT) ? lp.AT : transpose(lp.A);
+  const double zt = p.zero_tol, tol = p.bound_tol, ratio_tol = std::fmax(1.0e-9, p.bound_tol);
+
+  // _kernel_doubleton_equations_live_col_nnz (:245-271).
+  std::vector<int> col_nnz(size_t(n), 0);
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[j]) continue;
+    int cnt = 0;
+    for (int q = ATs.ptr[j]; q < ATs.ptr[j + 1]; ++q)
+      if (plan.keep_row[ATs.idx[q]] && std::fabs(ATs.val[q]) > zt) ++cnt;
+    col_nnz[j] = cnt;
+  }
+  // Candidates (:892-958) and fill-in acceptance (:960-987).
+  std::vector<uint8_t> active(size_t(m), 0);
+  std::vector<int> ke(size_t(m), -1), el(size_t(m), -1);
+  std::vector<double> kv(size_t(m), 0.0), ev(size_t(m), 0.0);
+  int acceptable = 0;
+  for (int i = 0; i < m; ++i) {
+    if (!plan.keep_row[i]) continue;
+    const double lhs = plan.AL[i], rhs = plan.AU[i];
+    if (!fin(lhs) || !fin(rhs) || std::fabs(lhs - rhs) > tol) continue;
+    int live = 0, c1 = -1, c2 = -1;
+    double v1 = 0.0, v2 = 0.0;
+    for (int q = A.ptr[i]; q < A.ptr[i + 1] && live <= 2; ++q) {
+      const int j = A.idx[q];
+      if (!plan.keep_col[j] || !(std::fabs(A.val[q]) > zt)) continue;
+      ++live;
+      if (live == 1) { c1 = j; v1 = A.val[q]; } else if (live == 2) { c2 = j; v2 = A.val[q]; }
+    }
+    if (live != 2) continue;
+    // _choose_doubleton_equations_columns (:170-214).
+    const bool i12 = integral_ratio(v1, v2, ratio_tol), i21 = integral_ratio(v2, v1, ratio_tol);
+    bool elim_first;
+    if (col_nnz[c1] == 1 && col_nnz[c2] != 1) elim_first = true;
+    else if (col_nnz[c1] != 1 && col_nnz[c2] == 1) elim_first = false;
+    else if (i12 && !i21) elim_first = false;
+    else if (i21 && !i12) elim_first = true;
+    else elim_first = col_nnz[c1] < col_nnz[c2];
+    const int e = elim_first ? c1 : c2, k = elim_first ? c2 : c1;
+    const double evl = elim_first ? v1 : v2, kvl = elim_first ? v2 : v1;
+    // _is_acceptable_doubleton_equations_pivot (:161-168).
+    if (std::fabs(evl) <= 0.0) continue;
+    const double pr = std::fabs(kvl / evl);
+    if (!(pr <= kDoubletonMaxPivotRatio && pr >= 1.0 / kDoubletonMaxPivotRatio)) continue;
+    if (col_nnz[e] > col_nnz[k] + p.doubleton_equations_max_fill_in_proxy + 1) continue;
+    if (fill_in_proxy(ATs, plan.keep_row, zt, k, e) > p.doubleton_equations_max_fill_in_proxy) continue;
+    active[i] = 1;
+    ke[i] = k; el[i] = e; kv[i] = kvl; ev[i] = evl;
+    ++acceptable;
+  }
+  // Matching rounds (:989-1027, :1604-1613): each round, a row that owns both
+  // of its unblocked columns (the smallest claiming row) is selected.
+  std::vector<uint8_t> blocked(size_t(n), 0), selected(size_t(m), 0);
+  for (int round = 0; round < kDoubletonRounds; ++round) {
+    std::vector<int> owner(size_t(n), INT_MAX);
+    for (int i = 0; i < m; ++i)
+      if (active[i] && !blocked[ke[i]] && !blocked[el[i]]) {
+        owner[ke[i]] = std::min(owner[ke[i]], i);
+        owner[el[i]] = std::min(owner[el[i]], i);
+      }
+    std::vector<int> won;
+    for (int i = 0; i < m; ++i)
+      if (active[i] && !blocked[ke[i]] && !blocked[el[i]] && owner[ke[i]] == i && owner[el[i]] == i) won.push_back(i);
+    for (int i : won) { selected[i] = 1; active[i] = 0; blocked[ke[i]] = blocked[el[i]] = 1; }
+  }
+  std::vector<int> rows;
+  for (int i = 0; i < m; ++i) if (selected[i]) rows.push_back(i);
+  const int sel = int(rows.size());
+  const double ratio = acceptable == 0 ? 0.0 : double(sel) / double(acceptable);
+  if (sel == 0 || sel < p.doubleton_equations_min_selected_per_batch || ratio < p.doubleton_equations_min_selected_ratio)
+    return;
+
+  // Apply (:1029-1117) against the values before the batch; keep and
+  // eliminated columns are distinct across the batch.
+  struct Rec { int e, k, row; double ev, kv, au, el, eu, kl, ku, nkl, nku, ec; };
+  std::vector<Rec> recs;
+  std::vector<uint8_t> subst(size_t(sel), 0), fixed(size_t(sel), 0);
+  std::vector<double> beta_of(size_t(sel), 0.0), alpha_of(size_t(sel), 0.0);
+  bool infeasible = false, any = false;
+  double obj = 0.0, fixed_obj = 0.0;
+  for (int t = 0; t < sel; ++t) {
+    const int row = rows[size_t(t)], k = ke[row], e = el[row];
+    const Rec r0{e, k, row, ev[row], kv[row], plan.AU[row], plan.l[e], plan.u[e], plan.l[k], plan.u[k], 0.0, 0.0,
+                 plan.c[e]};
+    const double alpha = -kv[row] / ev[row];
+    const double beta = plan.AU[row] / ev[row];
+    double ml = -INFINITY, mu = INFINITY;
+    if (fin(plan.l[e])) { const double b = (plan.l[e] - beta) / alpha; if (alpha > 0.0) ml = b; else mu = b; }
+    if (fin(plan.u[e])) { const double b = (plan.u[e] - beta) / alpha; if (alpha > 0.0) mu = b; else ml = b; }
+    if (ml > mu) std::swap(ml, mu);
+    const double nl = fin(ml) ? std::fmax(plan.l[k], ml) : plan.l[k];
+    const double nu = fin(mu) ? std::fmin(plan.u[k], mu) : plan.u[k];
+    if (nl > nu + p.bound_tol) { infeasible = true; continue; }
+    if (fin(nl) && fin(nu) && nu <= nl + p.bound_tol) {
+      const double at = 0.5 * (nl + nu);
+      plan.l[k] = at; plan.u[k] = at;
+      plan.keep_col[k] = 0;
+      fixed[size_t(t)] = 1;
+      fixed_obj += plan.c[k] * at;
+    } else {
+      plan.l[k] = nl; plan.u[k] = nu;
+      plan.c[k] += plan.c[e] * alpha;
+      plan.keep_row[row] = 0;
+      plan.keep_col[e] = 0;
+      subst[size_t(t)] = 1;
+      obj += r0.ec * beta;
+      Rec r = r0;
+      r.nkl = nl; r.nku = nu;
+      recs.push_back(r);
+    }
+    alpha_of[size_t(t)] = alpha;
+    beta_of[size_t(t)] = beta;
+    any = true;
+  }
+  if (infeasible) { plan.has_infeasible = true; return; }
+  if (!any) return;
+  if (p.record_postsolve_tape)
+    for (const Rec& r : recs)
+      plan.tape.add(DoubletonEquation, {r.e, r.k, r.row, 0},
+                    {r.ev, r.kv, r.au, r.el, r.eu, r.kl, r.ku, r.nkl, r.nku, r.ec, 0.0, 0.0});
+
+  // Row shifts (:1164-1189, :1191-1229), in stored column order per row: the
+  // eliminated columns contribute a * beta, fixed keep columns a * value.
+  std::vector<uint8_t> role(size_t(n), 0);
+  std::vector<double> value(size_t(n), 0.0);
+  for (int t = 0; t < sel; ++t) {
+    const int row = rows[size_t(t)];
+    if (subst[size_t(t)]) { role[size_t(el[row])] = 1; value[size_t(el[row])] = beta_of[size_t(t)]; }
+    if (fixed[size_t(t)]) { role[size_t(ke[row])] = 1; value[size_t(ke[row])] = plan.l[ke[row]]; }
+  }
+  for (int i = 0; i < m; ++i) {
+    if (!plan.keep_row[i]) continue;
+    double shift = 0.0;
+    bool touched = false;
+    for (int q = A.ptr[i]; q < A.ptr[i + 1]; ++q) {
+      const int j = A.idx[q];
+      if (role[j] && std::fabs(A.val[q]) > zt) { shift += A.val[q] * value[j]; touched = true; }
+    }
+    if (touched) { plan.AL[i] -= shift; plan.AU[i] -= shift; }
+  }
+
+  // New A (:1191-1489): every row merged with the substitution deltas
+  // alpha * a_(r, elim) at (r, keep), entries with |a| <= zero_tol dropped.
+  if (!recs.empty()) {
+    std::vector<std::vector<std::pair<int, double>>> delta(static_cast<size_t>(m));
+    for (int t = 0; t < sel; ++t) {
+      if (!subst[size_t(t)]) continue;
+      const int row = rows[size_t(t)], e = el[row], k = ke[row];
+      for (int q = ATs.ptr[e]; q < ATs.ptr[e + 1]; ++q) {
+        const int r = ATs.idx[q];
+        if (r != row && plan.keep_row[r] && std::fabs(ATs.val[q]) > zt)
+          delta[size_t(r)].push_back({k, alpha_of[size_t(t)] * ATs.val[q]});
+      }
+    }
+    Csr out;
+    out.rows = m;
+    out.cols = n;
+    out.ptr.assign(size_t(m) + 1, 0);
+    for (int i = 0; i < m; ++i) {
+      auto& d = delta[size_t(i)];
+      std::stable_sort(d.begin(), d.end(), [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+        return a.first < b.first;
+      });
+      int pp = A.ptr[i];
+      const int pe = A.ptr[i + 1];
+      size_t qq = 0;
+      while (pp < pe || qq < d.size()) {
+        const int sc = pp < pe ? A.idx[pp] : INT_MAX;
+        const int dc = qq < d.size() ? d[qq].first : INT_MAX;
+        const int col = std::min(sc, dc);
+        double merged = 0.0;
+        while (pp < pe && A.idx[pp] == col) merged += A.val[pp++];
+        while (qq < d.size() && d[qq].first == col) merged += d[qq++].second;
+        if (std::fabs(merged) > zt) { out.idx.push_back(col); out.val.push_back(merged); }
+      }
+      out.ptr[size_t(i) + 1] = int(out.idx.size());
+    }
+    plan.new_A = std::move(out);
+    plan.has_new_A = true;
+  }
+  plan.obj_delta += obj;
+  plan.obj_delta += fixed_obj;
+  plan.has_row_action = !recs.empty();
+  plan.has_col_action = true;
+  plan.has_change = true;
+}
+
+// ---- singleton columns ------------------------------------------------------
+
+namespace {
+enum SingletonAction : uint8_t {
+  kNone = 0, kSetRowSide = 1, kTightenLhs = 2, kTightenRhs = 3,
+  kEliminateFree = 4, kEliminateFreeAbove = 5, kEliminateFreeBelow = 6
+};
+
+struct RowActivityCache {
+  double fmin = 0.0, fmax = 0.0;
+  int min_neg = 0, min_pos = 0, max_neg = 0, max_pos = 0;
+  bool invalid = false;
+};
+
+// One entry's contribution (rule_singleton_columns.cu:555-654): NaN terms mark
+// the row invalid and contribute nothing.
+inline void cache_term(RowActivityCache& r, double a, double lj, double uj) {
+  const double tmin = a >= 0.0 ? a * lj : a * uj;
+  const double tmax = a >= 0.0 ? a * uj : a * lj;
+  if (std::isnan(tmin) || std::isnan(tmax)) { r.invalid = true; return; }
+  if (std::isinf(tmin)) (tmin < 0.0 ? r.min_neg : r.min_pos)++; else r.fmin += tmin;
+  if (std::isinf(tmax)) (tmax < 0.0 ? r.max_neg : r.max_pos)++; else r.fmax += tmax;
+}
+
+// _kernel_singleton_row_activity_cache / _long_row_activity_cache
+// (rule_singleton_columns.cu:555-754): rows of live length <= 1024 sum in
+// stored order; longer rows give live rank k to thread k mod 256, then a
+// shared-memory halving tree (stride 128 .. 1).
+RowActivityCache singleton_row_cache(const Lp& lp, const Plan& plan, const Stats& s, int row) {
+  RowActivityCache r;
+  if (!plan.keep_row[row]) return r;
+  const Csr& A = lp.A;
+  if (s.row_nnz[row] <= 1024) {
+    for (int p = A.ptr[row]; p < A.ptr[row + 1]; ++p) {
+      const int col = A.idx[p];
+      if (plan.keep_col[col]) cache_term(r, A.val[p], plan.l[col], plan.u[col]);
+    }
+    return r;
+  }
+  std::vector<RowActivityCache> part(256);
+  int rank = 0;
+  for (int p = A.ptr[row]; p < A.ptr[row + 1]; ++p) {
+    const int col = A.idx[p];
+    if (!plan.keep_col[col]) continue;
+    cache_term(part[size_t(rank % 256)], A.val[p], plan.l[col], plan.u[col]);
+    ++rank;
+  }
+  for (int stride = 128; stride > 0; stride >>= 1)
+    for (int t = 0; t < stride; ++t) {
+      RowActivityCache& a = part[size_t(t)];
+      const RowActivityCache& b = part[size_t(t + stride)];
+      a.fmin += b.fmin; a.fmax += b.fmax;
+      a.min_neg += b.min_neg; a.min_pos += b.min_pos; a.max_neg += b.max_neg; a.max_pos += b.max_pos;
+      a.invalid = a.invalid || b.invalid;
+    }
+  return part[0];
+}
+
+// _singleton_column_activity_bounds_from_cache (rule_singleton_columns.cu:756-816).
+bool rest_bounds(const RowActivityCache& r, double a, double lj, double uj, double& rest_min, double& rest_max) {
+  if (r.invalid) return false;
+  const double tmin = a >= 0.0 ? a * lj : a * uj;
+  const double tmax = a >= 0.0 ? a * uj : a * lj;
+  if (std::isnan(tmin) || std::isnan(tmax)) return false;
+  int min_neg = r.min_neg, min_pos = r.min_pos, max_neg = r.max_neg, max_pos = r.max_pos;
+  double vmin = r.fmin, vmax = r.fmax;
+  if (std::isinf(tmin)) (tmin < 0.0 ? min_neg : min_pos)--; else vmin -= tmin;
+  if (std::isinf(tmax)) (tmax < 0.0 ? max_neg : max_pos)--; else vmax -= tmax;
+  if (min_neg < 0 || min_pos < 0 || max_neg < 0 || max_pos < 0 || (min_neg > 0 && min_pos > 0) ||
+      (max_neg > 0 && max_pos > 0))
+    return false;
+  rest_min = min_neg > 0 ? -INFINITY : (min_pos > 0 ? INFINITY : vmin);
+  rest_max = max_neg > 0 ? -INFINITY : (max_pos > 0 ? INFINITY : vmax);
+  return !std::isnan(rest_min) && !std::isnan(rest_max);
+}
+
+// _singleton_column_direct_unbounded (rule_singleton_columns.cu:516-527).
+bool direct_unbounded(double cj, double a, double lhs, double rhs, double lb, double ub, double zt) {
+  return (cj > zt && a > zt && !fin(lhs) && !fin(lb)) || (cj > zt && a < -zt && !fin(rhs) && !fin(lb)) ||
+         (cj < -zt && a < -zt && !fin(lhs) && !fin(ub)) || (cj < -zt && a > zt && !fin(rhs) && !fin(ub));
+}
+
+// _singleton_column_implied_free_from_above / _below (rule_singleton_columns.cu:818-854).
+bool free_from_above(double a, double lhs, double rhs, double ub, double rmin, double rmax, double tol) {
+  if (!fin(ub)) return true;
+  double implied = INFINITY;
+  if (a > 0.0 && fin(rhs)) implied = (rhs - rmin) / a;
+  else if (a < 0.0 && fin(lhs)) implied = (lhs - rmax) / a;
+  return implied <= ub + tol;
+}
+bool free_from_below(double a, double lhs, double rhs, double lb, double rmin, double rmax, double tol) {
+  if (!fin(lb)) return true;
+  double implied = -INFINITY;
+  if (a > 0.0 && fin(lhs)) implied = (lhs - rmax) / a;
+  else if (a < 0.0 && fin(rhs)) implied = (rhs - rmin) / a;
+  return implied >= lb - tol;
+}
+
+// _singleton_column_active_side / _ineq_action (rule_singleton_columns.cu:856-903).
+uint8_t inequality_action(double cj, double a, double lhs, double rhs, bool above, bool below, double zt,
+                          double& side) {
+  if (above && below) {
+    if ((cj > zt && a > 0.0) || (cj < -zt && a < 0.0)) side = lhs;
+    else if ((cj > zt && a < 0.0) || (cj < -zt && a > 0.0)) side = rhs;
+    else side = fin(lhs) ? lhs : rhs;
+    return fin(side) ? kSetRowSide : kNone;
+  }
+  if (((cj < -zt && a > 0.0 && above) || (cj > zt && a < 0.0 && below)) && fin(rhs)) { side = rhs; return kTightenLhs; }
+  if (((cj > zt && a > 0.0 && below) || (cj < -zt && a < 0.0 && above)) && fin(lhs)) { side = lhs; return kTightenRhs; }
+  side = 0.0;
+  return kNone;
+}
+}  // namespace
+
+void rule_singleton_columns(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p) {
+  // apply_rule_singleton_columns (rule_singleton_columns.cu:1562-1827).
+  if (plan.has_infeasible || plan.has_unbounded || !p.enable_singleton_columns) return;
+  const int m = lp.m(), n = lp.n();
+  if (m == 0 || n == 0) return;
+  // Precheck (_kernel_count_singleton_column_support, :1141-1155).
+  bool any = false;
+  for (int j = 0; j < n && !any; ++j)
+    any = plan.keep_col[j] && s.singleton_col[j] && s.scol_row[j] >= 0 && plan.keep_row[size_t(s.scol_row[j])];
+  if (!any) return;
+
+  // 1. Propose (:905-1018): immutable actions, one owner per row
+  //    (EliminateFree first, then the smallest column).
+  std::vector<uint8_t> action(size_t(n), kNone);
+  std::vector<double> side(size_t(n), 0.0);
+  std::vector<int> owner(size_t(m), INT_MAX);
+  std::vector<int8_t> cached(size_t(m), 0);
+  std::vector<RowActivityCache> cache(static_cast<size_t>(m));
+  bool unbounded = false;
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[j] || !s.singleton_col[j]) continue;
+    const int row = s.scol_row[j];
+    if (row < 0 || row >= m || !plan.keep_row[row]) continue;
+    const double a = s.scol_val[j];
+    if (std::fabs(a) <= p.zero_tol) continue;
+    int live = 0;
+    for (int q = lp.A.ptr[row]; q < lp.A.ptr[row + 1] && live <= 1; ++q) live += plan.keep_col[lp.A.idx[q]] ? 1 : 0;
+    if (live <= 1) continue;
+    const double lhs = plan.AL[row], rhs = plan.AU[row], cj = plan.c[j];
+    if (direct_unbounded(cj, a, lhs, rhs, plan.l[j], plan.u[j], p.zero_tol)) { unbounded = true; continue; }
+    if (!cached[row]) { cache[row] = singleton_row_cache(lp, plan, s, row); cached[row] = 1; }
+    double rmin = 0.0, rmax = 0.0;
+    if (!rest_bounds(cache[row], a, plan.l[j], plan.u[j], rmin, rmax)) continue;
+    const double tol = p.bound_tol;
+    uint8_t act;
+    double sd;
+    if (fin(lhs) && fin(rhs) && std::fabs(lhs - rhs) <= tol) {
+      const double x1 = (rhs - rmin) / a, x2 = (rhs - rmax) / a;
+      const double ilb = std::fmin(x1, x2), iub = std::fmax(x1, x2);
+      const bool above = !fin(plan.u[j]) || iub <= plan.u[j] + tol;
+      const bool below = !fin(plan.l[j]) || ilb >= plan.l[j] - tol;
+      if (!(above || below)) continue;
+      act = above && below ? kEliminateFree : (above ? kEliminateFreeAbove : kEliminateFreeBelow);
+      sd = rhs;
+    } else {
+      const bool above = free_from_above(a, lhs, rhs, plan.u[j], rmin, rmax, tol);
+      const bool below = free_from_below(a, lhs, rhs, plan.l[j], rmin, rmax, tol);
+      act = inequality_action(cj, a, lhs, rhs, above, below, p.zero_tol, sd);
+      if (act == kNone) continue;
+    }
+    action[j] = act;
+    side[j] = sd;
+    const int key = act == kEliminateFree ? j - INT_MAX : j;
+    owner[row] = std::min(owner[row], key);
+  }
+  if (unbounded) { plan.has_unbounded = true; return; }
+
+  // 2. Stage (:1021-1073) against the unmodified plan.
+  std::vector<uint8_t> row_delete(size_t(m), 0), col_delete(size_t(n), 0), lo_change(size_t(m), 0),
+      hi_change(size_t(m), 0);
+  std::vector<double> AL_new(plan.AL), AU_new(plan.AU), contrib(size_t(n), 0.0);
+  bool any_elim = false, any_side = false;
+  for (int row = 0; row < m; ++row) {
+    const int j = owner[row] < 0 ? owner[row] + INT_MAX : owner[row];
+    if (j < 0 || j >= n) { owner[row] = INT_MAX; continue; }
+    owner[row] = j;
+    const uint8_t act = action[j];
+    const double lhs = plan.AL[row], rhs = plan.AU[row];
+    if (act == kEliminateFree || act == kEliminateFreeAbove || act == kEliminateFreeBelow) {
+      const double a = s.scol_val[j];
+      contrib[j] = plan.c[j] * rhs / a;
+      if (act == kEliminateFree) {
+        row_delete[row] = 1;
+      } else {
+        const bool above = act == kEliminateFreeAbove;
+        const double bound = above ? plan.l[j] : plan.u[j];
+        const bool keep_lower = above ? a < 0.0 : a > 0.0;
+        const double shifted = plan.AU[row] - a * bound;
+        if (keep_lower) { AL_new[row] = shifted; AU_new[row] = INFINITY; }
+        else { AL_new[row] = -INFINITY; AU_new[row] = shifted; }
+      }
+      col_delete[j] = 1;
+      any_elim = true;
+      continue;
+    }
+    if (act == kSetRowSide) {
+      const double sd = side[j];
+      if (!fin(lhs) || std::fabs(lhs - sd) > p.bound_tol) lo_change[row] = 1;
+      if (!fin(rhs) || std::fabs(rhs - sd) > p.bound_tol) hi_change[row] = 1;
+      AL_new[row] = sd;
+      AU_new[row] = sd;
+    } else if (act == kTightenLhs) {
+      lo_change[row] = 1;
+      AL_new[row] = rhs;
+    } else if (act == kTightenRhs) {
+      hi_change[row] = 1;
+      AU_new[row] = lhs;
+    }
+    any_side = true;
+  }
+  if (!any_elim && !any_side) return;
+
+  // Objective update of the surviving columns (:1075-1139): per column, in
+  // stored (row) order of its AT entries.
+  std::vector<double> c_new(plan.c);
+  if (any_elim) {
+    for (int col = 0; col < n; ++col) {
+      if (!plan.keep_col[col] || col_delete[col]) continue;
+      double updated = plan.c[col];
+      for (int q = lp.AT.ptr[col]; q < lp.AT.ptr[col + 1]; ++q) {
+        const int o = owner[size_t(lp.AT.idx[q])];
+        if (o < 0 || o >= n || !col_delete[o]) continue;
+        updated += -(plan.c[o] * lp.AT.val[q] / s.scol_val[o]);
+      }
+      c_new[col] = updated;
+    }
+  }
+  // Tape before commit (:1191-1560, :459-508).
+  if (any_elim && p.record_postsolve_tape) {
+    for (int row = 0; row < m; ++row) {
+      const int col = owner[row];
+      if (col < 0 || col >= n || !col_delete[col]) continue;
+      double pivot = 0.0;
+      std::vector<int> sidx;
+      std::vector<double> sval;
+      for (int q = lp.A.ptr[row]; q < lp.A.ptr[row + 1]; ++q) {
+        const int rc = lp.A.idx[q];
+        if (rc == col) pivot = lp.A.val[q];
+        else if (plan.keep_col[rc]) { sidx.push_back(rc); sval.push_back(lp.A.val[q]); }
+      }
+      if (std::fabs(pivot) <= p.zero_tol) continue;
+      std::vector<int> idx{col, row, int(sidx.size())};
+      idx.insert(idx.end(), sidx.begin(), sidx.end());
+      std::vector<double> val{pivot, side[col], plan.l[col], plan.u[col], plan.c[col], row_delete[row] ? 1.0 : 0.0};
+      val.insert(val.end(), sval.begin(), sval.end());
+      plan.tape.add(SingletonColumnSubstitution, idx, val);
+    }
+  }
+  if (any_side && p.record_postsolve_tape)
+    for (int row = 0; row < m; ++row)
+      if (lo_change[row] || hi_change[row]) plan.tape.add(RowDualShift, {row}, {0.0});
+  // Commit (:1157-1189).
+  for (int row = 0; row < m; ++row) {
+    if (row_delete[row]) plan.keep_row[row] = 0;
+    if (owner[row] >= 0 && owner[row] < n) { plan.AL[row] = AL_new[row]; plan.AU[row] = AU_new[row]; }
+  }
+  for (int j = 0; j < n; ++j) {
+    if (col_delete[j]) plan.keep_col[j] = 0;
+    if (any_elim && plan.keep_col[j]) plan.c[j] = c_new[j];
+  }
+  plan.obj_delta += domain_objective(contrib, plan);
+  plan.has_row_action = true;
+  plan.has_col_action = plan.has_col_action || any_elim;
+  plan.has_change = true;
+}
+
 namespace {
 inline void term_interval(double a, double lj, double uj, double& tmin, double& tmax) {
   if (a >= 0.0) { tmin = a * lj; tmax = a * uj; } else { tmin = a * uj; tmax = a * lj; }

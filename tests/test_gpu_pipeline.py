@@ -15,6 +15,8 @@ CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "sin
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
+SINGLETON = CLEANUP + ["singleton_columns"]
+FULL = PARALLEL + ["singleton_columns"]
 
 
 def bits(a):
@@ -33,8 +35,8 @@ def assert_same(gpu, orc):
     assert s.obj_constant_delta == o.obj_constant_delta
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
-@pytest.mark.parametrize("workload", ["random:400x1000", "small"])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
+@pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:400x1000", "slack:2000x5000"])
 def test_presolve_bitwise_vs_oracle(rules, workload):
     lp = lpgen.workload(workload, seed=0)
     params = params_with_rules(rules, enable_folding=0)
@@ -49,11 +51,12 @@ def test_presolve_bitwise_vs_oracle(rules, workload):
         device.free_summary(s)  # idempotent
 
 
-@pytest.mark.parametrize("seed", [0, 3])
-def test_postprocess_vs_oracle_and_highs(seed):
+@pytest.mark.parametrize("rules", [PROPAGATION, FULL])
+@pytest.mark.parametrize("workload,seed", [("random:400x1000", 0), ("random:400x1000", 3), ("slack:400x1000", 0)])
+def test_postprocess_vs_oracle_and_highs(rules, workload, seed):
     import torch
-    lp = lpgen.random_lp(400, 1000, seed=seed)
-    params = params_with_rules(PROPAGATION, enable_folding=0)
+    lp = lpgen.workload(workload, seed=seed)
+    params = params_with_rules(rules, enable_folding=0)
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
     try:

@@ -13,6 +13,8 @@ CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "sin
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
+SINGLETON = CLEANUP + ["singleton_columns"]
+FULL = PARALLEL + ["singleton_columns"]
 
 
 def test_dyadic_activity_matches_reference_fixture():
@@ -69,10 +71,11 @@ def test_det_sum_tree():
     assert pyoracle.det_sum(v) == total
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
-@pytest.mark.parametrize("seed", [0, 1])
-def test_postsolved_objective_matches_unreduced(rules, seed):
-    lp = lpgen.random_lp(400, 1000, seed=seed)
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
+@pytest.mark.parametrize("workload,seed", [("random:400x1000", 0), ("random:400x1000", 1), ("slack:400x1000", 0),
+                                           ("slack:400x1000", 1)])
+def test_postsolved_objective_matches_unreduced(rules, workload, seed):
+    lp = lpgen.workload(workload, seed=seed)
     res0, _, _ = lpsolve.solve(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values, lp.c, lp.AL, lp.AU, lp.l, lp.u)
     assert res0.status == 0
     r = pyoracle.presolve(lp, params_with_rules(rules))

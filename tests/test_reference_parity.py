@@ -27,6 +27,8 @@ CLEANUP = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "sin
 BUILT = CLEANUP + ["bound_strengthening"]
 PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
+SINGLETON = CLEANUP + ["singleton_columns"]
+FULL = PARALLEL + ["singleton_columns"]
 
 
 def run_reference(lp, rules, extra=None):
@@ -65,8 +67,8 @@ def close(a, b, rel=1e-12):
 
 
 @pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL])
-@pytest.mark.parametrize("workload", ["random:400x1000", "small"])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
+@pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:400x1000", "slack:2000x5000"])
 def test_structure_matches_reference(rules, workload):
     lp = lpgen.workload(workload, seed=0)
     ref = run_reference(lp, rules)
