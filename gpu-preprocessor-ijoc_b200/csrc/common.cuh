@@ -78,6 +78,19 @@ inline int grid_stride_blocks(int64_t n, int threads = kThreads, int per_sm = 8)
   return int(want < 1 ? 0 : (want < cap ? want : cap));
 }
 
+// Warp-aggregated append: every lane of the warp must call it; lanes with
+// `take` get consecutive slots (in lane order) from *counter, others get -1.
+__device__ __forceinline__ int warp_append(int32_t* counter, bool take) {
+  const unsigned mask = __ballot_sync(0xffffffffu, take);
+  if (!mask) return -1;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return take ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
+}
+
 // ---------------------------------------------------------------------------
 // Engine context: one stream (blocking w.r.t. the legacy default stream so
 // caller work on stream 0 is ordered before ours), a stream-ordered memory

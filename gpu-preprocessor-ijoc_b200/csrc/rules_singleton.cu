@@ -42,17 +42,6 @@ constexpr int kClaimed = INT_MAX - 1;   // row holds a candidate, no owner yet
 enum { kStUnbounded = 0, kStCand = 1, kStRows = 2, kStLong = 3, kStWin = 4, kStElim = 5, kStSide = 6,
        kStTouched = 7, kStWords = 8 };
 
-__device__ __forceinline__ int warp_append(int32_t* counter, bool take) {
-  const unsigned mask = __ballot_sync(0xffffffffu, take);
-  if (!mask) return -1;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(counter, __popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return take ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
-}
-
 __device__ __forceinline__ bool direct_unbounded(double cj, double a, double lhs, double rhs, double lb, double ub,
                                                  double zt) {
   // _singleton_column_direct_unbounded (rule_singleton_columns.cu:516-527).

@@ -73,7 +73,8 @@ int main(int argc, char** argv) {
       if (s == "--postsolve") { xs = argv[++a]; ys = argv[++a]; zs = argv[++a]; continue; }
       const auto eq = s.find('=');
       const std::string k = s.substr(0, eq);
-      const int v = std::stoi(s.substr(eq + 1));
+      const double dv = std::stod(s.substr(eq + 1));
+      const int v = static_cast<int>(dv);
 #define FLAG(name) else if (k == #name) p.name = v != 0
       if (false) {}
       FLAG(enable_folding); FLAG(enable_presolve);
@@ -83,6 +84,10 @@ int main(int argc, char** argv) {
       FLAG(enable_doubleton_equations); FLAG(enable_dual_fix); FLAG(enable_parallel_columns);
       FLAG(enable_structure_specific_rules); FLAG(enable_startup);
       else if (k == "max_iters") p.max_iters = v;
+      else if (k == "doubleton_equations_scan") p.doubleton_equations_scan = v != 0;
+      else if (k == "doubleton_equations_max_fill_in_proxy") p.doubleton_equations_max_fill_in_proxy = v;
+      else if (k == "doubleton_equations_min_selected_per_batch") p.doubleton_equations_min_selected_per_batch = v;
+      else if (k == "doubleton_equations_min_selected_ratio") p.doubleton_equations_min_selected_ratio = dv;
       else throw std::invalid_argument("unknown parameter " + k);
 #undef FLAG
     }

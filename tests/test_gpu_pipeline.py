@@ -17,6 +17,8 @@ PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 SINGLETON = CLEANUP + ["singleton_columns"]
 FULL = PARALLEL + ["singleton_columns"]
+ALL = FULL + ["doubleton_equations"]
+SMALL_BATCH = dict(doubleton_equations_min_selected_per_batch=1, doubleton_equations_min_selected_ratio=0.0)
 
 
 def bits(a):
@@ -51,12 +53,58 @@ def test_presolve_bitwise_vs_oracle(rules, workload):
         device.free_summary(s)  # idempotent
 
 
-@pytest.mark.parametrize("rules", [PROPAGATION, FULL])
+@pytest.mark.parametrize("workload,extra", [("random:400x1000", SMALL_BATCH), ("slack:2000x5000", SMALL_BATCH),
+                                            ("random:20000x50000", {})])
+def test_doubleton_bitwise_vs_oracle(workload, extra):
+    lp = lpgen.workload(workload, seed=0)
+    params = params_with_rules(ALL, enable_folding=0, **extra)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params)
+    try:
+        gpu = device.Result(s)
+        orc = pyoracle.presolve(lp, params)
+        assert_same(gpu, orc)
+        assert 13 in gpu.tape_types.tolist()   # the batch ran
+    finally:
+        device.free_summary(s)
+
+
+@pytest.mark.parametrize("workload,extra", [("slack:2000x5000", SMALL_BATCH), ("random:20000x50000", {})])
+def test_parallel_replay_matches_serial_oracle(workload, extra):
+    """Tapes of >= 1024 records replay as independent record groups on the
+    GPU; the result must equal the oracle's one-record-at-a-time replay bit
+    for bit, for any reduced point (here a seeded one inside the bounds)."""
+    import torch
+    lp = lpgen.workload(workload, seed=0)
+    params = params_with_rules(ALL, enable_folding=0, **extra)
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, params)
+    try:
+        gpu = device.Result(s)
+        assert len(gpu.tape_types) >= 1024
+        rng = np.random.default_rng(1)
+        lo = np.where(np.isfinite(gpu.l), gpu.l, -10.0)
+        hi = np.where(np.isfinite(gpu.u), gpu.u, lo + 20.0)
+        xr = lo + rng.random(s.reduced_cols) * (hi - lo)
+        yr = rng.standard_normal(s.reduced_rows)
+        zr = rng.standard_normal(s.reduced_cols)
+        x, y, z = device.postprocess(torch.from_numpy(xr).cuda(), torch.from_numpy(yr).cuda(),
+                                     torch.from_numpy(zr).cuda(), s, dlp)
+        orc = pyoracle.presolve(lp, params)
+        xo, yo, zo = orc.postsolve(xr, yr, zr)
+        assert np.array_equal(bits(x), bits(xo))
+        assert np.array_equal(bits(y), bits(yo))
+        assert np.array_equal(bits(z), bits(zo))
+    finally:
+        device.free_summary(s)
+
+
+@pytest.mark.parametrize("rules", [PROPAGATION, FULL, ALL])
 @pytest.mark.parametrize("workload,seed", [("random:400x1000", 0), ("random:400x1000", 3), ("slack:400x1000", 0)])
 def test_postprocess_vs_oracle_and_highs(rules, workload, seed):
     import torch
     lp = lpgen.workload(workload, seed=seed)
-    params = params_with_rules(rules, enable_folding=0)
+    params = params_with_rules(rules, enable_folding=0, **SMALL_BATCH)
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
     try:

@@ -15,6 +15,7 @@ PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 SINGLETON = CLEANUP + ["singleton_columns"]
 FULL = PARALLEL + ["singleton_columns"]
+ALL = FULL + ["doubleton_equations"]
 
 
 def test_dyadic_activity_matches_reference_fixture():
@@ -71,14 +72,16 @@ def test_det_sum_tree():
     assert pyoracle.det_sum(v) == total
 
 
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL, ALL])
 @pytest.mark.parametrize("workload,seed", [("random:400x1000", 0), ("random:400x1000", 1), ("slack:400x1000", 0),
                                            ("slack:400x1000", 1)])
 def test_postsolved_objective_matches_unreduced(rules, workload, seed):
     lp = lpgen.workload(workload, seed=seed)
     res0, _, _ = lpsolve.solve(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values, lp.c, lp.AL, lp.AU, lp.l, lp.u)
     assert res0.status == 0
-    r = pyoracle.presolve(lp, params_with_rules(rules))
+    # Small doubleton batches allowed so the rule runs at this size.
+    r = pyoracle.presolve(lp, params_with_rules(rules, doubleton_equations_min_selected_per_batch=1,
+                                                doubleton_equations_min_selected_ratio=0.0))
     s = r.summary
     assert not s.has_infeasible and not s.has_unbounded
     rr, yr, zr = lpsolve.solve(s.reduced_rows, s.reduced_cols, r.A_ptr, r.A_idx, r.A_val, r.c, r.AL, r.AU, r.l, r.u)

@@ -29,6 +29,8 @@ PROPAGATION = BUILT + ["infeasible_and_redundant_rows", "dual_fix"]
 PARALLEL = PROPAGATION + ["parallel_rows", "parallel_columns"]
 SINGLETON = CLEANUP + ["singleton_columns"]
 FULL = PARALLEL + ["singleton_columns"]
+ALL = FULL + ["doubleton_equations"]
+SMALL_BATCH = dict(doubleton_equations_min_selected_per_batch=1, doubleton_equations_min_selected_ratio=0.0)
 
 
 def run_reference(lp, rules, extra=None):
@@ -66,13 +68,13 @@ def close(a, b, rel=1e-12):
     return bool(np.all(ok))
 
 
-@pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
-@pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:400x1000", "slack:2000x5000"])
-def test_structure_matches_reference(rules, workload):
-    lp = lpgen.workload(workload, seed=0)
-    ref = run_reference(lp, rules)
-    params = params_with_rules(rules, enable_folding=0)
+needs_reference = pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
+
+
+def check_against_reference(lp, rules, extra=None):
+    extra = extra or {}
+    ref = run_reference(lp, rules, [f"{k}={v}" for k, v in extra.items()])
+    params = params_with_rules(rules, enable_folding=0, **extra)
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
     try:
@@ -93,5 +95,21 @@ def test_structure_matches_reference(rules, workload):
         # The oracle agrees with both.
         orc = pyoracle.presolve(lp, params)
         assert np.array_equal(orc.row_map, ref["row_map"]) and np.array_equal(orc.col_map, ref["col_map"])
+        return got
     finally:
         device.free_summary(s)
+
+
+@needs_reference
+@pytest.mark.parametrize("rules", [CLEANUP, BUILT, PROPAGATION, PARALLEL, SINGLETON, FULL])
+@pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:400x1000", "slack:2000x5000"])
+def test_structure_matches_reference(rules, workload):
+    check_against_reference(lpgen.workload(workload, seed=0), rules)
+
+
+@needs_reference
+@pytest.mark.parametrize("workload,extra", [("random:400x1000", SMALL_BATCH), ("slack:2000x5000", SMALL_BATCH),
+                                            ("random:20000x50000", {})])
+def test_doubleton_structure_matches_reference(workload, extra):
+    got = check_against_reference(lpgen.workload(workload, seed=0), ALL, extra)
+    assert 13 in got.tape_types.tolist()   # the batch ran
