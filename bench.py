@@ -35,7 +35,7 @@ WORKLOAD_DESC = "random LP m=2,000,000 n=5,000,000 + 2,000 hub rows (500-5000 nn
 METRIC = "presolve ms, HBM GB/s @25M nnz (presolve+postsolve ms per LP)"
 RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singleton_rows",
          "singleton_columns", "bound_strengthening", "infeasible_and_redundant_rows", "dual_fix",
-         "parallel_rows", "parallel_columns"]
+         "parallel_rows", "parallel_columns", "doubleton_equations"]
 
 
 def peaks():
@@ -136,6 +136,9 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) loop")
+    ap.add_argument("--no-kernel-table", action="store_true",
+                    help="skip the extra pass that times every kernel with CUDA events")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":
@@ -179,50 +182,64 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # Device-resident timed region (kernels timed per launch by CUDA events).
-    clocks = Clocks(local)
-    lib.gpp_kernel_launches(1)
-    lib.gpp_profile_enable(1)
-    barrier()
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pre_ms = []
+    # Device-resident timed region.
     out = (torch.empty(lp.n, dtype=torch.float64, device="cuda"), torch.empty(lp.m, dtype=torch.float64, device="cuda"),
            torch.empty(lp.n, dtype=torch.float64, device="cuda"))
+
+    def device_steps(k):
+        pre = []
+        for _ in range(k):
+            s = device.preprocess(dlp, params)
+            pre.append(1e3 * s.elapsed_seconds)
+            device.postsolve_device(*red, s, dlp, out)
+            device.free_summary(s)
+        return pre
+
+    clocks = Clocks(local)
+    lib.gpp_kernel_launches(1)
+    barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    for _ in range(args.steps):
-        s = device.preprocess(dlp, params)
-        pre_ms.append(1e3 * s.elapsed_seconds)
-        device.postsolve_device(*red, s, dlp, out)
-        device.free_summary(s)
+    pre_ms = device_steps(args.steps)
     t1.record(stream)
     barrier()
     clk = clocks.stop()
     step_ms = t0.elapsed_time(t1) / args.steps
     launches = int(lib.gpp_kernel_launches(0)) // args.steps
-    prof = capi.profile_read()
-    lib.gpp_profile_enable(0)
+    # Per-kernel table for the roofline: the same steps again with every
+    # launch bracketed by CUDA events (kept out of the timed region above).
+    prof = []
+    if not args.no_kernel_table:
+        lib.gpp_profile_enable(1)
+        barrier()
+        device_steps(args.steps)
+        barrier()
+        prof = capi.profile_read()
+        lib.gpp_profile_enable(0)
 
     # End to end through the C ABI from pinned host memory.
     host = {k: v.cpu().pin_memory() for k, v in dlp.t.items()}
     h2d = sum(v.numel() * v.element_size() for v in host.values())
     d2h = 8 * (lp.n + lp.m + lp.n)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        for k, v in host.items():
-            dlp.t[k].copy_(v, non_blocking=True)
-        s = device.preprocess(dlp, params)
-        device.postprocess(*red, s, dlp)
-        device.free_summary(s)
-    e1.record(stream)
-    barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
+    e2e_ms = None
+    if not args.no_e2e:
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            for k, v in host.items():
+                dlp.t[k].copy_(v, non_blocking=True)
+            s = device.preprocess(dlp, params)
+            device.postprocess(*red, s, dlp)
+            device.free_summary(s)
+        e1.record(stream)
+        barrier()
+        e2e_ms = e0.elapsed_time(e1) / args.steps
 
     if world > 1:
-        t = torch.tensor([step_ms, e2e_ms], device="cuda")
+        t = torch.tensor([step_ms, e2e_ms or 0.0], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, e2e_ms = float(t[0]), float(t[1])
+        step_ms, e2e_ms = float(t[0]), (float(t[1]) if e2e_ms is not None else None)
 
     peak, peak_kind = peaks()
     top = max(prof, key=lambda r: r[2]) if prof else None
@@ -263,7 +280,8 @@ def main():
                        "l2": "inputs (~1 GB) larger than L2; no flush",
                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "gpu_launches": launches,
-            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": None if e2e_ms is None else {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
+                                                "d2h_bytes_per_step": d2h},
             "roofline": roofline,
             "kernels": [{"name": n, "launches_per_step": l // args.steps, "ms_per_step": round(m / args.steps, 3)}
                         for n, l, m, b in kernels],

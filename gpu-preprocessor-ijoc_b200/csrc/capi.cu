@@ -80,6 +80,14 @@ void fill_summary(gpp_summary* s, gpp_record* rec, double preprocessing_seconds)
   s->elapsed_seconds = o.elapsed_seconds;
   s->preprocessing_seconds = preprocessing_seconds;
   s->obj_constant_delta = o.obj_constant_delta;
+  // FoldingPipelineSummary (folding_structs.hpp:94-109): the original sizes
+  // are the caller's model, the folded sizes what presolve ran on.
+  if (rec->folding.applied) {
+    s->original_rows = rec->folding.original_rows;
+    s->original_cols = rec->folding.original_cols;
+  }
+  s->folded_rows = rec->folding.applied ? rec->folding.folded_rows : s->original_rows;
+  s->folded_cols = rec->folding.applied ? rec->folding.folded_cols : s->original_cols;
   const gpp::WorkingLp& r = o.reduced;
   s->reduced_lp = gpp_lp{{r.A.rows, r.A.cols, r.A.nnz, r.A.ptr, r.A.idx, r.A.val},
                          {r.AT.rows, r.AT.cols, r.AT.nnz, r.AT.ptr, r.AT.idx, r.AT.val},
@@ -143,6 +151,35 @@ void gpp_default_params(gpp_params* p) {
   p->parallel_columns_scale_guard_max_group_size = 4;
   p->parallel_columns_scale_guard_min_groups = 128;
   p->enable_structure_specific_rules = 1;
+  p->enable_two_row_variable_elimination = 1;
+  p->two_row_variable_elimination_max_row_nnz = 8;
+  p->two_row_variable_elimination_safety_tol = 1.0e-8;
+  p->two_row_variable_elimination_min_candidates = 128;
+  p->two_row_variable_elimination_min_candidate_ratio = 0.01;
+  p->enable_zero_cost_product_variables = 1;
+  p->zero_cost_product_variables_min_candidates = 128;
+  p->zero_cost_product_variables_min_candidate_ratio = 0.01;
+  p->enable_piecewise_linear_reformulation_variable_pair = 1;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_probe_pairs = 256;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_min_pairs = 4096;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_min_potential_gain = 0.20;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_min_actual_gain = 0.20;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_max_tail_cols = 8;
+  p->piecewise_linear_reformulation_variable_pair_epigraph_max_quotient_terms_per_row = 5;
+  p->piecewise_linear_reformulation_variable_pair_shifted_antipodal_probe_pairs = 256;
+  p->piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_pairs = 4096;
+  p->piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_potential_gain = 0.20;
+  p->piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_actual_gain = 0.20;
+  p->piecewise_linear_reformulation_variable_pair_shifted_antipodal_max_quotient_terms_per_row = 6;
+  p->enable_column_domination = 1;
+  p->column_domination_probe_rows = 64;
+  p->column_domination_probe_cols = 256;
+  p->column_domination_probe_nnz = 256;
+  p->column_domination_min_fixed_cols = 4096;
+  p->column_domination_min_candidate_ratio = 0.20;
+  p->enable_piecewise_linear_reformulation_absolute_value = 1;
+  p->piecewise_linear_reformulation_absolute_value_residual_bound_mode = 0;
+  p->piecewise_linear_reformulation_absolute_value_residual_bound_as_free_min = 1.0e8;
   p->enable_redundant_variable_bounds = 0;
   p->enable_startup = 1;
   p->bound_strengthening_bound_only_nnz_round_budget = 8000000;
@@ -271,6 +308,32 @@ int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t* indice
     if (indices) *indices = r.indices;
     if (values) *values = r.values;
     if (fixed) *fixed = f;
+  });
+}
+
+int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32_t* col_color, double* row_scale,
+                           double* col_scale) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::FoldingResult& f = summary->record->folding;
+    if (!f.applied) return;
+    auto s = gpp::ctx().stream;
+    const size_t m = size_t(f.original_rows), n = size_t(f.original_cols);
+    if (row_color && m) check(cudaMemcpyAsync(row_color, f.row_color.p, 4 * m, cudaMemcpyDeviceToHost, s), "fold map");
+    if (col_color && n) check(cudaMemcpyAsync(col_color, f.col_color.p, 4 * n, cudaMemcpyDeviceToHost, s), "fold map");
+    if (row_scale && m) check(cudaMemcpyAsync(row_scale, f.row_scale.p, 8 * m, cudaMemcpyDeviceToHost, s), "fold map");
+    if (col_scale && n) check(cudaMemcpyAsync(col_scale, f.col_scale.p, 8 * n, cudaMemcpyDeviceToHost, s), "fold map");
+    gpp::ctx().sync("export folding map");
+  });
+}
+
+int gpp_unfold_solution(const gpp_summary* summary, const double* x_folded, const double* y_folded,
+                        const double* z_folded, double* x_out, double* y_out, double* z_out) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::FoldingResult& f = summary->record->folding;
+    if (!f.applied) throw std::invalid_argument("folding did not apply to this model");
+    gpp::unfold_to_host(f, x_folded, y_folded, z_folded, x_out, y_out, z_out);
   });
 }
 

@@ -9,12 +9,15 @@
 // chronological order by one thread per segment walk (the reference's serial
 // interpreter), and the closing projection runs one thread per column.
 #include "presolve.hpp"
+#include "sort.hpp"
 
 namespace gpp {
 
 namespace {
 
 constexpr double kTol = 1e-7;
+// Tapes shorter than this replay on one thread (the grouping costs more).
+constexpr int64_t kParallelMinRecords = 1024;
 enum : int {
   kFixedVariable = 0, kInfiniteBoundDualFix = 1, kSingletonColumnSubstitution = 2, kParallelColumn = 3,
   kParallelRow = 4, kDeletedRow = 5, kRowDualShift = 10, kRowImpliedBoundChange = 12, kDoubletonEquation = 13
@@ -332,6 +335,258 @@ __global__ void project_duals(int n, const uint8_t* __restrict__ prot, Model M, 
 
 SegView view(const PostsolveSegment& s) { return {s.types.p, s.is.p, s.vs.p, s.idx.p, s.val.p, s.count}; }
 
+// ---- component-parallel replay ----------------------------------------------
+//
+// Replaying the tape in reverse chronological order is equivalent to
+// replaying, in that order, each group of records that share a resource one
+// of them writes, with the groups independent of one another.  Resources are
+// the columns (x, z and the retrieval flag together) and the rows (y) of the
+// original model; per pass only what that pass reads or writes counts (x is
+// read-only in the dual pass, y and z untouched in the primal pass).  Records
+// that do nothing in a pass (variable bound changes, and the dual-only records
+// in the primal pass) drop out.  Groups come from a lock-free union-find over
+// the records; each group is replayed by one thread, newest record first.
+
+struct TapeView {
+  const SegView* segs;       // device array
+  const int64_t* starts;     // global index of each segment's first record, count+1 entries
+  int nseg;
+  int64_t total;
+  __device__ void at(int64_t g, int& type, const int32_t*& id, int64_t& ni, const double*& v, int64_t& nv) const {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (starts[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    const SegView& t = segs[lo];
+    const int64_t k = g - starts[lo];
+    type = t.types[k];
+    id = t.idx + t.is[k];
+    ni = t.is[k + 1] - t.is[k];
+    v = t.val + t.vs[k];
+    nv = t.vs[k + 1] - t.vs[k];
+  }
+};
+
+__device__ __forceinline__ bool replays_in(int type, bool dual) {
+  if (type == kFixedVariable || type == kInfiniteBoundDualFix || type == kSingletonColumnSubstitution ||
+      type == kParallelColumn || type == kDoubletonEquation)
+    return true;
+  return dual && (type == kRowDualShift || type == kParallelRow || type == kDeletedRow || type == kRowImpliedBoundChange);
+}
+
+// Calls visit(resource, writes) for every resource the record touches in the
+// pass; columns are 0..n-1, rows n..n+m-1.
+template <class F>
+__device__ void record_resources(int type, const int32_t* id, int64_t ni, int64_t nv, bool dual, int m, int n,
+                                 const Model& M, F visit) {
+  auto col = [&](int j, bool w) { if (j >= 0 && j < n) visit(j, w); };
+  auto row = [&](int i, bool w) { if (i >= 0 && i < m) visit(n + i, w); };
+  if (!dual) {
+    switch (type) {
+      case kFixedVariable: col(id[0], true); break;
+      case kInfiniteBoundDualFix: {
+        col(id[1], true);
+        int64_t ip = 3;
+        for (int r = 0; r < id[2] && ip < ni; ++r) {
+          const int len = id[ip];
+          for (int q = 0; q < len && ip + 1 + q < ni; ++q) col(id[ip + 1 + q], false);
+          ip += len + 1;
+        }
+        break;
+      }
+      case kSingletonColumnSubstitution:
+        col(id[0], true);
+        for (int q = 0; q < id[2] && 3 + q < ni; ++q) col(id[3 + q], false);
+        break;
+      case kParallelColumn: col(id[0], true); col(id[1], true); break;
+      case kDoubletonEquation: col(id[0], true); col(id[1], false); break;
+      default: break;
+    }
+    return;
+  }
+  switch (type) {
+    case kFixedVariable:
+      col(id[0], true);
+      for (int64_t q = 1; q < ni; ++q) row(id[q], false);
+      break;
+    case kInfiniteBoundDualFix: col(id[1], true); break;
+    case kSingletonColumnSubstitution: col(id[0], true); row(id[1], true); break;
+    case kParallelColumn: col(id[0], true); col(id[1], false); break;
+    case kDoubletonEquation:
+      col(id[0], true); col(id[1], true); row(id[2], true);
+      if (ni >= 4 && nv >= 12) {
+        for (int q = 0; q < id[3] && 4 + q < ni; ++q) row(id[4 + q], false);
+      } else if (M.present && id[0] >= 0 && id[0] < n) {
+        for (offset_t q = M.AT_ptr[id[0]]; q < M.AT_ptr[id[0] + 1]; ++q) row(M.AT_idx[q], false);
+      }
+      break;
+    case kRowDualShift: row(id[0], true); break;
+    case kParallelRow: if (ni >= 2) { row(id[0], true); row(id[1], true); } break;
+    case kDeletedRow:
+      if (ni >= 2) {
+        row(id[0], true); col(id[1], true);
+        if (M.present && id[1] >= 0 && id[1] < n)
+          for (offset_t q = M.AT_ptr[id[1]]; q < M.AT_ptr[id[1] + 1]; ++q) row(M.AT_idx[q], false);
+      }
+      break;
+    case kRowImpliedBoundChange:
+      if (ni >= 2) {
+        col(id[0], true); row(id[1], true);
+        if (M.present && id[1] >= 0 && id[1] < m)
+          for (offset_t q = M.A_ptr[id[1]]; q < M.A_ptr[id[1] + 1]; ++q) col(M.A_idx[q], true);
+      }
+      break;
+    default: break;
+  }
+}
+
+__global__ void cp_active(TapeView t, int dual, int32_t* __restrict__ flag) {
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < t.total; g += int64_t(gridDim.x) * blockDim.x) {
+    int type;
+    const int32_t* id;
+    int64_t ni, nv;
+    const double* v;
+    t.at(g, type, id, ni, v, nv);
+    flag[g] = replays_in(type, dual != 0) ? 1 : 0;
+  }
+}
+
+__global__ void cp_list(int64_t total, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                        int64_t* __restrict__ act, int32_t* __restrict__ parent) {
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x)
+    if (flag[g]) { act[pos[g]] = g; parent[pos[g]] = pos[g]; }
+}
+
+// First writer of each resource owns it.
+__global__ void cp_claim(TapeView t, const int64_t* __restrict__ act, int count, int dual, int m, int n, Model M,
+                         int32_t* __restrict__ owner) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    int type;
+    const int32_t* id;
+    int64_t ni, nv;
+    const double* v;
+    t.at(act[q], type, id, ni, v, nv);
+    record_resources(type, id, ni, nv, dual != 0, m, n, M, [&](int res, bool w) {
+      if (w) atomicCAS(owner + res, -1, q);
+    });
+  }
+}
+
+__device__ __forceinline__ int uf_root(int32_t* parent, int a) {
+  for (;;) {
+    const int b = *(volatile int32_t*)(parent + a);
+    if (b == a) return a;
+    a = b;
+  }
+}
+// Link the larger root under the smaller; a failed CAS means the root moved,
+// so retry from the new roots.  Links always point to smaller indices, so no
+// cycle can form and every retry makes progress.
+__device__ void uf_unite(int32_t* parent, int a, int b) {
+  for (;;) {
+    a = uf_root(parent, a);
+    b = uf_root(parent, b);
+    if (a == b) return;
+    const int hi = a > b ? a : b, lo = a > b ? b : a;
+    if (atomicCAS(parent + hi, hi, lo) == hi) return;
+  }
+}
+
+// Every record joins the owner of each resource it touches.
+__global__ void cp_connect(TapeView t, const int64_t* __restrict__ act, int count, int dual, int m, int n, Model M,
+                           const int32_t* __restrict__ owner, int32_t* __restrict__ parent) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    int type;
+    const int32_t* id;
+    int64_t ni, nv;
+    const double* v;
+    t.at(act[q], type, id, ni, v, nv);
+    record_resources(type, id, ni, nv, dual != 0, m, n, M, [&](int res, bool) {
+      const int o = owner[res];
+      if (o >= 0 && o != q) uf_unite(parent, q, o);
+    });
+  }
+}
+
+__global__ void cp_keys(int count, const int32_t* __restrict__ parent, uint64_t* __restrict__ keys,
+                        int32_t* __restrict__ vals) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    int r = q;
+    while (parent[r] != r) r = parent[r];
+    keys[q] = (uint64_t(uint32_t(r)) << 32) | uint32_t(q);
+    vals[q] = q;
+  }
+}
+
+__global__ void cp_heads(int count, const uint64_t* __restrict__ keys, int32_t* __restrict__ head) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+    head[q] = q == 0 || (keys[q] >> 32) != (keys[q - 1] >> 32) ? 1 : 0;
+}
+__global__ void cp_starts(int count, const int32_t* __restrict__ head, const int32_t* __restrict__ hpos,
+                          int32_t* __restrict__ start) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+    if (head[q]) start[hpos[q]] = q;
+}
+
+// One thread per group: its records (sorted ascending) replayed newest first.
+__global__ void cp_replay(TapeView t, const int64_t* __restrict__ act, const uint64_t* __restrict__ keys,
+                          const int32_t* __restrict__ start, int groups, int count, Sol s, Model M, int primal,
+                          int dual) {
+  for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < groups; gi += gridDim.x * blockDim.x) {
+    const int b = start[gi], e = gi + 1 < groups ? start[gi + 1] : count;
+    for (int q = e - 1; q >= b; --q) {
+      int type;
+      const int32_t* id;
+      int64_t ni, nv;
+      const double* v;
+      t.at(act[uint32_t(keys[q] & 0xffffffffu)], type, id, ni, v, nv);
+      replay_record(type, id, ni, v, nv, s, M, primal != 0, dual != 0);
+    }
+  }
+}
+
+void replay_parallel(const std::vector<PostsolveSegment>& segments, int m0, int n0, const Sol& s, const Model& M,
+                     bool dual, cudaStream_t st) {
+  std::vector<SegView> hv;
+  std::vector<int64_t> hs{0};
+  for (const auto& seg : segments) {
+    if (!seg.count) continue;
+    hv.push_back(view(seg));
+    hs.push_back(hs.back() + seg.count);
+  }
+  const int64_t total = hs.back();
+  if (!total) return;
+  DBuf<SegView> segs(hv.size(), st);
+  DBuf<int64_t> starts(hs.size(), st);
+  check(cudaMemcpyAsync(segs.p, hv.data(), sizeof(SegView) * hv.size(), cudaMemcpyHostToDevice, st), "tape views");
+  check(cudaMemcpyAsync(starts.p, hs.data(), sizeof(int64_t) * hs.size(), cudaMemcpyHostToDevice, st), "tape starts");
+  const TapeView t{segs.p, starts.p, int(hv.size()), total};
+  DBuf<int32_t> flag(size_t(total) + 1, st), pos(size_t(total) + 1, st);
+  GPP_LAUNCH(cp_active, grid_stride_blocks(total), kThreads, 0, st, t, int(dual), flag.p);
+  exclusive_scan_i32(flag.p, pos.p, total, st);
+  const int count = read_scalar(pos.p + total);
+  if (!count) return;
+  DBuf<int64_t> act(size_t(count), st);
+  DBuf<int32_t> parent(size_t(count), st), owner(size_t(m0) + size_t(n0), st);
+  GPP_LAUNCH(cp_list, grid_stride_blocks(total), kThreads, 0, st, total, flag.p, pos.p, act.p, parent.p);
+  check(cudaMemsetAsync(owner.p, 0xff, sizeof(int32_t) * (size_t(m0) + size_t(n0)), st), "owners");
+  const int g = grid_stride_blocks(count);
+  GPP_LAUNCH(cp_claim, g, kThreads, 0, st, t, act.p, count, int(dual), m0, n0, M, owner.p);
+  GPP_LAUNCH(cp_connect, g, kThreads, 0, st, t, act.p, count, int(dual), m0, n0, M, owner.p, parent.p);
+  DBuf<uint64_t> keys(size_t(count), st);
+  DBuf<int32_t> vals(size_t(count), st), head(size_t(count) + 1, st), hpos(size_t(count) + 1, st);
+  GPP_LAUNCH(cp_keys, g, kThreads, 0, st, count, parent.p, keys.p, vals.p);
+  radix_sort_pairs(keys.p, vals.p, count, st);
+  GPP_LAUNCH(cp_heads, g, kThreads, 0, st, count, keys.p, head.p);
+  exclusive_scan_i32(head.p, hpos.p, count, st);
+  const int groups = read_scalar(hpos.p + count);
+  DBuf<int32_t> gstart(size_t(groups), st);
+  GPP_LAUNCH(cp_starts, g, kThreads, 0, st, count, head.p, hpos.p, gstart.p);
+  GPP_LAUNCH(cp_replay, grid_stride_blocks(groups, 128), 128, 0, st, t, act.p, keys.p, gstart.p, groups, count, s, M,
+             int(!dual), int(dual));
+}
+
 }  // namespace
 
 void run_postsolve(const PresolveOutput& out, const double* x_red, const double* y_red, const double* z_red,
@@ -356,9 +611,14 @@ void run_postsolve(const PresolveOutput& out, const double* x_red, const double*
               original->AT.nzVal, original->c, original->l, original->u, true};
   }
   const Sol s{x, y, z, got.p};
-  for (int pass = 0; pass < 2; ++pass)
-    for (auto it = r.segments.rbegin(); it != r.segments.rend(); ++it)
-      GPP_LAUNCH(replay_serial, 1, 1, 0, st, view(*it), s, M, pass == 0, pass == 1);
+  if (r.records < kParallelMinRecords) {
+    for (int pass = 0; pass < 2; ++pass)
+      for (auto it = r.segments.rbegin(); it != r.segments.rend(); ++it)
+        GPP_LAUNCH(replay_serial, 1, 1, 0, st, view(*it), s, M, pass == 0, pass == 1);
+  } else {
+    replay_parallel(r.segments, m0, n0, s, M, false, st);
+    replay_parallel(r.segments, m0, n0, s, M, true, st);
+  }
   if (original && y && z && n0) {
     DBuf<uint8_t> prot(size_t(n0), st);
     prot.zero();

@@ -17,6 +17,9 @@
 //   * the matrix is rebuilt with alpha * a_(r,e) merged into (r, k) and
 //     entries |a| <= zero_tol dropped (:1191-1489); row sides shift by
 //     a * beta (and a * value for fixed keep columns).
+// With doubleton_equations_scan = 0 the reference's single-row mode runs
+// instead: the smallest acceptable row alone, its column-stored matrix update
+// and unfiltered row shifts (:273-512, :1814-2126).
 // Where the reference sums with atomicAdd (row shifts, objective deltas),
 // this engine sums in one fixed order: row shifts in stored column order per
 // row, objective deltas in ascending row order of the batch.
@@ -90,7 +93,25 @@ __device__ int fill_in_proxy(const offset_t* tptr, const int32_t* tidx, const do
   return fill;
 }
 
-// Candidates and acceptance (:892-987), one thread per row.
+// _doubleton_equations_fill_in_proxy_device (:216-243): stored entries of AT,
+// masks ignored (the single-row mode's proxy).
+__device__ int fill_in_proxy_stored(const offset_t* tptr, const int32_t* tidx, int keep, int elim) {
+  int fill = -1;
+  offset_t jj = tptr[keep], kk = tptr[elim];
+  const offset_t js = tptr[keep + 1], ks = tptr[elim + 1];
+  if (js <= jj || ks <= kk) return fill;
+  while (jj < js && kk < ks) {
+    const int kr = tidx[jj], er = tidx[kk];
+    if (kr == er) { ++jj; ++kk; }
+    else if (er < kr) { ++kk; ++fill; }
+    else ++jj;
+  }
+  return fill + int(ks - kk);
+}
+
+// Candidates and acceptance (:892-987; single-row mode :273-363), one thread
+// per row.  Live selects the batch mode's masked fill-in proxy.
+template <bool Live>
 __global__ void dt_candidates(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                               const double* __restrict__ val, const uint8_t* __restrict__ keep_row,
                               const uint8_t* __restrict__ keep_col, const int32_t* __restrict__ col_nnz,
@@ -130,10 +151,18 @@ __global__ void dt_candidates(int m, const offset_t* __restrict__ ptr, const int
     const double pr = fabs(kv / ev);
     if (!(pr <= kMaxPivotRatio && pr >= 1.0 / kMaxPivotRatio)) continue;
     if (col_nnz[e] > col_nnz[k] + max_fill + 1) continue;
-    if (fill_in_proxy(tptr, tidx, tval, keep_row, zt, k, e) > max_fill) continue;
+    const int fill = Live ? fill_in_proxy(tptr, tidx, tval, keep_row, zt, k, e) : fill_in_proxy_stored(tptr, tidx, k, e);
+    if (fill > max_fill) continue;
     flag[i] = 1;
     keep_c[i] = k; elim_c[i] = e; keep_v[i] = kv; elim_v[i] = ev;
   }
+}
+
+// The smallest flagged index (flag/pos from an exclusive scan).
+__global__ void dt_scatter_first(int count, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                                 int32_t* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+    if (flag[q] && pos[q] == 0) out[0] = q;
 }
 
 __global__ void dt_scatter(int count, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
@@ -448,16 +477,187 @@ __global__ void dt_rebuild(int m, const offset_t* __restrict__ ptr, const int32_
   }
 }
 
+// Single-row mode apply (:365-450): bounds, cost, masks and the record of
+// the target row; meta = {alpha, beta, objective term}.
+__global__ void dt_single_apply(const int32_t* __restrict__ acc, const int32_t* __restrict__ keep_c,
+                                const int32_t* __restrict__ elim_c, const double* __restrict__ keep_v,
+                                const double* __restrict__ elim_v, double bound_tol, double* __restrict__ l,
+                                double* __restrict__ u, double* __restrict__ c, const double* __restrict__ AU,
+                                uint8_t* __restrict__ keep_row, uint8_t* __restrict__ keep_col,
+                                double* __restrict__ meta, int32_t* __restrict__ rec_idx, double* __restrict__ rec_val,
+                                int32_t* st) {
+  const int row = acc[0], k = keep_c[row], e = elim_c[row];
+  const double kv = keep_v[row], ev = elim_v[row], rhs = AU[row];
+  const double le = l[e], ue = u[e], lk = l[k], uk = u[k], ce = c[e];
+  const double alpha = -kv / ev, beta = rhs / ev;
+  double ml = -INFINITY, mu = INFINITY;
+  if (isfinite(le)) { const double b = (le - beta) / alpha; if (alpha > 0.0) ml = b; else mu = b; }
+  if (isfinite(ue)) { const double b = (ue - beta) / alpha; if (alpha > 0.0) mu = b; else ml = b; }
+  if (ml > mu) { const double tmp = ml; ml = mu; mu = tmp; }
+  const double nl = isfinite(ml) ? fmax(lk, ml) : lk;
+  const double nu = isfinite(mu) ? fmin(uk, mu) : uk;
+  if (nl > nu + bound_tol) { st[kStInfeasible] = 1; return; }
+  l[k] = nl;
+  u[k] = nu;
+  c[k] = c[k] + ce * alpha;
+  keep_row[row] = 0;
+  keep_col[e] = 0;
+  meta[0] = alpha;
+  meta[1] = beta;
+  meta[2] = ce * beta;
+  rec_idx[0] = e; rec_idx[1] = k; rec_idx[2] = row; rec_idx[3] = 0;
+  rec_val[0] = ev; rec_val[1] = kv; rec_val[2] = rhs; rec_val[3] = le; rec_val[4] = ue; rec_val[5] = lk;
+  rec_val[6] = uk; rec_val[7] = nl; rec_val[8] = nu; rec_val[9] = ce; rec_val[10] = 0.0; rec_val[11] = 0.0;
+  st[kStAny] = 1;
+}
+
+// Every row with an entry in the eliminated column shifts by a * beta (the
+// first stored entry of that row, as the reference's search does).
+__global__ void dt_single_shift(const int32_t* __restrict__ acc, const int32_t* __restrict__ elim_c,
+                                const offset_t* __restrict__ tptr, const int32_t* __restrict__ tidx,
+                                const double* __restrict__ tval, const double* __restrict__ meta,
+                                const int32_t* __restrict__ st, double* __restrict__ AL, double* __restrict__ AU) {
+  if (!st[kStAny]) return;
+  const int e = elim_c[acc[0]];
+  const offset_t b = tptr[e], end = tptr[e + 1];
+  for (offset_t q = b + blockIdx.x * blockDim.x + threadIdx.x; q < end; q += offset_t(gridDim.x) * blockDim.x) {
+    const int r = tidx[q];
+    bool first = true;
+    for (offset_t q2 = b; q2 < q && first; ++q2) first = tidx[q2] != r;
+    if (!first) continue;
+    const double shift = tval[q] * meta[1];
+    AL[r] -= shift;
+    AU[r] -= shift;
+  }
+}
+
+// Single-row mode matrix (:452-500, :1814-1946): stored entries kept, the
+// keep column of each row becomes a_k + alpha * a_e (inserted in column order
+// when absent, dropped when |.| <= zero_tol); the target row is copied.
+template <bool Write>
+__global__ void dt_single_rows(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                               const double* __restrict__ val, const int32_t* __restrict__ acc,
+                               const int32_t* __restrict__ keep_c, const int32_t* __restrict__ elim_c,
+                               const double* __restrict__ meta, double zt, int32_t* __restrict__ cnt,
+                               const offset_t* __restrict__ optr, int32_t* __restrict__ oidx,
+                               double* __restrict__ oval) {
+  const int target = acc[0], e = elim_c[target], k = keep_c[target];
+  const double alpha = meta[0];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const offset_t first = ptr[r], last = ptr[r + 1];
+    offset_t w = Write ? optr[r] : 0;
+    if (r == target) {
+      for (offset_t q = first; q < last; ++q) {
+        if (Write) { oidx[w] = idx[q]; oval[w] = val[q]; }
+        ++w;
+      }
+    } else if (first < last) {
+      bool ep = false, kp = false;
+      double are = 0.0, old = 0.0;
+      for (offset_t q = first; q < last; ++q) {
+        if (idx[q] == e) { ep = true; are = val[q]; } else if (idx[q] == k) { kp = true; old = val[q]; }
+      }
+      const double nk = old + alpha * are;
+      const bool insert = ep && !kp && fabs(nk) > zt;
+      bool inserted = !insert;
+      for (offset_t q = first; q < last; ++q) {
+        const int col = idx[q];
+        if (insert && !inserted && col > k) {
+          if (Write) { oidx[w] = k; oval[w] = nk; }
+          ++w;
+          inserted = true;
+        }
+        if (col == k) {
+          if (fabs(nk) > zt) {
+            if (Write) { oidx[w] = k; oval[w] = nk; }
+            ++w;
+          }
+        } else {
+          if (Write) { oidx[w] = col; oval[w] = val[q]; }
+          ++w;
+        }
+      }
+      if (insert && !inserted) {
+        if (Write) { oidx[w] = k; oval[w] = nk; }
+        ++w;
+      }
+    }
+    if (!Write) cnt[r] = int32_t(w);
+  }
+}
+
 int warp_grid(int64_t items) {
   return int(std::max<int64_t>(1, std::min<int64_t>((items + 7) / 8, int64_t(kNumSMs) * 16)));
+}
+
+// Single-row mode (doubleton_equations_scan = 0; rule_doubleton_equations.cu:
+// 1948-2126): the smallest acceptable row (over the stored AT, unsorted as
+// given) is substituted alone.
+void doubleton_single_row(Plan& plan, const WorkingLp& lp, const gpp_params& p) {
+  const int m = lp.m(), n = lp.n();
+  if (m == 0 || n == 0) return;
+  auto s = ctx().stream;
+  const double zt = p.zero_tol, ratio_tol = std::fmax(1.0e-9, p.bound_tol);
+  DBuf<int32_t> col_nnz(size_t(n), s), flag(size_t(m) + 1, s), pos(size_t(m) + 1, s), keep_c(size_t(m), s),
+      elim_c(size_t(m), s);
+  DBuf<double> keep_v(size_t(m), s), elim_v(size_t(m), s);
+  GPP_LAUNCH(dt_col_nnz, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val, plan.keep_row.p,
+             plan.keep_col.p, zt, col_nnz.p);
+  GPP_LAUNCH(dt_candidates<false>, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val,
+             plan.keep_row.p, plan.keep_col.p, col_nnz.p, plan.AL.p, plan.AU.p, zt, p.bound_tol, ratio_tol,
+             p.doubleton_equations_max_fill_in_proxy, lp.AT.ptr, lp.AT.idx, lp.AT.val, flag.p, keep_c.p, elim_c.p,
+             keep_v.p, elim_v.p);
+  exclusive_scan_i32(flag.p, pos.p, m, s);
+  if (read_scalar(pos.p + m) == 0) return;
+  DBuf<int32_t> acc(size_t(1), s);
+  GPP_LAUNCH(dt_scatter_first, grid_stride_blocks(m), kThreads, 0, s, m, flag.p, pos.p, acc.p);
+  Status st;
+  st.clear(kStWords);
+  DBuf<double> meta(3, s), rec_val(12, s);
+  DBuf<int32_t> rec_idx(4, s);
+  GPP_LAUNCH(dt_single_apply, 1, 1, 0, s, acc.p, keep_c.p, elim_c.p, keep_v.p, elim_v.p, p.bound_tol, plan.l.p,
+             plan.u.p, plan.c.p, plan.AU.p, plan.keep_row.p, plan.keep_col.p, meta.p, rec_idx.p, rec_val.p, st.d);
+  GPP_LAUNCH(dt_single_shift, kNumSMs, kThreads, 0, s, acc.p, elim_c.p, lp.AT.ptr, lp.AT.idx, lp.AT.val, meta.p, st.d,
+             plan.AL.p, plan.AU.p);
+  const int32_t* f = st.read(kStWords);
+  if (f[kStInfeasible]) { plan.has_infeasible = true; return; }
+  if (p.record_postsolve_tape) {
+    PostsolveSegment seg = make_segment(1, 4, 12);
+    const int64_t offs[2] = {0, 4}, voffs[2] = {0, 12};
+    const int32_t type = 13;  // DoubletonEquation
+    check(cudaMemcpyAsync(seg.types.p, &type, sizeof(type), cudaMemcpyHostToDevice, s), "doubleton record type");
+    check(cudaMemcpyAsync(seg.is.p, offs, sizeof(offs), cudaMemcpyHostToDevice, s), "doubleton record offsets");
+    check(cudaMemcpyAsync(seg.vs.p, voffs, sizeof(voffs), cudaMemcpyHostToDevice, s), "doubleton record offsets");
+    check(cudaMemcpyAsync(seg.idx.p, rec_idx.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToDevice, s), "doubleton record");
+    check(cudaMemcpyAsync(seg.val.p, rec_val.p, 12 * sizeof(double), cudaMemcpyDeviceToDevice, s), "doubleton record");
+    ctx().sync("doubleton record");
+    plan.tape.push_back(std::move(seg));
+  }
+  DBuf<int32_t> cnt(size_t(m) + 1, s);
+  GPP_LAUNCH(dt_single_rows<false>, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val, acc.p,
+             keep_c.p, elim_c.p, meta.p, zt, cnt.p, nullptr, nullptr, nullptr);
+  DevCsr out;
+  out.rows = m;
+  out.cols = n;
+  out.ptr = dalloc<offset_t>(size_t(m) + 1);
+  exclusive_scan_i32(cnt.p, out.ptr, m, s);
+  out.nnz = read_scalar(out.ptr + m);
+  out.idx = dalloc<int32_t>(size_t(out.nnz));
+  out.val = dalloc<double>(size_t(out.nnz));
+  GPP_LAUNCH(dt_single_rows<true>, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val, acc.p,
+             keep_c.p, elim_c.p, meta.p, zt, nullptr, out.ptr, out.idx, out.val);
+  if (plan.has_new_A) free_csr(plan.new_A);
+  plan.new_A = out;
+  plan.has_new_A = true;
+  plan.obj_delta += read_scalar(meta.p + 2);
+  plan.has_row_action = plan.has_col_action = plan.has_change = true;
 }
 
 }  // namespace
 
 void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params& p) {
   if (plan.has_infeasible || plan.has_unbounded) return;
-  if (!p.doubleton_equations_scan)
-    throw std::invalid_argument("doubleton_equations_scan = 0 (single-row mode) is not available in this build");
+  if (!p.doubleton_equations_scan) { doubleton_single_row(plan, lp, p); return; }
   const int m = lp.m(), n = lp.n();
   if (m == 0 || n == 0) return;
   auto s = ctx().stream;
@@ -480,7 +680,7 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
   DBuf<double> keep_v(size_t(m), s), elim_v(size_t(m), s);
   GPP_LAUNCH(dt_col_nnz, grid_stride_blocks(n), kThreads, 0, s, n, AT.ptr, AT.idx, AT.val, plan.keep_row.p,
              plan.keep_col.p, zt, col_nnz.p);
-  GPP_LAUNCH(dt_candidates, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val,
+  GPP_LAUNCH(dt_candidates<true>, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val,
              plan.keep_row.p, plan.keep_col.p, col_nnz.p, plan.AL.p, plan.AU.p, zt, tol, ratio_tol,
              p.doubleton_equations_max_fill_in_proxy, AT.ptr, AT.idx, AT.val, flag.p, keep_c.p, elim_c.p, keep_v.p,
              elim_v.p);

@@ -50,8 +50,39 @@ _PARAM_FIELDS = [
     ("parallel_columns_max_abs_ratio", f64, 2.0),
     ("parallel_columns_scale_guard_max_group_size", i32, 4),
     ("parallel_columns_scale_guard_min_groups", i32, 128),
-    ("enable_structure_specific_rules", u8, 1), ("enable_redundant_variable_bounds", u8, 0),
-    ("enable_startup", u8, 1), ("bound_strengthening_bound_only_nnz_round_budget", i64, 8_000_000),
+    ("enable_structure_specific_rules", u8, 1),
+    ("enable_two_row_variable_elimination", u8, 1),
+    ("two_row_variable_elimination_max_row_nnz", i32, 8),
+    ("two_row_variable_elimination_safety_tol", f64, 1.0e-8),
+    ("two_row_variable_elimination_min_candidates", i32, 128),
+    ("two_row_variable_elimination_min_candidate_ratio", f64, 0.01),
+    ("enable_zero_cost_product_variables", u8, 1),
+    ("zero_cost_product_variables_min_candidates", i32, 128),
+    ("zero_cost_product_variables_min_candidate_ratio", f64, 0.01),
+    ("enable_piecewise_linear_reformulation_variable_pair", u8, 1),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_probe_pairs", i32, 256),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_min_pairs", i32, 4096),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_min_potential_gain", f64, 0.20),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_min_actual_gain", f64, 0.20),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_max_tail_cols", i32, 8),
+    ("piecewise_linear_reformulation_variable_pair_epigraph_max_quotient_terms_per_row", i32, 5),
+    ("piecewise_linear_reformulation_variable_pair_shifted_antipodal_probe_pairs", i32, 256),
+    ("piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_pairs", i32, 4096),
+    ("piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_potential_gain", f64, 0.20),
+    ("piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_actual_gain", f64, 0.20),
+    ("piecewise_linear_reformulation_variable_pair_shifted_antipodal_max_quotient_terms_per_row", i32, 6),
+    ("enable_column_domination", u8, 1),
+    ("column_domination_probe_rows", i32, 64),
+    ("column_domination_probe_cols", i32, 256),
+    ("column_domination_probe_nnz", i32, 256),
+    ("column_domination_min_fixed_cols", i32, 4096),
+    ("column_domination_min_candidate_ratio", f64, 0.20),
+    ("enable_piecewise_linear_reformulation_absolute_value", u8, 1),
+    ("piecewise_linear_reformulation_absolute_value_residual_bound_mode", u8, 0),
+    ("piecewise_linear_reformulation_absolute_value_residual_bound_as_free_min", f64, 1.0e8),
+    ("enable_redundant_variable_bounds", u8, 0),
+    ("enable_startup", u8, 1),
+    ("bound_strengthening_bound_only_nnz_round_budget", i64, 8000000),
 ]
 
 
@@ -91,7 +122,8 @@ class Summary(C.Structure):
                 ("stopped_at_iteration_limit", u8), ("has_change", u8), ("has_infeasible", u8),
                 ("has_unbounded", u8), ("presolve_enabled", u8), ("folding_applied", u8),
                 ("owns_reduced_lp", u8), ("elapsed_seconds", f64), ("preprocessing_seconds", f64),
-                ("obj_constant_delta", f64), ("reduced_lp", Lp), ("record", C.c_void_p)]
+                ("obj_constant_delta", f64), ("reduced_lp", Lp), ("record", C.c_void_p),
+                ("folded_rows", i32), ("folded_cols", i32)]
 
 
 _lib = None
@@ -123,6 +155,8 @@ def load():
         "gpp_parallel_row_hashes": (C.c_int, [P(Csr), vp, vp, C.c_int, vp]),
         "gpp_sort_pairs": (C.c_int, [vp, vp, i64]),
         "gpp_sort_pairs_static": (C.c_int, [vp, vp, i64, vp]),
+        "gpp_export_folding_map": (C.c_int, [C.POINTER(Summary), vp, vp, vp, vp]),
+        "gpp_unfold_solution": (C.c_int, [C.POINTER(Summary), vp, vp, vp, vp, vp, vp]),
         "gpp_device_free": (None, [vp]),
         "gpp_last_error": (C.c_char_p, []),
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
@@ -142,6 +176,7 @@ EXPORTED = [
     "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
     "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_free",
+    "gpp_export_folding_map", "gpp_unfold_solution",
     "gpp_last_error", "gpp_kernel_launches", "gpp_profile_enable", "gpp_profile_read",
 ]
 

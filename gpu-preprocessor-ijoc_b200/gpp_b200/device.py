@@ -185,3 +185,27 @@ def postsolve_device(x_red, y_red, z_red, summary: capi.Summary, original: Devic
     _raise(capi.load().gpp_postsolve_device(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
                                             *(ptr(t) for t in out)))
     return out
+
+
+def fold_map(summary: capi.Summary):
+    """folding::copy_map_to_host: (row_color, col_color, row_scale, col_scale) or None."""
+    if not summary.folding_applied:
+        return None
+    rc = np.zeros(summary.original_rows, np.int32)
+    cc = np.zeros(summary.original_cols, np.int32)
+    rs = np.zeros(summary.original_rows)
+    cs = np.zeros(summary.original_cols)
+    _raise(capi.load().gpp_export_folding_map(C.byref(summary), *(a.ctypes.data_as(C.c_void_p)
+                                                                  for a in (rc, cc, rs, cs))))
+    return rc, cc, rs, cs
+
+
+def unfold(x_folded, y_folded, z_folded, summary: capi.Summary):
+    """folding::unfold_solution_device_to_host: folded-model CUDA tensors -> original-model host arrays."""
+    x = np.zeros(summary.original_cols)
+    y = np.zeros(summary.original_rows)
+    z = np.zeros(summary.original_cols)
+    _raise(capi.load().gpp_unfold_solution(C.byref(summary), ptr(x_folded), ptr(y_folded), ptr(z_folded),
+                                           x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                           z.ctypes.data_as(C.c_void_p)))
+    return x, y, z

@@ -271,6 +271,31 @@ def _add_slacks(lp: HostLP, act, frac: float, seed: int) -> HostLP:
     return HostLP(m, n + k, ptr, idx, val, c, AL, AU, l, u)
 
 
+def replicated_lp(m: int, n: int, copies: int, seed: int = 0) -> HostLP:
+    """`copies` identical copies of random_lp(m, n) on the block diagonal plus
+    one coupling row (sum of all variables <= a slack bound): a model with an
+    exact symmetry, so colour refinement folds it back to about one copy."""
+    base = random_lp(m, n, seed)
+    rows, cols, vals = [], [], []
+    counts = np.diff(base.row_ptr).astype(np.int64)
+    r_base = np.repeat(np.arange(m, dtype=np.int64), counts)
+    for k in range(copies):
+        rows.append(r_base + k * m)
+        cols.append(base.col_idx.astype(np.int64) + k * n)
+        vals.append(base.values)
+    mt, nt = m * copies + 1, n * copies
+    rows.append(np.full(nt, mt - 1, dtype=np.int64))
+    cols.append(np.arange(nt, dtype=np.int64))
+    vals.append(np.ones(nt))
+    ptr, idx, val = coo_to_csr(mt, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
+    finite_u = np.where(np.isfinite(base.u), base.u, 10.0)
+    cap = float(copies * finite_u.sum()) * 2.0 + 1.0
+    AL = np.concatenate([np.tile(base.AL, copies), [-INF]])
+    AU = np.concatenate([np.tile(base.AU, copies), [cap]])
+    return HostLP(mt, nt, ptr, idx, val, np.tile(base.c, copies), AL, AU, np.tile(base.l, copies),
+                  np.tile(base.u, copies)).ensure_transpose()
+
+
 def qap_lp(N: int, seed: int = 0) -> HostLP:
     """Adams-Johnson QAP relaxation in the reference exporter's row/column order."""
     rng = np.random.default_rng(seed)
@@ -341,7 +366,8 @@ def qap_lp(N: int, seed: int = 0) -> HostLP:
 
 def workload(name: str, seed: int = 0) -> HostLP:
     """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
-    'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows), 'qap:N'."""
+    'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows),
+    'replicated:MxN*K' (K identical copies plus a coupling row), 'qap:N'."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -354,6 +380,11 @@ def workload(name: str, seed: int = 0) -> HostLP:
     if name.startswith("slack:"):
         m, n = (int(v) for v in name.split(":")[1].split("x"))
         return random_lp(m, n, seed, slack_frac=0.3)
+    if name.startswith("replicated:"):
+        spec = name.split(":")[1]
+        mn, k = spec.split("*")
+        m, n = (int(v) for v in mn.split("x"))
+        return replicated_lp(m, n, int(k), seed)
     if name.startswith("qap:"):
         return qap_lp(int(name.split(":")[1]), seed)
     raise ValueError(f"unknown workload {name!r}")

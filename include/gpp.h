@@ -108,10 +108,41 @@ typedef struct gpp_params {
   double parallel_columns_max_abs_ratio;
   int32_t parallel_columns_scale_guard_max_group_size;
   int32_t parallel_columns_scale_guard_min_groups;
-  /* Master switch of the structure-specific startup rules.  They are outside
-   * this engine's scope: a nonzero value is accepted only when the startup
-   * detectors provably cannot fire (see gpp_presolve's documentation). */
+  /* The structure-specific startup rules (column domination, two-row
+   * variable elimination, zero-cost product variables, the piecewise-linear
+   * reformulations) and their settings are carried for layout parity with
+   * PresolveParams; this engine does not run those rules, so the Startup
+   * phase only consumes its iteration. */
   uint8_t enable_structure_specific_rules;
+  uint8_t enable_two_row_variable_elimination;
+  int32_t two_row_variable_elimination_max_row_nnz;
+  double two_row_variable_elimination_safety_tol;
+  int32_t two_row_variable_elimination_min_candidates;
+  double two_row_variable_elimination_min_candidate_ratio;
+  uint8_t enable_zero_cost_product_variables;
+  int32_t zero_cost_product_variables_min_candidates;
+  double zero_cost_product_variables_min_candidate_ratio;
+  uint8_t enable_piecewise_linear_reformulation_variable_pair;
+  int32_t piecewise_linear_reformulation_variable_pair_epigraph_probe_pairs;
+  int32_t piecewise_linear_reformulation_variable_pair_epigraph_min_pairs;
+  double piecewise_linear_reformulation_variable_pair_epigraph_min_potential_gain;
+  double piecewise_linear_reformulation_variable_pair_epigraph_min_actual_gain;
+  int32_t piecewise_linear_reformulation_variable_pair_epigraph_max_tail_cols;
+  int32_t piecewise_linear_reformulation_variable_pair_epigraph_max_quotient_terms_per_row;
+  int32_t piecewise_linear_reformulation_variable_pair_shifted_antipodal_probe_pairs;
+  int32_t piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_pairs;
+  double piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_potential_gain;
+  double piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_actual_gain;
+  int32_t piecewise_linear_reformulation_variable_pair_shifted_antipodal_max_quotient_terms_per_row;
+  uint8_t enable_column_domination;
+  int32_t column_domination_probe_rows;
+  int32_t column_domination_probe_cols;
+  int32_t column_domination_probe_nnz;
+  int32_t column_domination_min_fixed_cols;
+  double column_domination_min_candidate_ratio;
+  uint8_t enable_piecewise_linear_reformulation_absolute_value;
+  uint8_t piecewise_linear_reformulation_absolute_value_residual_bound_mode;
+  double piecewise_linear_reformulation_absolute_value_residual_bound_as_free_min;
   uint8_t enable_redundant_variable_bounds;
   uint8_t enable_startup;
   int64_t bound_strengthening_bound_only_nnz_round_budget;
@@ -145,6 +176,8 @@ typedef struct gpp_summary {
   double obj_constant_delta;
   gpp_lp reduced_lp;               /* device arrays; borrowed from the input when !owns_reduced_lp */
   gpp_record* record;
+  int32_t folded_rows;             /* sizes of the folded model (the original sizes when not folded) */
+  int32_t folded_cols;
 } gpp_summary;
 
 /* ---- Plain pipeline: preprocess / postprocess / free_summary ------------- */
@@ -200,6 +233,20 @@ GPP_API int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t
 GPP_API int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t* index_starts,
                     int64_t* value_starts, int32_t* indices, double* vals,
                     int32_t* fixed_idx, double* fixed_val);
+
+/* folding::copy_map_to_host (folding/folding.hpp:22): the 1-based colour of
+ * every original row / column and the unfold scales 1/|colour|, as HOST
+ * arrays (m0, n0, m0, n0; any may be NULL).  Returns GPP_OK with nothing
+ * written when folding did not apply (summary->folding_applied == 0). */
+GPP_API int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32_t* col_color,
+                                   double* row_scale, double* col_scale);
+
+/* folding::unfold_solution_device_to_host (folding/folding.hpp:40-44): map a
+ * solution of the folded model (DEVICE arrays of folded_cols, folded_rows,
+ * folded_cols entries; any may be NULL) to the original model on the HOST:
+ * x_j = x_f[C(j)], y_i = y_f[R(i)] / |R(i)|, z_j = z_f[C(j)] / |C(j)|. */
+GPP_API int gpp_unfold_solution(const gpp_summary* summary, const double* x_folded, const double* y_folded,
+                                const double* z_folded, double* x_out, double* y_out, double* z_out);
 
 /* ---- Kernel-level entry points (rule / kernel parity tests) -------------- */
 

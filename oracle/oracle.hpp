@@ -119,6 +119,16 @@ uint64_t row_hash(const Csr& A, int row, const uint8_t* keep_col, int mode);
 uint64_t row_hash_tol(const Csr& A, int row, const uint8_t* keep_col, int mode, double tol);
 uint64_t col_hash(const Csr& AT, int col, const uint8_t* keep_row, double tol);
 
+// --- folding (oracle_folding.cpp) -----------------------------------------
+struct Fold {
+  bool applied = false;
+  int rows = 0, cols = 0;              // original sizes
+  Lp folded;
+  std::vector<int> row_color, col_color;     // 1-based colour per original row / column
+  std::vector<double> row_scale, col_scale;  // 1 / colour size
+};
+Fold fold(const Lp& lp, double tol);
+
 // --- pipeline -------------------------------------------------------------
 Result presolve(const Lp& lp, const gpp_params& params);
 void postsolve(const Result& r, const Lp& original, const double* x_red, const double* y_red,

@@ -37,6 +37,7 @@ struct orc_lp {
 struct orc_result {
   oracle::Result r;
   oracle::Lp original;
+  oracle::Fold fold;
 };
 
 const char* orc_last_error() { return g_error.c_str(); }
@@ -55,10 +56,20 @@ static oracle::Lp to_lp(const orc_lp* h) {
 }
 
 int orc_presolve(const orc_lp* h, const gpp_params* p, orc_result** out) {
+  // run_gpu_presolve_with_folding (folding.cu:172-213): fold first when
+  // enabled, then presolve whichever model results.
   try {
     auto* res = new orc_result;
     res->original = to_lp(h);
-    res->r = oracle::presolve(res->original, *p);
+    if (p->enable_folding) res->fold = oracle::fold(res->original, p->folding_tolerance);
+    const oracle::Lp& input = res->fold.applied ? res->fold.folded : res->original;
+    res->r = oracle::presolve(input, *p);
+    auto& s = res->r.summary;
+    s.folding_applied = res->fold.applied ? 1 : 0;
+    s.original_rows = res->original.m();
+    s.original_cols = res->original.n();
+    s.folded_rows = input.m();
+    s.folded_cols = input.n();
     *out = res;
     return 0;
   } catch (const std::exception& e) {
@@ -106,13 +117,38 @@ void orc_tape(const orc_result* r, int32_t* types, int64_t* is, int64_t* vs, int
   cp(fixed_idx, R.fixed_idx); cp(fixed_val, R.fixed_val);
 }
 
+// copy_map_to_host (folding_map.cu:250-270); returns 1 when folding applied.
+int orc_fold_map(const orc_result* r, int32_t* row_color, int32_t* col_color, double* row_scale, double* col_scale) {
+  const auto& f = r->fold;
+  if (!f.applied) return 0;
+  auto cp = [](auto* dst, const auto& v) { if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0])); };
+  cp(row_color, f.row_color); cp(col_color, f.col_color); cp(row_scale, f.row_scale); cp(col_scale, f.col_scale);
+  return 1;
+}
+
 int orc_trace_count(const orc_result* r) { return int(r->r.trace.size()); }
 const char* orc_trace(const orc_result* r, int k) { return r->r.trace[size_t(k)].c_str(); }
 
 int orc_postsolve(const orc_result* r, const double* x_red, const double* y_red, const double* z_red,
                   double* x, double* y, double* z) {
   try {
-    oracle::postsolve(r->r, r->original, x_red, y_red, z_red, x, y, z);
+    if (!r->fold.applied) {
+      oracle::postsolve(r->r, r->original, x_red, y_red, z_red, x, y, z);
+      return 0;
+    }
+    // postsolve_and_unfold_to_host (folding.cu:215-261): postsolve on the
+    // folded model, then x_j = x_f[C(j)], y_i = y_f[R(i)]/|R|, z_j = z_f[C(j)]/|C|.
+    const oracle::Lp& F = r->fold.folded;
+    std::vector<double> xf(static_cast<size_t>(F.n())), yf(static_cast<size_t>(F.m())), zf(static_cast<size_t>(F.n()));
+    oracle::postsolve(r->r, F, x_red, y_red, z_red, xf.data(), yf.data(), zf.data());
+    const auto& fd = r->fold;
+    for (int j = 0; j < fd.cols; ++j) {
+      const int k = fd.col_color[size_t(j)] - 1;
+      if (x) x[j] = xf[size_t(k)];
+      if (z) z[j] = zf[size_t(k)] * fd.col_scale[size_t(j)];
+    }
+    if (y)
+      for (int i = 0; i < fd.rows; ++i) y[i] = yf[size_t(fd.row_color[size_t(i)] - 1)] * fd.row_scale[size_t(i)];
     return 0;
   } catch (const std::exception& e) {
     g_error = e.what();

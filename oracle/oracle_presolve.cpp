@@ -252,6 +252,16 @@ Result presolve(const Lp& lp, const gpp_params& p) {
   res.record.cols.resize(size_t(lp.n()));
   for (int i = 0; i < lp.m(); ++i) res.record.rows[size_t(i)] = i;
   for (int j = 0; j < lp.n(); ++j) res.record.cols[size_t(j)] = j;
+  if (!p.enable_presolve) {
+    // run_optional_gpu_presolve with presolve off (folding.cu:145-170).
+    S.reduced_rows = lp.m();
+    S.reduced_cols = lp.n();
+    S.reduced_nnz = lp.A.nnz();
+    S.presolve_enabled = 0;
+    res.reduced = lp;
+    return res;
+  }
+  S.presolve_enabled = 1;
   Engine e(p, res);
   e.cur = lp;
   const auto t0 = std::chrono::steady_clock::now();

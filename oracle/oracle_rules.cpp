@@ -245,13 +245,140 @@ int fill_in_proxy(const Csr& AT, const std::vector<uint8_t>& keep_row, double zt
 }
 }  // namespace
 
+namespace {
+// _doubleton_equations_fill_in_proxy_device (rule_doubleton_equations.cu:216-243):
+// over the stored entries of AT, masks ignored.
+int fill_in_proxy_stored(const Csr& AT, int keep, int elim) {
+  int fill = -1;
+  int jj = AT.ptr[keep], kk = AT.ptr[elim];
+  const int js = AT.ptr[keep + 1], ks = AT.ptr[elim + 1];
+  if (js <= jj || ks <= kk) return fill;
+  while (jj < js && kk < ks) {
+    const int kr = AT.idx[jj], er = AT.idx[kk];
+    if (kr == er) { ++jj; ++kk; }
+    else if (er < kr) { ++kk; ++fill; }
+    else ++jj;
+  }
+  return fill + (ks - kk);
+}
+
+// Single-row mode (doubleton_equations_scan = 0; rule_doubleton_equations.cu:
+// 273-512, 1814-2126): the smallest acceptable row is substituted; every row
+// side shifts by a_(r,elim) * beta, and the matrix keeps its stored entries
+// except the keep column, which becomes a_(r,keep) + alpha * a_(r,elim).
+void doubleton_single_row(Plan& plan, const Lp& lp, const gpp_params& p) {
+  const int m = lp.m(), n = lp.n();
+  if (m == 0 || n == 0) return;
+  const Csr& A = lp.A;
+  const double zt = p.zero_tol, tol = p.bound_tol, ratio_tol = std::fmax(1.0e-9, p.bound_tol);
+  std::vector<int> col_nnz(size_t(n), 0);
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[j]) continue;
+    for (int q = lp.AT.ptr[j]; q < lp.AT.ptr[j + 1]; ++q)
+      if (plan.keep_row[lp.AT.idx[q]] && std::fabs(lp.AT.val[q]) > zt) ++col_nnz[j];
+  }
+  int target = -1, e = -1, k = -1;
+  double ev = 0.0, kv = 0.0;
+  for (int i = 0; i < m && target < 0; ++i) {
+    if (!plan.keep_row[i]) continue;
+    const double lhs = plan.AL[i], rhs = plan.AU[i];
+    if (!fin(lhs) || !fin(rhs) || std::fabs(lhs - rhs) > tol) continue;
+    int live = 0, c1 = -1, c2 = -1;
+    double v1 = 0.0, v2 = 0.0;
+    for (int q = A.ptr[i]; q < A.ptr[i + 1] && live <= 2; ++q) {
+      const int j = A.idx[q];
+      if (!plan.keep_col[j] || !(std::fabs(A.val[q]) > zt)) continue;
+      ++live;
+      if (live == 1) { c1 = j; v1 = A.val[q]; } else if (live == 2) { c2 = j; v2 = A.val[q]; }
+    }
+    if (live != 2) continue;
+    const bool i12 = integral_ratio(v1, v2, ratio_tol), i21 = integral_ratio(v2, v1, ratio_tol);
+    bool elim_first;
+    if (col_nnz[c1] == 1 && col_nnz[c2] != 1) elim_first = true;
+    else if (col_nnz[c1] != 1 && col_nnz[c2] == 1) elim_first = false;
+    else if (i12 && !i21) elim_first = false;
+    else if (i21 && !i12) elim_first = true;
+    else elim_first = col_nnz[c1] < col_nnz[c2];
+    const int ce = elim_first ? c1 : c2, ck = elim_first ? c2 : c1;
+    const double cev = elim_first ? v1 : v2, ckv = elim_first ? v2 : v1;
+    if (std::fabs(cev) <= 0.0) continue;
+    const double pr = std::fabs(ckv / cev);
+    if (!(pr <= kDoubletonMaxPivotRatio && pr >= 1.0 / kDoubletonMaxPivotRatio)) continue;
+    if (col_nnz[ce] > col_nnz[ck] + p.doubleton_equations_max_fill_in_proxy + 1) continue;
+    if (fill_in_proxy_stored(lp.AT, ck, ce) > p.doubleton_equations_max_fill_in_proxy) continue;
+    target = i; e = ce; k = ck; ev = cev; kv = ckv;
+  }
+  if (target < 0) return;
+  const double rhs = plan.AU[target];
+  const double le = plan.l[e], ue = plan.u[e], lk = plan.l[k], uk = plan.u[k], ce = plan.c[e];
+  const double alpha = -kv / ev, beta = rhs / ev;
+  double ml = -INFINITY, mu = INFINITY;
+  if (fin(le)) { const double b = (le - beta) / alpha; if (alpha > 0.0) ml = b; else mu = b; }
+  if (fin(ue)) { const double b = (ue - beta) / alpha; if (alpha > 0.0) mu = b; else ml = b; }
+  if (ml > mu) std::swap(ml, mu);
+  const double nl = fin(ml) ? std::fmax(lk, ml) : lk;
+  const double nu = fin(mu) ? std::fmin(uk, mu) : uk;
+  if (nl > nu + p.bound_tol) { plan.has_infeasible = true; return; }
+  for (int q = lp.AT.ptr[e]; q < lp.AT.ptr[e + 1]; ++q) {
+    const int r = lp.AT.idx[q];
+    bool first = true;
+    for (int q2 = lp.AT.ptr[e]; q2 < q; ++q2) first = first && lp.AT.idx[q2] != r;
+    if (!first) continue;
+    const double shift = lp.AT.val[q] * beta;
+    plan.AL[r] -= shift;
+    plan.AU[r] -= shift;
+  }
+  plan.l[k] = nl;
+  plan.u[k] = nu;
+  plan.c[k] += ce * alpha;
+  plan.keep_row[target] = 0;
+  plan.keep_col[e] = 0;
+  if (p.record_postsolve_tape)
+    plan.tape.add(DoubletonEquation, {e, k, target, 0}, {ev, kv, rhs, le, ue, lk, uk, nl, nu, ce, 0.0, 0.0});
+  Csr out;
+  out.rows = m;
+  out.cols = n;
+  out.ptr.assign(size_t(m) + 1, 0);
+  for (int r = 0; r < m; ++r) {
+    const int first = A.ptr[r], last = A.ptr[r + 1];
+    if (r == target) {
+      for (int q = first; q < last; ++q) { out.idx.push_back(A.idx[q]); out.val.push_back(A.val[q]); }
+    } else if (first < last) {
+      bool ep = false, kp = false;
+      double are = 0.0, old = 0.0;
+      for (int q = first; q < last; ++q) {
+        if (A.idx[q] == e) { ep = true; are = A.val[q]; } else if (A.idx[q] == k) { kp = true; old = A.val[q]; }
+      }
+      const double nk = old + alpha * are;
+      const bool insert = ep && !kp && std::fabs(nk) > zt;
+      bool inserted = !insert;
+      for (int q = first; q < last; ++q) {
+        const int col = A.idx[q];
+        if (insert && !inserted && col > k) { out.idx.push_back(k); out.val.push_back(nk); inserted = true; }
+        if (col == k) {
+          if (std::fabs(nk) > zt) { out.idx.push_back(k); out.val.push_back(nk); }
+        } else {
+          out.idx.push_back(col);
+          out.val.push_back(A.val[q]);
+        }
+      }
+      if (insert && !inserted) { out.idx.push_back(k); out.val.push_back(nk); }
+    }
+    out.ptr[size_t(r) + 1] = int(out.idx.size());
+  }
+  plan.new_A = std::move(out);
+  plan.has_new_A = true;
+  plan.obj_delta += ce * beta;
+  plan.has_row_action = plan.has_col_action = plan.has_change = true;
+}
+}  // namespace
+
 void rule_doubleton_equations(Plan& plan, const Lp& lp, const gpp_params& p) {
   // apply_rule_doubleton_equations -> _batch -> _batch_once
   // (rule_doubleton_equations.cu:1512-1812, 1948-1957): one batch of
   // non-overlapping doubleton equalities per call.
   if (plan.has_infeasible || plan.has_unbounded) return;
-  if (!p.doubleton_equations_scan)
-    throw std::runtime_error("oracle: doubleton_equations_scan = 0 (single-row mode) is not restated");
+  if (!p.doubleton_equations_scan) { doubleton_single_row(plan, lp, p); return; }
   const int m = lp.m(), n = lp.n();
   if (m == 0 || n == 0) return;
   const Csr& A = lp.A;

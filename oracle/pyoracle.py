@@ -48,6 +48,7 @@ def lib():
         _lib.orc_trace.argtypes = [vp, C.c_int]
         _lib.orc_trace.restype = C.c_char_p
         _lib.orc_postsolve.argtypes = [vp] * 7
+        _lib.orc_fold_map.argtypes = [vp] * 5
         _lib.orc_last_error.restype = C.c_char_p
         _lib.orc_row_activity_summary.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double,
                                                   vp, vp, vp, vp, vp, vp, vp]
@@ -104,6 +105,16 @@ class OracleResult:
                                               self.fixed_val)))
         self.trace = [L.orc_trace(handle, k).decode() for k in range(L.orc_trace_count(handle))]
         self.m0, self.n0 = lp.m, lp.n
+
+    def fold_map(self):
+        """(row_color, col_color, row_scale, col_scale) when folding applied, else None."""
+        s = self.summary
+        if not s.folding_applied:
+            return None
+        rc, cc = np.zeros(self.m0, np.int32), np.zeros(self.n0, np.int32)
+        rs, cs = np.zeros(self.m0), np.zeros(self.n0)
+        lib().orc_fold_map(self._h, ptr(rc), ptr(cc), ptr(rs), ptr(cs))
+        return rc, cc, rs, cs
 
     def postsolve(self, x_red, y_red, z_red):
         x = np.zeros(self.n0)

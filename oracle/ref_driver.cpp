@@ -84,6 +84,7 @@ int main(int argc, char** argv) {
       FLAG(enable_doubleton_equations); FLAG(enable_dual_fix); FLAG(enable_parallel_columns);
       FLAG(enable_structure_specific_rules); FLAG(enable_startup);
       else if (k == "max_iters") p.max_iters = v;
+      else if (k == "folding_tolerance") p.folding_tolerance = dv;
       else if (k == "doubleton_equations_scan") p.doubleton_equations_scan = v != 0;
       else if (k == "doubleton_equations_max_fill_in_proxy") p.doubleton_equations_max_fill_in_proxy = v;
       else if (k == "doubleton_equations_min_selected_per_batch") p.doubleton_equations_min_selected_per_batch = v;
@@ -163,6 +164,13 @@ int main(int argc, char** argv) {
       save(out, "u", down(L.u, size_t(L.A.cols)));
       save(out, "AL", down(L.AL, size_t(L.A.rows)));
       save(out, "AU", down(L.AU, size_t(L.A.rows)));
+    }
+    if (s.folding_applied) {
+      const auto map = gp::folding::copy_map_to_host(s.folding.map);
+      save(out, "row_color", map.row_color_id);
+      save(out, "col_color", map.col_color_id);
+      save(out, "row_scale", map.row_scale);
+      save(out, "col_scale", map.col_scale);
     }
     // Fills the record's host views; postsolve keeps using the device state.
     auto& record = const_cast<gp::presolve::PresolveRecordGpu&>(ps.record);

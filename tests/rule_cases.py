@@ -33,16 +33,19 @@ class Run:
     """Presolve `lp` with `rules` on 'oracle' or 'gpu' and keep host copies."""
 
     def __init__(self, backend, lp, rules, **extra):
-        params = params_with_rules(rules, enable_folding=0, **extra)
+        extra.setdefault("enable_folding", 0)
+        params = params_with_rules(rules, **extra)
         if backend == "oracle":
             import pyoracle
             self.r = pyoracle.presolve(lp, params)
+            self.fold = self.r.fold_map()
         else:
             from gpp_b200 import device
             dlp = device.DeviceLp(lp)
             s = device.preprocess(dlp, params)
             try:
                 self.r = device.Result(s)
+                self.fold = device.fold_map(s)
                 self.r.summary = type(s).from_buffer_copy(s)   # free_summary clears s
             finally:
                 device.free_summary(s)

@@ -52,7 +52,8 @@ def run_reference(lp, rules, extra=None):
             "AT_val": np.float64, "c": np.float64, "l": np.float64, "u": np.float64, "AL": np.float64,
             "AU": np.float64, "row_map": np.int32, "col_map": np.int32, "fixed_idx": np.int32,
             "fixed_val": np.float64, "tape_types": np.int32, "tape_is": np.int32, "tape_vs": np.int32,
-            "tape_idx": np.int32, "tape_val": np.float64}
+            "tape_idx": np.int32, "tape_val": np.float64, "row_color": np.int32, "col_color": np.int32,
+            "row_scale": np.float64, "col_scale": np.float64}
     for k, dt in spec.items():
         p = os.path.join(d, k)
         out[k] = np.fromfile(p, dtype=dt) if os.path.exists(p) else None
@@ -79,6 +80,8 @@ def check_against_reference(lp, rules, extra=None):
     s = device.preprocess(dlp, params)
     try:
         got = device.Result(s)
+        got.fold = device.fold_map(s)
+        got.summary = type(s).from_buffer_copy(s)
         m = ref["meta"]
         assert (s.reduced_rows, s.reduced_cols, s.reduced_nnz) == (
             int(m["reduced_rows"]), int(m["reduced_cols"]), int(m["reduced_nnz"]))
@@ -113,3 +116,34 @@ def test_structure_matches_reference(rules, workload):
 def test_doubleton_structure_matches_reference(workload, extra):
     got = check_against_reference(lpgen.workload(workload, seed=0), ALL, extra)
     assert 13 in got.tape_types.tolist()   # the batch ran
+
+
+@needs_reference
+@pytest.mark.parametrize("workload", ["replicated:100x250*4", "replicated:400x1000*3", "random:400x1000"])
+def test_folding_matches_reference(workload):
+    """The default pipeline with folding on: the fold decision, folded sizes,
+    colour maps and the presolve of the folded model equal the reference's."""
+    lp = lpgen.workload(workload, seed=0)
+    got = check_against_reference(lp, ALL, {"enable_folding": 1})
+    ref = run_reference(lp, ALL, ["enable_folding=1"])
+    m = ref["meta"]
+    assert got.summary.folding_applied == int(m["folding_applied"])
+    assert (got.summary.folded_rows, got.summary.folded_cols) == (int(m["folded_rows"]), int(m["folded_cols"]))
+    if got.summary.folding_applied:
+        assert np.array_equal(got.fold[0], ref["row_color"]) and np.array_equal(got.fold[1], ref["col_color"])
+        assert np.array_equal(got.fold[2], ref["row_scale"]) and np.array_equal(got.fold[3], ref["col_scale"])
+
+
+@needs_reference
+@pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:2000x5000", "random:20000x50000"])
+def test_reference_startup_rules_do_not_fire(workload):
+    """This engine carries but does not run the reference's structure-specific
+    startup rules.  On these workloads the reference's own detectors reject
+    them: its output with the rules on equals its output with them off, so the
+    engine's parity holds for the reference's default settings too."""
+    lp = lpgen.workload(workload, seed=0)
+    on = run_reference(lp, ALL, ["enable_structure_specific_rules=1"])
+    off = run_reference(lp, ALL)
+    for k in ("row_map", "col_map", "A_idx", "tape_types"):
+        assert np.array_equal(on[k], off[k]), k
+    assert on["meta"]["iterations"] == off["meta"]["iterations"]

@@ -89,3 +89,26 @@ def test_keep_column_fixed_when_bounds_close(backend):
     assert r.fixed_idx.tolist() == [0]
     assert r.row_map.tolist() == [0, 1] and r.col_map.tolist() == [1]
     assert abs(r.AU[0] - (0.0 - 1.0 * (2.0 + 0.5e-10))) < 1e-15
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_eliminates_doubleton_equation_row_single_row_mode(backend):
+    # test_eliminates_doubleton_equation_row: doubleton_equations_scan = 0.
+    lp = make_lp(2, [[(0, 1.0), (1, 2.0)]], c=[3.0, 5.0], l=[0.0, -INF], u=[10.0, INF], AL=[4.0], AU=[4.0])
+    r = Run(backend, lp, RULE, doubleton_equations_scan=0, doubleton_equations_max_fill_in_proxy=10)
+    assert r.row_map.tolist() == [] and r.col_map.tolist() == [1]
+    assert abs(r.c[0] - (-1.0)) < 1e-12
+    assert abs(r.s.obj_constant_delta - 12.0) < 1e-12
+    assert r.tape_types.tolist() == [DOUBLETON]
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_single_row_mode_substitutes_one_row_per_call(backend):
+    # Two independent doubletons: one substitution per rule call, the smallest
+    # row first; the scheduler's next aggregation round takes the other only
+    # after nnz progress, which this tiny LP never makes.
+    lp = make_lp(4, [[(0, 1.0), (1, 1.0)], [(2, 1.0), (3, 2.0)]], c=[1.0, 2.0, 3.0, 4.0], l=[-INF] * 4,
+                 u=[INF] * 4, AL=[1.0, 2.0], AU=[1.0, 2.0])
+    r = Run(backend, lp, RULE, doubleton_equations_scan=0)
+    assert r.tape_types.tolist() == [DOUBLETON]
+    assert r.tape_idx.tolist()[2] == 0
