@@ -91,6 +91,32 @@ __device__ __forceinline__ int warp_append(int32_t* counter, bool take) {
   return take ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
 }
 
+// Block-aggregated append: one atomic per block instead of one per warp (a
+// per-warp atomic on one address serialises a grid-wide sweep).  Every
+// thread of the block must call it the same number of times.
+__device__ __forceinline__ int block_append(int32_t* counter, bool take) {
+  __shared__ int warp_base[32];
+  __shared__ int block_base;
+  const unsigned mask = __ballot_sync(0xffffffffu, take);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_base[warp] = __popc(mask);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int total = 0;
+    const int warps = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < warps; ++w) {
+      const int c = warp_base[w];
+      warp_base[w] = total;
+      total += c;
+    }
+    block_base = total ? atomicAdd(counter, total) : 0;
+  }
+  __syncthreads();
+  const int slot = take ? block_base + warp_base[warp] + __popc(mask & ((1u << lane) - 1u)) : -1;
+  __syncthreads();
+  return slot;
+}
+
 // ---------------------------------------------------------------------------
 // Engine context: one stream (blocking w.r.t. the legacy default stream so
 // caller work on stream 0 is ordered before ours), a stream-ordered memory

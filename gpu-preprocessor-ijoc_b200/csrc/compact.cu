@@ -10,6 +10,7 @@
 // second streaming pass.  The general transpose below is only needed for an
 // input A^T that is not row-sorted and for matrices rebuilt by a rule.
 #include "engine.cuh"
+#include "sort.hpp"
 
 #include <algorithm>
 
@@ -155,90 +156,29 @@ __global__ void histogram(const int32_t* __restrict__ idx, offset_t nnz, int32_t
   for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * blockDim.x)
     atomicAdd(counts + idx[p], 1);
 }
-__global__ void scatter_rows(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                             const double* __restrict__ val, int32_t* __restrict__ cursor,
-                             int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
-    for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) {
-      const int q = atomicAdd(cursor + idx[p], 1);
-      out_idx[q] = r;
-      out_val[q] = val[p];
-    }
-}
-// Sort every row of (idx, val) by idx.  Rows of up to 32 entries: insertion
-// sort by one thread; up to 4096: bitonic sort in shared memory by one block;
-// longer: rank by counting (each entry's rank = number of smaller keys).
-__global__ void sort_rows_short(int rows, const offset_t* __restrict__ ptr, int32_t* idx, double* val) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
-    const offset_t a = ptr[r], e = ptr[r + 1];
-    if (e - a > 32) continue;
-    for (offset_t i = a + 1; i < e; ++i) {
-      const int k = idx[i];
-      const double v = val[i];
-      offset_t j = i - 1;
-      while (j >= a && idx[j] > k) { idx[j + 1] = idx[j]; val[j + 1] = val[j]; --j; }
-      idx[j + 1] = k;
-      val[j + 1] = v;
-    }
+// Column keys and entry positions of M, in stored (row-major) order.
+__global__ void transpose_keys(offset_t nnz, const int32_t* __restrict__ idx, uint64_t* __restrict__ keys,
+                               int32_t* __restrict__ pos) {
+  for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * blockDim.x) {
+    keys[p] = uint64_t(uint32_t(idx[p]));
+    pos[p] = int32_t(p);
   }
 }
-__global__ void sort_rows_long(const int32_t* __restrict__ rows_list, const int32_t* __restrict__ count,
-                               const offset_t* __restrict__ ptr, int32_t* idx, double* val,
-                               int32_t* scratch_idx, double* scratch_val) {
-  __shared__ int skey[4096];
-  __shared__ int spos[4096];
-  for (int q = blockIdx.x; q < *count; q += gridDim.x) {
-    const int r = rows_list[q];
-    const offset_t a = ptr[r], e = ptr[r + 1];
-    const int len = int(e - a);
-    if (len <= 32) continue;
-    if (len <= 4096) {
-      int pow2 = 1;
-      while (pow2 < len) pow2 <<= 1;
-      for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
-        skey[i] = i < len ? idx[a + i] : 0x7fffffff;
-        spos[i] = i;
-      }
-      __syncthreads();
-      for (int k = 2; k <= pow2; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
-            const int x = i ^ j;
-            if (x > i) {
-              const bool up = (i & k) == 0;
-              if ((skey[i] > skey[x]) == up) {
-                const int tk = skey[i]; skey[i] = skey[x]; skey[x] = tk;
-                const int tp = spos[i]; spos[i] = spos[x]; spos[x] = tp;
-              }
-            }
-          }
-          __syncthreads();
-        }
-      for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        scratch_idx[a + i] = skey[i];
-        scratch_val[a + i] = val[a + spos[i]];
-      }
-      __syncthreads();
-      for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        idx[a + i] = scratch_idx[a + i];
-        val[a + i] = scratch_val[a + i];
-      }
-      __syncthreads();
-    } else {
-      for (offset_t i = a + threadIdx.x; i < e; i += blockDim.x) {
-        const int k = idx[i];
-        offset_t rank = 0;
-        for (offset_t j = a; j < e; ++j) rank += idx[j] < k;
-        scratch_idx[a + rank] = k;
-        scratch_val[a + rank] = val[i];
-      }
-      __syncthreads();
-      for (offset_t i = a + threadIdx.x; i < e; i += blockDim.x) {
-        idx[i] = scratch_idx[i];
-        val[i] = scratch_val[i];
-      }
-      __syncthreads();
-    }
+// Row of every stored entry: one warp per row writes its run.
+__global__ void row_of_entry(int rows, const offset_t* __restrict__ ptr, int32_t* __restrict__ row) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps)
+    for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) row[p] = r;
+}
+// Entries in (column, row) order: gather their rows and values.
+__global__ void transpose_gather(offset_t nnz, const int32_t* __restrict__ pos, const int32_t* __restrict__ row,
+                                 const double* __restrict__ val, int32_t* __restrict__ out_idx,
+                                 double* __restrict__ out_val) {
+  for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nnz; q += int64_t(gridDim.x) * blockDim.x) {
+    const int32_t p = pos[q];
+    out_idx[q] = row[p];
+    out_val[q] = val[p];
   }
 }
 
@@ -307,6 +247,9 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
 }
 
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
+  // A stable radix sort of the stored entries by column: entries of one
+  // column keep their row-major order, i.e. ascending rows (duplicates in
+  // stored order), which is the row-sorted CSR of M^T.
   DevCsr t;
   t.rows = M.cols;
   t.cols = M.rows;
@@ -320,22 +263,16 @@ DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
   t.val = dalloc<double>(size_t(M.nnz));
   DBuf<int32_t> cnt(size_t(t.rows) + 1, s);
   cnt.zero();
-  GPP_LAUNCH(histogram, grid_stride_blocks(M.nnz), kThreads, 0, s, M.idx, M.nnz, cnt.p);
+  const int g = grid_stride_blocks(M.nnz);
+  GPP_LAUNCH(histogram, g, kThreads, 0, s, M.idx, M.nnz, cnt.p);
   exclusive_scan_i32(cnt.p, t.ptr, t.rows, s);
-  DBuf<int32_t> cursor(size_t(t.rows), s);
-  cursor.copy_from(t.ptr, size_t(t.rows));
-  GPP_LAUNCH(scatter_rows, grid_stride_blocks(M.rows), kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, cursor.p,
-             t.idx, t.val);
-  GPP_LAUNCH(sort_rows_short, grid_stride_blocks(t.rows), kThreads, 0, s, t.rows, t.ptr, t.idx, t.val);
-  RowSchedule sch;
-  build_schedule(sch, t, nullptr, s);
-  DBuf<int32_t> sidx(size_t(M.nnz), s);
-  DBuf<double> sval(size_t(M.nnz), s);
-  // Rows longer than 32 are in the medium or long queue.
-  GPP_LAUNCH(sort_rows_long, roles_medium(t.rows), kThreads, 0, s, sch.medium.p, sch.counts.p, t.ptr, t.idx,
-             t.val, sidx.p, sval.p);
-  GPP_LAUNCH(sort_rows_long, roles_long(t.rows), kThreads, 0, s, sch.long_rows.p, sch.counts.p + 1, t.ptr,
-             t.idx, t.val, sidx.p, sval.p);
+  DBuf<uint64_t> keys(size_t(M.nnz), s);
+  DBuf<int32_t> pos(size_t(M.nnz), s), row(size_t(M.nnz), s);
+  GPP_LAUNCH(transpose_keys, g, kThreads, 0, s, M.nnz, M.idx, keys.p, pos.p);
+  radix_sort_pairs(keys.p, pos.p, M.nnz, s);
+  GPP_LAUNCH(row_of_entry, std::max(1, std::min((M.rows + 7) / 8, kNumSMs * 16)), kThreads, 0, s, M.rows, M.ptr,
+             row.p);
+  GPP_LAUNCH(transpose_gather, g, kThreads, 0, s, M.nnz, pos.p, row.p, M.val, t.idx, t.val);
   return t;
 }
 

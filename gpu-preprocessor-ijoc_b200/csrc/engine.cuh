@@ -79,6 +79,11 @@ struct Stats {
   DBuf<uint8_t> empty_row, singleton_row, empty_col, singleton_col;
   DBuf<double> srow_val, scol_val;
   DBuf<unsigned long long> live_nnz;
+  // Incremental refresh: the masks the statistics describe, the rows and
+  // columns deleted since, and which of them need their flags recomputed.
+  bool valid = false;
+  DBuf<uint8_t> seen_row, seen_col, dirty_row, dirty_col;
+  DBuf<int32_t> deleted, counters;
 };
 
 struct WorkingLp {

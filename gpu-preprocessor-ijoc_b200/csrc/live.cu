@@ -29,17 +29,11 @@ __global__ void classify_rows(const offset_t* __restrict__ ptr, int m, const int
                               int32_t* __restrict__ medium, int32_t* __restrict__ longq,
                               int32_t* __restrict__ counts) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
   const int len = row < m ? row_len(ptr, live_deg, row) : 0;
   for (int g = 0; g < 2; ++g) {
     const bool sel = row < m && (g == 0 ? (len > kShortRow && len <= kLongRow) : len > kLongRow);
-    const unsigned mask = __ballot_sync(0xffffffffu, sel);
-    if (!mask) continue;
-    const int leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(counts + g, __popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (sel) (g == 0 ? medium : longq)[base + __popc(mask & ((1u << lane) - 1u))] = row;
+    const int at = block_append(counts + g, sel);
+    if (sel) (g == 0 ? medium : longq)[at] = row;
   }
 }
 
@@ -388,16 +382,133 @@ void allocate_stats(Stats& st, int32_t m, int32_t n) {
   st.col_nnz.alloc(size_t(n), s); st.empty_col.alloc(size_t(n), s); st.singleton_col.alloc(size_t(n), s);
   st.scol_row.alloc(size_t(n), s); st.scol_val.alloc(size_t(n), s);
   st.live_nnz.alloc(1, s);
+  st.seen_row.alloc(size_t(m), s); st.seen_col.alloc(size_t(n), s);
+  st.dirty_row.alloc(size_t(m), s); st.dirty_col.alloc(size_t(n), s);
+  st.dirty_row.zero(); st.dirty_col.zero();
+  st.deleted.alloc(size_t(m) + size_t(n), s);
+  st.counters.alloc(2, s);
+  st.valid = false;
 }
+
+namespace {
+
+// ---- incremental refresh ---------------------------------------------------
+//
+// Masks only lose entries between two materialisations, so the statistics of
+// the current masks follow from those of the previous ones: a deleted row
+// takes one off the degree of every still-kept column it touches (and a
+// deleted column likewise for rows), the live total drops by the entries that
+// stopped being live, and only rows / columns whose degree changed need their
+// empty / singleton flags and singleton support recomputed.  The result is
+// the full recount's exactly (integer counts, and the support of a degree-1
+// row is its only live entry).
+
+// Rows (first m) and columns (next n) whose mask went from kept to deleted.
+__global__ void inc_deleted(int m, int n, const uint8_t* __restrict__ seen_row, const uint8_t* __restrict__ keep_row,
+                            const uint8_t* __restrict__ seen_col, const uint8_t* __restrict__ keep_col,
+                            int32_t* __restrict__ list, int32_t* counters) {
+  const int stride = gridDim.x * blockDim.x;
+  const int top = (max(m, n) + stride - 1) / stride * stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < top; i += stride) {
+    const bool dr = i < m && seen_row[i] && !keep_row[i];
+    const bool dc = i < n && seen_col[i] && !keep_col[i];
+    const int pr = block_append(counters, dr);
+    if (dr) list[pr] = i;
+    const int pc = block_append(counters + 1, dc);
+    if (dc) list[m + pc] = i;
+  }
+}
+
+// One warp per deleted outer item: its own statistics are reset, and every
+// still-kept inner item it touches loses one degree and is marked dirty.
+// `total` (rows only) drops by the item's old degree; `cross_total` (columns
+// only) drops by one per kept row it leaves.
+__global__ void inc_walk(const int32_t* __restrict__ list, const int32_t* __restrict__ count, const offset_t* __restrict__ ptr,
+                         const int32_t* __restrict__ idx, const uint8_t* __restrict__ keep_inner,
+                         int32_t* __restrict__ degree, uint8_t* __restrict__ empty, uint8_t* __restrict__ singleton,
+                         int32_t* __restrict__ support, double* __restrict__ coefficient,
+                         int32_t* __restrict__ inner_degree, uint8_t* __restrict__ inner_dirty,
+                         unsigned long long* total, unsigned long long* cross_total) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int k = *count;
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < k; w += warps) {
+    const int r = list[w];
+    unsigned int left = 0;
+    for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) {
+      const int c = idx[p];
+      if (keep_inner[c]) {
+        atomicSub(inner_degree + c, 1);
+        inner_dirty[c] = 1;
+        ++left;
+      }
+    }
+    for (int off = 16; off; off >>= 1) left += __shfl_down_sync(0xffffffffu, left, off);
+    if (lane == 0) {
+      if (total) atomicAdd(total, 0ULL - (unsigned long long)degree[r]);
+      if (cross_total && left) atomicAdd(cross_total, 0ULL - (unsigned long long)left);
+      degree[r] = 0; empty[r] = 0; singleton[r] = 0; support[r] = -1; coefficient[r] = 0.0;
+    }
+  }
+}
+
+// Flags of the dirty kept items; a degree-1 item finds its only live entry.
+__global__ void inc_fix(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                        const double* __restrict__ val, const uint8_t* __restrict__ keep_outer,
+                        const uint8_t* __restrict__ keep_inner, uint8_t* __restrict__ dirty,
+                        const int32_t* __restrict__ degree, uint8_t* __restrict__ empty,
+                        uint8_t* __restrict__ singleton, int32_t* __restrict__ support,
+                        double* __restrict__ coefficient) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    if (!dirty[r]) continue;
+    dirty[r] = 0;
+    if (!keep_outer[r]) continue;
+    const int d = degree[r];
+    empty[r] = d == 0;
+    singleton[r] = d == 1;
+    int sup = -1;
+    double coef = 0.0;
+    if (d == 1)
+      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p)
+        if (keep_inner[idx[p]]) { sup = idx[p]; coef = val[p]; }
+    support[r] = sup;
+    coefficient[r] = coef;
+  }
+}
+
+}  // namespace
 
 void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
   // refresh_live_stats (gpu_presolve_kernels.cu:493-517).
   auto s = ctx().stream;
-  st.live_nnz.zero();
-  live_stats_side(lp.A, plan.keep_row.p, plan.keep_col.p, st.row_nnz.p, st.empty_row.p, st.singleton_row.p,
-                  st.srow_col.p, st.srow_val.p, st.live_nnz.p, s);
-  live_stats_side(lp.AT, plan.keep_col.p, plan.keep_row.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p,
-                  st.scol_row.p, st.scol_val.p, nullptr, s);
+  const int m = lp.m(), n = lp.n();
+  if (!st.valid) {
+    st.live_nnz.zero();
+    live_stats_side(lp.A, plan.keep_row.p, plan.keep_col.p, st.row_nnz.p, st.empty_row.p, st.singleton_row.p,
+                    st.srow_col.p, st.srow_val.p, st.live_nnz.p, s);
+    live_stats_side(lp.AT, plan.keep_col.p, plan.keep_row.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p,
+                    st.scol_row.p, st.scol_val.p, nullptr, s);
+  } else {
+    st.counters.zero();
+    GPP_LAUNCH(inc_deleted, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, m, n, st.seen_row.p, plan.keep_row.p,
+               st.seen_col.p, plan.keep_col.p, st.deleted.p, st.counters.p);
+    const int g = kNumSMs * 8;
+    GPP_LAUNCH(inc_walk, g, kThreads, 0, s, st.deleted.p, st.counters.p, lp.A.ptr, lp.A.idx, plan.keep_col.p,
+               st.row_nnz.p, st.empty_row.p, st.singleton_row.p, st.srow_col.p, st.srow_val.p, st.col_nnz.p,
+               st.dirty_col.p, st.live_nnz.p, nullptr);
+    GPP_LAUNCH(inc_walk, g, kThreads, 0, s, st.deleted.p + m, st.counters.p + 1, lp.AT.ptr, lp.AT.idx,
+               plan.keep_row.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p, st.scol_row.p, st.scol_val.p,
+               st.row_nnz.p, st.dirty_row.p, nullptr, st.live_nnz.p);
+    GPP_LAUNCH(inc_fix, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p,
+               plan.keep_col.p, st.dirty_row.p, st.row_nnz.p, st.empty_row.p, st.singleton_row.p, st.srow_col.p,
+               st.srow_val.p);
+    GPP_LAUNCH(inc_fix, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val, plan.keep_col.p,
+               plan.keep_row.p, st.dirty_col.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p, st.scol_row.p,
+               st.scol_val.p);
+  }
+  st.seen_row.copy_from(plan.keep_row.p, size_t(m));
+  st.seen_col.copy_from(plan.keep_col.p, size_t(n));
+  st.valid = true;
 }
 
 void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,

@@ -34,6 +34,10 @@ namespace gpp {
 namespace {
 
 constexpr int kRounds = 8;
+// Rows longer than this with at most kBlockMergeDeltas deltas are rebuilt by
+// a block (dt_rebuild_block) instead of one lane.
+constexpr int kBlockMergeRow = 64;
+constexpr int kBlockMergeDeltas = 2048;
 constexpr double kMaxPivotRatio = 1.0e3;
 enum { kStInfeasible = 0, kStAny = 1, kStSubst = 2, kStFixed = 3, kStTouched = 4, kStWords = 5 };
 enum : uint8_t { kPairNone = 0, kPairSubst = 1, kPairFixed = 2 };
@@ -470,10 +474,127 @@ __global__ void dt_rebuild(int m, const offset_t* __restrict__ ptr, const int32_
         out += __popc(mask);
       }
       if (!Write && lane == 0) cnt[r] = int32_t(out);
+    } else if (sorted && p1 - p0 > kBlockMergeRow && q1 - q0 <= kBlockMergeDeltas) {
+      continue;  // dt_rebuild_block
     } else if (lane == 0) {
       if (Write) merge_row<true>(p0, p1, idx, val, q0, q1, dcol, dv, zt, oidx + optr[r], oval + optr[r]);
       else cnt[r] = merge_row<false>(p0, p1, idx, val, q0, q1, dcol, dv, zt, nullptr, nullptr);
     }
+  }
+}
+
+// Long rows with deltas (of a strictly sorted matrix): the rows the warp
+// kernel leaves out, listed once.
+__global__ void dt_long_delta_rows(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ dptr,
+                                   int32_t* __restrict__ list, int32_t* counter) {
+  const int stride = gridDim.x * blockDim.x;
+  const int top = (m + stride - 1) / stride * stride;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < top; r += stride) {
+    const bool take = r < m && dptr[r + 1] > dptr[r] && ptr[r + 1] - ptr[r] > kBlockMergeRow &&
+                      dptr[r + 1] - dptr[r] <= kBlockMergeDeltas;
+    const int at = block_append(counter, take);
+    if (take) list[at] = r;
+  }
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sm, int& total) {
+  sm[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < kThreads; off <<= 1) {
+    const int t = threadIdx.x >= unsigned(off) ? sm[threadIdx.x - off] : 0;
+    __syncthreads();
+    sm[threadIdx.x] += t;
+    __syncthreads();
+  }
+  total = sm[kThreads - 1];
+  const int ex = sm[threadIdx.x] - v;
+  __syncthreads();
+  return ex;
+}
+
+// The same merge as merge_row, one block per row: source entries are merged
+// with their matching delta in parallel, the deltas without a source entry
+// ("new" deltas, few) are placed by binary search, and block scans give every
+// kept entry its output slot.  Valid for strictly sorted rows and sorted,
+// unique delta columns.
+template <bool Write>
+__global__ void __launch_bounds__(kThreads)
+dt_rebuild_block(const int32_t* __restrict__ list, const int32_t* __restrict__ count, const offset_t* __restrict__ ptr,
+                 const int32_t* __restrict__ idx, const double* __restrict__ val, const int32_t* __restrict__ dptr,
+                 const int32_t* __restrict__ dcol, const double* __restrict__ dv, double zt, int32_t* __restrict__ cnt,
+                 const offset_t* __restrict__ optr, int32_t* __restrict__ oidx, double* __restrict__ oval) {
+  __shared__ int scan[kThreads];
+  __shared__ int kcol[kBlockMergeDeltas];
+  __shared__ int kins[kBlockMergeDeltas];
+  __shared__ double kval[kBlockMergeDeltas];
+  const int rows = *count;
+  for (int q = blockIdx.x; q < rows; q += gridDim.x) {
+    const int r = list[q];
+    const offset_t p0 = ptr[r];
+    const int len = int(ptr[r + 1] - p0);
+    const int q0 = dptr[r], nd = dptr[r + 1] - q0;
+    // New deltas (no source entry in their column) that survive, in column order.
+    int nk = 0;
+    for (int c0 = 0; c0 < nd; c0 += kThreads) {
+      const int d = c0 + threadIdx.x;
+      int flag = 0, col = 0, ins = 0;
+      double v = 0.0;
+      if (d < nd) {
+        col = dcol[q0 + d];
+        int lo = 0, hi = len;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (idx[p0 + mid] < col) lo = mid + 1; else hi = mid; }
+        ins = lo;
+        v = 0.0 + dv[q0 + d];
+        flag = (lo == len || idx[p0 + lo] != col) && fabs(v) > zt;
+      }
+      int total;
+      const int ex = block_exclusive_scan(flag, scan, total);
+      if (flag) { kcol[nk + ex] = col; kins[nk + ex] = ins; kval[nk + ex] = v; }
+      nk += total;
+      __syncthreads();
+    }
+    const offset_t base = Write ? optr[r] : 0;
+    int running = 0;
+    for (int c0 = 0; c0 < len; c0 += kThreads) {
+      const int i = c0 + threadIdx.x;
+      int keep = 0, col = 0;
+      double merged = 0.0;
+      if (i < len) {
+        col = idx[p0 + i];
+        merged = 0.0 + val[p0 + i];
+        int lo = 0, hi = nd;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (dcol[q0 + mid] < col) lo = mid + 1; else hi = mid; }
+        if (lo < nd && dcol[q0 + lo] == col) merged += dv[q0 + lo];
+        keep = fabs(merged) > zt;
+      }
+      int total;
+      const int ex = block_exclusive_scan(keep, scan, total);
+      if (Write && i < len) {
+        // New deltas inserted before source entry i: kins <= i.
+        int lo = 0, hi = nk;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (kins[mid] <= i) lo = mid + 1; else hi = mid; }
+        if (keep) {
+          oidx[base + running + ex + lo] = col;
+          oval[base + running + ex + lo] = merged;
+        }
+        // The new deltas that sit right before entry i.
+        int first = lo;
+        while (first > 0 && kins[first - 1] == i) --first;
+        for (int t = first; t < lo; ++t) {
+          oidx[base + running + ex + t] = kcol[t];
+          oval[base + running + ex + t] = kval[t];
+        }
+      }
+      running += total;
+    }
+    if (Write) {
+      // New deltas after the last source entry.
+      for (int t = threadIdx.x; t < nk; t += kThreads)
+        if (kins[t] == len) { oidx[base + running + t] = kcol[t]; oval[base + running + t] = kval[t]; }
+    } else if (threadIdx.x == 0) {
+      cnt[r] = running + nk;
+    }
+    __syncthreads();
   }
 }
 
@@ -776,9 +897,16 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
     }
     exclusive_scan_i32(row_cnt.p, dptr.p, m, s);
     const bool a_sorted = rows_strictly_sorted(lp.A, s);
-    DBuf<int32_t> cnt(size_t(m) + 1, s);
+    DBuf<int32_t> cnt(size_t(m) + 1, s), long_rows(size_t(m), s), long_count(1, s);
+    long_count.zero();
+    if (a_sorted)
+      GPP_LAUNCH(dt_long_delta_rows, grid_stride_blocks(m), kThreads, 0, s, m, lp.A.ptr, dptr.p, long_rows.p,
+                 long_count.p);
     GPP_LAUNCH(dt_rebuild<false>, warp_grid(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val, dptr.p, dcol.p,
                dv.p, zt, a_sorted, cnt.p, nullptr, nullptr, nullptr);
+    if (a_sorted)
+      GPP_LAUNCH(dt_rebuild_block<false>, kNumSMs * 4, kThreads, 0, s, long_rows.p, long_count.p, lp.A.ptr, lp.A.idx,
+                 lp.A.val, dptr.p, dcol.p, dv.p, zt, cnt.p, nullptr, nullptr, nullptr);
     DevCsr out;
     out.rows = m;
     out.cols = n;
@@ -789,6 +917,9 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
     out.val = dalloc<double>(size_t(out.nnz));
     GPP_LAUNCH(dt_rebuild<true>, warp_grid(m), kThreads, 0, s, m, lp.A.ptr, lp.A.idx, lp.A.val, dptr.p, dcol.p,
                dv.p, zt, a_sorted, nullptr, out.ptr, out.idx, out.val);
+    if (a_sorted)
+      GPP_LAUNCH(dt_rebuild_block<true>, kNumSMs * 4, kThreads, 0, s, long_rows.p, long_count.p, lp.A.ptr, lp.A.idx,
+                 lp.A.val, dptr.p, dcol.p, dv.p, zt, nullptr, out.ptr, out.idx, out.val);
     if (plan.has_new_A) free_csr(plan.new_A);
     plan.new_A = out;
     plan.has_new_A = true;

@@ -312,7 +312,9 @@ __global__ void count_guard_groups(int count, const uint64_t* __restrict__ sh, c
                                    double coeff_tol, double obj_tol, double max_abs, int max_size, int stop_after,
                                    int32_t* __restrict__ out) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
-    if (atomicAdd(out, 0) >= stop_after) return;
+    // Early exit once enough groups are counted: a plain (volatile) read, as
+    // an atomic read of one address from every thread serialises them.
+    if (*(volatile int32_t*)out >= stop_after) return;
     const uint64_t hs = sh[s];
     if (s > 0 && sh[s - 1] == hs) continue;
     int e = s;

@@ -62,7 +62,7 @@ __global__ void sc_candidates(int n, int m, const uint8_t* __restrict__ keep_col
                               int32_t* __restrict__ owner, int32_t* __restrict__ cand, int32_t* __restrict__ rows,
                               int32_t* __restrict__ long_rows, int32_t* st) {
   const int stride = gridDim.x * blockDim.x;
-  const int top = (n + 31) / 32 * 32;
+  const int top = (n + stride - 1) / stride * stride;   // every thread of a block runs the same trips
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < top; j += stride) {
     bool take = false, claim = false, is_long = false;
     if (j < n && keep_col[j] && singleton[j]) {
@@ -78,11 +78,11 @@ __global__ void sc_candidates(int n, int m, const uint8_t* __restrict__ keep_col
         }
       }
     }
-    const int pc = warp_append(st + kStCand, take);
+    const int pc = block_append(st + kStCand, take);
     if (take) cand[pc] = j;
-    const int pr = warp_append(st + kStRows, claim);
+    const int pr = block_append(st + kStRows, claim);
     if (claim) rows[pr] = srow[j];
-    const int pl = warp_append(st + kStLong, is_long);
+    const int pl = block_append(st + kStLong, is_long);
     if (is_long) long_rows[pl] = srow[j];
   }
 }
@@ -290,8 +290,9 @@ __global__ void sc_stage(const int32_t* __restrict__ rows, int32_t* st, int n, c
                          int32_t* __restrict__ winners, int64_t* __restrict__ contrib_idx,
                          double* __restrict__ contrib_val) {
   const int count = st[kStRows];
-  const int top = (count + 31) / 32 * 32;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < top; q += gridDim.x * blockDim.x) {
+  const int stride = gridDim.x * blockDim.x;
+  const int top = (count + stride - 1) / stride * stride;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < top; q += stride) {
     int row = -1, j = -1;
     uint8_t k = 0;
     double contrib = 0.0;
@@ -344,9 +345,9 @@ __global__ void sc_stage(const int32_t* __restrict__ rows, int32_t* st, int n, c
       if (k) kind[row] = k;
     }
     const bool elim = k == kRowElimKept || k == kRowElimDeleted;
-    const int pe = warp_append(st + kStElim, elim);
+    const int pe = block_append(st + kStElim, elim);
     if (elim) { contrib_idx[pe] = j; contrib_val[pe] = contrib; }
-    const int pw = warp_append(st + kStWin, k != 0);
+    const int pw = block_append(st + kStWin, k != 0);
     if (k) winners[pw] = row;
   }
 }

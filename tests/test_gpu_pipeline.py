@@ -135,10 +135,3 @@ def test_identity_when_presolve_disabled():
         assert s.reduced_lp.A.rowPtr == dlp.t["A_ptr"].data_ptr()
     finally:
         device.free_summary(s)
-
-
-def test_folding_request_fails_loudly_until_built():
-    lp = lpgen.random_lp(200, 500, seed=1)
-    dlp = device.DeviceLp(lp)
-    with pytest.raises(RuntimeError):
-        device.preprocess(dlp, params_with_rules(BUILT, enable_folding=1))

@@ -75,7 +75,7 @@ needs_reference = pytest.mark.skipif(not os.path.exists(DRIVER), reason="referen
 def check_against_reference(lp, rules, extra=None):
     extra = extra or {}
     ref = run_reference(lp, rules, [f"{k}={v}" for k, v in extra.items()])
-    params = params_with_rules(rules, enable_folding=0, **extra)
+    params = params_with_rules(rules, **{"enable_folding": 0, **extra})
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
     try:
