@@ -159,7 +159,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     lib = capi.load()
     lp = lpgen.workload(args.workload, seed=0)
-    params = params_with_rules(RULES, enable_folding=0)
+    params = params_with_rules(RULES, enable_folding=1)
     dlp = device.DeviceLp(lp)
     stream = torch.cuda.current_stream()
 
@@ -173,6 +173,7 @@ def main():
             red = (torch.from_numpy(x0).cuda(), torch.zeros(s.reduced_rows, dtype=torch.float64, device="cuda"),
                    torch.zeros(s.reduced_cols, dtype=torch.float64, device="cuda"))
             reduced = (s.reduced_rows, s.reduced_cols, s.reduced_nnz, s.iterations)
+            folded = s.folding_applied
         device.postprocess(*red, s, dlp)
         device.free_summary(s)
     torch.cuda.synchronize()
@@ -274,7 +275,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD_DESC, "rows": lp.m, "cols": lp.n, "nnz": lp.nnz,
-                       "rules": RULES, "folding": False,
+                       "rules": RULES, "folding": True, "folding_applied": bool(folded),
                        "reduced": {"rows": reduced[0], "cols": reduced[1], "nnz": reduced[2], "iterations": reduced[3]},
                        "presolve_ms": round(statistics.mean(pre_ms), 3),
                        "l2": "inputs (~1 GB) larger than L2; no flush",

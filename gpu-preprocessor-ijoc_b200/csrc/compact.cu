@@ -44,7 +44,7 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
       const int nr = outer_map[r];
       if (nr < 0) continue;
       int c = 0;
-      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) c += inner_map[idx[p]] >= 0;
+      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) c += inner_map[__ldcs(idx + p)] >= 0;
       out_counts[nr] = c;
     }
     return;
@@ -57,7 +57,7 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
       const int nr = outer_map[r];
       if (nr < 0) continue;
       int c = 0;
-      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) c += inner_map[idx[p]] >= 0;
+      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) c += inner_map[__ldcs(idx + p)] >= 0;
       for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
       if (lane == 0) out_counts[nr] = c;
     }
@@ -69,7 +69,7 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
     const int nr = outer_map[r];
     if (nr < 0) continue;  // block-uniform
     int c = 0;
-    for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads) c += inner_map[idx[p]] >= 0;
+    for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads) c += inner_map[__ldcs(idx + p)] >= 0;
     for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
     if ((threadIdx.x & 31) == 0) scount[threadIdx.x >> 5] = c;
     __syncthreads();
@@ -98,8 +98,8 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
       if (nr < 0) continue;
       offset_t w = out_ptr[nr];
       for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) {
-        const int c = inner_map[idx[p]];
-        if (c >= 0) { out_idx[w] = c; out_val[w] = val[p]; ++w; }
+        const int c = inner_map[__ldcs(idx + p)];
+        if (c >= 0) { out_idx[w] = c; out_val[w] = __ldcs(val + p); ++w; }
       }
     }
     return;
@@ -114,12 +114,12 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
       offset_t w = out_ptr[nr];
       for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += 32) {
         const offset_t p = chunk + lane;
-        const int c = p < ptr[r + 1] ? inner_map[idx[p]] : -1;
+        const int c = p < ptr[r + 1] ? inner_map[__ldcs(idx + p)] : -1;
         const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
         if (c >= 0) {
           const offset_t o = w + __popc(mask & ((1u << lane) - 1u));
           out_idx[o] = c;
-          out_val[o] = val[p];
+          out_val[o] = __ldcs(val + p);
         }
         w += __popc(mask);
       }
@@ -135,7 +135,7 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
     offset_t w = out_ptr[nr];
     for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += kThreads) {
       const offset_t p = chunk + threadIdx.x;
-      const int c = p < ptr[r + 1] ? inner_map[idx[p]] : -1;
+      const int c = p < ptr[r + 1] ? inner_map[__ldcs(idx + p)] : -1;
       const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
       if (lane == 0) wcount[warp] = __popc(mask);
       __syncthreads();
@@ -144,7 +144,7 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
       if (c >= 0) {
         const offset_t o = w + before + __popc(mask & ((1u << lane) - 1u));
         out_idx[o] = c;
-        out_val[o] = val[p];
+        out_val[o] = __ldcs(val + p);
       }
       w += total;
       __syncthreads();

@@ -73,16 +73,16 @@ struct ActivityTerm {
   const double* u;
   double zero_tol;
   __device__ __forceinline__ void operator()(offset_t p, double& lo, double& hi, int& ni, int& pi) const {
-    const double a = val[p];
+    const double a = __ldcs(val + p);   // streamed once: keep L2 for the gathered bounds
     if constexpr (Plain) {
       // Plain sums of the redundant-row test: infinities propagate.
-      const int col = idx[p];
+      const int col = __ldcs(idx + p);
       lo += a >= 0.0 ? a * l[col] : a * u[col];
       hi += a >= 0.0 ? a * u[col] : a * l[col];
       return;
     }
     if (fabs(a) <= zero_tol) return;
-    const int col = idx[p];
+    const int col = __ldcs(idx + p);
     const double tlo = a >= 0.0 ? a * l[col] : a * u[col];
     const double thi = a >= 0.0 ? a * u[col] : a * l[col];
     if (isfinite(tlo)) lo += tlo; else if (tlo < 0.0) ++ni;
@@ -111,7 +111,7 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
       for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
-        if ((keep_row && !keep_row[i]) || (keep_col && !keep_col[idx[p]])) continue;
+        if ((keep_row && !keep_row[i]) || (keep_col && !keep_col[__ldcs(idx + p)])) continue;
         term(p, lo, hi, ni, pi);
       }
       min_fin[i] = lo; max_fin[i] = hi;
@@ -199,7 +199,7 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
       offset_t pos = -1;
       if (active)
         for (offset_t p = first; p < last; ++p)
-          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+          if (!keep_inner || keep_inner[__ldcs(idx + p)]) { ++count; pos = p; }
       stats_write(r, active, count, pos, idx, val, degree, empty, singleton, support, coefficient, nullptr);
       acc += unsigned(count);
     }
@@ -213,7 +213,7 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
       long long pos = -1;
       if (active)
         for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
-          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+          if (!keep_inner || keep_inner[__ldcs(idx + p)]) { ++count; pos = p; }
       for (int off = 16; off; off >>= 1) {
         count += __shfl_down_sync(0xffffffffu, count, off);
         pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
@@ -232,7 +232,7 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
       long long pos = -1;
       if (active)
         for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads)
-          if (!keep_inner || keep_inner[idx[p]]) { ++count; pos = p; }
+          if (!keep_inner || keep_inner[__ldcs(idx + p)]) { ++count; pos = p; }
       for (int off = 16; off; off >>= 1) {
         count += __shfl_down_sync(0xffffffffu, count, off);
         pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));

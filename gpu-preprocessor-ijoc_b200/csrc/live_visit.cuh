@@ -22,7 +22,7 @@ __device__ __forceinline__ void live_visit(offset_t first, offset_t last, const 
   int carry = 0;
   for (offset_t chunk = first; chunk < last; chunk += W) {
     const offset_t p = chunk + lane;
-    const bool live = p < last && keep[idx[p]];
+    const bool live = p < last && keep[__ldcs(idx + p)];
     const unsigned mask = __ballot_sync(0xffffffffu, live);
     int rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
     int c = __popc(mask);

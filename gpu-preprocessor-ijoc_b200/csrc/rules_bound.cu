@@ -81,14 +81,23 @@ struct CandArgs {
   double* cand_u;
 };
 
-__device__ __forceinline__ void candidate_entry(const CandArgs& g, int i, offset_t p) {
-  const int j = g.idx[p];
+// The row's sides and activity summary, loaded once per row.
+struct RowCtx {
+  double al, au, mn, mx;
+  int ni, pi;
+};
+__device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
+  return RowCtx{g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i]};
+}
+
+__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p) {
+  const int j = __ldcs(g.idx + p);   // CSR streamed once: keep L2 for the gathered bounds
   if (!g.keep_col[j]) return;
-  const double a = g.val[p];
+  const double a = __ldcs(g.val + p);
   if (fabs(a) <= g.zero_tol) return;
   const double ol = g.l[j], ou = g.u[j];
   double il, iu;
-  implied_bounds(a, ol, ou, g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i], il, iu);
+  implied_bounds(a, ol, ou, rc.al, rc.au, rc.mn, rc.mx, rc.ni, rc.pi, il, iu);
   double nl = ol, nu = ou;
   if (isfinite(il)) nl = fmax(nl, il);
   if (isfinite(iu)) nu = fmin(nu, iu);
@@ -96,32 +105,47 @@ __device__ __forceinline__ void candidate_entry(const CandArgs& g, int i, offset
   if (nu < ou) atomic_min_d(&g.cand_u[j], nu);
 }
 
+// Entry-parallel form of the candidate sweep: the candidates are combined by
+// atomic max / min, which is order-free, so instead of row roles every thread
+// takes consecutive stored entries (coalesced loads, full memory-level
+// parallelism) and finds their row by a binary search over the tile's row
+// pointers, staged in shared memory.
+constexpr int kEntryTile = 2048;
+constexpr int kTileRows = 2048;
+
+__device__ __forceinline__ int row_of(const offset_t* ptr, int lo, int hi, offset_t p) {
+  // Largest r in [lo, hi) with ptr[r] <= p.
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (ptr[mid] <= p) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(kThreads)
-candidates_kernel(int m, CandArgs g, const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
-                  const int32_t* __restrict__ counts, int short_blocks, int medium_blocks) {
-  const int b = blockIdx.x;
-  if (b < short_blocks) {
-    for (int i = b * blockDim.x + threadIdx.x; i < m; i += short_blocks * blockDim.x) {
-      if (g.ptr[i + 1] - g.ptr[i] > kShortRow || !g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-      for (offset_t p = g.ptr[i]; p < g.ptr[i + 1]; ++p) candidate_entry(g, i, p);
+candidates_entries(int m, offset_t nnz, CandArgs g) {
+  __shared__ offset_t sptr[kTileRows + 1];
+  __shared__ int srow[2];
+  for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
+    const offset_t last = min(nnz, base + kEntryTile) - 1;
+    if (threadIdx.x == 0) {
+      srow[0] = row_of(g.ptr, 0, m, base);
+      srow[1] = row_of(g.ptr, 0, m, last);
     }
-    return;
-  }
-  if (b < short_blocks + medium_blocks) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
-      const int i = medium[q];
+    __syncthreads();
+    const int r0 = srow[0], r1 = srow[1];
+    const bool staged = r1 - r0 + 1 <= kTileRows;
+    if (staged)
+      for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
+    __syncthreads();
+    for (int k = 0; k < kEntryTile / kThreads; ++k) {
+      const offset_t p = base + offset_t(k) * kThreads + threadIdx.x;
+      if (p > last) break;
+      const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
       if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-      for (offset_t p = g.ptr[i] + lane; p < g.ptr[i + 1]; p += 32) candidate_entry(g, i, p);
+      candidate_entry(g, row_ctx(g, i), p);
     }
-    return;
-  }
-  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
-  for (int q = lb; q < counts[1]; q += nlong) {
-    const int i = longq[q];
-    if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-    for (offset_t p = g.ptr[i] + threadIdx.x; p < g.ptr[i + 1]; p += kThreads) candidate_entry(g, i, p);
+    __syncthreads();
   }
 }
 
@@ -330,15 +354,13 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                        mn.p, mx.p, ni.p, pi.p, s);
   const RowSummary rs{mn.p, mx.p, ni.p, pi.p};
   {
-    const RowSchedule& sch = stored_schedule(lp.A);
-    const int sb = grid_stride_blocks(m, kThreads, 16), mb = std::min<int>(kNumSMs * 8, (m + 7) / 8),
-              lb = std::min<int>(kNumSMs * 4, m);
     CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, plan.keep_col.p, stats.row_nnz.p, plan.AL.p,
                plan.AU.p, plan.l.p, plan.u.p, rs, p.zero_tol, cl.p, cu.p};
     const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + double(n) + 4.0 * m + 16.0 * m + 24.0 * m +
                          16.0 * n + 16.0 * n;
-    GPP_LAUNCH_BYTES(candidates_kernel, bytes, sb + mb + lb, kThreads, 0, s, m, g, sch.medium.p, sch.long_rows.p, sch.counts.p,
-               sb, mb);
+    const int64_t tiles = (int64_t(lp.A.nnz) + kEntryTile - 1) / kEntryTile;
+    GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(tiles, kNumSMs * 8))),
+                     kThreads, 0, s, m, lp.A.nnz, g);
   }
   col_max_abs(lp.AT, plan.keep_row.p, vmax.p, s);
   DBuf<double> fl(size_t(n), s), fu(size_t(n), s), fixv(size_t(n), s);

@@ -43,26 +43,56 @@ __global__ void mark_touched_rows(int n, const offset_t* __restrict__ at_ptr, co
   }
 }
 
-// Row sums over selected columns in stored (ascending column) order; one
-// thread per touched row, every other row gets 0.
-__global__ void row_gather_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                  const double* __restrict__ val, const uint8_t* __restrict__ keep_row,
-                                  const uint8_t* __restrict__ touched, const uint8_t* __restrict__ selected,
+// Kept touched rows are listed; every other row's sum is 0.
+__global__ void list_touched_rows(int m, const uint8_t* __restrict__ keep_row, const uint8_t* __restrict__ touched,
+                                  int32_t* __restrict__ list, int32_t* counter, double* __restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  const int top = (m + stride - 1) / stride * stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < top; i += stride) {
+    const bool take = i < m && keep_row[i] && touched[i];
+    if (i < m && !take) out[i] = 0.0;
+    const int at = block_append(counter, take);
+    if (take) list[at] = i;
+  }
+}
+
+// Row sums over selected columns, added in stored (ascending column) order:
+// one warp per listed row computes 32 terms at a time and lane 0 adds them in
+// order, so long rows no longer serialise on one thread's loads.
+__global__ void row_gather_kernel(const int32_t* __restrict__ list, const int32_t* __restrict__ count,
+                                  const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                  const double* __restrict__ val, const uint8_t* __restrict__ selected,
                                   const double* __restrict__ value, const double* __restrict__ radius,
                                   double* __restrict__ out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int k = *count;
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < k; w += warps) {
+    const int i = list[w];
     double acc = 0.0;
-    if (keep_row[i] && touched[i])
-      for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
-        const int j = idx[p];
-        if (!selected[j]) continue;
-        if (radius) {
-          if (radius[j] > 0.0) acc += fabs(val[p]) * radius[j];
-        } else {
-          acc += val[p] * value[j];
+    for (offset_t chunk = ptr[i]; chunk < ptr[i + 1]; chunk += 32) {
+      const offset_t p = chunk + lane;
+      double term = 0.0;
+      bool has = false;
+      if (p < ptr[i + 1]) {
+        const int j = __ldcs(idx + p);
+        if (selected[j]) {
+          if (radius) {
+            if (radius[j] > 0.0) { has = true; term = fabs(__ldcs(val + p)) * radius[j]; }
+          } else {
+            has = true;
+            term = __ldcs(val + p) * value[j];
+          }
         }
       }
-    out[i] = acc;
+      const unsigned hv = __ballot_sync(0xffffffffu, has);
+      if (!hv) continue;
+      for (int q = 0; q < 32; ++q) {
+        const double v = __shfl_sync(0xffffffffu, term, q);
+        if (hv >> q & 1u) acc += v;
+      }
+    }
+    if (lane == 0) out[i] = acc;
   }
 }
 
@@ -198,11 +228,15 @@ __global__ void singleton_rows_commit(int m, int n, const uint8_t* __restrict__ 
 void row_gather_shift(const DevCsr& A, const DevCsr& AT, const uint8_t* keep_row, const uint8_t* selected,
                       const double* value, const double* radius, double* out, cudaStream_t s) {
   DBuf<uint8_t> touched(size_t(std::max(A.rows, 1)), s);
+  DBuf<int32_t> list(size_t(std::max(A.rows, 1)), s), count(1, s);
   touched.zero();
+  count.zero();
   GPP_LAUNCH(mark_touched_rows, grid_stride_blocks(AT.rows), kThreads, 0, s, AT.rows, AT.ptr, AT.idx, selected, radius,
              touched.p);
-  GPP_LAUNCH(row_gather_kernel, grid_stride_blocks(A.rows), kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, keep_row,
-             touched.p, selected, value, radius, out);
+  GPP_LAUNCH(list_touched_rows, grid_stride_blocks(A.rows), kThreads, 0, s, A.rows, keep_row, touched.p, list.p,
+             count.p, out);
+  GPP_LAUNCH(row_gather_kernel, kNumSMs * 16, kThreads, 0, s, list.p, count.p, A.ptr, A.idx, A.val, selected, value,
+             radius, out);
 }
 
 double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_t n, cudaStream_t s) {

@@ -45,14 +45,49 @@ __global__ void digit_presence(const uint64_t* __restrict__ keys, int64_t n, uin
   if (threadIdx.x < 64 && local[threadIdx.x]) atomicOr(&seen[threadIdx.x], local[threadIdx.x]);
 }
 
-__global__ void digit_scatter(const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals, int64_t n, int shift,
-                              const int32_t* __restrict__ offsets, int64_t tiles, uint64_t* __restrict__ out_keys,
-                              int32_t* __restrict__ out_vals) {
-  __shared__ int32_t running[256];
+// Stable scatter of one tile: the tile's keys are first ranked into a
+// digit-sorted order in shared memory (warp ranks from __match_any_sync,
+// warps ordered through shared counters, rounds in tile order), then written
+// out so consecutive threads store consecutive slots of one digit's run:
+// coalesced runs instead of one sector per key.
+__global__ void __launch_bounds__(kThreads)
+digit_scatter(const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals, int64_t n, int shift,
+              const int32_t* __restrict__ offsets, int64_t tiles, uint64_t* __restrict__ out_keys,
+              int32_t* __restrict__ out_vals) {
+  __shared__ int32_t running[256];      // next tile-local slot of each digit
+  __shared__ int32_t digit_start[256];  // tile-local start of each digit's run
+  __shared__ int32_t global_start[256]; // global position of the run's first slot
   __shared__ int32_t warp_digit_count[8][256];
+  __shared__ uint64_t local_keys[kTile];
+  __shared__ int32_t local_vals[kTile];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  running[threadIdx.x] = offsets[int64_t(threadIdx.x) * tiles + blockIdx.x];
   const int64_t base = int64_t(blockIdx.x) * kTile;
+  const int tile_n = int(min(int64_t(kTile), n - base));
+  // Tile-local digit counts (the scan of the digit-major table gives the
+  // global start of this tile's run of each digit).
+  global_start[threadIdx.x] = offsets[int64_t(threadIdx.x) * tiles + blockIdx.x];
+  running[threadIdx.x] = 0;
+  __syncthreads();
+  for (int k = 0; k < kItems; ++k) {
+    const int64_t i = base + int64_t(k) * kThreads + threadIdx.x;
+    if (i < n) atomicAdd(&running[int((keys[i] >> shift) & 0xff)], 1);
+  }
+  __syncthreads();
+  // Exclusive scan of the 256 tile counts (one thread per digit).
+  {
+    __shared__ int32_t scan[256];
+    scan[threadIdx.x] = running[threadIdx.x];
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+      const int32_t t = threadIdx.x >= unsigned(off) ? scan[threadIdx.x - off] : 0;
+      __syncthreads();
+      scan[threadIdx.x] += t;
+      __syncthreads();
+    }
+    digit_start[threadIdx.x] = scan[threadIdx.x] - running[threadIdx.x];
+    running[threadIdx.x] = digit_start[threadIdx.x];
+  }
+  __syncthreads();
   for (int k = 0; k < kItems; ++k) {
     // Elements of this round: consecutive within the round, warp-major.
     const int64_t i = base + int64_t(k) * kThreads + threadIdx.x;
@@ -65,20 +100,27 @@ __global__ void digit_scatter(const uint64_t* __restrict__ keys, const int32_t* 
     __syncthreads();
     if (valid && rank_in_warp == 0) warp_digit_count[warp][d] = __popc(peers);
     __syncthreads();
-    int before = 0;
-    if (valid)
-      for (int w = 0; w < warp; ++w) before += warp_digit_count[w][d];
     if (valid) {
-      const int64_t dst = int64_t(running[d]) + before + rank_in_warp;
-      out_keys[dst] = key;
-      out_vals[dst] = vals[i];
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += warp_digit_count[w][d];
+      const int slot = running[d] + before + rank_in_warp;
+      local_keys[slot] = key;
+      local_vals[slot] = vals[i];
     }
     __syncthreads();
-    // Advance the running offsets by this round's per-digit totals.
     int total = 0;
     for (int w = 0; w < 8; ++w) total += warp_digit_count[w][threadIdx.x];
     running[threadIdx.x] += total;
     __syncthreads();
+  }
+  // Write the digit-sorted tile: slot q of digit d goes to global_start[d] +
+  // (q - digit_start[d]).
+  for (int q = threadIdx.x; q < tile_n; q += kThreads) {
+    const uint64_t key = local_keys[q];
+    const int d = int((key >> shift) & 0xff);
+    const int64_t dst = int64_t(global_start[d]) + (q - digit_start[d]);
+    out_keys[dst] = key;
+    out_vals[dst] = local_vals[q];
   }
 }
 
