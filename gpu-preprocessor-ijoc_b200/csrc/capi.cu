@@ -443,6 +443,14 @@ int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, void* stre
   return guarded([&] { gpp::radix_sort_pairs_static(keys, values, n, static_cast<cudaStream_t>(stream)); });
 }
 
+int gpp_device_alloc(void** ptr, size_t bytes) {
+  return guarded([&] {
+    if (!ptr) throw std::invalid_argument("null argument");
+    *ptr = nullptr;
+    if (bytes) check(cudaMalloc(ptr, bytes), "cudaMalloc");
+  });
+}
+
 void gpp_device_free(void* p) {
   if (!p) return;
   try {

@@ -157,6 +157,7 @@ def load():
         "gpp_sort_pairs_static": (C.c_int, [vp, vp, i64, vp]),
         "gpp_export_folding_map": (C.c_int, [C.POINTER(Summary), vp, vp, vp, vp]),
         "gpp_unfold_solution": (C.c_int, [C.POINTER(Summary), vp, vp, vp, vp, vp, vp]),
+        "gpp_device_alloc": (C.c_int, [C.POINTER(vp), C.c_size_t]),
         "gpp_device_free": (None, [vp]),
         "gpp_last_error": (C.c_char_p, []),
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
@@ -175,7 +176,7 @@ EXPORTED = [
     "gpp_default_params", "gpp_preprocess", "gpp_run_presolve", "gpp_postprocess",
     "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
-    "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_free",
+    "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_alloc", "gpp_device_free",
     "gpp_export_folding_map", "gpp_unfold_solution",
     "gpp_last_error", "gpp_kernel_launches", "gpp_profile_enable", "gpp_profile_read",
 ]

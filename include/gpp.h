@@ -312,6 +312,11 @@ GPP_API int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n);
 #define GPP_SORT_STATIC_MAX_PAIRS (1 << 20)
 GPP_API int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, void* stream);
 
+/* Device allocation of `bytes` bytes with cudaMalloc (the C++ layer's
+ * postsolve_gpu returns such arrays, as the reference's does,
+ * cpp/src/presolve/gpu_postsolve.cu:545-556).  Release with gpp_device_free or
+ * cudaFree.  bytes = 0 gives NULL. */
+GPP_API int gpp_device_alloc(void** device_ptr, size_t bytes);
 GPP_API void gpp_device_free(void* device_ptr);
 
 /* Last error message of the calling thread ("" when none). */
