@@ -137,6 +137,8 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) loop")
+    ap.add_argument("--kernel-table-out", default=None,
+                    help="write every kernel's launches, ms and bytes per step to this CSV file")
     ap.add_argument("--no-kernel-table", action="store_true",
                     help="skip the extra pass that times every kernel with CUDA events")
     args = ap.parse_args()
@@ -198,6 +200,7 @@ def main():
 
     clocks = Clocks(local)
     lib.gpp_kernel_launches(1)
+    lib.gpp_host_syncs(1)
     barrier()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
@@ -207,6 +210,7 @@ def main():
     clk = clocks.stop()
     step_ms = t0.elapsed_time(t1) / args.steps
     launches = int(lib.gpp_kernel_launches(0)) // args.steps
+    syncs = int(lib.gpp_host_syncs(0)) // args.steps
     # Per-kernel table for the roofline: the same steps again with every
     # launch bracketed by CUDA events (kept out of the timed region above).
     prof = []
@@ -217,6 +221,11 @@ def main():
         barrier()
         prof = capi.profile_read()
         lib.gpp_profile_enable(0)
+        if args.kernel_table_out and rank == 0:
+            with open(args.kernel_table_out, "w") as f:
+                f.write("kernel,launches_per_step,ms_per_step,bytes_per_step\n")
+                for n, l, m, b in sorted(prof, key=lambda r: -r[2]):
+                    f.write(f"{n},{l / args.steps:.1f},{m / args.steps:.4f},{b / args.steps:.0f}\n")
 
     # End to end through the C ABI from pinned host memory.
     host = {k: v.cpu().pin_memory() for k, v in dlp.t.items()}
@@ -281,6 +290,7 @@ def main():
                        "l2": "inputs (~1 GB) larger than L2; no flush",
                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "gpu_launches": launches,
+            "host_syncs_per_step": syncs,
             "e2e": None if e2e_ms is None else {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
                                                 "d2h_bytes_per_step": d2h},
             "roofline": roofline,

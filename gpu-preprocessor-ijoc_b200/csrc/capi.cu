@@ -491,4 +491,10 @@ uint64_t gpp_kernel_launches(int reset) {
   return v;
 }
 
+uint64_t gpp_host_syncs(int reset) {
+  const uint64_t v = gpp::sync_counter();
+  if (reset) gpp::sync_counter() = 0;
+  return v;
+}
+
 }  // extern "C"

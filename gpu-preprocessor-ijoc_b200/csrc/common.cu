@@ -11,6 +11,10 @@ uint64_t& launch_counter() {
   static thread_local uint64_t count = 0;
   return count;
 }
+uint64_t& sync_counter() {
+  static thread_local uint64_t n = 0;
+  return n;
+}
 
 Context::Context() {
   check(cudaGetDevice(&device), "cudaGetDevice");
@@ -58,81 +62,88 @@ const int32_t* Status::read(int words) {
 }
 
 namespace {
-constexpr int kScanTile = 2048;  // 256 threads x 8 items
+constexpr int kScanTile = 2048;  // 256 threads x 8 consecutive items
+constexpr int kScanWarps = kThreads / 32;
+
+// Block-wide sum of one value per thread (integers: any order); every
+// thread gets the result.  Contains __syncthreads.
+template <class T>
+__device__ __forceinline__ T block_total(T v, T* warp_sums) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = v;
+  __syncthreads();
+  T t = 0;
+#pragma unroll
+  for (int w = 0; w < kScanWarps; ++w) t += warp_sums[w];
+  __syncthreads();
+  return t;
+}
+
+// Block-wide exclusive scan of one value per thread, in thread order.
+// Contains __syncthreads.
+template <class T>
+__device__ __forceinline__ T block_exclusive(T v, T* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T peer = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += peer;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  T before = 0;
+#pragma unroll
+  for (int w = 0; w < kScanWarps; ++w) before += w < warp ? warp_sums[w] : T(0);
+  __syncthreads();
+  return before + incl - v;
+}
 
 template <class T>
-__global__ void tile_reduce(const T* __restrict__ in, int64_t n, T* __restrict__ tile_sums) {
-  __shared__ T sm[kThreads];
+__global__ void __launch_bounds__(kThreads) tile_reduce(const T* __restrict__ in, int64_t n, T* __restrict__ tile_sums) {
+  __shared__ T warp_sums[kScanWarps];
   const int64_t base = int64_t(blockIdx.x) * kScanTile;
   T acc = 0;
+#pragma unroll
   for (int k = 0; k < kScanTile / kThreads; ++k) {
     const int64_t i = base + int64_t(k) * kThreads + threadIdx.x;
     if (i < n) acc += in[i];
   }
-  sm[threadIdx.x] = acc;
-  __syncthreads();
-  for (int h = kThreads / 2; h > 0; h >>= 1) {
-    if (threadIdx.x < h) sm[threadIdx.x] += sm[threadIdx.x + h];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = sm[0];
+  acc = block_total(acc, warp_sums);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = acc;
 }
 
-// Exclusive scan of tile sums in one block of 1024 threads.
+// Each block scans its tile (thread t owns 8 consecutive items) from the sum
+// of all earlier tiles, which it adds up itself; the last block writes the
+// total to out[n].  `in` and `out` may alias: a thread reads its own items
+// before it writes them, and no thread touches another's.
 template <class T>
-__global__ void scan_tile_sums(T* sums, int64_t count, T* total_out) {
-  __shared__ T sm[1024];
-  const int64_t per = (count + 1023) / 1024;
-  const int64_t b = int64_t(threadIdx.x) * per;
-  T local = 0;
-  for (int64_t k = 0; k < per && b + k < count; ++k) local += sums[b + k];
-  sm[threadIdx.x] = local;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const T v = threadIdx.x >= unsigned(off) ? sm[threadIdx.x - off] : T(0);
-    __syncthreads();
-    sm[threadIdx.x] += v;
-    __syncthreads();
-  }
-  T run = threadIdx.x ? sm[threadIdx.x - 1] : T(0);
-  for (int64_t k = 0; k < per && b + k < count; ++k) {
-    const T v = sums[b + k];
-    sums[b + k] = run;
-    run += v;
-  }
-  if (threadIdx.x == 1023) *total_out = sm[1023];
-}
-
-// Each block rescans its tile: thread t owns 8 consecutive items.
-template <class T>
-__global__ void tile_scan(const T* __restrict__ in, int64_t n, const T* __restrict__ tile_offsets,
-                          T* __restrict__ out) {
-  __shared__ T sm[kThreads];
+__global__ void __launch_bounds__(kThreads) tile_scan(const T* __restrict__ in, int64_t n,
+                                                     const T* __restrict__ tile_sums, T* __restrict__ out) {
+  __shared__ T warp_sums[kScanWarps];
+  T offset = 0;
+  for (int k = threadIdx.x; k < int(blockIdx.x); k += kThreads) offset += tile_sums[k];
+  offset = block_total(offset, warp_sums);
   const int64_t base = int64_t(blockIdx.x) * kScanTile + int64_t(threadIdx.x) * 8;
   T v[8];
   T local = 0;
+#pragma unroll
   for (int k = 0; k < 8; ++k) {
     v[k] = base + k < n ? in[base + k] : T(0);
     local += v[k];
   }
-  sm[threadIdx.x] = local;
-  __syncthreads();
-  for (int off = 1; off < kThreads; off <<= 1) {
-    const T t = threadIdx.x >= unsigned(off) ? sm[threadIdx.x - off] : T(0);
-    __syncthreads();
-    sm[threadIdx.x] += t;
-    __syncthreads();
-  }
-  T run = tile_offsets[blockIdx.x] + (threadIdx.x ? sm[threadIdx.x - 1] : T(0));
+  T run = offset + block_exclusive(local, warp_sums);
+#pragma unroll
   for (int k = 0; k < 8; ++k) {
     if (base + k < n) out[base + k] = run;
     run += v[k];
   }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kThreads - 1) out[n] = run;
 }
 
-template <class T>
-__global__ void write_total(T* out, int64_t n, const T* total) { out[n] = *total; }
-
+// Exclusive scan of n items into out[0..n], out[n] the total: one launch up
+// to kScanTile items, two above.
 template <class T>
 void exclusive_scan(const T* in, T* out, int64_t n, cudaStream_t s) {
   if (n <= 0) {
@@ -140,13 +151,13 @@ void exclusive_scan(const T* in, T* out, int64_t n, cudaStream_t s) {
     return;
   }
   const int64_t tiles = (n + kScanTile - 1) / kScanTile;
-  DBuf<T> sums(size_t(tiles) + 1, s);
+  if (tiles == 1) {
+    GPP_LAUNCH(tile_scan<T>, 1, kThreads, 0, s, in, n, static_cast<const T*>(nullptr), out);
+    return;
+  }
+  DBuf<T> sums(size_t(tiles), s);
   GPP_LAUNCH(tile_reduce<T>, int(tiles), kThreads, 0, s, in, n, sums.p);
-  GPP_LAUNCH(scan_tile_sums<T>, 1, 1024, 0, s, sums.p, tiles, sums.p + tiles);
-  // tile_scan reads in[] before out[] is written only within the same tile;
-  // `in` and `out` may alias.
   GPP_LAUNCH(tile_scan<T>, int(tiles), kThreads, 0, s, in, n, sums.p, out);
-  GPP_LAUNCH(write_total<T>, 1, 1, 0, s, out, n, sums.p + tiles);
 }
 
 __global__ void det_sum_chunks(const double* __restrict__ v, int64_t n, double* __restrict__ out) {
@@ -178,6 +189,7 @@ double det_sum(const double* v, int64_t n, cudaStream_t s) {
   GPP_LAUNCH(det_sum_chunks, int(chunks), kThreads, 0, s, v, n, part.p);
   std::vector<double> h(static_cast<size_t>(chunks));
   check(cudaMemcpyAsync(h.data(), part.p, sizeof(double) * size_t(chunks), cudaMemcpyDeviceToHost, s), "det_sum d2h");
+  ++sync_counter();
   check(cudaStreamSynchronize(s), "det_sum sync");
   double total = 0.0;
   for (double x : h) total += x;

@@ -18,6 +18,7 @@ namespace gpp {
 
 using offset_t = gpp_offset;
 constexpr int kThreads = 256;
+constexpr int kEntryTile = 2048;    // stored entries per tile of the entry-parallel sweeps
 constexpr int kShortRow = 8;      // rows of live length <= 8: one thread per row
 constexpr int kLongRow = 1024;    // rows of live length > 1024: one block per row
 constexpr int kNumSMs = 148;      // B200
@@ -38,6 +39,7 @@ inline void check(cudaError_t e, const char* ctx) {
 
 // Kernel launch counter (per host thread) for the benchmark's launch report.
 uint64_t& launch_counter();
+uint64_t& sync_counter();   // host waits on the engine stream, calling thread
 
 // Optional per-launch timing (CUDA events on the launching stream) used by
 // the benchmark's roofline report; off unless gpp_profile_enable(1).
@@ -76,6 +78,38 @@ inline int grid_stride_blocks(int64_t n, int threads = kThreads, int per_sm = 8)
   const int64_t want = (n + threads - 1) / threads;
   const int64_t cap = int64_t(kNumSMs) * per_sm;
   return int(want < 1 ? 0 : (want < cap ? want : cap));
+}
+
+// Order-free max / min of doubles as single 64-bit integer reductions (RED,
+// no value returned, nothing for the thread to wait on).  A double whose sign
+// bit is clear orders like its bits read as a signed integer; one whose sign
+// bit is set orders in reverse of its bits read as an unsigned integer, and
+// every such pattern compares above every clear-sign pattern as unsigned and
+// below it as signed.  So max = signed max for clear-sign values and unsigned
+// min for set-sign values (min the other way round), which equals the
+// load-and-CAS loop of the reference (rule_bound_strengthening.cu:299-335)
+// for every input except the tie +0 / -0, where the CAS result depends on the
+// arrival order and this one does not (max keeps +0, min keeps -0).  NaN
+// values must not be passed.
+__device__ __forceinline__ void red_max_f64(double* addr, double v) {
+  const long long bits = __double_as_longlong(v);
+  if (bits >= 0) atomicMax(reinterpret_cast<long long*>(addr), bits);
+  else atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(bits));
+}
+__device__ __forceinline__ void red_min_f64(double* addr, double v) {
+  const long long bits = __double_as_longlong(v);
+  if (bits >= 0) atomicMin(reinterpret_cast<long long*>(addr), bits);
+  else atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(bits));
+}
+
+// Largest r in [lo, hi) with ptr[r] <= p: for a stored position p of a CSR
+// matrix (ptr non-decreasing), the row that holds p (never an empty row).
+__device__ __forceinline__ int row_of(const offset_t* ptr, int lo, int hi, offset_t p) {
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (ptr[mid] <= p) lo = mid; else hi = mid;
+  }
+  return lo;
 }
 
 // Warp-aggregated append: every lane of the warp must call it; lanes with
@@ -130,7 +164,10 @@ struct Context {
   ~Context();
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
-  void sync(const char* ctx) { check(cudaStreamSynchronize(stream), ctx); }
+  void sync(const char* ctx) {
+    ++sync_counter();
+    check(cudaStreamSynchronize(stream), ctx);
+  }
 };
 Context& ctx();
 

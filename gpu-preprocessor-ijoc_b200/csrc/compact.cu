@@ -50,16 +50,20 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
     return;
   }
   if (b < short_blocks + medium_blocks) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Four medium rows per warp, eight lanes each.
+    const int g = threadIdx.x & 7;
     const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
-      const int r = medium[q];
-      const int nr = outer_map[r];
-      if (nr < 0) continue;
-      int c = 0;
-      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32) c += inner_map[__ldcs(idx + p)] >= 0;
-      for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
-      if (lane == 0) out_counts[nr] = c;
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < counts[0]; q0 += nwarps * 4) {
+      const int q = q0 + ((threadIdx.x & 31) >> 3);
+      int nr = -1, c = 0;
+      if (q < counts[0]) {
+        const int r = medium[q];
+        nr = outer_map[r];
+        if (nr >= 0)
+          for (offset_t p = ptr[r] + g; p < ptr[r + 1]; p += 8) c += inner_map[__ldcs(idx + p)] >= 0;
+      }
+      for (int off = 4; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off, 8);
+      if (g == 0 && nr >= 0) out_counts[nr] = c;
     }
     return;
   }
@@ -105,23 +109,36 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
     return;
   }
   if (b < short_blocks + medium_blocks) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Four medium rows per warp, eight lanes each, eight stored entries per
+    // round; a group ballot ranks the kept entries of a round in stored order.
+    // Every lane runs the warp's largest number of rounds, so the ballots stay
+    // warp-uniform.
+    const int g = threadIdx.x & 7;
+    const unsigned shift = unsigned(threadIdx.x & 24);
     const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
-      const int r = medium[q];
-      const int nr = outer_map[r];
-      if (nr < 0) continue;
-      offset_t w = out_ptr[nr];
-      for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += 32) {
-        const offset_t p = chunk + lane;
-        const int c = p < ptr[r + 1] ? inner_map[__ldcs(idx + p)] : -1;
-        const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < counts[0]; q0 += nwarps * 4) {
+      const int q = q0 + ((threadIdx.x & 31) >> 3);
+      offset_t first = 0, end = 0, w = 0;
+      if (q < counts[0]) {
+        const int r = medium[q];
+        const int nr = outer_map[r];
+        if (nr >= 0) {
+          first = ptr[r];
+          end = ptr[r + 1];
+          w = out_ptr[nr];
+        }
+      }
+      const int rounds = __reduce_max_sync(0xffffffffu, int((end - first + 7) >> 3));
+      for (int k = 0; k < rounds; ++k) {
+        const offset_t p = first + offset_t(k) * 8 + g;
+        const int c = p < end ? inner_map[__ldcs(idx + p)] : -1;
+        const unsigned bits = (__ballot_sync(0xffffffffu, c >= 0) >> shift) & 0xFFu;
         if (c >= 0) {
-          const offset_t o = w + __popc(mask & ((1u << lane) - 1u));
+          const offset_t o = w + __popc(bits & ((1u << g) - 1u));
           out_idx[o] = c;
           out_val[o] = __ldcs(val + p);
         }
-        w += __popc(mask);
+        w += __popc(bits);
       }
     }
     return;
@@ -182,10 +199,14 @@ __global__ void transpose_gather(offset_t nnz, const int32_t* __restrict__ pos, 
   }
 }
 
+// Four rows per warp, eight lanes per row, each lane comparing the pairs
+// (p - 1, p) of its stride.
 __global__ void check_sorted(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                              int32_t* bad) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
-    for (offset_t p = ptr[r] + 1; p < ptr[r + 1]; ++p)
+  const int g = threadIdx.x & 7;
+  const int groups = gridDim.x * (blockDim.x >> 3);
+  for (int r = blockIdx.x * (blockDim.x >> 3) + (threadIdx.x >> 3); r < rows; r += groups)
+    for (offset_t p = ptr[r] + 1 + g; p < ptr[r + 1]; p += 8)
       if (idx[p - 1] >= idx[p]) { atomicExch(bad, 1); break; }
 }
 
@@ -278,10 +299,16 @@ DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
 
 bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s) {
   if (M.rows <= 0 || M.nnz <= 1) return true;
+  // A matrix does not change between materialisations, so the answer is kept
+  // with its cached schedule.
+  const RowSchedule& sch = stored_schedule(M);
+  if (sch.sorted >= 0) return sch.sorted != 0;
   DBuf<int32_t> bad(1, s);
   bad.zero();
-  GPP_LAUNCH(check_sorted, grid_stride_blocks(M.rows), kThreads, 0, s, M.rows, M.ptr, M.idx, bad.p);
-  return read_scalar(bad.p) == 0;
+  GPP_LAUNCH(check_sorted, std::max(1, std::min((M.rows + 31) / 32, kNumSMs * 16)), kThreads, 0, s, M.rows, M.ptr,
+             M.idx, bad.p);
+  sch.sorted = read_scalar(bad.p) == 0 ? 1 : 0;
+  return sch.sorted != 0;
 }
 
 void gather_by_map(double* dst, const double* src, const int32_t* old_to_new, int32_t n_old, cudaStream_t s) {
@@ -293,6 +320,7 @@ void compose_map(int32_t* next, const int32_t* prev, const int32_t* old_to_new, 
 }
 
 void free_csr(DevCsr& M) {
+  forget_schedule(M.ptr);
   dfree(M.ptr);
   dfree(M.idx);
   dfree(M.val);

@@ -23,6 +23,11 @@ struct DevCsr {
 // and long queues list the remaining rows for warp- and block-per-row work.
 struct RowSchedule {
   DBuf<int32_t> medium, long_rows, counts;  // counts[0] medium, counts[1] long
+  // Stored schedules only: for every tile of kEntryTile stored entries, the
+  // rows that hold its first (x) and last (y) entry.
+  DBuf<int2> tile_rows;
+  int64_t tiles = 0;
+  mutable int sorted = -1;  // rows strictly ascending: -1 not yet checked, else 0 / 1
   const offset_t* ptr = nullptr;
   int32_t rows = -1;
   offset_t nnz = -1;
@@ -35,6 +40,9 @@ void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees
 // Cached stored-length schedule (A and AT slots), invalidated per materialisation.
 const RowSchedule& stored_schedule(const DevCsr& M);
 void invalidate_schedules();
+// Drops any cached schedule of the matrix whose row pointers are `ptr` (called
+// when that matrix is freed, since its memory can come back for another).
+void forget_schedule(const offset_t* ptr);
 
 struct PostsolveSegment {
   DBuf<int32_t> types;

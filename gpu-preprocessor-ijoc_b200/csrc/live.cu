@@ -204,21 +204,28 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
       acc += unsigned(count);
     }
   } else if (b < short_blocks + medium_blocks) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Four medium rows per warp, eight lanes each: counts and the last live
+    // position are order-free, and four rows' loads are in flight at once.
+    const int g = threadIdx.x & 7;
     const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
-      const int r = medium[q];
-      const bool active = !keep_outer || keep_outer[r];
-      int count = 0;
+    const int nmedium = counts[0];
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < nmedium; q0 += nwarps * 4) {
+      const int q = q0 + ((threadIdx.x & 31) >> 3);
+      int r = -1, count = 0;
+      bool active = false;
       long long pos = -1;
-      if (active)
-        for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
-          if (!keep_inner || keep_inner[__ldcs(idx + p)]) { ++count; pos = p; }
-      for (int off = 16; off; off >>= 1) {
-        count += __shfl_down_sync(0xffffffffu, count, off);
-        pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off));
+      if (q < nmedium) {
+        r = medium[q];
+        active = !keep_outer || keep_outer[r];
+        if (active)
+          for (offset_t p = ptr[r] + g; p < ptr[r + 1]; p += 8)
+            if (!keep_inner || keep_inner[__ldcs(idx + p)]) { ++count; pos = p; }
       }
-      if (lane == 0) {
+      for (int off = 4; off; off >>= 1) {
+        count += __shfl_down_sync(0xffffffffu, count, off, 8);
+        pos = max(pos, __shfl_down_sync(0xffffffffu, pos, off, 8));
+      }
+      if (g == 0 && r >= 0) {
         stats_write(r, active, count, offset_t(pos), idx, val, degree, empty, singleton, support, coefficient, nullptr);
         acc += unsigned(count);
       }
@@ -276,15 +283,21 @@ col_max_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __rest
     return;
   }
   if (b < short_blocks + medium_blocks) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Four medium rows per warp, eight lanes each (the max is order-free).
+    const int g = threadIdx.x & 7;
     const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < counts[0]; q += nwarps) {
-      const int r = medium[q];
+    const int nmedium = counts[0];
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < nmedium; q0 += nwarps * 4) {
+      const int q = q0 + ((threadIdx.x & 31) >> 3);
+      int r = -1;
       double v = 0.0;
-      for (offset_t p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
-        if (!keep_row || keep_row[idx[p]]) v = fmax(v, fabs(val[p]));
-      for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-      if (lane == 0) out[r] = v;
+      if (q < nmedium) {
+        r = medium[q];
+        for (offset_t p = ptr[r] + g; p < ptr[r + 1]; p += 8)
+          if (!keep_row || keep_row[__ldcs(idx + p)]) v = fmax(v, fabs(__ldcs(val + p)));
+      }
+      for (int off = 4; off; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off, 8));
+      if (g == 0 && r >= 0) out[r] = v;
     }
     return;
   }
@@ -335,6 +348,22 @@ ScheduleCache& schedule_cache() {
 
 }  // namespace
 
+namespace {
+// Row r writes the tiles whose first stored position, or last one (the last
+// tile ends at nnz - 1), falls in [ptr[r], ptr[r+1]): every tile gets both
+// rows with no search, in one pass over the row pointers.
+__global__ void tile_rows_kernel(int rows, offset_t nnz, const offset_t* __restrict__ ptr, int2* __restrict__ tile_rows) {
+  constexpr int64_t T = kEntryTile;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const int64_t a = ptr[r], b = ptr[r + 1];
+    if (a == b) continue;
+    for (int64_t t = (a + T - 1) / T; t * T < b; ++t) tile_rows[t].x = r;
+    for (int64_t t = (a + T) / T - 1; (t + 1) * T <= b; ++t) tile_rows[t].y = r;
+    if (b == nnz) tile_rows[(nnz - 1) / T].y = r;
+  }
+}
+}  // namespace
+
 void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees, cudaStream_t st) {
   const size_t rows = size_t(std::max(M.rows, 1));
   if (s.medium.n < rows) s.medium.alloc(rows, st);
@@ -343,6 +372,13 @@ void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees
   check(cudaMemsetAsync(s.counts.p, 0, 2 * sizeof(int32_t), st), "schedule counts");
   GPP_LAUNCH(classify_rows, blocks_for(M.rows), kThreads, 0, st, M.ptr, M.rows, live_degrees, s.medium.p,
              s.long_rows.p, s.counts.p);
+  s.tiles = 0;
+  s.sorted = -1;
+  if (!live_degrees && M.rows > 0 && M.nnz > 0) {
+    s.tiles = (int64_t(M.nnz) + kEntryTile - 1) / kEntryTile;
+    if (s.tile_rows.n < size_t(s.tiles)) s.tile_rows.alloc(size_t(s.tiles), st);
+    GPP_LAUNCH(tile_rows_kernel, grid_stride_blocks(M.rows), kThreads, 0, st, M.rows, M.nnz, M.ptr, s.tile_rows.p);
+  }
   s.ptr = M.ptr;
   s.rows = M.rows;
   s.nnz = M.nnz;
@@ -359,6 +395,12 @@ const RowSchedule& stored_schedule(const DevCsr& M) {
 }
 
 void invalidate_schedules() { ++schedule_cache().epoch; }
+
+void forget_schedule(const offset_t* ptr) {
+  if (!ptr) return;
+  for (auto& s : schedule_cache().slots)
+    if (s.ptr == ptr) s.ptr = nullptr;
+}
 
 void live_stats_side(const DevCsr& M, const uint8_t* keep_outer, const uint8_t* keep_inner, int32_t* degree,
                      uint8_t* empty, uint8_t* singleton, int32_t* support, double* coefficient,

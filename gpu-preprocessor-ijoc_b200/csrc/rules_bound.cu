@@ -13,26 +13,6 @@ namespace gpp {
 
 namespace {
 
-__device__ __forceinline__ double atomic_max_d(double* addr, double v) {
-  auto* a = reinterpret_cast<unsigned long long*>(addr);
-  unsigned long long old = *a, assumed;
-  do {
-    assumed = old;
-    if (__longlong_as_double((long long)assumed) >= v) break;
-    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
-  } while (assumed != old);
-  return __longlong_as_double((long long)old);
-}
-__device__ __forceinline__ double atomic_min_d(double* addr, double v) {
-  auto* a = reinterpret_cast<unsigned long long*>(addr);
-  unsigned long long old = *a, assumed;
-  do {
-    assumed = old;
-    if (__longlong_as_double((long long)assumed) <= v) break;
-    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
-  } while (assumed != old);
-  return __longlong_as_double((long long)old);
-}
 
 struct RowSummary {
   const double* mn;
@@ -101,8 +81,8 @@ __device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx&
   double nl = ol, nu = ou;
   if (isfinite(il)) nl = fmax(nl, il);
   if (isfinite(iu)) nu = fmin(nu, iu);
-  if (nl > ol) atomic_max_d(&g.cand_l[j], nl);
-  if (nu < ou) atomic_min_d(&g.cand_u[j], nu);
+  if (nl > ol) red_max_f64(&g.cand_l[j], nl);
+  if (nu < ou) red_min_f64(&g.cand_u[j], nu);
 }
 
 // Entry-parallel form of the candidate sweep: the candidates are combined by
@@ -110,30 +90,15 @@ __device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx&
 // takes consecutive stored entries (coalesced loads, full memory-level
 // parallelism) and finds their row by a binary search over the tile's row
 // pointers, staged in shared memory.
-constexpr int kEntryTile = 2048;
 constexpr int kTileRows = 2048;
 
-__device__ __forceinline__ int row_of(const offset_t* ptr, int lo, int hi, offset_t p) {
-  // Largest r in [lo, hi) with ptr[r] <= p.
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (ptr[mid] <= p) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
 __global__ void __launch_bounds__(kThreads)
-candidates_entries(int m, offset_t nnz, CandArgs g) {
+candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g) {
   __shared__ offset_t sptr[kTileRows + 1];
-  __shared__ int srow[2];
   for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
     const offset_t last = min(nnz, base + kEntryTile) - 1;
-    if (threadIdx.x == 0) {
-      srow[0] = row_of(g.ptr, 0, m, base);
-      srow[1] = row_of(g.ptr, 0, m, last);
-    }
-    __syncthreads();
-    const int r0 = srow[0], r1 = srow[1];
+    const int2 span = tile_rows[base / kEntryTile];   // rows of the tile's first and last entry
+    const int r0 = span.x, r1 = span.y;
     const bool staged = r1 - r0 + 1 <= kTileRows;
     if (staged)
       for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
@@ -358,9 +323,9 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                plan.AU.p, plan.l.p, plan.u.p, rs, p.zero_tol, cl.p, cu.p};
     const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + double(n) + 4.0 * m + 16.0 * m + 24.0 * m +
                          16.0 * n + 16.0 * n;
-    const int64_t tiles = (int64_t(lp.A.nnz) + kEntryTile - 1) / kEntryTile;
-    GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(tiles, kNumSMs * 8))),
-                     kThreads, 0, s, m, lp.A.nnz, g);
+    const RowSchedule& sch = stored_schedule(lp.A);
+    GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(sch.tiles, kNumSMs * 8))),
+                     kThreads, 0, s, lp.A.nnz, sch.tile_rows.p, g);
   }
   col_max_abs(lp.AT, plan.keep_row.p, vmax.p, s);
   DBuf<double> fl(size_t(n), s), fu(size_t(n), s), fixv(size_t(n), s);

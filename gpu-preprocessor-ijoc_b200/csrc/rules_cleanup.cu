@@ -12,26 +12,6 @@ namespace gpp {
 
 namespace {
 
-__device__ __forceinline__ double atomic_max_d(double* addr, double v) {
-  auto* a = reinterpret_cast<unsigned long long*>(addr);
-  unsigned long long old = *a, assumed;
-  do {
-    assumed = old;
-    if (__longlong_as_double((long long)assumed) >= v) break;
-    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
-  } while (assumed != old);
-  return __longlong_as_double((long long)old);
-}
-__device__ __forceinline__ double atomic_min_d(double* addr, double v) {
-  auto* a = reinterpret_cast<unsigned long long*>(addr);
-  unsigned long long old = *a, assumed;
-  do {
-    assumed = old;
-    if (__longlong_as_double((long long)assumed) <= v) break;
-    old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
-  } while (assumed != old);
-  return __longlong_as_double((long long)old);
-}
 
 // Rows touched by a selected column (with positive radius in radius mode).
 __global__ void mark_touched_rows(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
@@ -201,8 +181,8 @@ __global__ void singleton_row_bounds(int m, int n, const uint8_t* __restrict__ k
     const double a = sval[i];
     if (!(col >= 0 && col < n && fabs(a) > zero_tol)) continue;
     const double lo = AL[i], hi = AU[i];
-    atomic_max_d(&cand_l[col], a > 0.0 ? lo / a : hi / a);
-    atomic_min_d(&cand_u[col], a > 0.0 ? hi / a : lo / a);
+    red_max_f64(&cand_l[col], a > 0.0 ? lo / a : hi / a);
+    red_min_f64(&cand_u[col], a > 0.0 ? hi / a : lo / a);
     remove[i] = 1;
   }
 }

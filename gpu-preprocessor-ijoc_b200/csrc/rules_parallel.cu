@@ -97,6 +97,59 @@ __device__ void row_hash_warp(const RowHashArgs& g, int i) {
   }
 }
 
+// Four rows per warp, eight lanes (a group) per row, eight stored entries per
+// round.  A first sweep finds the live length and the first live entry (the
+// pivot); the second forms the hash: the XOR aggregate is order-free, the
+// sequential fold visits the group's live entries of each round in stored
+// order through shuffles.  Every lane runs the same number of rounds (the
+// warp's maximum), so ballots and shuffles stay warp-uniform; rounds past a
+// row's end have no live entry.
+__device__ void row_hash_grouped(const RowHashArgs& g, int i) {
+  const int lane = threadIdx.x & 31, group = lane >> 3, gl = lane & 7;
+  const unsigned shift = unsigned(group * 8);
+  const bool keep = i >= 0 && g.keep_row[i];
+  const offset_t a = keep ? g.ptr[i] : 0, e = keep ? g.ptr[i + 1] : 0;
+  const int rounds = __reduce_max_sync(0xffffffffu, int((e - a + 7) >> 3));
+  int len = 0;
+  offset_t first = -1;
+  for (int k = 0; k < rounds; ++k) {
+    const offset_t p = a + offset_t(k) * 8 + gl;
+    const bool live = p < e && (!g.keep_col || g.keep_col[__ldcs(g.idx + p)]);
+    const unsigned bits = (__ballot_sync(0xffffffffu, live) >> shift) & 0xFFu;
+    if (first < 0 && bits) first = a + offset_t(k) * 8 + (__ffs(bits) - 1);
+    len += __popc(bits);
+  }
+  const bool trivial = !keep || len == 0 || fabs(g.val[first]) <= g.tol;
+  const double pivot = trivial ? 1.0 : g.val[first];
+  const offset_t from = trivial ? e : first;
+  const int rounds2 = __reduce_max_sync(0xffffffffu, int((e - from + 7) >> 3));
+  uint64_t h = mix(kFnvOffset, uint64_t(len)), agg = 0;
+  for (int k = 0; k < rounds2; ++k) {
+    const offset_t p = from + offset_t(k) * 8 + gl;
+    const bool live = p < e && (!g.keep_col || g.keep_col[__ldcs(g.idx + p)]);
+    const uint64_t col = live ? uint64_t(__ldcs(g.idx + p)) : 0;
+    const uint64_t b = live ? dbits(__ldcs(g.val + p) / pivot) : 0;
+    if (g.use_xor) {
+      if (live) agg ^= mix(mix(kFnvOffset, col), b);
+    } else {
+      const unsigned bits = (__ballot_sync(0xffffffffu, live) >> shift) & 0xFFu;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const uint64_t ct = __shfl_sync(0xffffffffu, col, t, 8);
+        const uint64_t bt = __shfl_sync(0xffffffffu, b, t, 8);
+        if ((bits >> t) & 1u) h = mix(mix(h, ct), bt);
+      }
+    }
+  }
+  if (g.use_xor)
+    for (int off = 4; off; off >>= 1) agg ^= __shfl_xor_sync(0xffffffffu, agg, off, 8);
+  if (gl == 0 && i >= 0) {
+    if (!g.keep_row[i]) g.out[i] = uint64_t(i);
+    else if (trivial) g.out[i] = mix(kFnvOffset, uint64_t(i));
+    else g.out[i] = g.use_xor ? mix(h, agg) : h;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads)
 row_hash_kernel(int rows, RowHashArgs g, const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
                 const int32_t* __restrict__ counts, int short_blocks) {
@@ -106,10 +159,16 @@ row_hash_kernel(int rows, RowHashArgs g, const int32_t* __restrict__ medium, con
       if (g.ptr[i + 1] - g.ptr[i] <= kShortRow) row_hash_thread(g, i);
     return;
   }
-  const int warp = threadIdx.x >> 5;
+  // Medium rows four to a warp; long rows (> kLongRow stored entries) one to
+  // a warp, so that no group waits through a long row's rounds.
   const int nwarps = (gridDim.x - short_blocks) * (kThreads / 32);
-  const int wid = (b - short_blocks) * (kThreads / 32) + warp;
-  for (int q = wid; q < counts[0] + counts[1]; q += nwarps) row_hash_warp(g, q < counts[0] ? medium[q] : longq[q - counts[0]]);
+  const int wid = (b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5);
+  const int nmedium = counts[0];
+  for (int q0 = wid * 4; q0 < nmedium; q0 += nwarps * 4) {
+    const int q = q0 + ((threadIdx.x & 31) >> 3);
+    row_hash_grouped(g, q < nmedium ? medium[q] : -1);
+  }
+  for (int q = wid; q < counts[1]; q += nwarps) row_hash_warp(g, longq[q]);
 }
 
 __global__ void gather_live(int n, const uint8_t* __restrict__ keep, const int32_t* __restrict__ pos,

@@ -114,8 +114,13 @@ struct CacheOut {
 };
 
 // _kernel_singleton_row_activity_cache (:555-614) for rows of live length
-// <= 1024: one warp per row loads 32 entries at a time; lane 0 accumulates them
-// in stored order, exactly the reference's sequential loop.
+// <= 1024: one warp per row loads 32 entries at a time.  The reference's
+// sequential loop skips a NaN term entirely, counts an infinite term and adds
+// a finite one; the counts and the NaN flag are order-free, so they come from
+// ballots, and the finite sums are formed in stored order by the same
+// shuffle-add chain on every lane.  A skipped term enters the chain as +0.0,
+// which is exact: a sum that starts at +0.0 never becomes -0.0 in
+// round-to-nearest, and x + (+0.0) == x for every other x.
 __global__ void sc_cache_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ st,
                               const int32_t* __restrict__ row_nnz, const offset_t* __restrict__ ptr,
                               const int32_t* __restrict__ idx, const double* __restrict__ val,
@@ -128,28 +133,33 @@ __global__ void sc_cache_rows(const int32_t* __restrict__ rows, const int32_t* _
     const int row = rows[w];
     if (row_nnz[row] > kLongRow) continue;
     RowCache r{0.0, 0.0, 0, 0, 0, 0, 0};
-    for (offset_t chunk = ptr[row]; chunk < ptr[row + 1]; chunk += 32) {
+    const offset_t end = ptr[row + 1];
+    for (offset_t chunk = ptr[row]; chunk < end; chunk += 32) {
       const offset_t p = chunk + lane;
       double tmin = 0.0, tmax = 0.0;
-      int live = 0;
-      if (p < ptr[row + 1]) {
-        const int col = idx[p];
+      bool live = false;
+      if (p < end) {
+        const int col = __ldcs(idx + p);
         if (keep_col[col]) {
-          live = 1;
-          const double a = val[p];
+          live = true;
+          const double a = __ldcs(val + p);
           tmin = a >= 0.0 ? a * l[col] : a * u[col];
           tmax = a >= 0.0 ? a * u[col] : a * l[col];
         }
       }
-      const unsigned lv = __ballot_sync(0xffffffffu, live);
-      for (int k = 0; k < 32; ++k) {
-        const double a_min = __shfl_sync(0xffffffffu, tmin, k);
-        const double a_max = __shfl_sync(0xffffffffu, tmax, k);
-        if (lane == 0 && (lv >> k & 1u)) {
-          if (isnan(a_min) || isnan(a_max)) { r.invalid = 1; continue; }
-          if (isinf(a_min)) { if (a_min < 0.0) ++r.min_neg; else ++r.min_pos; } else { r.fmin += a_min; }
-          if (isinf(a_max)) { if (a_max < 0.0) ++r.max_neg; else ++r.max_pos; } else { r.fmax += a_max; }
-        }
+      const bool nan = live && (isnan(tmin) || isnan(tmax));
+      const bool counted = live && !nan;
+      r.invalid |= __any_sync(0xffffffffu, nan);
+      r.min_neg += __popc(__ballot_sync(0xffffffffu, counted && isinf(tmin) && tmin < 0.0));
+      r.min_pos += __popc(__ballot_sync(0xffffffffu, counted && isinf(tmin) && tmin > 0.0));
+      r.max_neg += __popc(__ballot_sync(0xffffffffu, counted && isinf(tmax) && tmax < 0.0));
+      r.max_pos += __popc(__ballot_sync(0xffffffffu, counted && isinf(tmax) && tmax > 0.0));
+      const double fmin_term = counted && isfinite(tmin) ? tmin : 0.0;
+      const double fmax_term = counted && isfinite(tmax) ? tmax : 0.0;
+      const int n = int(min(offset_t(32), end - chunk));
+      for (int k = 0; k < n; ++k) {
+        r.fmin += __shfl_sync(0xffffffffu, fmin_term, k);
+        r.fmax += __shfl_sync(0xffffffffu, fmax_term, k);
       }
     }
     if (lane == 0) out.store(row, r);

@@ -335,6 +335,11 @@ GPP_API int gpp_profile_read(int index, char* name, size_t name_len, int64_t* la
  * the last reset (used by the benchmark to report its launch count). */
 GPP_API uint64_t gpp_kernel_launches(int reset);
 
+/* Number of times the library waited on its stream from the calling thread
+ * (to read a count, a flag or a size back) since the last reset: each wait
+ * leaves the GPU idle until the host launches again. */
+GPP_API uint64_t gpp_host_syncs(int reset);
+
 #ifdef __cplusplus
 }
 #endif

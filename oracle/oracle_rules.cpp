@@ -11,6 +11,17 @@ namespace oracle {
 
 namespace {
 inline bool fin(double x) { return std::isfinite(x); }
+// Order-free max / min of candidate bounds, as the engine's 64-bit integer
+// reductions combine them: the reference's load-and-CAS loop
+// (rule_bound_strengthening.cu:299-335) for every input except the tie
+// +0 / -0, which the loop resolves by arrival order; here max keeps +0 and
+// min keeps -0.
+inline void max_into(double& cur, double v) {
+  if (v > cur || (v == 0.0 && cur == 0.0 && std::signbit(cur) && !std::signbit(v))) cur = v;
+}
+inline void min_into(double& cur, double v) {
+  if (v < cur || (v == 0.0 && cur == 0.0 && !std::signbit(cur) && std::signbit(v))) cur = v;
+}
 }
 
 void refresh_stats(Stats& s, const Lp& lp, const Plan& plan) {
@@ -172,8 +183,8 @@ void rule_singleton_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_par
     const double lo = plan.AL[i], hi = plan.AU[i];
     const double il = a > 0.0 ? lo / a : hi / a;
     const double iu = a > 0.0 ? hi / a : lo / a;
-    if (!(cl[col] >= il)) cl[col] = il;   // atomic_max_double
-    if (!(cu[col] <= iu)) cu[col] = iu;   // atomic_min_double
+    max_into(cl[col], il);   // atomic_max_double
+    min_into(cu[col], iu);   // atomic_min_double
     remove[i] = 1;
     any_remove = true;
   }
@@ -896,8 +907,8 @@ void rule_bound_strengthening(Plan& plan, const Lp& lp, const Stats& s, const gp
       double nl = ol, nu = ou;
       if (fin(il)) nl = std::fmax(nl, il);
       if (fin(iu)) nu = std::fmin(nu, iu);
-      if (nl > ol && !(cl[j] >= nl)) cl[j] = nl;
-      if (nu < ou && !(cu[j] <= nu)) cu[j] = nu;
+      if (nl > ol) max_into(cl[j], nl);
+      if (nu < ou) min_into(cu[j], nu);
     }
   }
   std::vector<double> cmax(n);

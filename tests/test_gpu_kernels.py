@@ -98,21 +98,62 @@ def test_live_stats_and_col_max_vs_oracle():
     assert np.array_equal(out.cpu().numpy(), pyoracle.col_max_abs(lp.n, lp.m, lp.at_ptr, lp.at_idx, lp.at_val, keep_r))
 
 
-def test_compaction_and_transpose_vs_numpy():
+def sparse_rows(m, n, lengths, seed):
+    """CSR with the given row lengths, distinct sorted columns per row."""
+    rng = np.random.default_rng(seed)
+    ptr_ = np.zeros(m + 1, np.int64)
+    ptr_[1:] = np.cumsum(lengths)
+    idx = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lengths if k] or [np.zeros(0, int)])
+    val = rng.standard_normal(idx.size)
+    return ptr_.astype(np.int32), idx.astype(np.int32), val
+
+
+def compaction_case(name):
     rng = np.random.default_rng(11)
-    lp = lpgen.random_lp(2500, 6000, seed=11, hub_rows=4)
-    keep_r = (rng.random(lp.m) < 0.7).astype(np.uint8)
-    keep_c = (rng.random(lp.n) < 0.6).astype(np.uint8)
-    A, keep = dev_csr(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values)
+    if name == "random_hubs":
+        lp = lpgen.random_lp(2500, 6000, seed=11, hub_rows=4)
+        m, n, p_, i_, v_ = lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values
+        return m, n, p_, i_, v_, (rng.random(m) < 0.7).astype(np.uint8), (rng.random(n) < 0.6).astype(np.uint8)
+    if name == "empty_runs":
+        # Leading, trailing and long interior runs of empty rows.
+        m, n = 60000, 3000
+        lengths = np.zeros(m, np.int64)
+        lengths[5000:55000:97] = rng.integers(1, 40, size=len(range(5000, 55000, 97)))
+        p_, i_, v_ = sparse_rows(m, n, lengths, 12)
+        return m, n, p_, i_, v_, (rng.random(m) < 0.8).astype(np.uint8), (rng.random(n) < 0.7).astype(np.uint8)
+    if name == "long_rows":
+        # Rows of thousands of entries interleaved with short and empty rows.
+        m, n = 40, 20000
+        lengths = rng.integers(0, 30, size=m)
+        lengths[[3, 17, 18, 39]] = [9000, 4500, 12000, 7000]
+        p_, i_, v_ = sparse_rows(m, n, lengths, 13)
+        keep_r = np.ones(m, np.uint8)
+        keep_r[17] = 0
+        return m, n, p_, i_, v_, keep_r, (rng.random(n) < 0.5).astype(np.uint8)
+    if name == "nothing_left":
+        # Kept rows, kept columns, but no kept entry: every new pointer is 0.
+        m, n = 3000, 600
+        lengths = rng.integers(0, 6, size=m)
+        p_, i_, v_ = sparse_rows(m, 500, lengths, 14)   # columns 500.. hold no entry
+        keep_c = np.zeros(n, np.uint8)
+        keep_c[500:503] = 1
+        return m, n, p_, i_, v_, (rng.random(m) < 0.5).astype(np.uint8), keep_c
+    raise ValueError(name)
+
+
+@pytest.mark.parametrize("case", ["random_hubs", "empty_runs", "long_rows", "nothing_left"])
+def test_compaction_and_transpose_vs_numpy(case):
+    m, n, row_ptr, col_idx, values, keep_r, keep_c = compaction_case(case)
+    A, keep = dev_csr(m, n, row_ptr, col_idx, values)
     Ao, ATo = capi.Csr(), capi.Csr()
     dkr, dkc = to_device(keep_r, np.uint8), to_device(keep_c, np.uint8)   # kept alive across the call
     _raise(capi.load().gpp_compact_and_transpose(C.byref(A), ptr(dkr), ptr(dkc), C.byref(Ao), C.byref(ATo)))
-    rmap = np.cumsum(keep_r) - 1
-    cmap = np.cumsum(keep_c) - 1
-    rows = np.repeat(np.arange(lp.m), np.diff(lp.row_ptr))
-    sel = keep_r[rows].astype(bool) & keep_c[lp.col_idx].astype(bool)
+    rmap = np.cumsum(keep_r.astype(np.int64)) - 1
+    cmap = np.cumsum(keep_c.astype(np.int64)) - 1
+    rows = np.repeat(np.arange(m), np.diff(row_ptr))
+    sel = keep_r[rows].astype(bool) & keep_c[col_idx].astype(bool)
     m2, n2 = int(keep_r.sum()), int(keep_c.sum())
-    ptr2, idx2, val2 = lpgen.coo_to_csr(m2, rmap[rows[sel]], cmap[lp.col_idx[sel]], lp.values[sel])
+    ptr2, idx2, val2 = lpgen.coo_to_csr(m2, rmap[rows[sel]], cmap[col_idx[sel]], values[sel])
     tp, ti, tv = lpgen.csr_transpose(m2, n2, ptr2, idx2, val2)
     assert Ao.rows == m2 and Ao.cols == n2 and Ao.nnz == idx2.size
     assert np.array_equal(_d2h(Ao.rowPtr, m2 + 1, np.int32), ptr2)
