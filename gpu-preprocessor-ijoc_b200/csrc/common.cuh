@@ -80,6 +80,16 @@ inline int grid_stride_blocks(int64_t n, int threads = kThreads, int per_sm = 8)
   return int(want < 1 ? 0 : (want < cap ? want : cap));
 }
 
+// Column bounds packed for the row sweeps: {l_j, u_j} in one 16-byte record,
+// so a gathered column costs one memory sector instead of three (l, u and the
+// keep mask).  A removed column holds one reserved NaN bit pattern in both
+// fields; a kept column holds its bounds as they are (any value, NaN
+// included), so the sweeps' arithmetic is unchanged.
+constexpr unsigned long long kRemovedColumnBits = 0x7FF00000DEADC01EULL;
+__device__ __forceinline__ bool removed_column(double2 b) {
+  return static_cast<unsigned long long>(__double_as_longlong(b.x)) == kRemovedColumnBits;
+}
+
 // Order-free max / min of doubles as single 64-bit integer reductions (RED,
 // no value returned, nothing for the thread to wait on).  A double whose sign
 // bit is clear orders like its bits read as a signed integer; one whose sign

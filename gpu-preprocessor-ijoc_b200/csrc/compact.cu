@@ -28,6 +28,15 @@ __global__ void prefix_to_map(const uint8_t* __restrict__ keep, const int32_t* _
     old_to_new[i] = keep[i] ? prefix[i] : -1;
 }
 
+// Copy roles.  Rows of up to kLongRow stored entries go four to a warp,
+// eight lanes per row, the warp's four rows consecutive (so its loads and
+// stores cover one contiguous stretch of the matrix); longer rows take a whole
+// block.  Entries are copied in stored order, so the schedule is free.
+// First of the four consecutive rows of this warp in the group role.
+__device__ __forceinline__ int warp_first_row(int block) {
+  return (block * (kThreads / 32) + int(threadIdx.x >> 5)) * 4;
+}
+
 // Count kept entries of kept rows: short rows by thread, medium by warp,
 // long by block (roles as in live.cu).
 __global__ void __launch_bounds__(kThreads)
@@ -86,45 +95,30 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
 }
 
 // Stable copy of kept entries (order preserving), remapping inner indices.
+// In the group role a ballot over the group's eight lanes ranks the kept
+// entries of each round of eight stored entries; every lane runs the warp's
+// largest number of rounds, so the ballots stay warp-uniform.
 __global__ void __launch_bounds__(kThreads)
 copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
           const double* __restrict__ val, const int32_t* __restrict__ outer_map,
-          const int32_t* __restrict__ inner_map, const int32_t* __restrict__ medium,
-          const int32_t* __restrict__ longq, const int32_t* __restrict__ counts, int short_blocks,
-          int medium_blocks, const offset_t* __restrict__ out_ptr, int32_t* __restrict__ out_idx,
-          double* __restrict__ out_val) {
+          const int32_t* __restrict__ inner_map, const int32_t* __restrict__ longq,
+          const int32_t* __restrict__ counts, int group_blocks, const offset_t* __restrict__ out_ptr,
+          int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
   __shared__ int wcount[8];
   const int b = blockIdx.x;
-  if (b < short_blocks) {
-    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
-      const int nr = outer_map[r];
-      if (nr < 0) continue;
-      offset_t w = out_ptr[nr];
-      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) {
-        const int c = inner_map[__ldcs(idx + p)];
-        if (c >= 0) { out_idx[w] = c; out_val[w] = __ldcs(val + p); ++w; }
-      }
-    }
-    return;
-  }
-  if (b < short_blocks + medium_blocks) {
-    // Four medium rows per warp, eight lanes each, eight stored entries per
-    // round; a group ballot ranks the kept entries of a round in stored order.
-    // Every lane runs the warp's largest number of rounds, so the ballots stay
-    // warp-uniform.
+  if (b < group_blocks) {
     const int g = threadIdx.x & 7;
     const unsigned shift = unsigned(threadIdx.x & 24);
-    const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < counts[0]; q0 += nwarps * 4) {
-      const int q = q0 + ((threadIdx.x & 31) >> 3);
+    const int stride = group_blocks * kThreads / 8;
+    for (int r0 = warp_first_row(b); r0 < rows; r0 += stride) {
+      const int r = r0 + int((threadIdx.x & 31) >> 3);
       offset_t first = 0, end = 0, w = 0;
-      if (q < counts[0]) {
-        const int r = medium[q];
-        const int nr = outer_map[r];
+      if (r < rows) {
+        const offset_t a = ptr[r], e = ptr[r + 1];
+        const int nr = e - a > kLongRow ? -1 : outer_map[r];
         if (nr >= 0) {
-          first = ptr[r];
-          end = ptr[r + 1];
+          first = a;
+          end = e;
           w = out_ptr[nr];
         }
       }
@@ -143,7 +137,7 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
     }
     return;
   }
-  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
+  const int lb = b - group_blocks, nlong = gridDim.x - group_blocks;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int q = lb; q < counts[1]; q += nlong) {
     const int r = longq[q];
@@ -225,8 +219,6 @@ __global__ void compose_kernel(int32_t* __restrict__ next, const int32_t* __rest
   }
 }
 
-int roles_short(int rows) { return grid_stride_blocks(rows, kThreads, 16); }
-int roles_medium(int rows) { return std::min<int>(kNumSMs * 8, (rows + 7) / 8); }
 int roles_long(int rows) { return std::min<int>(kNumSMs * 4, rows); }
 
 }  // namespace
@@ -251,19 +243,23 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
     return out;
   }
   const RowSchedule& sch = stored_schedule(M);
-  const int sb = roles_short(M.rows), mb = roles_medium(M.rows), lb = roles_long(M.rows);
+  const int gb = std::max(1, std::min((M.rows + 31) / 32, kNumSMs * 16));
+  const int lb = roles_long(M.rows);
+  // Counting reads only: short rows one per thread (more rows in flight),
+  // medium rows four per warp, long rows one per block.
+  const int sb = grid_stride_blocks(M.rows, kThreads, 16), mb = std::min<int>(kNumSMs * 8, (M.rows + 7) / 8);
   DBuf<int32_t> counts(size_t(outer_new) + 1, s);
   const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * outer_new;
-  GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map, sch.medium.p,
-             sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
+  GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map,
+                   sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
   exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
   out.nnz = read_scalar(out.ptr + outer_new);
   out.idx = dalloc<int32_t>(size_t(out.nnz));
   out.val = dalloc<double>(size_t(out.nnz));
   const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +
                             4.0 * (outer_new + 1) + 12.0 * out.nnz;
-  GPP_LAUNCH_BYTES(copy_kept, copy_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map, inner_map,
-             sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, out.ptr, out.idx, out.val);
+  GPP_LAUNCH_BYTES(copy_kept, copy_bytes, gb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map,
+                   inner_map, sch.long_rows.p, sch.counts.p, gb, out.ptr, out.idx, out.val);
   return out;
 }
 

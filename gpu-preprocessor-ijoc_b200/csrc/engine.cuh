@@ -111,6 +111,12 @@ void live_stats_side(const DevCsr& M, const uint8_t* keep_outer, const uint8_t* 
                      double* coefficient, unsigned long long* total, cudaStream_t s);
 void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan);
 void allocate_stats(Stats& st, int32_t m, int32_t n);
+// Packs {l_j, u_j} of every column (a removed one as the reserved NaN pair).
+void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int32_t n, double2* lu,
+                 cudaStream_t s);
+void row_activity_summary_packed(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
+                                 const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,
+                                 int32_t* max_inf, cudaStream_t s);
 void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,
                           const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
                           double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,

@@ -69,51 +69,52 @@ template <bool Plain>
 struct ActivityTerm {
   const int32_t* idx;
   const double* val;
-  const double* l;
-  const double* u;
+  const double2* lu;
   double zero_tol;
-  __device__ __forceinline__ void operator()(offset_t p, double& lo, double& hi, int& ni, int& pi) const {
+  // The term of live stored entry p whose column bounds are b.
+  __device__ __forceinline__ void operator()(offset_t p, double2 b, double& lo, double& hi, int& ni, int& pi) const {
     const double a = __ldcs(val + p);   // streamed once: keep L2 for the gathered bounds
     if constexpr (Plain) {
       // Plain sums of the redundant-row test: infinities propagate.
-      const int col = __ldcs(idx + p);
-      lo += a >= 0.0 ? a * l[col] : a * u[col];
-      hi += a >= 0.0 ? a * u[col] : a * l[col];
+      lo += a >= 0.0 ? a * b.x : a * b.y;
+      hi += a >= 0.0 ? a * b.y : a * b.x;
       return;
     }
     if (fabs(a) <= zero_tol) return;
-    const int col = __ldcs(idx + p);
-    const double tlo = a >= 0.0 ? a * l[col] : a * u[col];
-    const double thi = a >= 0.0 ? a * u[col] : a * l[col];
+    const double tlo = a >= 0.0 ? a * b.x : a * b.y;
+    const double thi = a >= 0.0 ? a * b.y : a * b.x;
     if (isfinite(tlo)) lo += tlo; else if (tlo < 0.0) ++ni;
     if (isfinite(thi)) hi += thi; else if (thi > 0.0) ++pi;
   }
+  __device__ __forceinline__ double2 bounds(offset_t p) const { return lu[__ldcs(idx + p)]; }
 };
 
 template <bool Plain>
 __global__ void __launch_bounds__(kThreads)
 activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                const double* __restrict__ val, const double* __restrict__ l, const double* __restrict__ u,
-                double zero_tol, const uint8_t* __restrict__ keep_row, const uint8_t* __restrict__ keep_col,
-                const int32_t* __restrict__ live_deg, const int32_t* __restrict__ medium,
-                const int32_t* __restrict__ longq, const int32_t* __restrict__ counts, int short_blocks,
-                int medium_blocks, double* __restrict__ min_fin, double* __restrict__ max_fin,
-                int32_t* __restrict__ min_inf, int32_t* __restrict__ max_inf) {
+                const double* __restrict__ val, const double2* __restrict__ lu, double zero_tol,
+                const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ live_deg,
+                const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
+                const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
+                double* __restrict__ min_fin, double* __restrict__ max_fin, int32_t* __restrict__ min_inf,
+                int32_t* __restrict__ max_inf) {
   __shared__ int slots[256];
   __shared__ int warp_counts[8];
   __shared__ double dagg[8];
   __shared__ int iagg[8];
-  const ActivityTerm<Plain> term{idx, val, l, u, zero_tol};
+  const ActivityTerm<Plain> term{idx, val, lu, zero_tol};
+  const auto live_at = [&](offset_t p) { return !removed_column(term.bounds(p)); };
   const int b = blockIdx.x;
   if (b < short_blocks) {
     for (int i = b * blockDim.x + threadIdx.x; i < m; i += short_blocks * blockDim.x) {
       if (row_len(ptr, live_deg, i) > kShortRow) continue;
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
-      for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
-        if ((keep_row && !keep_row[i]) || (keep_col && !keep_col[__ldcs(idx + p)])) continue;
-        term(p, lo, hi, ni, pi);
-      }
+      if (!keep_row || keep_row[i])
+        for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+          const double2 bnd = term.bounds(p);
+          if (!removed_column(bnd)) term(p, bnd, lo, hi, ni, pi);
+        }
       min_fin[i] = lo; max_fin[i] = hi;
       if (min_inf) { min_inf[i] = ni; max_inf[i] = pi; }
     }
@@ -128,10 +129,10 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
       const offset_t first = ptr[row], last = ptr[row + 1];
-      const uint8_t* mask = live_deg && live_deg[row] == int(last - first) ? nullptr : keep_col;
+      const bool all_live = live_deg && live_deg[row] == int(last - first);
       if (!keep_row || keep_row[row])
-        live_visit<32>(first, last, idx, mask, slots + warp * 32, nullptr,
-                       [&](offset_t p) { term(p, lo, hi, ni, pi); });
+        live_visit_by<32>(first, last, all_live, live_at, slots + warp * 32, nullptr,
+                          [&](offset_t p) { term(p, term.bounds(p), lo, hi, ni, pi); });
       lo = warp_sum_down(lo); hi = warp_sum_down(hi); ni = warp_sum_down(ni); pi = warp_sum_down(pi);
       if (lane == 0) {
         min_fin[row] = lo; max_fin[row] = hi;
@@ -148,10 +149,10 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
     double lo = 0.0, hi = 0.0;
     int ni = 0, pi = 0;
     const offset_t first = ptr[row], last = ptr[row + 1];
-    const uint8_t* mask = live_deg && live_deg[row] == int(last - first) ? nullptr : keep_col;
+    const bool all_live = live_deg && live_deg[row] == int(last - first);
     if (!keep_row || keep_row[row])
-      live_visit<256>(first, last, idx, mask, slots, warp_counts,
-                      [&](offset_t p) { term(p, lo, hi, ni, pi); });
+      live_visit_by<256>(first, last, all_live, live_at, slots, warp_counts,
+                         [&](offset_t p) { term(p, term.bounds(p), lo, hi, ni, pi); });
     lo = block_sum_cub_order(lo, dagg);
     hi = block_sum_cub_order(hi, dagg);
     ni = block_sum_cub_order(ni, iagg);
@@ -162,6 +163,13 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
     }
     __syncthreads();
   }
+}
+
+__global__ void pack_bounds_kernel(int n, const double* __restrict__ l, const double* __restrict__ u,
+                                   const uint8_t* __restrict__ keep, double2* __restrict__ lu) {
+  const double removed = __longlong_as_double(static_cast<long long>(kRemovedColumnBits));
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    lu[j] = !keep || keep[j] ? make_double2(l[j], u[j]) : make_double2(removed, removed);
 }
 
 // Live degree / singleton support.  Counts and the max live position are
@@ -553,12 +561,17 @@ void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
   st.valid = true;
 }
 
-void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,
-                          const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
-                          double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,
-                          cudaStream_t s) {
-  // compute_row_activity_summary (gpu_presolve_kernels.cu:744-787).
-  if (!A.rows) return;
+void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int32_t n, double2* lu,
+                 cudaStream_t s) {
+  if (n <= 0) return;
+  GPP_LAUNCH_BYTES(pack_bounds_kernel, 33.0 * n, grid_stride_blocks(n), kThreads, 0, s, n, l, u, keep_col, lu);
+}
+
+namespace {
+template <bool Plain>
+void launch_activity(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
+                     const int32_t* live_deg, double* lo, double* hi, int32_t* ni, int32_t* pi, double out_bytes,
+                     cudaStream_t s) {
   static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
   const RowSchedule* sch;
   if (live_deg) {
@@ -569,12 +582,37 @@ void row_activity_summary(const DevCsr& A, const double* l, const double* u, dou
   }
   const Roles r = roles_for(A.rows);
   // Algorithmic bytes (each array charged once): row pointers, column indices
-  // and values, column bounds, masks, live degrees, four outputs.
+  // and values, packed column bounds, row mask, live degrees, the outputs.
   const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
-                       (keep_col ? A.cols : 0) + (live_deg ? 4.0 * A.rows : 0) + 24.0 * A.rows;
-  GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s, A.rows, A.ptr,
-             A.idx, A.val, l, u, zero_tol, keep_row, keep_col, live_deg, sch->medium.p, sch->long_rows.p,
-             sch->counts.p, r.short_blocks, r.medium_blocks, min_fin, max_fin, min_inf, max_inf);
+                       (live_deg ? 4.0 * A.rows : 0) + out_bytes * A.rows;
+  const int grid = r.short_blocks + r.medium_blocks + r.long_blocks;
+  if constexpr (Plain)
+    GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
+  else
+    GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
+}
+}  // namespace
+
+void row_activity_summary_packed(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
+                                 const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,
+                                 int32_t* max_inf, cudaStream_t s) {
+  // compute_row_activity_summary (gpu_presolve_kernels.cu:744-787).
+  if (!A.rows) return;
+  launch_activity<false>(A, lu, zero_tol, keep_row, live_deg, min_fin, max_fin, min_inf, max_inf, 24.0, s);
+}
+
+void row_activity_summary(const DevCsr& A, const double* l, const double* u, double zero_tol,
+                          const uint8_t* keep_row, const uint8_t* keep_col, const int32_t* live_deg,
+                          double* min_fin, double* max_fin, int32_t* min_inf, int32_t* max_inf,
+                          cudaStream_t s) {
+  if (!A.rows) return;
+  DBuf<double2> lu(size_t(std::max(A.cols, 1)), s);
+  pack_bounds(l, u, keep_col, A.cols, lu.p, s);
+  row_activity_summary_packed(A, lu.p, zero_tol, keep_row, live_deg, min_fin, max_fin, min_inf, max_inf, s);
 }
 
 void row_plain_minmax(const DevCsr& A, const double* l, const double* u, const uint8_t* keep_row,
@@ -582,21 +620,9 @@ void row_plain_minmax(const DevCsr& A, const double* l, const double* u, const u
                       cudaStream_t s) {
   // Row sums of the redundant-row rule (rule_infeasible_and_redundant_rows.cu:46-156).
   if (!A.rows) return;
-  static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
-  const RowSchedule* sch;
-  if (live_deg) {
-    build_schedule(*live_schedule, A, live_deg, s);
-    sch = live_schedule;
-  } else {
-    sch = &stored_schedule(A);
-  }
-  const Roles r = roles_for(A.rows);
-  const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
-                       (keep_col ? A.cols : 0) + (live_deg ? 4.0 * A.rows : 0) + 16.0 * A.rows;
-  GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, r.short_blocks + r.medium_blocks + r.long_blocks, kThreads, 0, s,
-                   A.rows, A.ptr, A.idx, A.val, l, u, 0.0, keep_row, keep_col, live_deg, sch->medium.p,
-                   sch->long_rows.p, sch->counts.p, r.short_blocks, r.medium_blocks, row_min, row_max,
-                   (int32_t*)nullptr, (int32_t*)nullptr);
+  DBuf<double2> lu(size_t(std::max(A.cols, 1)), s);
+  pack_bounds(l, u, keep_col, A.cols, lu.p, s);
+  launch_activity<true>(A, lu.p, 0.0, keep_row, live_deg, row_min, row_max, nullptr, nullptr, 16.0, s);
 }
 
 void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStream_t s) {

@@ -49,12 +49,10 @@ struct CandArgs {
   const int32_t* idx;
   const double* val;
   const uint8_t* keep_row;
-  const uint8_t* keep_col;
   const int32_t* row_nnz;
   const double* AL;
   const double* AU;
-  const double* l;
-  const double* u;
+  const double2* lu;   // packed column bounds, removed columns marked
   RowSummary rs;
   double zero_tol;
   double* cand_l;
@@ -72,10 +70,11 @@ __device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
 
 __device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p) {
   const int j = __ldcs(g.idx + p);   // CSR streamed once: keep L2 for the gathered bounds
-  if (!g.keep_col[j]) return;
+  const double2 b = g.lu[j];
+  if (removed_column(b)) return;
   const double a = __ldcs(g.val + p);
   if (fabs(a) <= g.zero_tol) return;
-  const double ol = g.l[j], ou = g.u[j];
+  const double ol = b.x, ou = b.y;
   double il, iu;
   implied_bounds(a, ol, ou, rc.al, rc.au, rc.mn, rc.mx, rc.ni, rc.pi, il, iu);
   double nl = ol, nu = ou;
@@ -315,14 +314,16 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
   cu.copy_from(plan.u.p, size_t(n));
   Status st;
   st.clear(5);
-  row_activity_summary(lp.A, plan.l.p, plan.u.p, p.zero_tol, plan.keep_row.p, plan.keep_col.p, stats.row_nnz.p,
-                       mn.p, mx.p, ni.p, pi.p, s);
+  // One packed bounds array serves the activity sweep and the candidate sweep.
+  DBuf<double2> lu(size_t(n), s);
+  pack_bounds(plan.l.p, plan.u.p, plan.keep_col.p, n, lu.p, s);
+  row_activity_summary_packed(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p, s);
   const RowSummary rs{mn.p, mx.p, ni.p, pi.p};
   {
-    CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, plan.keep_col.p, stats.row_nnz.p, plan.AL.p,
-               plan.AU.p, plan.l.p, plan.u.p, rs, p.zero_tol, cl.p, cu.p};
-    const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + double(n) + 4.0 * m + 16.0 * m + 24.0 * m +
-                         16.0 * n + 16.0 * n;
+    CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, stats.row_nnz.p, plan.AL.p, plan.AU.p, lu.p, rs,
+               p.zero_tol, cl.p, cu.p};
+    const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + 4.0 * m + 16.0 * m + 24.0 * m + 16.0 * n +
+                         16.0 * n;
     const RowSchedule& sch = stored_schedule(lp.A);
     GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(sch.tiles, kNumSMs * 8))),
                      kThreads, 0, s, lp.A.nnz, sch.tile_rows.p, g);
