@@ -38,6 +38,17 @@ RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singl
          "parallel_rows", "parallel_columns", "doubleton_equations"]
 
 
+# DRAM bytes (read + write) per launch from one ncu --set full capture of the
+# full-size workload (summarised under profiles/): the mean over the captured
+# launches, which are the step's first (full-size) launches.
+MEASURED_TRAFFIC = {
+    "copy_kept": 673.1e6,
+    "activity_kernel<false>": 1312.5e6,
+    "activity_kernel<true>": 1165.2e6,
+    "candidates_entries": 1216.9e6,
+}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -86,6 +97,85 @@ class Clocks:
                     reasons.add(name)
         os.unlink(self.file.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons)}
+
+
+BATCH_DESC = ("config-0-style LPs, m log-uniform in [1,000, 200,000], n = 2.5m, seeds 1000+k "
+              "(the batched-form workload)")
+
+
+def batch_jobs(count):
+    """(m, seed) of every LP of the batched workload."""
+    import numpy as np
+    rng = np.random.default_rng(7)
+    ms = np.exp(rng.uniform(np.log(1000.0), np.log(200000.0), size=count)).astype(int)
+    return [(int(m), 1000 + k) for k, m in enumerate(ms)]
+
+
+def make_batch_lp(job):
+    """Generates one LP of the batched workload (runs in a spawned worker process)."""
+    from gpp_b200 import lpgen
+    m, seed = job
+    lp = lpgen.random_lp(m, int(2.5 * m), seed=seed)
+    lp.ensure_transpose()
+    return lp
+
+
+def run_batched(lps, params, max_workers):
+    """Batched form against looping the plain form over the same LPs, inputs resident on the GPU.
+
+    Returns the JSON object of the batched measurement."""
+    import numpy as np
+    import torch
+    from gpp_b200 import device
+    dlps = [device.DeviceLp(lp) for lp in lps]
+    torch.cuda.synchronize()
+
+    def zeros(s):
+        return (torch.zeros(s.reduced_cols, dtype=torch.float64, device="cuda"),
+                torch.zeros(s.reduced_rows, dtype=torch.float64, device="cuda"),
+                torch.zeros(s.reduced_cols, dtype=torch.float64, device="cuda"))
+
+    def key(s):
+        return (s.reduced_rows, s.reduced_cols, s.reduced_nnz, s.iterations, s.has_infeasible, s.has_unbounded,
+                s.obj_constant_delta)
+
+    # Looping the plain form: presolve + postsolve of one LP after another.
+    t0 = time.perf_counter()
+    plain_keys, plain_lat = [], []
+    for d in dlps:
+        s = device.preprocess(d, params)
+        device.postprocess(*zeros(s), s, d)
+        plain_keys.append(key(s))
+        plain_lat.append(s.preprocessing_seconds)
+        device.free_summary(s)
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+
+    workers = device.batch_autotune(dlps, params, max_workers=max_workers)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sums, _ = device.preprocess_batch(dlps, params, workers=workers)
+    reds = [zeros(s) for s in sums]
+    device.postprocess_batch([r[0] for r in reds], [r[1] for r in reds], [r[2] for r in reds], sums, dlps,
+                             workers=workers)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    match = sum(key(s) == k for s, k in zip(sums, plain_keys))
+    lat = [s.preprocessing_seconds for s in sums]
+    for s in sums:
+        device.free_summary(s)
+    nnz = sum(lp.nnz for lp in lps)
+    pct = lambda v, q: round(1e3 * float(np.percentile(v, q)), 3)
+    return {"lps": len(lps), "nnz_total": int(nnz), "workload": BATCH_DESC, "workers": workers,
+            "lps_per_s": round(len(lps) / t_batch, 2), "looped_lps_per_s": round(len(lps) / t_loop, 2),
+            "speedup_vs_looped": round(t_loop / t_batch, 2), "batch_s": round(t_batch, 3),
+            "looped_s": round(t_loop, 3),
+            "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "looped_p50": pct(plain_lat, 50),
+                           "looped_p99": pct(plain_lat, 99),
+                           "definition": "per-LP presolve wall time (preprocessing_seconds) inside each run"},
+            "match_plain": f"{match}/{len(lps)}",
+            "timing": "wall clock around presolve + postsolve of all LPs, device inputs resident, "
+                      "reduced solutions all-zero"}
 
 
 def dist_env():
@@ -137,6 +227,9 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) loop")
+    ap.add_argument("--batch", type=int, default=512,
+                    help="LPs in the batched-form measurement (0 skips it; N=1 only)")
+    ap.add_argument("--batch-max-workers", type=int, default=32)
     ap.add_argument("--kernel-table-out", default=None,
                     help="write every kernel's launches, ms and bytes per step to this CSV file")
     ap.add_argument("--no-kernel-table", action="store_true",
@@ -246,6 +339,15 @@ def main():
         barrier()
         e2e_ms = e0.elapsed_time(e1) / args.steps
 
+    # The batched workload is generated by spawned processes (after the timed
+    # loops, so they do not compete with them for host cores; they overlap the
+    # single-core CPU baseline instead).
+    batch_pool = batch_result = None
+    if args.batch > 0 and world == 1:
+        import multiprocessing as mp
+        batch_pool = mp.get_context("spawn").Pool(max(1, min(32, (os.cpu_count() or 2) - 2)))
+        batch_result = batch_pool.map_async(make_batch_lp, batch_jobs(args.batch), chunksize=1)
+
     if world > 1:
         t = torch.tensor([step_ms, e2e_ms or 0.0], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -264,7 +366,8 @@ def main():
             roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                         "launches_per_step": nl // args.steps, "avg_launch_us": round(1e3 * ms / nl, 2),
-                        "bytes_per_launch": int(by / nl), "traffic": None}
+                        "bytes_per_launch": int(by / nl),
+                        "traffic": MEASURED_TRAFFIC.get(name)}
     kernels = sorted(prof, key=lambda r: -r[2])[:8]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -278,6 +381,11 @@ def main():
             if wall:
                 cpu = {"value": round(1e3 * wall[0], 1), "unit": "ms", "cores": 1, "kind": "reference",
                        "sample": f"one PSLP 0.0.11 presolve of the full workload ({WORKLOAD_DESC}) on 1 host core"}
+    batched = None
+    if batch_result is not None:
+        batched = run_batched(batch_result.get(), params, args.batch_max_workers)
+        batch_pool.close()
+        batch_pool.join()
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": round(step_ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -297,6 +405,7 @@ def main():
             "kernels": [{"name": n, "launches_per_step": l // args.steps, "ms_per_step": round(m / args.steps, 3)}
                         for n, l, m, b in kernels],
             "cpu_baseline": cpu,
+            "batched": batched,
             "clocks": clk,
         }))
     if world > 1:

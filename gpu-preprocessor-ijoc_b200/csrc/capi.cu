@@ -2,10 +2,19 @@
 // exceptions and maps them to the status codes the header documents; the C++
 // API in include/gpu_preprocessor/ maps them back to the reference's
 // exception types.
+#include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <cmath>
+#include <functional>
 #include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "folding.hpp"
 #include "presolve.hpp"
@@ -24,6 +33,15 @@ const char* last_error();
 using gpp::check;
 
 namespace {
+
+constexpr int kDefaultBatchWorkers = 8;
+constexpr int kAutotuneSample = 32;
+
+// A batch whose items failed: carries the first failing item's status (the
+// message is already set).
+struct BatchFailure {
+  int status;
+};
 
 template <class F>
 int guarded(F f) {
@@ -49,6 +67,8 @@ int guarded(F f) {
   } catch (const std::exception& e) {
     gpp::set_last_error(e.what());
     return GPP_ERR_RUNTIME;
+  } catch (const BatchFailure& f) {
+    return f.status;
   }
 }
 
@@ -106,6 +126,163 @@ void identity_output(const gpp_lp& lp, gpp::PresolveOutput& o) {
   o.reduced.c = lp.c; o.reduced.AL = lp.AL; o.reduced.AU = lp.AU; o.reduced.l = lp.l; o.reduced.u = lp.u;
   o.reduced.obj = lp.obj_constant;
   o.owns_reduced = false;
+}
+
+// The body of gpp_preprocess.  `device_sync` waits for all work on the
+// device before the timer starts, as the reference's pipeline timing does;
+// the batched form skips it so that its workers do not wait on each other.
+void preprocess_into(const gpp_lp* lp, const gpp_params* params, gpp_summary* out, bool device_sync) {
+  if (!lp || !params || !out) throw std::invalid_argument("null argument");
+  validate_lp(*lp);
+  auto rec = std::make_unique<gpp_record>();
+  rec->presolve_enabled = params->enable_presolve != 0;
+  gpp::ctx().sync("before preprocessing timer");
+  if (device_sync) check(cudaDeviceSynchronize(), "before preprocessing timer");
+  const auto t0 = std::chrono::steady_clock::now();
+  if (params->enable_folding) gpp::run_folding(*lp, params->folding_tolerance, rec->folding);
+  const gpp_lp& input = rec->folding.applied ? rec->folding.folded : *lp;
+  if (params->enable_presolve) gpp::run_presolve(input, *params, rec->out);
+  else identity_output(input, rec->out);
+  gpp::ctx().sync("preprocessing completion");
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  fill_summary(out, rec.get(), secs);
+  rec.release();
+}
+
+// The body of gpp_postprocess.
+void postprocess_into(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
+                      const gpp_lp* original, double* x_out, double* y_out, double* z_out) {
+  if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+  const gpp_record* rec = summary->record;
+  auto s = gpp::ctx().stream;
+  const int n0 = summary->original_cols, m0 = summary->original_rows;
+  if (!rec->presolve_enabled && !rec->folding.applied) {
+    auto copy = [&](double* dst, const double* src, int n) {
+      if (dst && src && n) check(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "copy identity");
+    };
+    copy(x_out, x_red, n0); copy(y_out, y_red, m0); copy(z_out, z_red, n0);
+    gpp::ctx().sync("identity postprocess");
+    return;
+  }
+  const int pn = rec->out.record.n0, pm = rec->out.record.m0;
+  gpp::DBuf<double> x(size_t(std::max(pn, 1)), s), y(size_t(std::max(pm, 1)), s), z(size_t(std::max(pn, 1)), s);
+  if (!rec->presolve_enabled) {
+    if (pn) { check(cudaMemcpyAsync(x.p, x_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "x");
+              check(cudaMemcpyAsync(z.p, z_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "z"); }
+    if (pm) check(cudaMemcpyAsync(y.p, y_red, sizeof(double) * pm, cudaMemcpyDeviceToDevice, s), "y");
+  } else {
+    const gpp_lp* model = rec->folding.applied ? &rec->folding.folded : original;
+    gpp::run_postsolve(rec->out, x_red, y_red, z_red, model, x.p, y.p, z.p);
+  }
+  if (rec->folding.applied) {
+    gpp::unfold_to_host(rec->folding, x.p, y.p, z.p, x_out, y_out, z_out);
+  } else {
+    if (x_out && pn) check(cudaMemcpyAsync(x_out, x.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "x d2h");
+    if (y_out && pm) check(cudaMemcpyAsync(y_out, y.p, sizeof(double) * pm, cudaMemcpyDeviceToHost, s), "y d2h");
+    if (z_out && pn) check(cudaMemcpyAsync(z_out, z.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "z d2h");
+  }
+  gpp::ctx().sync("postprocess");
+}
+
+// ---- batched form ----------------------------------------------------------
+// A persistent pool of host threads.  Each thread keeps its own engine context
+// (stream, schedules, status buffer), so LPs given to different threads run
+// concurrently on the GPU and their host round-trips overlap.  Threads live
+// until process exit: their contexts are created once, not per batch.
+class WorkerPool {
+ public:
+  static WorkerPool& get() {
+    static WorkerPool* pool = new WorkerPool;   // never destroyed: detached threads use it until exit
+    return *pool;
+  }
+
+  // Runs task(order[0]), task(order[1]), ... on `workers` threads (the caller
+  // is one of them), each item exactly once, every thread with `device`
+  // current.  One batch at a time.
+  void run(int workers, int device, const std::vector<int>& order, const std::function<void(int)>& task) {
+    std::lock_guard<std::mutex> one_batch(batch_mutex_);
+    workers = std::max(1, workers);
+    {
+      std::unique_lock<std::mutex> lock(m_);
+      while (int(threads_) < workers - 1) {
+        std::thread([this, id = int(threads_)] { loop(id); }).detach();
+        ++threads_;
+      }
+      order_ = &order;
+      task_ = &task;
+      device_ = device;
+      next_.store(0);
+      active_ = workers - 1;
+      running_ = workers - 1;
+      ++generation_;
+    }
+    cv_.notify_all();
+    drain();
+    std::unique_lock<std::mutex> lock(m_);
+    done_.wait(lock, [this] { return running_ == 0; });
+    order_ = nullptr;
+    task_ = nullptr;
+  }
+
+ private:
+  void drain() {
+    for (size_t i = next_.fetch_add(1); i < order_->size(); i = next_.fetch_add(1)) (*task_)((*order_)[i]);
+  }
+  void loop(int id) {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lock(m_);
+        cv_.wait(lock, [&] { return generation_ != seen; });
+        seen = generation_;
+        if (id >= active_) continue;
+      }
+      cudaSetDevice(device_);
+      drain();
+      std::lock_guard<std::mutex> lock(m_);
+      if (--running_ == 0) done_.notify_all();
+    }
+  }
+
+  std::mutex batch_mutex_, m_;
+  std::condition_variable cv_, done_;
+  size_t threads_ = 0;
+  uint64_t generation_ = 0;
+  int active_ = 0, running_ = 0, device_ = 0;
+  std::atomic<size_t> next_{0};
+  const std::vector<int>* order_ = nullptr;
+  const std::function<void(int)>* task_ = nullptr;
+};
+
+// LP indices, largest nnz first (longest jobs start first, so the last
+// finishers are short ones).
+std::vector<int> largest_first(const gpp_lp* lps, int32_t count) {
+  std::vector<int> order(static_cast<size_t>(count));
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lps[a].A.nnz > lps[b].A.nnz; });
+  return order;
+}
+
+// Runs one item per LP under the status mapping of the plain entry points;
+// returns GPP_OK or the first failing status in LP order, whose message
+// becomes the caller's last error.
+int run_batch(int32_t count, int workers, const std::vector<int>& order, int32_t* status,
+              const std::function<void(int)>& body) {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::vector<int32_t> st(static_cast<size_t>(count), GPP_OK);
+  std::vector<std::string> msg(static_cast<size_t>(count));
+  WorkerPool::get().run(workers, dev, order, [&](int k) {
+    st[size_t(k)] = guarded([&] { body(k); });
+    if (st[size_t(k)] != GPP_OK) msg[size_t(k)] = gpp::last_error();
+  });
+  if (status) std::copy(st.begin(), st.end(), status);
+  for (int32_t k = 0; k < count; ++k)
+    if (st[size_t(k)] != GPP_OK) {
+      gpp::set_last_error("LP " + std::to_string(k) + ": " + msg[size_t(k)]);
+      return st[size_t(k)];
+    }
+  return GPP_OK;
 }
 
 }  // namespace
@@ -205,23 +382,7 @@ int gpp_run_presolve(const gpp_lp* lp, const gpp_params* params, int keep_reduce
 
 int gpp_preprocess(const gpp_lp* lp, const gpp_params* params, gpp_summary* out) {
   // folding::run_gpu_presolve_with_folding(lp, params, true, true) (folding.cu:172-213).
-  return guarded([&] {
-    if (!lp || !params || !out) throw std::invalid_argument("null argument");
-    validate_lp(*lp);
-    auto rec = std::make_unique<gpp_record>();
-    rec->presolve_enabled = params->enable_presolve != 0;
-    gpp::ctx().sync("before preprocessing timer");
-    check(cudaDeviceSynchronize(), "before preprocessing timer");
-    const auto t0 = std::chrono::steady_clock::now();
-    if (params->enable_folding) gpp::run_folding(*lp, params->folding_tolerance, rec->folding);
-    const gpp_lp& input = rec->folding.applied ? rec->folding.folded : *lp;
-    if (params->enable_presolve) gpp::run_presolve(input, *params, rec->out);
-    else identity_output(input, rec->out);
-    gpp::ctx().sync("preprocessing completion");
-    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    fill_summary(out, rec.get(), secs);
-    rec.release();
-  });
+  return guarded([&] { preprocess_into(lp, params, out, true); });
 }
 
 int gpp_postsolve_device(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
@@ -237,38 +398,7 @@ int gpp_postsolve_device(const double* x_red, const double* y_red, const double*
 int gpp_postprocess(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
                     const gpp_lp* original, double* x_out, double* y_out, double* z_out) {
   // postsolve_and_unfold_to_host (folding.cu:215-261).
-  return guarded([&] {
-    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
-    const gpp_record* rec = summary->record;
-    auto s = gpp::ctx().stream;
-    const int n0 = summary->original_cols, m0 = summary->original_rows;
-    if (!rec->presolve_enabled && !rec->folding.applied) {
-      auto copy = [&](double* dst, const double* src, int n) {
-        if (dst && src && n) check(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "copy identity");
-      };
-      copy(x_out, x_red, n0); copy(y_out, y_red, m0); copy(z_out, z_red, n0);
-      gpp::ctx().sync("identity postprocess");
-      return;
-    }
-    const int pn = rec->out.record.n0, pm = rec->out.record.m0;
-    gpp::DBuf<double> x(size_t(std::max(pn, 1)), s), y(size_t(std::max(pm, 1)), s), z(size_t(std::max(pn, 1)), s);
-    if (!rec->presolve_enabled) {
-      if (pn) { check(cudaMemcpyAsync(x.p, x_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "x");
-                check(cudaMemcpyAsync(z.p, z_red, sizeof(double) * pn, cudaMemcpyDeviceToDevice, s), "z"); }
-      if (pm) check(cudaMemcpyAsync(y.p, y_red, sizeof(double) * pm, cudaMemcpyDeviceToDevice, s), "y");
-    } else {
-      const gpp_lp* model = rec->folding.applied ? &rec->folding.folded : original;
-      gpp::run_postsolve(rec->out, x_red, y_red, z_red, model, x.p, y.p, z.p);
-    }
-    if (rec->folding.applied) {
-      gpp::unfold_to_host(rec->folding, x.p, y.p, z.p, x_out, y_out, z_out);
-    } else {
-      if (x_out && pn) check(cudaMemcpyAsync(x_out, x.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "x d2h");
-      if (y_out && pm) check(cudaMemcpyAsync(y_out, y.p, sizeof(double) * pm, cudaMemcpyDeviceToHost, s), "y d2h");
-      if (z_out && pn) check(cudaMemcpyAsync(z_out, z.p, sizeof(double) * pn, cudaMemcpyDeviceToHost, s), "z d2h");
-    }
-    gpp::ctx().sync("postprocess");
-  });
+  return guarded([&] { postprocess_into(x_red, y_red, z_red, summary, original, x_out, y_out, z_out); });
 }
 
 void gpp_free_summary(gpp_summary* summary) {
@@ -497,4 +627,72 @@ uint64_t gpp_host_syncs(int reset) {
   return v;
 }
 
+
+int gpp_preprocess_batch(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t workers,
+                         gpp_summary* out, int32_t* status) {
+  if (count < 0 || (count > 0 && (!lps || !params || !out))) {
+    gpp::set_last_error("gpp_preprocess_batch: null argument or negative count");
+    return GPP_ERR_INVALID;
+  }
+  if (count == 0) return GPP_OK;
+  const int w = workers > 0 ? workers : kDefaultBatchWorkers;
+  return guarded([&] {
+    check(cudaDeviceSynchronize(), "before batch");   // inputs queued on any stream are complete
+    for (int32_t k = 0; k < count; ++k) out[k] = gpp_summary{};
+    const int rc = run_batch(count, w, largest_first(lps, count), status,
+                             [&](int k) { preprocess_into(&lps[k], params, &out[k], false); });
+    if (rc != GPP_OK) throw BatchFailure{rc};
+  });
+}
+
+int gpp_postprocess_batch(const double* const* x_red, const double* const* y_red, const double* const* z_red,
+                          const gpp_summary* summaries, const gpp_lp* originals, int32_t count, int32_t workers,
+                          double* const* x_out, double* const* y_out, double* const* z_out, int32_t* status) {
+  if (count < 0 || (count > 0 && (!summaries || !originals))) {
+    gpp::set_last_error("gpp_postprocess_batch: null argument or negative count");
+    return GPP_ERR_INVALID;
+  }
+  if (count == 0) return GPP_OK;
+  const int w = workers > 0 ? workers : kDefaultBatchWorkers;
+  auto at = [](auto a, int k) { return a ? a[k] : nullptr; };
+  return guarded([&] {
+    check(cudaDeviceSynchronize(), "before batch");
+    const int rc = run_batch(count, w, largest_first(originals, count), status, [&](int k) {
+      postprocess_into(at(x_red, k), at(y_red, k), at(z_red, k), &summaries[k], &originals[k], at(x_out, k),
+                       at(y_out, k), at(z_out, k));
+    });
+    if (rc != GPP_OK) throw BatchFailure{rc};
+  });
+}
+
+int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
+                       int32_t* best_workers) {
+  if (count <= 0 || !lps || !params || !best_workers || max_workers < 1) {
+    gpp::set_last_error("gpp_batch_autotune: empty batch, null argument or max_workers < 1");
+    return GPP_ERR_INVALID;
+  }
+  return guarded([&] {
+    // A sample that keeps the batch's size mix: every k-th LP of the
+    // largest-first order, at most kAutotuneSample of them.
+    const std::vector<int> order = largest_first(lps, count);
+    const int stride = std::max<int>(1, (count + kAutotuneSample - 1) / kAutotuneSample);
+    std::vector<gpp_lp> sample;
+    for (size_t i = 0; i < order.size(); i += size_t(stride)) sample.push_back(lps[order[i]]);
+    std::vector<gpp_summary> out(sample.size());
+    double best_rate = -1.0;
+    int best = 1;
+    for (int w = 1; w <= max_workers; w *= 2) {
+      check(cudaDeviceSynchronize(), "autotune");
+      const auto t0 = std::chrono::steady_clock::now();
+      const int rc = gpp_preprocess_batch(sample.data(), int32_t(sample.size()), params, w, out.data(), nullptr);
+      const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      for (auto& o : out) gpp_free_summary(&o);
+      if (rc != GPP_OK) throw BatchFailure{rc};
+      const double rate = double(sample.size()) / std::max(secs, 1e-9);
+      // A larger pool must beat the best so far by 5% to be chosen.
+      if (rate > best_rate * 1.05) { best_rate = rate; best = w; }
+    }
+    *best_workers = best;
+  });
+}
 }  // extern "C"

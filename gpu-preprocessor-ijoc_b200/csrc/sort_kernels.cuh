@@ -63,29 +63,29 @@ digit_scatter(const uint64_t* __restrict__ keys, const int32_t* __restrict__ val
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t base = int64_t(blockIdx.x) * kTile;
   const int tile_n = int(min(int64_t(kTile), n - base));
-  // Tile-local digit counts (the scan of the digit-major table gives the
-  // global start of this tile's run of each digit).
-  global_start[threadIdx.x] = offsets[int64_t(threadIdx.x) * tiles + blockIdx.x];
-  running[threadIdx.x] = 0;
-  __syncthreads();
-  for (int k = 0; k < kItems; ++k) {
-    const int64_t i = base + int64_t(k) * kThreads + threadIdx.x;
-    if (i < n) atomicAdd(&running[int((keys[i] >> shift) & 0xff)], 1);
-  }
-  __syncthreads();
-  // Exclusive scan of the 256 tile counts (one thread per digit).
+  // The scanned digit-major table holds this tile's run start of every
+  // digit; the next entry (the same digit's next tile, or the next digit's
+  // first tile) minus it is the tile's count of that digit, so no recount.
+  const int64_t at = int64_t(threadIdx.x) * tiles + blockIdx.x;
+  const int32_t start_d = offsets[at];
+  const int32_t count_d = offsets[at + 1] - start_d;
+  global_start[threadIdx.x] = start_d;
   {
-    __shared__ int32_t scan[256];
-    scan[threadIdx.x] = running[threadIdx.x];
-    __syncthreads();
-    for (int off = 1; off < 256; off <<= 1) {
-      const int32_t t = threadIdx.x >= unsigned(off) ? scan[threadIdx.x - off] : 0;
-      __syncthreads();
-      scan[threadIdx.x] += t;
-      __syncthreads();
+    // Exclusive scan of the 256 tile counts, one digit per thread.
+    __shared__ int32_t warp_total[8];
+    int32_t incl = count_d;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int32_t peer = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += peer;
     }
-    digit_start[threadIdx.x] = scan[threadIdx.x] - running[threadIdx.x];
-    running[threadIdx.x] = digit_start[threadIdx.x];
+    if (lane == 31) warp_total[warp] = incl;
+    __syncthreads();
+    int32_t before = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) before += w < warp ? warp_total[w] : 0;
+    digit_start[threadIdx.x] = before + incl - count_d;
+    running[threadIdx.x] = before + incl - count_d;
   }
   __syncthreads();
   for (int k = 0; k < kItems; ++k) {

@@ -34,7 +34,7 @@ namespace {
 
 constexpr int64_t kStaticPairs = GPP_SORT_STATIC_MAX_PAIRS;
 constexpr int64_t kStaticTiles = (kStaticPairs + kTile - 1) / kTile;
-constexpr int64_t kStaticCounts = 256 * kStaticTiles;
+constexpr int64_t kStaticCounts = 256 * kStaticTiles + 1;   // digit-major table and its total
 constexpr size_t kKeysOffset = 0;
 constexpr size_t kValsOffset = kKeysOffset + sizeof(uint64_t) * size_t(kStaticPairs);
 constexpr size_t kCountsOffset = kValsOffset + sizeof(int32_t) * size_t(kStaticPairs);
@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_counts_one_block(int32_t* _
     counts[i] = run;
     run += v;
   }
+  if (threadIdx.x == kScanThreads - 1) counts[n] = sm[kScanThreads - 1];   // the total, read by the scatter
 }
 
 void launched(const char* what) {

@@ -162,6 +162,9 @@ def load():
         "gpp_last_error": (C.c_char_p, []),
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
         "gpp_host_syncs": (C.c_uint64, [C.c_int]),
+        "gpp_preprocess_batch": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, vp, vp]),
+        "gpp_postprocess_batch": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp]),
+        "gpp_batch_autotune": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, P(C.c_int32)]),
         "gpp_profile_enable": (None, [C.c_int]),
         "gpp_profile_read": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(i64), P(f64), P(f64)]),
     }
@@ -179,7 +182,8 @@ EXPORTED = [
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
     "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_alloc", "gpp_device_free",
     "gpp_export_folding_map", "gpp_unfold_solution",
-    "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs", "gpp_profile_enable", "gpp_profile_read",
+    "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
+    "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune", "gpp_profile_enable", "gpp_profile_read",
 ]
 
 

@@ -209,3 +209,57 @@ def unfold(x_folded, y_folded, z_folded, summary: capi.Summary):
                                            x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
                                            z.ctypes.data_as(C.c_void_p)))
     return x, y, z
+
+
+def _ptr_array(values):
+    arr = (C.c_void_p * max(1, len(values)))()
+    for k, v in enumerate(values):
+        arr[k] = v
+    return arr
+
+
+def preprocess_batch(dlps, params=None, workers: int = 0):
+    """gpp_preprocess_batch: one summary per LP (each as gpp_preprocess gives it) and the per-LP statuses.
+
+    Raises on a failed batch after freeing the summaries it made."""
+    lib = capi.load()
+    params = params or capi.Params.defaults()
+    lps = (capi.Lp * len(dlps))(*[d.struct() for d in dlps])
+    out = (capi.Summary * len(dlps))()
+    status = np.zeros(len(dlps), np.int32)
+    rc = lib.gpp_preprocess_batch(C.cast(lps, C.c_void_p), len(dlps), C.byref(params), workers,
+                                  C.cast(out, C.c_void_p), status.ctypes.data_as(C.c_void_p))
+    summaries = [out[k] for k in range(len(dlps))]
+    if rc != 0:
+        for s in summaries:
+            free_summary(s)
+        _raise(rc)
+    return summaries, status
+
+
+def postprocess_batch(xs, ys, zs, summaries, dlps, workers: int = 0):
+    """gpp_postprocess_batch: xs/ys/zs are per-LP CUDA float64 tensors (or None) in reduced order;
+    returns per-LP host (x, y, z) in original order."""
+    lib = capi.load()
+    k = len(summaries)
+    outs = [(np.zeros(s.original_cols), np.zeros(s.original_rows), np.zeros(s.original_cols)) for s in summaries]
+    sums = (capi.Summary * k)(*summaries)
+    lps = (capi.Lp * k)(*[d.struct() for d in dlps])
+    dev = [_ptr_array([ptr(v[i]) if v is not None and v[i] is not None else None for i in range(k)])
+           for v in (xs, ys, zs)]
+    host = [_ptr_array([o[j].ctypes.data for o in outs]) for j in range(3)]
+    status = np.zeros(k, np.int32)
+    _raise(lib.gpp_postprocess_batch(*(C.cast(a, C.c_void_p) for a in dev), C.cast(sums, C.c_void_p),
+                                     C.cast(lps, C.c_void_p), k, workers,
+                                     *(C.cast(a, C.c_void_p) for a in host), status.ctypes.data_as(C.c_void_p)))
+    return outs
+
+
+def batch_autotune(dlps, params=None, max_workers: int = 32) -> int:
+    """gpp_batch_autotune: the worker count of the best sampled throughput."""
+    lib = capi.load()
+    params = params or capi.Params.defaults()
+    lps = (capi.Lp * len(dlps))(*[d.struct() for d in dlps])
+    best = C.c_int32(0)
+    _raise(lib.gpp_batch_autotune(C.cast(lps, C.c_void_p), len(dlps), C.byref(params), max_workers, C.byref(best)))
+    return int(best.value)

@@ -248,6 +248,38 @@ GPP_API int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_colo
 GPP_API int gpp_unfold_solution(const gpp_summary* summary, const double* x_folded, const double* y_folded,
                                 const double* z_folded, double* x_out, double* y_out, double* z_out);
 
+/* ---- Batched form --------------------------------------------------------- */
+
+/* Presolves `count` independent LPs (lps[k] -> out[k]), each exactly as
+ * gpp_preprocess would: the same rules, the same results.  The LPs are spread
+ * over `workers` host threads of the library (workers <= 0: 8), each with its
+ * own stream on the current device, largest LP first, so that many small LPs
+ * keep the GPU busy while each one waits on its own host round-trips.  The
+ * threads are created on first use and kept until exit.  status[k] (may be
+ * NULL) receives LP k's status; the return value is GPP_OK or the first
+ * failing LP's status, with gpp_last_error naming that LP.  Free every out[k]
+ * with gpp_free_summary, whether or not the batch succeeded.  The reference has
+ * no batched entry point; this is the batched form of its plain path. */
+GPP_API int gpp_preprocess_batch(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t workers,
+                                 gpp_summary* out, int32_t* status);
+
+/* gpp_postprocess for each LP of a batch, on the same worker threads:
+ * x_red[k], y_red[k], z_red[k] are LP k's reduced solution (device; the
+ * arrays of pointers, and any entry, may be NULL), x_out[k], y_out[k],
+ * z_out[k] its host outputs in original order. */
+GPP_API int gpp_postprocess_batch(const double* const* x_red, const double* const* y_red,
+                                  const double* const* z_red, const gpp_summary* summaries,
+                                  const gpp_lp* originals, int32_t count, int32_t workers,
+                                  double* const* x_out, double* const* y_out, double* const* z_out,
+                                  int32_t* status);
+
+/* Chooses the worker count for a batch: times gpp_preprocess_batch on a
+ * sample of up to 32 of the LPs (every k-th by size) with 1, 2, 4, ... up to
+ * max_workers threads and writes the count of the best throughput (a larger
+ * count must win by 5%). */
+GPP_API int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
+                               int32_t* best_workers);
+
 /* ---- Kernel-level entry points (rule / kernel parity tests) -------------- */
 
 /* compute_row_activity_summary (presolve/gpu_presolve_kernels.hpp:76-86):
