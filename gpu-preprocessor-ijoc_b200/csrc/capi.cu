@@ -666,7 +666,7 @@ int gpp_postprocess_batch(const double* const* x_red, const double* const* y_red
 }
 
 int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
-                       int32_t* best_workers) {
+                       int32_t* best_workers, double* rates) {
   if (count <= 0 || !lps || !params || !best_workers || max_workers < 1) {
     gpp::set_last_error("gpp_batch_autotune: empty batch, null argument or max_workers < 1");
     return GPP_ERR_INVALID;
@@ -680,7 +680,7 @@ int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* param
     for (size_t i = 0; i < order.size(); i += size_t(stride)) sample.push_back(lps[order[i]]);
     std::vector<gpp_summary> out(sample.size());
     double best_rate = -1.0;
-    int best = 1;
+    int best = 1, tried = 0;
     for (int w = 1; w <= max_workers; w *= 2) {
       check(cudaDeviceSynchronize(), "autotune");
       const auto t0 = std::chrono::steady_clock::now();
@@ -689,6 +689,8 @@ int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* param
       for (auto& o : out) gpp_free_summary(&o);
       if (rc != GPP_OK) throw BatchFailure{rc};
       const double rate = double(sample.size()) / std::max(secs, 1e-9);
+      if (rates) rates[tried] = rate;
+      ++tried;
       // A larger pool must beat the best so far by 5% to be chosen.
       if (rate > best_rate * 1.05) { best_rate = rate; best = w; }
     }

@@ -2,6 +2,8 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <chrono>
+#include <string>
 #include <memory>
 #include <mutex>
 
@@ -21,12 +23,29 @@ Context::Context() {
   // Blocking stream: implicitly ordered after work the caller queued on the
   // legacy default stream, as the reference's synchronous API assumes.
   check(cudaStreamCreateWithFlags(&stream, cudaStreamDefault), "cudaStreamCreate");
-  cudaMemPool_t pool;
-  check(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
+  // A pool of this context alone: with one pool per host thread, the batched
+  // form's workers neither share a pool lock nor get ordered after each other
+  // by block reuse across their streams.
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
   uint64_t keep = UINT64_MAX;  // keep freed blocks in the pool between presolve calls
   check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool threshold");
   check(cudaMallocHost(reinterpret_cast<void**>(&host_status), sizeof(int32_t) * kStatusWords),
         "cudaMallocHost status");
+}
+
+void Context::sync(const char* label) {
+  ++sync_counter();
+  if (!profiling()) {
+    check(cudaStreamSynchronize(stream), label);
+    return;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  check(cudaStreamSynchronize(stream), label);
+  profile_sync(label, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
 }
 
 Context::~Context() {
@@ -48,7 +67,11 @@ Context& ctx() {
   return *(*per_device)[size_t(dev)];
 }
 
-Status::Status() { check(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().stream), "status alloc"); }
+Status::Status() {
+  check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().pool,
+                                ctx().stream),
+        "status alloc");
+}
 Status::~Status() { if (d) cudaFreeAsync(d, ctx().stream); }
 void Status::clear(int words) {
   check(cudaMemsetAsync(d, 0, sizeof(int32_t) * size_t(words), ctx().stream), "status clear");
@@ -119,8 +142,8 @@ __global__ void __launch_bounds__(kThreads) tile_reduce(const T* __restrict__ in
 // total to out[n].  `in` and `out` may alias: a thread reads its own items
 // before it writes them, and no thread touches another's.
 template <class T>
-__global__ void __launch_bounds__(kThreads) tile_scan(const T* __restrict__ in, int64_t n,
-                                                     const T* __restrict__ tile_sums, T* __restrict__ out) {
+__global__ void __launch_bounds__(kThreads) tile_scan(const T* in, int64_t n, const T* __restrict__ tile_sums,
+                                                     T* out) {
   __shared__ T warp_sums[kScanWarps];
   T offset = 0;
   for (int k = threadIdx.x; k < int(blockIdx.x); k += kThreads) offset += tile_sums[k];
@@ -142,19 +165,54 @@ __global__ void __launch_bounds__(kThreads) tile_scan(const T* __restrict__ in, 
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kThreads - 1) out[n] = run;
 }
 
+// Scan of up to kSmallScan items in one block of 1024 threads: thread t owns
+// a run of consecutive items; the runs' sums are scanned across the block by
+// warp shuffles and one shared round of warp totals.  `in` and `out` may
+// alias (each thread reads its items before writing them).
+constexpr int kSmallScanThreads = 1024;
+constexpr int64_t kSmallScan = 32 * kSmallScanThreads;
+
+template <class T>
+__global__ void __launch_bounds__(kSmallScanThreads) small_scan(const T* in, int64_t n, T* out) {
+  __shared__ T warp_sums[kSmallScanThreads / 32];
+  const int64_t per = (n + kSmallScanThreads - 1) / kSmallScanThreads;
+  const int64_t begin = int64_t(threadIdx.x) * per;
+  const int64_t end = min(n, begin + per);
+  T local = 0;
+  for (int64_t i = begin; i < end; ++i) local += in[i];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T incl = local;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T peer = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += peer;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  T before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_sums[w];
+  T run = before + incl - local;
+  for (int64_t i = begin; i < end; ++i) {
+    const T v = in[i];
+    out[i] = run;
+    run += v;
+  }
+  if (threadIdx.x == kSmallScanThreads - 1) out[n] = before + incl;
+}
+
 // Exclusive scan of n items into out[0..n], out[n] the total: one launch up
-// to kScanTile items, two above.
+// to kSmallScan items, two above.
 template <class T>
 void exclusive_scan(const T* in, T* out, int64_t n, cudaStream_t s) {
   if (n <= 0) {
     check(cudaMemsetAsync(out, 0, sizeof(T), s), "scan empty");
     return;
   }
-  const int64_t tiles = (n + kScanTile - 1) / kScanTile;
-  if (tiles == 1) {
-    GPP_LAUNCH(tile_scan<T>, 1, kThreads, 0, s, in, n, static_cast<const T*>(nullptr), out);
+  if (n <= kSmallScan) {
+    GPP_LAUNCH(small_scan<T>, 1, kSmallScanThreads, 0, s, in, n, out);
     return;
   }
+  const int64_t tiles = (n + kScanTile - 1) / kScanTile;
   DBuf<T> sums(size_t(tiles), s);
   GPP_LAUNCH(tile_reduce<T>, int(tiles), kThreads, 0, s, in, n, sums.p);
   GPP_LAUNCH(tile_scan<T>, int(tiles), kThreads, 0, s, in, n, sums.p, out);
@@ -217,9 +275,10 @@ namespace {
 thread_local std::string g_last_error;
 
 struct ProfileRecord {
-  const char* name;
+  std::string name;
   double bytes;
-  cudaEvent_t begin, end;
+  cudaEvent_t begin, end;   // null for a host wait, whose host time is host_ms
+  double host_ms;
 };
 struct ProfileState {
   bool on = false;
@@ -244,7 +303,10 @@ cudaEvent_t profile_event() {
   return p.pool[p.next++];
 }
 void profile_record(const char* name, double bytes, cudaEvent_t begin, cudaEvent_t end) {
-  profile_state().records.push_back({name, bytes, begin, end});
+  profile_state().records.push_back({name, bytes, begin, end, 0.0});
+}
+void profile_sync(const char* label, double ms) {
+  profile_state().records.push_back({std::string("sync: ") + label, 0.0, nullptr, nullptr, ms});
 }
 void profile_enable(bool on) {
   auto& p = profile_state();
@@ -258,8 +320,8 @@ std::vector<ProfileSummary> profile_summary() {
   check(cudaDeviceSynchronize(), "profile sync");
   std::vector<ProfileSummary> out;
   for (const auto& r : p.records) {
-    float ms = 0.f;
-    check(cudaEventElapsedTime(&ms, r.begin, r.end), "cudaEventElapsedTime");
+    float ms = float(r.host_ms);
+    if (r.begin) check(cudaEventElapsedTime(&ms, r.begin, r.end), "cudaEventElapsedTime");
     ProfileSummary* s = nullptr;
     for (auto& o : out)
       if (o.name == r.name) s = &o;

@@ -168,16 +168,16 @@ __device__ __forceinline__ int block_append(int32_t* counter, bool take) {
 struct Context {
   cudaStream_t stream = nullptr;
   int device = -1;
+  cudaMemPool_t pool = nullptr;   // this context's own stream-ordered pool
   int32_t* host_status = nullptr;   // pinned, kStatusWords ints
   static constexpr int kStatusWords = 64;
   Context();
   ~Context();
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
-  void sync(const char* ctx) {
-    ++sync_counter();
-    check(cudaStreamSynchronize(stream), ctx);
-  }
+  // Waits for the engine stream (`ctx` names the call site; while profiling,
+  // each wait is recorded as "sync: <ctx>" with its host time).
+  void sync(const char* ctx);
 };
 Context& ctx();
 
@@ -192,7 +192,8 @@ struct DBuf {
     release();
     s = stream ? stream : ctx().stream;
     n = count;
-    if (count) check(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s), "cudaMallocAsync");
+    if (count) check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().pool, s),
+                     "cudaMallocFromPoolAsync");
   }
   void release() {
     if (p) cudaFreeAsync(p, s);
@@ -230,7 +231,9 @@ struct DBuf {
 template <class T>
 T* dalloc(size_t count) {
   T* p = nullptr;
-  if (count) check(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().stream), "cudaMallocAsync");
+  if (count)
+    check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().pool, ctx().stream),
+          "cudaMallocFromPoolAsync");
   return p;
 }
 inline void dfree(void* p) {
@@ -285,6 +288,7 @@ struct ProfileSummary {
   double bytes;
 };
 void profile_enable(bool on);
+void profile_sync(const char* label, double ms);
 std::vector<ProfileSummary> profile_summary();
 
 // Thread-local error message for the C ABI.

@@ -164,7 +164,7 @@ def load():
         "gpp_host_syncs": (C.c_uint64, [C.c_int]),
         "gpp_preprocess_batch": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, vp, vp]),
         "gpp_postprocess_batch": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp]),
-        "gpp_batch_autotune": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, P(C.c_int32)]),
+        "gpp_batch_autotune": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, P(C.c_int32), vp]),
         "gpp_profile_enable": (None, [C.c_int]),
         "gpp_profile_read": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(i64), P(f64), P(f64)]),
     }

@@ -157,17 +157,19 @@ def preprocess(dlp: DeviceLp, params=None) -> capi.Summary:
     return s
 
 
-def postprocess(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp):
-    """x/y/z_red: torch CUDA float64 tensors in reduced order; returns host numpy x, y, z."""
+def postprocess(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp, out=None):
+    """x/y/z_red: torch CUDA float64 tensors in reduced order; returns host x, y, z in original order.
+
+    ``out`` may give the three host arrays (numpy arrays, or CPU torch tensors such as
+    page-locked ones, which download faster); otherwise numpy arrays are allocated."""
     lib = capi.load()
-    x = np.zeros(summary.original_cols)
-    y = np.zeros(summary.original_rows)
-    z = np.zeros(summary.original_cols)
+    if out is None:
+        out = (np.zeros(summary.original_cols), np.zeros(summary.original_rows), np.zeros(summary.original_cols))
+    addr = [a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr() for a in out]
     lp = original.struct()
     _raise(lib.gpp_postprocess(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
-                               x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
-                               z.ctypes.data_as(C.c_void_p)))
-    return x, y, z
+                               *(C.c_void_p(v) for v in addr)))
+    return out
 
 
 def free_summary(summary: capi.Summary) -> None:
@@ -255,11 +257,14 @@ def postprocess_batch(xs, ys, zs, summaries, dlps, workers: int = 0):
     return outs
 
 
-def batch_autotune(dlps, params=None, max_workers: int = 32) -> int:
-    """gpp_batch_autotune: the worker count of the best sampled throughput."""
+def batch_autotune(dlps, params=None, max_workers: int = 32):
+    """gpp_batch_autotune: (best worker count, {worker count: sampled LPs/s})."""
     lib = capi.load()
     params = params or capi.Params.defaults()
     lps = (capi.Lp * len(dlps))(*[d.struct() for d in dlps])
     best = C.c_int32(0)
-    _raise(lib.gpp_batch_autotune(C.cast(lps, C.c_void_p), len(dlps), C.byref(params), max_workers, C.byref(best)))
-    return int(best.value)
+    counts = [1 << k for k in range(max_workers.bit_length()) if (1 << k) <= max_workers]
+    rates = np.zeros(len(counts))
+    _raise(lib.gpp_batch_autotune(C.cast(lps, C.c_void_p), len(dlps), C.byref(params), max_workers, C.byref(best),
+                                  rates.ctypes.data_as(C.c_void_p)))
+    return int(best.value), {w: round(float(r), 2) for w, r in zip(counts, rates)}

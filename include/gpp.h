@@ -276,9 +276,10 @@ GPP_API int gpp_postprocess_batch(const double* const* x_red, const double* cons
 /* Chooses the worker count for a batch: times gpp_preprocess_batch on a
  * sample of up to 32 of the LPs (every k-th by size) with 1, 2, 4, ... up to
  * max_workers threads and writes the count of the best throughput (a larger
- * count must win by 5%). */
+ * count must win by 5%).  `rates` (may be NULL; one entry per count tried,
+ * floor(log2(max_workers)) + 1 of them) receives the sampled LPs/s. */
 GPP_API int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
-                               int32_t* best_workers);
+                               int32_t* best_workers, double* rates);
 
 /* ---- Kernel-level entry points (rule / kernel parity tests) -------------- */
 

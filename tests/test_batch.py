@@ -94,5 +94,5 @@ def test_batch_failure_stays_with_its_lp():
 
 def test_autotune_picks_a_power_of_two():
     dlps = [device.DeviceLp(lp) for lp in batch_lps()]
-    best = device.batch_autotune(dlps, capi.Params.defaults(), max_workers=8)
-    assert best in (1, 2, 4, 8)
+    best, curve = device.batch_autotune(dlps, capi.Params.defaults(), max_workers=8)
+    assert best in (1, 2, 4, 8) and sorted(curve) == [1, 2, 4, 8] and all(r > 0 for r in curve.values())
