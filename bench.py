@@ -390,6 +390,29 @@ def main():
             if wall:
                 cpu = {"value": round(1e3 * wall[0], 1), "unit": "ms", "cores": 1, "kind": "reference",
                        "sample": f"one PSLP 0.0.11 presolve of the full workload ({WORKLOAD_DESC}) on 1 host core"}
+    # Learned round schedule on the same LP (held out: the schedule is trained
+    # on LPs of at most 500,000 rows): presolve time and the share of the
+    # plain run's nnz removal it keeps.
+    learned = None
+    from gpp_b200 import schedule
+    if rank == 0 and os.path.exists(schedule.MODEL_FILE):
+        w_sched, skip_below, stop_above = schedule.load_model()
+        with schedule.Model(w_sched, skip_below, stop_above) as model:
+            times, kept_nnz = [], None
+            for it in range(max(args.warmup, 3) + args.steps):
+                s = schedule.scheduled_preprocess(dlp, params, model)
+                if it >= max(args.warmup, 3):
+                    times.append(1e3 * s.elapsed_seconds)
+                kept_nnz = s.reduced_nnz
+                device.free_summary(s)
+        plain_ms = statistics.mean(pre_ms)
+        removed_plain = lp.nnz - reduced[2]
+        learned = {"presolve_ms": round(statistics.mean(times), 3), "plain_presolve_ms": round(plain_ms, 3),
+                   "time_ratio": round(statistics.mean(times) / plain_ms, 4),
+                   "nnz_removal_kept": round((lp.nnz - kept_nnz) / removed_plain, 5) if removed_plain else 1.0,
+                   "skip_below": skip_below, "stop_above": stop_above,
+                   "model": "2x64 FP32 MLP, trained on plain-loop traces"}
+
     batched = None
     if batch_result is not None:
         batched = run_batched(batch_result.get(), params, args.batch_max_workers)
@@ -415,6 +438,7 @@ def main():
                         for n, l, m, b in kernels],
             "cpu_baseline": cpu,
             "batched": batched,
+            "learned_schedule": learned,
             "clocks": clk,
         }))
     if world > 1:

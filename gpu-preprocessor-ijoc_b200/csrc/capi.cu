@@ -18,7 +18,12 @@
 
 #include "folding.hpp"
 #include "presolve.hpp"
+#include "schedule_mlp.hpp"
 #include "sort.hpp"
+
+struct gpp_schedule_model {
+  std::unique_ptr<gpp::MlpSchedule> policy;
+};
 
 struct gpp_record {
   gpp::PresolveOutput out;
@@ -131,7 +136,8 @@ void identity_output(const gpp_lp& lp, gpp::PresolveOutput& o) {
 // The body of gpp_preprocess.  `device_sync` waits for all work on the
 // device before the timer starts, as the reference's pipeline timing does;
 // the batched form skips it so that its workers do not wait on each other.
-void preprocess_into(const gpp_lp* lp, const gpp_params* params, gpp_summary* out, bool device_sync) {
+void preprocess_into(const gpp_lp* lp, const gpp_params* params, gpp_summary* out, bool device_sync,
+                     gpp::SchedulePolicy* policy = nullptr, std::vector<gpp::RoundRecord>* trace = nullptr) {
   if (!lp || !params || !out) throw std::invalid_argument("null argument");
   validate_lp(*lp);
   auto rec = std::make_unique<gpp_record>();
@@ -141,7 +147,7 @@ void preprocess_into(const gpp_lp* lp, const gpp_params* params, gpp_summary* ou
   const auto t0 = std::chrono::steady_clock::now();
   if (params->enable_folding) gpp::run_folding(*lp, params->folding_tolerance, rec->folding);
   const gpp_lp& input = rec->folding.applied ? rec->folding.folded : *lp;
-  if (params->enable_presolve) gpp::run_presolve(input, *params, rec->out);
+  if (params->enable_presolve) gpp::run_presolve(input, *params, rec->out, policy, trace);
   else identity_output(input, rec->out);
   gpp::ctx().sync("preprocessing completion");
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -695,6 +701,74 @@ int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* param
       if (rate > best_rate * 1.05) { best_rate = rate; best = w; }
     }
     *best_workers = best;
+  });
+}
+
+int gpp_preprocess_traced(const gpp_lp* lp, const gpp_params* params, gpp_summary* out, float* features,
+                          int32_t* round_info, int64_t* round_nnz, int32_t max_rounds, int32_t* rounds) {
+  return guarded([&] {
+    if (!rounds || max_rounds < 0) throw std::invalid_argument("gpp_preprocess_traced: bad round buffer");
+    std::vector<gpp::RoundRecord> trace;
+    preprocess_into(lp, params, out, true, nullptr, &trace);
+    *rounds = int32_t(trace.size());
+    for (size_t r = 0; r < trace.size() && int32_t(r) < max_rounds; ++r) {
+      const auto& t = trace[r];
+      if (features) std::copy(t.features, t.features + gpp::kScheduleFeatures, features + r * gpp::kScheduleFeatures);
+      if (round_info) {
+        round_info[4 * r + 0] = t.phase;
+        round_info[4 * r + 1] = t.iteration;
+        round_info[4 * r + 2] = int32_t(t.ran);
+        round_info[4 * r + 3] = int32_t(t.changed);
+      }
+      if (round_nnz) {
+        round_nnz[2 * r + 0] = t.nnz_before;
+        round_nnz[2 * r + 1] = t.nnz_after;
+      }
+    }
+  });
+}
+
+int gpp_schedule_model_create(const float* params, double skip_below, double stop_above,
+                              gpp_schedule_model** out) {
+  return guarded([&] {
+    if (!params || !out || !(skip_below >= 0.0 && skip_below <= 1.0) || !(stop_above >= 0.0))
+      throw std::invalid_argument("gpp_schedule_model_create: null argument or threshold out of range");
+    auto m = std::make_unique<gpp_schedule_model>();
+    m->policy = std::make_unique<gpp::MlpSchedule>(params, skip_below, stop_above);
+    *out = m.release();
+  });
+}
+
+void gpp_schedule_model_free(gpp_schedule_model* model) { delete model; }
+
+int gpp_preprocess_scheduled(const gpp_lp* lp, const gpp_params* params, gpp_schedule_model* model,
+                             gpp_summary* out) {
+  return guarded([&] {
+    if (!model) throw std::invalid_argument("gpp_preprocess_scheduled: null model");
+    preprocess_into(lp, params, out, true, model->policy.get(), nullptr);
+  });
+}
+
+int gpp_mlp_train(float* params, const float* X, const float* Y, const float* M, int64_t n, int32_t epochs,
+                  int32_t batch, float lr, uint64_t seed, float* loss_per_epoch) {
+  return guarded([&] {
+    if (!params || !X || !Y || !M) throw std::invalid_argument("gpp_mlp_train: null argument");
+    gpp::mlp_train(params, X, Y, M, n, epochs, batch, lr, seed, loss_per_epoch);
+  });
+}
+
+int gpp_mlp_forward(const float* params, const float* X, int64_t n, float* probs) {
+  return guarded([&] {
+    if (!params || (n > 0 && (!X || !probs))) throw std::invalid_argument("gpp_mlp_forward: null argument");
+    gpp::mlp_forward(params, X, n, probs);
+  });
+}
+
+int gpp_mlp_gradients(const float* params, const float* X, const float* Y, const float* M, int64_t n, float* grads,
+                      float* loss) {
+  return guarded([&] {
+    if (!params || !X || !Y || !M || !grads) throw std::invalid_argument("gpp_mlp_gradients: null argument");
+    gpp::mlp_gradients(params, X, Y, M, n, grads, loss);
   });
 }
 }  // extern "C"

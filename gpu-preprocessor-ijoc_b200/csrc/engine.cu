@@ -217,7 +217,8 @@ bool good_progress(int64_t before, int64_t after, int64_t d) { return before >= 
 
 }  // namespace
 
-void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out) {
+void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out, SchedulePolicy* policy,
+                  std::vector<RoundRecord>* trace) {
   Engine e(p, out);
   WorkingLp& cur = e.cur;
   cur.A = DevCsr{input.A.rows, input.A.cols, input.A.nnz, input.A.rowPtr, input.A.colVal, input.A.nzVal};
@@ -245,6 +246,19 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out)
   auto deferred = [&](bool enabled, const char* name, auto rule) {
     return !time_exceeded() && e.deferred_rule(enabled, name, rule);
   };
+  // Round schedule: `skip` gates rules for the current round (a policy's
+  // choice; 0 in the plain loop), `ran` / `changed` record what the gated
+  // rules did.
+  uint32_t skip = 0, ran = 0, changed_rules = 0;
+  auto gate = [&](int rule, bool enabled) {
+    const bool run = enabled && !(skip >> rule & 1u);
+    if (run) ran |= 1u << rule;
+    return run;
+  };
+  auto note = [&](int rule, bool ch) {
+    if (ch) changed_rules |= 1u << rule;
+    return ch;
+  };
   auto cleanup = [&]() {
     out.trace.push_back("phase=cleanup");
     bool ch = deferred(p.enable_infeasible_and_fixed_variables, "infeasible_and_fixed_variables",
@@ -252,14 +266,15 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out)
     ch = deferred(p.enable_empty_columns, "empty_columns", [&] { rule_empty_columns(e.plan, cur, e.stats, p); }) || ch;
     ch = deferred(p.enable_empty_rows, "empty_rows", [&] { rule_empty_rows(e.plan, cur, e.stats, p); }) || ch;
     ch = deferred(p.enable_singleton_rows, "singleton_rows", [&] { rule_singleton_rows(e.plan, cur, e.stats, p); }) || ch;
-    ch = deferred(p.enable_singleton_columns, "singleton_columns",
-                  [&] { rule_singleton_columns(e.plan, cur, e.stats, p); }) || ch;
+    ch = note(kGateSingletonColumns,
+              deferred(gate(kGateSingletonColumns, p.enable_singleton_columns), "singleton_columns",
+                       [&] { rule_singleton_columns(e.plan, cur, e.stats, p); })) || ch;
     return ch;
   };
   auto propagation = [&]() {
     out.trace.push_back("phase=propagation");
     bool bounds_changed = false;
-    if (p.enable_bound_strengthening && !e.terminal && !time_exceeded()) {
+    if (gate(kGateBoundStrengthening, p.enable_bound_strengthening) && !e.terminal && !time_exceeded()) {
       e.prepare();
       const int n = cur.n();
       e.ref_bounds.alloc(size_t(2 * std::max(n, 1)), ctx().stream);
@@ -267,12 +282,16 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out)
       check(cudaMemcpyAsync(e.ref_bounds.p + n, e.plan.u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx().stream), "ref u");
       e.plan.ref_l = e.ref_bounds.p;
       e.plan.ref_u = e.ref_bounds.p + n;
-      bounds_changed = e.deferred_rule(true, "bound_strengthening",
-                                       [&] { rule_bound_strengthening(e.plan, cur, e.stats, p); });
+      bounds_changed = note(kGateBoundStrengthening,
+                            e.deferred_rule(true, "bound_strengthening",
+                                            [&] { rule_bound_strengthening(e.plan, cur, e.stats, p); }));
     }
-    deferred(p.enable_infeasible_and_redundant_rows, "infeasible_and_redundant_rows",
-             [&] { rule_redundant_rows(e.plan, cur, e.stats, p); });
-    deferred(p.enable_dual_fix, "dual_fix", [&] { rule_dual_fix(e.plan, cur, e.stats, p); });
+    const bool tail = gate(kGateRedundantRowsDualFix, p.enable_infeasible_and_redundant_rows || p.enable_dual_fix);
+    bool tail_changed = deferred(tail && p.enable_infeasible_and_redundant_rows, "infeasible_and_redundant_rows",
+                                 [&] { rule_redundant_rows(e.plan, cur, e.stats, p); });
+    tail_changed = deferred(tail && p.enable_dual_fix, "dual_fix", [&] { rule_dual_fix(e.plan, cur, e.stats, p); }) ||
+                   tail_changed;
+    note(kGateRedundantRowsDualFix, tail_changed);
     return bounds_changed;
   };
 
@@ -289,12 +308,47 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out)
     if (m >= 512 && m <= 2048 && n >= 128 * m && n <= 256 * m && initial_live >= 2048 * m && initial_live <= 8192 * m)
       limit = std::max(limit, std::min(2, configured));
   }
+  // Host-side state of the round features.
+  const int64_t initial_rows = std::max<int64_t>(1, cur.m());
+  const int64_t initial_nnz_all = std::max<int64_t>(1, initial_live);
+  int64_t removed_prev = 0, removed_prev2 = 0;
+  int round = 0;
+  bool last_changed[kGatedRules] = {};
+  int last_ran[kGatedRules];
+  for (int& r : last_ran) r = -1;
+  const bool scheduled = policy || trace;
   while (p.max_iters > 0 && !e.terminal && !time_exceeded()) {
     if (phase != Cleanup) {
       if (out.iterations >= p.max_iters) { out.stopped_at_iteration_limit = true; break; }
       ++out.iterations;
     }
     const int64_t before = e.live_nnz();
+    RoundRecord rec;
+    skip = ran = changed_rules = 0;
+    if (scheduled) {
+      float* f = rec.features;
+      f[int(phase)] = 1.0f;
+      f[4] = float(round) / 32.0f;
+      f[5] = float(double(before) / double(initial_nnz_all));
+      f[6] = float(double(removed_prev) / double(initial_nnz_all));
+      f[7] = float(double(removed_prev2) / double(initial_nnz_all));
+      for (int g = 0; g < kGatedRules; ++g) {
+        f[8 + g] = last_changed[g] ? 1.0f : 0.0f;
+        f[14 + g] = last_ran[g] < 0 ? 1.0f : std::min(1.0f, float(round - last_ran[g]) / 16.0f);
+      }
+      f[20] = float(bound_only_rounds) / 8.0f;
+      f[21] = float(std::log10(double(initial_nnz_all)) / 8.0);
+      f[22] = float(1.0 - double(before) / double(initial_nnz_all));
+      f[23] = float(double(cur.m()) / double(initial_rows));
+      rec.phase = int32_t(phase);
+      rec.iteration = out.iterations;
+      rec.nnz_before = before;
+      if (policy) {
+        bool stop = false;
+        skip = policy->decide(f, &stop);
+        if (stop) break;
+      }
+    }
     if (phase == Cleanup) {
       const uint64_t ser = e.deletion_serial;
       const bool changed = cleanup();
@@ -312,21 +366,46 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out)
       if (phase == Aggregation) bound_only_rounds = 0;
     } else if (phase == Aggregation) {
       out.trace.push_back("phase=aggregation");
-      if (!time_exceeded())
-        e.materialized_rule(p.enable_doubleton_equations, "doubleton_equations",
-                            [&](Plan& pl) { rule_doubleton_equations(pl, cur, p); });
+      if (!time_exceeded() && gate(kGateDoubleton, p.enable_doubleton_equations))
+        e.materialized_rule(true, "doubleton_equations", [&](Plan& pl) { rule_doubleton_equations(pl, cur, p); });
       const int64_t after = e.live_nnz();
+      note(kGateDoubleton, after < before);
       phase = good_progress(before, after, min_dec) ? Cleanup : Parallel;
     } else {
       out.trace.push_back("phase=parallel");
-      bool changed = deferred(p.enable_parallel_rows, "parallel_rows",
-                              [&] { rule_parallel_rows(e.plan, cur, e.stats, p); });
-      changed = deferred(p.enable_parallel_columns, "parallel_columns",
-                         [&] { rule_parallel_columns(e.plan, cur, e.stats, p); }) || changed;
+      bool changed = note(kGateParallelRows,
+                          deferred(gate(kGateParallelRows, p.enable_parallel_rows), "parallel_rows",
+                                   [&] { rule_parallel_rows(e.plan, cur, e.stats, p); }));
+      changed = note(kGateParallelColumns,
+                     deferred(gate(kGateParallelColumns, p.enable_parallel_columns), "parallel_columns",
+                              [&] { rule_parallel_columns(e.plan, cur, e.stats, p); })) || changed;
       e.materialize("2");
       const int64_t after = e.live_nnz();
-      if (!(changed && good_progress(before, after, min_dec))) break;
+      const bool stop_loop = !(changed && good_progress(before, after, min_dec));
+      if (scheduled) {
+        rec.ran = ran; rec.changed = changed_rules; rec.nnz_after = after;
+        if (trace) trace->push_back(rec);
+      }
+      if (stop_loop) break;
       phase = Cleanup;
+      if (scheduled) {
+        removed_prev2 = removed_prev;
+        removed_prev = before - after;
+        for (int g = 0; g < kGatedRules; ++g)
+          if (ran >> g & 1u) { last_ran[g] = round; last_changed[g] = (changed_rules >> g & 1u) != 0; }
+        ++round;
+      }
+      continue;
+    }
+    if (scheduled) {
+      const int64_t after = e.live_nnz();
+      rec.ran = ran; rec.changed = changed_rules; rec.nnz_after = after;
+      if (trace) trace->push_back(rec);
+      removed_prev2 = removed_prev;
+      removed_prev = before - after;
+      for (int g = 0; g < kGatedRules; ++g)
+        if (ran >> g & 1u) { last_ran[g] = round; last_changed[g] = (changed_rules >> g & 1u) != 0; }
+      ++round;
     }
   }
   e.materialize("finalize");

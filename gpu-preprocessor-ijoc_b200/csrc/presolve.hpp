@@ -23,7 +23,50 @@ struct PresolveOutput {
   std::vector<std::string> trace;
 };
 
-void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out);
+// ---- round schedule ---------------------------------------------------------
+// One round is one step of the phase machine (Cleanup, Propagation,
+// Aggregation or Parallel).  Six rules can be gated per round.
+enum GatedRule : int {
+  kGateSingletonColumns = 0,
+  kGateBoundStrengthening = 1,
+  kGateRedundantRowsDualFix = 2,
+  kGateDoubleton = 3,
+  kGateParallelRows = 4,
+  kGateParallelColumns = 5,
+  kGatedRules = 6
+};
+constexpr int kScheduleFeatures = 24;
+
+// What the host knows at the start of a round, normalised to about [0, 1]:
+//  0-3   phase one-hot (Cleanup, Propagation, Aggregation, Parallel)
+//  4     round index / 32
+//  5     live nnz / initial nnz
+//  6, 7  nnz removed by the previous round and the one before, / initial nnz
+//  8-13  per gated rule: 1 if it changed the model the last time it ran
+//  14-19 per gated rule: rounds since it last ran / 16 (1 if never)
+//  20    consecutive bound-only propagation rounds / 8
+//  21    log10(initial nnz) / 8
+//  22    share of the initial nnz removed so far
+//  23    kept rows / initial rows (as of the last materialisation)
+struct RoundRecord {
+  int32_t phase = 0;          // 0 Cleanup, 1 Propagation, 2 Aggregation, 3 Parallel
+  int32_t iteration = 0;
+  uint32_t ran = 0;           // bit per gated rule that ran this round
+  uint32_t changed = 0;       // bit per gated rule that changed the model
+  int64_t nnz_before = 0, nnz_after = 0;
+  float features[kScheduleFeatures] = {};
+};
+
+// Decides, per round, which gated rules to skip and whether to stop; the plain
+// phase machine is what runs when no policy is given.
+struct SchedulePolicy {
+  virtual ~SchedulePolicy() = default;
+  // Returns the skip mask (bit per gated rule); sets *stop to end presolve.
+  virtual uint32_t decide(const float* features, bool* stop) = 0;
+};
+
+void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
+                  SchedulePolicy* policy = nullptr, std::vector<RoundRecord>* trace = nullptr);
 
 // postsolve_gpu (cpp/src/presolve/gpu_postsolve.cu:535-670): device arrays
 // x_org (n0), y_org (m0), z_org (n0) receive the original-space solution.

@@ -163,6 +163,13 @@ def load():
         "gpp_kernel_launches": (C.c_uint64, [C.c_int]),
         "gpp_host_syncs": (C.c_uint64, [C.c_int]),
         "gpp_preprocess_batch": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, vp, vp]),
+        "gpp_preprocess_traced": (C.c_int, [P(Lp), P(Params), P(Summary), vp, vp, vp, C.c_int32, P(C.c_int32)]),
+        "gpp_schedule_model_create": (C.c_int, [vp, C.c_double, C.c_double, P(vp)]),
+        "gpp_schedule_model_free": (None, [vp]),
+        "gpp_preprocess_scheduled": (C.c_int, [P(Lp), P(Params), vp, P(Summary)]),
+        "gpp_mlp_train": (C.c_int, [vp, vp, vp, vp, i64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, vp]),
+        "gpp_mlp_forward": (C.c_int, [vp, vp, i64, vp]),
+        "gpp_mlp_gradients": (C.c_int, [vp, vp, vp, vp, i64, vp, vp]),
         "gpp_postprocess_batch": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp]),
         "gpp_batch_autotune": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, P(C.c_int32), vp]),
         "gpp_profile_enable": (None, [C.c_int]),
@@ -183,7 +190,9 @@ EXPORTED = [
     "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_alloc", "gpp_device_free",
     "gpp_export_folding_map", "gpp_unfold_solution",
     "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
-    "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune", "gpp_profile_enable", "gpp_profile_read",
+    "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
+    "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free", "gpp_preprocess_scheduled",
+    "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
 ]
 
 

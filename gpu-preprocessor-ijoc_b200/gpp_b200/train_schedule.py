@@ -1,0 +1,116 @@
+"""Trains the learned round schedule.
+
+    python -m gpp_b200.train_schedule --out schedule_model.npz [--lps 600] [--seed 0]
+
+1. Draws training LPs from the plain-presolve generator (lpgen.random_lp) with
+   m log-uniform in [1,000, 500,000] and n = 2.5 m (generated by spawned
+   processes), and records a trace of the plain phase machine on each.
+2. Trains the schedule MLP on the rounds of all traces (the library's CUDA
+   kernels; Adam, masked binary cross-entropy).
+3. Chooses the two decision thresholds on held-out LPs (skip a rule below
+   one probability, stop above another): the pair with the least total
+   presolve time among those that keep at least 98% of the plain run's nnz
+   removal on every held-out LP (the plain loop -- skip nothing, never stop
+   -- if none does).
+4. Writes parameters, thresholds and training notes to --out.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import sys
+import time
+
+import numpy as np
+
+KEEP_SHARE = 0.98
+SKIP_BELOW = (0.5, 0.3, 0.15, 0.05, 0.0)
+STOP_ABOVE = (0.5, 0.8, 0.95, 0.99, 1.0)   # 1.0: never stop
+
+
+def _draw(job):
+    from gpp_b200 import lpgen
+    m, seed = job
+    lp = lpgen.random_lp(m, int(2.5 * m), seed=seed)
+    lp.ensure_transpose()
+    return lp
+
+
+def jobs(count, seed, lo=1000, hi=500000):
+    rng = np.random.default_rng(seed)
+    ms = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).astype(int)
+    return [(int(m), int(seed * 100000 + k)) for k, m in enumerate(ms)]
+
+
+def removal(lp, s):
+    return lp.nnz - s.reduced_nnz
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--lps", type=int, default=600)
+    ap.add_argument("--holdout", type=int, default=40)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--max-m", type=int, default=500000)
+    args = ap.parse_args(argv)
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(max(1, min(32, (os.cpu_count() or 2) - 1))) as pool:
+        train_lps = pool.map(_draw, jobs(args.lps, args.seed + 1, hi=args.max_m), chunksize=1)
+        hold_lps = pool.map(_draw, jobs(args.holdout, args.seed + 2, hi=args.max_m), chunksize=1)
+
+    from gpp_b200 import capi, device, schedule
+    params = capi.Params.defaults()
+    X, Y, M = [], [], []
+    t0 = time.perf_counter()
+    for lp in train_lps:
+        d = device.DeviceLp(lp)
+        s, tr = schedule.traced_preprocess(d, params)
+        device.free_summary(s)
+        y, m = schedule.labels(tr)
+        X.append(tr["features"]); Y.append(y); M.append(m)
+        del d
+    X, Y, M = (np.concatenate(a) for a in (X, Y, M))
+    trace_s = time.perf_counter() - t0
+    w, loss = schedule.train(X, Y, M, epochs=args.epochs, seed=args.seed)
+
+    # Threshold on held-out LPs: plain first, then each threshold.
+    dlps = [device.DeviceLp(lp) for lp in hold_lps]
+    plain_t, plain_r = [], []
+    for lp, d in zip(hold_lps, dlps):
+        s = device.preprocess(d, params)   # warm caches once
+        device.free_summary(s)
+        s = device.preprocess(d, params)
+        plain_t.append(s.preprocessing_seconds)
+        plain_r.append(removal(lp, s))
+        device.free_summary(s)
+    table = {}
+    for skip_below in SKIP_BELOW:
+        for stop_above in STOP_ABOVE:
+            times, kept = [], []
+            with schedule.Model(w, skip_below, stop_above) as model:
+                for lp, d, pr in zip(hold_lps, dlps, plain_r):
+                    s = schedule.scheduled_preprocess(d, params, model)
+                    times.append(s.preprocessing_seconds)
+                    kept.append(removal(lp, s) / pr if pr > 0 else 1.0)
+                    device.free_summary(s)
+            table[f"{skip_below}/{stop_above}"] = {
+                "skip_below": skip_below, "stop_above": stop_above,
+                "time_ratio": float(np.sum(times) / np.sum(plain_t)), "min_kept": float(np.min(kept)),
+                "mean_kept": float(np.mean(kept))}
+    ok = [v for v in table.values() if v["min_kept"] >= KEEP_SHARE]
+    best = min(ok, key=lambda v: v["time_ratio"]) if ok else {"skip_below": 0.0, "stop_above": 1.0}
+    notes = {"samples": int(len(X)), "train_lps": args.lps, "holdout_lps": args.holdout, "trace_seconds": trace_s,
+             "final_loss": float(loss[-1]) if len(loss) else None, "thresholds": table, "chosen": best,
+             "positive_rate": [float(x) for x in (Y * M).sum(0) / np.maximum(M.sum(0), 1)]}
+    schedule.save_model(args.out, w, best["skip_below"], best["stop_above"], loss=loss, notes=json.dumps(notes))
+    print(json.dumps(notes, indent=1))
+
+
+if __name__ == "__main__":
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    main()

@@ -281,6 +281,53 @@ GPP_API int gpp_postprocess_batch(const double* const* x_red, const double* cons
 GPP_API int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
                                int32_t* best_workers, double* rates);
 
+/* ---- Learned round schedule -------------------------------------------------
+ * The plain phase machine (Cleanup, Propagation, Aggregation, Parallel) runs
+ * one phase per round.  A schedule model may, per round, skip any of six gated
+ * rules (singleton columns, bound strengthening, redundant rows + dual fix,
+ * doubleton equations, parallel rows, parallel columns) and stop presolve.
+ * The model is a small FP32 MLP with GPP_SCHEDULE_FEATURES inputs, two hidden
+ * layers of GPP_SCHEDULE_HIDDEN units and GPP_SCHEDULE_OUTPUTS logits (one per
+ * gated rule, "the rule will change the model this round", then "stop").
+ * The reference has no counterpart; its plain loop stays the default here. */
+#define GPP_SCHEDULE_FEATURES 24
+#define GPP_SCHEDULE_HIDDEN 64
+#define GPP_SCHEDULE_OUTPUTS 7
+/* W1[24][64], b1[64], W2[64][64], b2[64], W3[64][7], b3[7], row-major. */
+#define GPP_SCHEDULE_PARAMS (24 * 64 + 64 + 64 * 64 + 64 + 64 * 7 + 7)
+
+/* gpp_preprocess that also records every round: features[r * 24 + i],
+ * round_info[4 r ..] = phase (0 Cleanup, 1 Propagation, 2 Aggregation,
+ * 3 Parallel), iteration, gated rules that ran (bit mask), gated rules that
+ * changed the model (bit mask); round_nnz[2 r ..] = live nnz before and after
+ * the round.  At most max_rounds are written; *rounds gets the count.  The
+ * presolve result is the plain one. */
+GPP_API int gpp_preprocess_traced(const gpp_lp* lp, const gpp_params* params, gpp_summary* out, float* features,
+                                  int32_t* round_info, int64_t* round_nnz, int32_t max_rounds, int32_t* rounds);
+
+typedef struct gpp_schedule_model gpp_schedule_model;
+/* A model from GPP_SCHEDULE_PARAMS host floats.  Per round it skips gated rule
+ * g when sigmoid(logit g) < skip_below and stops when sigmoid(stop logit) >
+ * stop_above (skip_below = 0 keeps every rule; stop_above >= 1 never stops).
+ * One model may be used by one host thread at a time. */
+GPP_API int gpp_schedule_model_create(const float* params, double skip_below, double stop_above,
+                                      gpp_schedule_model** out);
+GPP_API void gpp_schedule_model_free(gpp_schedule_model* model);
+/* gpp_preprocess with the rounds scheduled by `model`. */
+GPP_API int gpp_preprocess_scheduled(const gpp_lp* lp, const gpp_params* params, gpp_schedule_model* model,
+                                     gpp_summary* out);
+
+/* Training and inference of the schedule MLP on the GPU (host arrays in and
+ * out).  X is n x 24, Y and M (labels and 0/1 masks) are n x 7; the loss is
+ * the mean over samples of the masked binary cross-entropy of the logits.
+ * gpp_mlp_train runs `epochs` epochs of Adam (minibatches of `batch`, order
+ * shuffled by `seed`) from and into `params`; loss_per_epoch may be NULL. */
+GPP_API int gpp_mlp_train(float* params, const float* X, const float* Y, const float* M, int64_t n, int32_t epochs,
+                          int32_t batch, float lr, uint64_t seed, float* loss_per_epoch);
+GPP_API int gpp_mlp_forward(const float* params, const float* X, int64_t n, float* probs);
+GPP_API int gpp_mlp_gradients(const float* params, const float* X, const float* Y, const float* M, int64_t n,
+                              float* grads, float* loss);
+
 /* ---- Kernel-level entry points (rule / kernel parity tests) -------------- */
 
 /* compute_row_activity_summary (presolve/gpu_presolve_kernels.hpp:76-86):
