@@ -22,7 +22,7 @@ FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-li
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
          "--extended-lambda", "-I", os.path.join(HERE, "..", "include")]
 UNITS = ["common.cu", "live.cu", "compact.cu", "recovery.cu", "rules_cleanup.cu", "rules_bound.cu", "rules_propagation.cu", "sort.cu", "sort_static.cu", "rules_parallel.cu", "rules_singleton.cu", "rules_doubleton.cu",
-         "engine.cu", "postsolve.cu", "folding.cu", "schedule_mlp.cu", "capi.cu"]
+         "engine.cu", "postsolve.cu", "folding.cu", "schedule_mlp.cu", "mps_reader.cpp", "capi.cu"]
 
 
 def _compile(unit: str) -> str:

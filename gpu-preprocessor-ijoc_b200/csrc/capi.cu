@@ -19,7 +19,16 @@
 #include "folding.hpp"
 #include "presolve.hpp"
 #include "schedule_mlp.hpp"
+#include "mps_reader.hpp"
+
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
 #include "sort.hpp"
+
+struct gpp_mps_model {
+  gpp::MpsModel m;
+};
 
 struct gpp_schedule_model {
   std::unique_ptr<gpp::MlpSchedule> policy;
@@ -769,6 +778,155 @@ int gpp_mlp_gradients(const float* params, const float* X, const float* Y, const
   return guarded([&] {
     if (!params || !X || !Y || !M || !grads) throw std::invalid_argument("gpp_mlp_gradients: null argument");
     gpp::mlp_gradients(params, X, Y, M, n, grads, loss);
+  });
+}
+
+int gpp_mps_read(const char* path, gpp_mps_model** out) {
+  try {
+    if (!path || !out) throw std::invalid_argument("gpp_mps_read: null argument");
+    auto m = std::make_unique<gpp_mps_model>();
+    m->m = gpp::read_mps_file(path);
+    *out = m.release();
+    gpp::set_last_error("");
+    return GPP_OK;
+  } catch (const std::invalid_argument& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_INVALID;
+  } catch (const std::exception& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_RUNTIME;
+  }
+}
+
+int gpp_mps_read_string(const char* text, gpp_mps_model** out) {
+  try {
+    if (!text || !out) throw std::invalid_argument("gpp_mps_read_string: null argument");
+    auto m = std::make_unique<gpp_mps_model>();
+    m->m = gpp::read_mps_text(text);
+    *out = m.release();
+    gpp::set_last_error("");
+    return GPP_OK;
+  } catch (const std::invalid_argument& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_INVALID;
+  } catch (const std::exception& e) {
+    gpp::set_last_error(e.what());
+    return GPP_ERR_RUNTIME;
+  }
+}
+
+int gpp_mps_info(const gpp_mps_model* model, int32_t* rows, int32_t* cols, int64_t* nnz, double* obj_constant,
+                 char* name, size_t name_len) {
+  if (!model) return GPP_ERR_INVALID;
+  const gpp::MpsModel& m = model->m;
+  if (rows) *rows = m.rows;
+  if (cols) *cols = m.cols;
+  if (nnz) *nnz = int64_t(m.csr_val.size());
+  if (obj_constant) *obj_constant = m.obj_constant;
+  if (name && name_len) {
+    const size_t k = std::min(name_len - 1, m.name.size());
+    std::memcpy(name, m.name.data(), k);
+    name[k] = '\0';
+  }
+  return GPP_OK;
+}
+
+int gpp_mps_arrays(const gpp_mps_model* model, int64_t* row_ptr, int32_t* col_idx, double* csr_val, int64_t* col_ptr,
+                   int32_t* row_idx, double* csc_val, double* c, double* AL, double* AU, double* l, double* u) {
+  if (!model) return GPP_ERR_INVALID;
+  const gpp::MpsModel& m = model->m;
+  auto put = [](auto* dst, const auto& v) { if (dst) std::copy(v.begin(), v.end(), dst); };
+  put(row_ptr, m.row_ptr); put(col_idx, m.col_idx); put(csr_val, m.csr_val);
+  put(col_ptr, m.col_ptr); put(row_idx, m.row_idx); put(csc_val, m.csc_val);
+  put(c, m.cost); put(AL, m.row_lower); put(AU, m.row_upper); put(l, m.col_lower); put(u, m.col_upper);
+  return GPP_OK;
+}
+
+void gpp_mps_free(gpp_mps_model* model) { delete model; }
+
+int gpp_mps_upload(const gpp_mps_model* model, gpp_lp* out) {
+  return guarded([&] {
+    if (!model || !out) throw std::invalid_argument("gpp_mps_upload: null argument");
+    const gpp::MpsModel& m = model->m;
+    const int64_t nnz = int64_t(m.csr_val.size());
+    if (nnz > int64_t(INT32_MAX)) throw std::length_error("nnz exceeds the 32-bit offset range of this build");
+    *out = gpp_lp{};
+    auto up = [](const auto& v, auto** dst) {
+      using T = std::remove_pointer_t<std::remove_reference_t<decltype(*dst)>>;
+      check(cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * std::max<size_t>(v.size(), 1)), "cudaMalloc");
+      if (!v.empty()) check(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+    };
+    try {
+      const std::vector<gpp_offset> rp(m.row_ptr.begin(), m.row_ptr.end()), cp(m.col_ptr.begin(), m.col_ptr.end());
+      out->A = {m.rows, m.cols, gpp_offset(nnz), nullptr, nullptr, nullptr};
+      out->AT = {m.cols, m.rows, gpp_offset(nnz), nullptr, nullptr, nullptr};
+      up(rp, &out->A.rowPtr); up(m.col_idx, &out->A.colVal); up(m.csr_val, &out->A.nzVal);
+      up(cp, &out->AT.rowPtr); up(m.row_idx, &out->AT.colVal); up(m.csc_val, &out->AT.nzVal);
+      up(m.cost, &out->c); up(m.row_lower, &out->AL); up(m.row_upper, &out->AU);
+      up(m.col_lower, &out->l); up(m.col_upper, &out->u);
+      out->obj_constant = m.obj_constant;
+    } catch (...) {
+      gpp_lp_free(out);
+      throw;
+    }
+  });
+}
+
+void gpp_lp_free(gpp_lp* lp) {
+  if (!lp) return;
+  for (void* p : {static_cast<void*>(lp->A.rowPtr), static_cast<void*>(lp->A.colVal), static_cast<void*>(lp->A.nzVal),
+                  static_cast<void*>(lp->AT.rowPtr), static_cast<void*>(lp->AT.colVal),
+                  static_cast<void*>(lp->AT.nzVal), static_cast<void*>(lp->c), static_cast<void*>(lp->AL),
+                  static_cast<void*>(lp->AU), static_cast<void*>(lp->l), static_cast<void*>(lp->u)})
+    if (p) cudaFree(p);
+  *lp = gpp_lp{};
+}
+
+int gpp_export_reduced(const gpp_summary* summary, const char* out_dir, const char* model_name) {
+  return guarded([&] {
+    if (!summary || !summary->record || !out_dir) throw std::invalid_argument("gpp_export_reduced: null argument");
+    namespace fs = std::filesystem;
+    const fs::path dir(out_dir);
+    fs::create_directories(dir);
+    const gpp_lp& lp = summary->reduced_lp;
+    std::ofstream meta(dir / "meta.txt");
+    if (!meta) throw std::runtime_error("failed to open export meta");
+    meta << std::setprecision(17);
+    meta << "format gpu_preprocessor_reduced_lp_v1\noffset_bits 32\n";
+    meta << "model " << (model_name ? model_name : "") << "\n";
+    meta << "status " << (summary->has_infeasible ? "infeasible" : summary->has_unbounded ? "unbounded" : "ok") << "\n";
+    meta << "original_rows " << summary->original_rows << "\noriginal_cols " << summary->original_cols << "\n";
+    meta << "folding_applied " << int(summary->folding_applied) << "\nfolded_rows " << summary->folded_rows
+         << "\nfolded_cols " << summary->folded_cols << "\n";
+    meta << "reduced_rows " << summary->reduced_rows << "\nreduced_cols " << summary->reduced_cols
+         << "\nreduced_nnz " << summary->reduced_nnz << "\n";
+    meta << "obj_constant " << lp.obj_constant << "\nobjective_shift " << summary->obj_constant_delta << "\n";
+    meta << "preprocessing_seconds " << summary->preprocessing_seconds << "\npresolve_seconds "
+         << summary->elapsed_seconds << "\n";
+    meta << "iterations " << summary->iterations << "\n";
+    if (!meta) throw std::runtime_error("failed to write export meta");
+    auto write = [&](const char* name, const void* dev, size_t bytes) {
+      std::vector<char> host(bytes);
+      if (bytes) check(cudaMemcpy(host.data(), dev, bytes, cudaMemcpyDeviceToHost), "export copy");
+      std::ofstream f(dir / name, std::ios::binary);
+      f.write(host.data(), std::streamsize(bytes));
+      if (!f) throw std::runtime_error(std::string("failed to write ") + name);
+    };
+    const size_t m = size_t(lp.A.rows), n = size_t(lp.A.cols), nnz = size_t(lp.A.nnz);
+    if (m == 0) {
+      const int32_t zero = 0;
+      std::ofstream f(dir / "A_rowPtr_i32.bin", std::ios::binary);
+      f.write(reinterpret_cast<const char*>(&zero), sizeof(zero));
+    } else {
+      write("A_rowPtr_i32.bin", lp.A.rowPtr, sizeof(gpp_offset) * (m + 1));
+    }
+    write("A_colVal_i32.bin", lp.A.colVal, sizeof(int32_t) * nnz);
+    write("A_nzVal_f64.bin", lp.A.nzVal, sizeof(double) * nnz);
+    write("c_f64.bin", lp.c, sizeof(double) * n);
+    write("l_f64.bin", lp.l, sizeof(double) * n);
+    write("u_f64.bin", lp.u, sizeof(double) * n);
+    write("AL_f64.bin", lp.AL, sizeof(double) * m);
+    write("AU_f64.bin", lp.AU, sizeof(double) * m);
   });
 }
 }  // extern "C"

@@ -164,6 +164,14 @@ def load():
         "gpp_host_syncs": (C.c_uint64, [C.c_int]),
         "gpp_preprocess_batch": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, vp, vp]),
         "gpp_preprocess_traced": (C.c_int, [P(Lp), P(Params), P(Summary), vp, vp, vp, C.c_int32, P(C.c_int32)]),
+        "gpp_mps_read": (C.c_int, [C.c_char_p, P(vp)]),
+        "gpp_mps_read_string": (C.c_int, [C.c_char_p, P(vp)]),
+        "gpp_mps_info": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(i64), P(f64), C.c_char_p, C.c_size_t]),
+        "gpp_mps_arrays": (C.c_int, [vp] + [vp] * 11),
+        "gpp_mps_free": (None, [vp]),
+        "gpp_mps_upload": (C.c_int, [vp, P(Lp)]),
+        "gpp_lp_free": (None, [P(Lp)]),
+        "gpp_export_reduced": (C.c_int, [P(Summary), C.c_char_p, C.c_char_p]),
         "gpp_schedule_model_create": (C.c_int, [vp, C.c_double, C.c_double, P(vp)]),
         "gpp_schedule_model_free": (None, [vp]),
         "gpp_preprocess_scheduled": (C.c_int, [P(Lp), P(Params), vp, P(Summary)]),
@@ -191,6 +199,8 @@ EXPORTED = [
     "gpp_export_folding_map", "gpp_unfold_solution",
     "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
     "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
+    "gpp_mps_read", "gpp_mps_read_string", "gpp_mps_info", "gpp_mps_arrays", "gpp_mps_free", "gpp_mps_upload",
+    "gpp_lp_free", "gpp_export_reduced",
     "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
 ]

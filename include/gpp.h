@@ -281,6 +281,43 @@ GPP_API int gpp_postprocess_batch(const double* const* x_red, const double* cons
 GPP_API int gpp_batch_autotune(const gpp_lp* lps, int32_t count, const gpp_params* params, int32_t max_workers,
                                int32_t* best_workers, double* rates);
 
+/* ---- Host I/O: MPS input, reduced-LP export -------------------------------- */
+
+/* A continuous LP read from an MPS file (the reference's mps_reader::read_mps,
+ * cpp/mps_reader/include/mps_reader/mpsreader.hpp:13-18, same arrays for the
+ * same file): free format, or fixed columns when free parsing fails; ROWS,
+ * COLUMNS (integer markers read as bounds only), RHS (an RHS on the objective
+ * row is the negated objective constant), RANGES, BOUNDS (FR MI PL BV LO UP FX
+ * LI UI), OBJSENSE MIN.  Duplicate coefficients are summed.  Errors:
+ * GPP_ERR_INVALID with the parser's message. */
+typedef struct gpp_mps_model gpp_mps_model;
+GPP_API int gpp_mps_read(const char* path, gpp_mps_model** out);
+GPP_API int gpp_mps_read_string(const char* text, gpp_mps_model** out);
+/* Sizes, objective constant and model name (NUL-terminated, truncated to
+ * name_len); any pointer may be NULL. */
+GPP_API int gpp_mps_info(const gpp_mps_model* model, int32_t* rows, int32_t* cols, int64_t* nnz,
+                         double* obj_constant, char* name, size_t name_len);
+/* Host copies: CSR (row_ptr[rows+1], col_idx, csr_val), CSC (col_ptr[cols+1],
+ * row_idx, csc_val; columns in file order, rows ascending), c[cols],
+ * AL/AU[rows], l/u[cols]; any pointer may be NULL. */
+GPP_API int gpp_mps_arrays(const gpp_mps_model* model, int64_t* row_ptr, int32_t* col_idx, double* csr_val,
+                           int64_t* col_ptr, int32_t* row_idx, double* csc_val, double* c, double* AL, double* AU,
+                           double* l, double* u);
+GPP_API void gpp_mps_free(gpp_mps_model* model);
+/* The model on the current device as a gpp_lp with A and AT = A^T (the
+ * reference's tools upload_lp, cpp/tools/gpu_preprocessor_tool_common.hpp:
+ * 108-141); the arrays are cudaMalloc'd and released by gpp_lp_free. */
+GPP_API int gpp_mps_upload(const gpp_mps_model* model, gpp_lp* out);
+GPP_API void gpp_lp_free(gpp_lp* lp);
+
+/* Writes the reduced LP of a summary to `out_dir` in the reference's export
+ * format (cpp/tools/gpu_preprocessor_export_reduced.cpp:17-64, format
+ * gpu_preprocessor_reduced_lp_v1): meta.txt and the raw little-endian arrays
+ * A_rowPtr_i32, A_colVal_i32, A_nzVal_f64, c_f64, l_f64, u_f64, AL_f64,
+ * AU_f64 (.bin).  meta.txt has the reference's keys except folding_seconds,
+ * which this engine does not time separately. */
+GPP_API int gpp_export_reduced(const gpp_summary* summary, const char* out_dir, const char* model_name);
+
 /* ---- Learned round schedule -------------------------------------------------
  * The plain phase machine (Cleanup, Propagation, Aggregation, Parallel) runs
  * one phase per round.  A schedule model may, per round, skip any of six gated
