@@ -123,16 +123,34 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
         }
       }
       const int rounds = __reduce_max_sync(0xffffffffu, int((end - first + 7) >> 3));
-      for (int k = 0; k < rounds; ++k) {
-        const offset_t p = first + offset_t(k) * 8 + g;
-        const int c = p < end ? inner_map[__ldcs(idx + p)] : -1;
-        const unsigned bits = (__ballot_sync(0xffffffffu, c >= 0) >> shift) & 0xFFu;
-        if (c >= 0) {
-          const offset_t o = w + __popc(bits & ((1u << g) - 1u));
-          out_idx[o] = c;
-          out_val[o] = __ldcs(val + p);
+      // Four rounds per step: their index loads, then their column-map
+      // gathers and value loads, are all in flight before the first ballot.
+      constexpr int kBatch = 4;
+      for (int k0 = 0; k0 < rounds; k0 += kBatch) {
+        int col[kBatch];
+        double v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          const offset_t p = first + offset_t(k0 + u) * 8 + g;
+          col[u] = k0 + u < rounds && p < end ? __ldcs(idx + p) : -1;
         }
-        w += __popc(bits);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          const offset_t p = first + offset_t(k0 + u) * 8 + g;
+          col[u] = col[u] >= 0 ? inner_map[col[u]] : -1;
+          v[u] = col[u] >= 0 ? __ldcs(val + p) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          if (k0 + u >= rounds) break;   // warp-uniform
+          const unsigned bits = (__ballot_sync(0xffffffffu, col[u] >= 0) >> shift) & 0xFFu;
+          if (col[u] >= 0) {
+            const offset_t o = w + __popc(bits & ((1u << g) - 1u));
+            out_idx[o] = col[u];
+            out_val[o] = v[u];
+          }
+          w += __popc(bits);
+        }
       }
     }
     return;

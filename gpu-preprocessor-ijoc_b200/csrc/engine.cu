@@ -239,8 +239,16 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
   };
 
   if (p.enable_startup && p.max_iters > 0 && !time_exceeded()) {
-    // Structure-specific startup detectors are outside this engine's scope;
-    // the Startup phase still consumes its iteration (gpu_presolve.cu:2453).
+    // Startup (gpu_presolve.cu:2361-2454): the structure-specific rules, all
+    // off when enable_structure_specific_rules is (:2088-2094).  Column
+    // domination is the one implemented; its reductions are applied before
+    // Cleanup, as the reference applies its startup batch.  Two-row variable
+    // elimination, zero-cost product variables and the piecewise-linear
+    // reformulations are not run.  The phase consumes one iteration (:2453).
+    if (p.enable_structure_specific_rules && p.enable_column_domination && !e.terminal) {
+      if (e.deferred_rule(true, "column_domination", [&] { rule_column_domination(e.plan, cur, p); }))
+        e.materialize("startup");
+    }
     ++out.iterations;
   }
   auto deferred = [&](bool enabled, const char* name, auto rule) {

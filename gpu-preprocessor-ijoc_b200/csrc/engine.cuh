@@ -160,6 +160,8 @@ void rule_singleton_columns(Plan& plan, const WorkingLp& lp, const Stats& s, con
 void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_redundant_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_dual_fix(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
+// rules_startup.cu: structure-specific Startup rules.
+void rule_column_domination(Plan& plan, const WorkingLp& lp, const gpp_params& p);
 void rule_parallel_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_parallel_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params& p);

@@ -364,10 +364,38 @@ def qap_lp(N: int, seed: int = 0) -> HostLP:
     return HostLP(m, n, ptr, idx, val, c, AL, AU, l, u).ensure_transpose()
 
 
+def setcover_lp(m: int, n: int, seed: int = 0, witness: bool = True) -> HostLP:
+    """Unit set-covering LP  min c'x, sum_{j in row i} x_j >= 1, 0 <= x <= 1,
+    every coefficient 1: the structure the column-domination startup rule
+    accepts.  The first max(1, n // 4) columns cost 1 and cover every row
+    (column i mod that count is in row i) so each row holds a cost-1
+    witness; every column gets 1 + Poisson(2) further distinct rows, and the
+    remaining columns an integer cost uniform in [1, 2 * degree], so about
+    half of them cost more than their degree.  ``witness=False`` raises the
+    cost-1 columns to 2, which leaves rows without a witness."""
+    rng = np.random.default_rng(seed)
+    cheap = max(1, n // 4)
+    rows = [np.arange(m, dtype=np.int64)]
+    cols = [np.arange(m, dtype=np.int64) % cheap]
+    extra = 1 + rng.poisson(2.0, size=n)
+    rows.append(rng.integers(0, m, size=int(extra.sum())))
+    cols.append(np.repeat(np.arange(n, dtype=np.int64), extra))
+    r, cidx = np.concatenate(rows), np.concatenate(cols)
+    key = np.unique(r * n + cidx)                       # distinct (row, column) pairs
+    r, cidx = key // n, key % n
+    ptr, idx, val = coo_to_csr(m, r, cidx, np.ones(len(r)))
+    degree = np.bincount(cidx, minlength=n)
+    c = np.floor(rng.uniform(1.0, 2.0 * np.maximum(degree, 1) + 1.0)).astype(np.float64)
+    c[:cheap] = 1.0 if witness else 2.0
+    AL, AU = np.ones(m), np.full(m, INF)
+    return HostLP(m, n, ptr, idx, val, c, AL, AU, np.zeros(n), np.ones(n)).ensure_transpose()
+
+
 def workload(name: str, seed: int = 0) -> HostLP:
     """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
     'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows),
-    'replicated:MxN*K' (K identical copies plus a coupling row), 'qap:N'."""
+    'replicated:MxN*K' (K identical copies plus a coupling row), 'setcover:MxN' (unit set covering),
+    'qap:N'."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -385,6 +413,9 @@ def workload(name: str, seed: int = 0) -> HostLP:
         mn, k = spec.split("*")
         m, n = (int(v) for v in mn.split("x"))
         return replicated_lp(m, n, int(k), seed)
+    if name.startswith("setcover:"):
+        m, n = (int(v) for v in name.split(":")[1].split("x"))
+        return setcover_lp(m, n, seed)
     if name.startswith("qap:"):
         return qap_lp(int(name.split(":")[1]), seed)
     raise ValueError(f"unknown workload {name!r}")

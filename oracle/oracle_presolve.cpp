@@ -267,8 +267,13 @@ Result presolve(const Lp& lp, const gpp_params& p) {
   const auto t0 = std::chrono::steady_clock::now();
 
   if (p.enable_startup && p.max_iters > 0) {
-    // Structure-specific startup rules are outside this engine's scope; the
-    // Startup phase still consumes one iteration (gpu_presolve.cu:2453).
+    // Startup (gpu_presolve.cu:2361-2454): of the structure-specific rules,
+    // column domination, applied before Cleanup; the phase consumes one
+    // iteration (:2453).
+    if (p.enable_structure_specific_rules && p.enable_column_domination) {
+      if (e.deferred_rule(true, "column_domination", [&] { rule_column_domination(e.plan, e.cur, p); }))
+        e.materialize("startup");
+    }
     ++S.iterations;
   }
   auto cleanup = [&]() {

@@ -1464,4 +1464,43 @@ void rule_parallel_columns(Plan& plan, const Lp& lp, const Stats&, const gpp_par
   plan.has_col_action = plan.has_change = true;
 }
 
+void rule_column_domination(Plan& plan, const Lp& lp, const gpp_params& p) {
+  // analyze_column_domination / build_column_domination_plan
+  // (rule_column_domination.cu:248-379): strict unit set covering only.
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  const int nnz = lp.A.ptr[size_t(m)];
+  const int min_fixed = std::max(1, p.column_domination_min_fixed_cols);
+  if (m <= 0 || nnz <= 0 || n < min_fixed) return;
+  for (int i = 0; i < m; ++i) {
+    if (plan.AL[size_t(i)] != 1.0 || !(std::isinf(plan.AU[size_t(i)]) && plan.AU[size_t(i)] > 0.0)) return;
+    bool witness = false;
+    for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1] && !witness; ++q)
+      witness = plan.c[size_t(lp.A.idx[size_t(q)])] == 1.0;
+    if (!witness) return;
+  }
+  for (int j = 0; j < n; ++j) {
+    const double cj = plan.c[size_t(j)];
+    if (plan.l[size_t(j)] != 0.0 || plan.u[size_t(j)] != 1.0) return;
+    if (!(std::isfinite(cj) && cj >= 1.0 && std::floor(cj) == cj)) return;
+  }
+  for (int q = 0; q < nnz; ++q)
+    if (lp.A.val[size_t(q)] != 1.0 || lp.AT.val[size_t(q)] != 1.0) return;
+  std::vector<uint8_t> dominated(size_t(n), 0);
+  int count = 0;
+  for (int j = 0; j < n; ++j) {
+    dominated[size_t(j)] = plan.c[size_t(j)] > double(lp.AT.ptr[size_t(j) + 1] - lp.AT.ptr[size_t(j)]);
+    count += dominated[size_t(j)];
+  }
+  if (count < min_fixed || double(count) / double(n) + 1.0e-15 < p.column_domination_min_candidate_ratio) return;
+  for (int j = 0; j < n; ++j)
+    if (dominated[size_t(j)]) {
+      plan.keep_col[size_t(j)] = 0;
+      plan.l[size_t(j)] = 0.0;
+      plan.u[size_t(j)] = 0.0;
+    }
+  plan.has_col_action = plan.has_change = true;
+}
+
 }  // namespace oracle
+

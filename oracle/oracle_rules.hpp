@@ -12,6 +12,7 @@ void rule_singleton_columns(Plan& plan, const Lp& lp, const Stats& s, const gpp_
 void rule_bound_strengthening(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p);
 void rule_redundant_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p);
 void rule_dual_fix(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p);
+void rule_column_domination(Plan& plan, const Lp& lp, const gpp_params& p);
 void rule_parallel_rows(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p);
 void rule_parallel_columns(Plan& plan, const Lp& lp, const Stats& s, const gpp_params& p);
 void rule_doubleton_equations(Plan& plan, const Lp& lp, const gpp_params& p);

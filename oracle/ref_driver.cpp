@@ -83,6 +83,11 @@ int main(int argc, char** argv) {
       FLAG(enable_parallel_rows); FLAG(enable_empty_columns); FLAG(enable_singleton_columns);
       FLAG(enable_doubleton_equations); FLAG(enable_dual_fix); FLAG(enable_parallel_columns);
       FLAG(enable_structure_specific_rules); FLAG(enable_startup);
+      FLAG(enable_column_domination); FLAG(enable_two_row_variable_elimination);
+      FLAG(enable_zero_cost_product_variables); FLAG(enable_piecewise_linear_reformulation_variable_pair);
+      FLAG(enable_piecewise_linear_reformulation_absolute_value);
+      else if (k == "column_domination_min_fixed_cols") p.column_domination_min_fixed_cols = v;
+      else if (k == "column_domination_min_candidate_ratio") p.column_domination_min_candidate_ratio = dv;
       else if (k == "max_iters") p.max_iters = v;
       else if (k == "folding_tolerance") p.folding_tolerance = dv;
       else if (k == "doubleton_equations_scan") p.doubleton_equations_scan = v != 0;

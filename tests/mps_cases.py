@@ -23,7 +23,8 @@ def number(v, rng, fixed):
     elif form == "trail_dot":
         s = f"{round(v):d}."
     elif form == "lead_dot":
-        s = f"{abs(v) % 1:.7f}"[1:] if abs(v) % 1 else "0.5"
+        frac = f"{abs(v) % 1:.7f}"[1:] if abs(v) % 1 else ".5"
+        s = ("-" if v < 0 else "") + frac
     else:
         s = f"{v:.25f}"
     if fixed and len(s) > 12:
@@ -116,6 +117,59 @@ def write_mps(rng, m=12, n=20, fixed=False):
                 lines.append(f" {t:<2} {'BND':<8}  {c:<8}" + (f"  {v:>12}" if v is not None else ""))
             else:
                 lines.append(f" {t} BND {c}" + (f" {v}" if v is not None else ""))
+    lines.append("ENDATA")
+    return "\n".join(lines) + "\n"
+
+
+def lp_to_mps(lp, name="planted"):
+    """Free-format MPS text of a host LP (row sides as E/L/G plus RANGES for
+    two-sided rows; LO/UP/FX/FR/MI bounds); values written with repr.  A free
+    row is written as an L row with right-hand side 1e9, which no feasible
+    point of these models reaches."""
+    rows = [f"R{i}" for i in range(lp.m)]
+    lines = [f"NAME {name}", "ROWS", " N OBJ"]
+    kinds = []
+    for i in range(lp.m):
+        lo, hi = lp.AL[i], lp.AU[i]
+        k = "E" if lo == hi else "L" if np.isneginf(lo) else "G"
+        kinds.append(k)
+        lines.append(f" {k} {rows[i]}")
+    lines.append("COLUMNS")
+    lp = lp.ensure_transpose()
+    ptr, idx = lp.at_ptr, lp.at_idx
+    for j in range(lp.n):
+        cells = [("OBJ", lp.c[j])] if lp.c[j] != 0.0 else []
+        cells += [(rows[idx[q]], lp.at_val[q]) for q in range(ptr[j], ptr[j + 1])]
+        if not cells:
+            cells = [("OBJ", 0.0)]
+        for r, v in cells:
+            lines.append(f"    C{j} {r} {float(v)!r}")
+    lines.append("RHS")
+    for i, k in enumerate(kinds):
+        side = lp.AU[i] if k == "L" else lp.AL[i]
+        if np.isposinf(side):
+            side = 1.0e9
+        if side != 0.0:
+            lines.append(f"    RHS {rows[i]} {float(side)!r}")
+    lines.append("RANGES")
+    for i, k in enumerate(kinds):
+        if k == "G" and np.isfinite(lp.AU[i]):
+            lines.append(f"    RNG {rows[i]} {float(lp.AU[i] - lp.AL[i])!r}")
+    lines.append("BOUNDS")
+    for j in range(lp.n):
+        lo, hi = lp.l[j], lp.u[j]
+        if lo == hi:
+            lines.append(f" FX BND C{j} {float(lo)!r}")
+            continue
+        if np.isneginf(lo) and np.isposinf(hi):
+            lines.append(f" FR BND C{j}")
+            continue
+        if np.isneginf(lo):
+            lines.append(f" MI BND C{j}")
+        elif lo != 0.0:
+            lines.append(f" LO BND C{j} {float(lo)!r}")
+        if np.isfinite(hi):
+            lines.append(f" UP BND C{j} {float(hi)!r}")
     lines.append("ENDATA")
     return "\n".join(lines) + "\n"
 

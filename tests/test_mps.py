@@ -120,8 +120,8 @@ def test_both_readers_reject(case):
 
 @pytest.mark.gpu
 def test_upload_and_export_reduced(tmp_path):
-    text = mps_cases.write_mps(np.random.default_rng(77), m=300, n=700)
-    model = mps.MpsModel(text=text)
+    from gpp_b200 import lpgen
+    model = mps.MpsModel(text=mps_cases.lp_to_mps(lpgen.random_lp(300, 700, seed=77)))
     lp_c = model.upload()
     dlp = device.DeviceLp(model.host_lp())
     params = capi.Params.defaults()
@@ -130,6 +130,7 @@ def test_upload_and_export_reduced(tmp_path):
         s1 = capi.Summary()
         device._raise(capi.load().gpp_preprocess(C.byref(lp_c), C.byref(params), C.byref(s1)))
         s2 = device.preprocess(dlp, params)
+        assert s1.has_infeasible == 0 and s1.has_unbounded == 0 and s1.reduced_nnz > 0
         r1, r2 = device.Result(s1), device.Result(s2)
         for k in ("A_ptr", "A_idx", "A_val", "c", "l", "u", "AL", "AU", "row_map", "col_map", "tape_val"):
             assert np.array_equal(getattr(r1, k).view(np.uint8), getattr(r2, k).view(np.uint8)), k

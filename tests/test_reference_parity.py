@@ -73,7 +73,7 @@ needs_reference = pytest.mark.skipif(not os.path.exists(DRIVER), reason="referen
 
 
 def check_against_reference(lp, rules, extra=None):
-    extra = extra or {}
+    extra = {"enable_structure_specific_rules": 0, **(extra or {})}
     ref = run_reference(lp, rules, [f"{k}={v}" for k, v in extra.items()])
     params = params_with_rules(rules, **{"enable_folding": 0, **extra})
     dlp = device.DeviceLp(lp)
@@ -137,10 +137,11 @@ def test_folding_matches_reference(workload):
 @needs_reference
 @pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:2000x5000", "random:20000x50000"])
 def test_reference_startup_rules_do_not_fire(workload):
-    """This engine carries but does not run the reference's structure-specific
-    startup rules.  On these workloads the reference's own detectors reject
-    them: its output with the rules on equals its output with them off, so the
-    engine's parity holds for the reference's default settings too."""
+    """Of the reference's structure-specific startup rules this engine runs
+    column domination only.  On these workloads the reference's own detectors
+    reject all of them: its output with the rules on equals its output with
+    them off, so the engine's parity holds for the reference's default
+    settings too."""
     lp = lpgen.workload(workload, seed=0)
     on = run_reference(lp, ALL, ["enable_structure_specific_rules=1"])
     off = run_reference(lp, ALL)
