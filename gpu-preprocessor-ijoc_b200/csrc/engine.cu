@@ -241,14 +241,21 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
   if (p.enable_startup && p.max_iters > 0 && !time_exceeded()) {
     // Startup (gpu_presolve.cu:2361-2454): the structure-specific rules, all
     // off when enable_structure_specific_rules is (:2088-2094).  Column
-    // domination is the one implemented; its reductions are applied before
-    // Cleanup, as the reference applies its startup batch.  Two-row variable
-    // elimination, zero-cost product variables and the piecewise-linear
+    // domination, two-row variable elimination and zero-cost product
+    // variables share one plan, each seeing the deletions of those before it,
+    // and the plan is applied once before Cleanup.  The piecewise-linear
     // reformulations are not run.  The phase consumes one iteration (:2453).
-    if (p.enable_structure_specific_rules && p.enable_column_domination && !e.terminal) {
-      if (e.deferred_rule(true, "column_domination", [&] { rule_column_domination(e.plan, cur, p); }))
-        e.materialize("startup");
-    }
+    const bool batch = p.enable_structure_specific_rules &&
+                       (p.enable_column_domination || p.enable_two_row_variable_elimination ||
+                        p.enable_zero_cost_product_variables);
+    if (batch && e.deferred_rule(true, "startup_projection_batch", [&] {
+          if (p.enable_column_domination) rule_column_domination(e.plan, cur, p);
+          if (p.enable_two_row_variable_elimination && !time_exceeded())
+            rule_two_row_variable_elimination(e.plan, cur, p);
+          if (p.enable_zero_cost_product_variables && !time_exceeded())
+            rule_zero_cost_product_variables(e.plan, cur, p);
+        }))
+      e.materialize("startup");
     ++out.iterations;
   }
   auto deferred = [&](bool enabled, const char* name, auto rule) {

@@ -162,6 +162,8 @@ void rule_redundant_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const 
 void rule_dual_fix(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 // rules_startup.cu: structure-specific Startup rules.
 void rule_column_domination(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+void rule_two_row_variable_elimination(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+void rule_zero_cost_product_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p);
 void rule_parallel_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_parallel_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params& p);

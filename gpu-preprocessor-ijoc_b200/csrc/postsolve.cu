@@ -20,7 +20,8 @@ constexpr double kTol = 1e-7;
 constexpr int64_t kParallelMinRecords = 1024;
 enum : int {
   kFixedVariable = 0, kInfiniteBoundDualFix = 1, kSingletonColumnSubstitution = 2, kParallelColumn = 3,
-  kParallelRow = 4, kDeletedRow = 5, kRowDualShift = 10, kRowImpliedBoundChange = 12, kDoubletonEquation = 13
+  kParallelRow = 4, kDeletedRow = 5, kRowDualShift = 10, kRowImpliedBoundChange = 12, kDoubletonEquation = 13,
+  kFmeCol = 14
 };
 
 __device__ __forceinline__ bool pfin(double x) { return x > -INFINITY && x < INFINITY; }
@@ -161,6 +162,27 @@ __device__ void replay_record(int type, const int32_t* id, int64_t ni, const dou
       x[col] = ext;
     }
     if (dual && z) { z[col] = 0.0; s.got[col] = 1; }
+  } else if (type == kFmeCol) {
+    // replay_projected_column (postsolve_projected_variables.cuh:10-66):
+    // x = max of the lower expressions (else min of the upper ones, else 0);
+    // the column's reduced cost and its rows' duals are zero.
+    const int K = id[0], col = id[1], L = id[3 + K];
+    int64_t meta = 4 + K, at = 4 + K + 2 * int64_t(L), vp = 0;
+    if (primal) {
+      double lo = -INFINITY, hi = INFINITY;
+      bool has_lo = false, has_hi = false;
+      for (int e = 0; e < L; ++e) {
+        const int orient = id[meta++];
+        const int len = id[meta++];
+        double cand = v[vp];
+        for (int t = 0; t < len; ++t) cand += v[vp + 1 + t] * x[id[at++]];
+        if (orient > 0) { lo = fmax(lo, cand); has_lo = true; } else { hi = fmin(hi, cand); has_hi = true; }
+        vp += 1 + len;
+      }
+      x[col] = has_lo ? lo : (has_hi ? hi : 0.0);
+    }
+    if (dual && z) { z[col] = 0.0; s.got[col] = 1; }
+    if (dual && y) for (int t = 0; t < K; ++t) y[id[2 + t]] = 0.0;
   } else if (dual && type == kRowDualShift) {
     if (y) y[id[0]] += v[0];
   } else if (dual && type == kParallelRow && ni >= 2 && nv >= 5) {
@@ -370,7 +392,7 @@ struct TapeView {
 
 __device__ __forceinline__ bool replays_in(int type, bool dual) {
   if (type == kFixedVariable || type == kInfiniteBoundDualFix || type == kSingletonColumnSubstitution ||
-      type == kParallelColumn || type == kDoubletonEquation)
+      type == kParallelColumn || type == kDoubletonEquation || type == kFmeCol)
     return true;
   return dual && (type == kRowDualShift || type == kParallelRow || type == kDeletedRow || type == kRowImpliedBoundChange);
 }
@@ -401,6 +423,17 @@ __device__ void record_resources(int type, const int32_t* id, int64_t ni, int64_
         break;
       case kParallelColumn: col(id[0], true); col(id[1], true); break;
       case kDoubletonEquation: col(id[0], true); col(id[1], false); break;
+      case kFmeCol:
+        if (ni >= 4) {
+          const int K = id[0];
+          col(id[1], true);
+          if (3 + K < ni) {
+            const int terms = id[2 + K];
+            const int64_t first = int64_t(4 + K) + 2 * int64_t(id[3 + K]);
+            for (int t = 0; t < terms && first + t < ni; ++t) col(id[first + t], false);
+          }
+        }
+        break;
       default: break;
     }
     return;
@@ -419,6 +452,12 @@ __device__ void record_resources(int type, const int32_t* id, int64_t ni, int64_
         for (int q = 0; q < id[3] && 4 + q < ni; ++q) row(id[4 + q], false);
       } else if (M.present && id[0] >= 0 && id[0] < n) {
         for (offset_t q = M.AT_ptr[id[0]]; q < M.AT_ptr[id[0] + 1]; ++q) row(M.AT_idx[q], false);
+      }
+      break;
+    case kFmeCol:
+      if (ni >= 2) {
+        col(id[1], true);
+        for (int t = 0; t < id[0] && 2 + t < ni; ++t) row(id[2 + t], true);
       }
       break;
     case kRowDualShift: row(id[0], true); break;

@@ -22,7 +22,7 @@ __device__ __forceinline__ int map_idx(int x, const int32_t* map, int n) { retur
 enum : int {
   kFixedVariable = 0, kInfiniteBoundDualFix = 1, kSingletonColumnSubstitution = 2, kParallelColumn = 3,
   kParallelRow = 4, kDeletedRow = 5, kRowLowerBoundChange = 8, kRowUpperBoundChange = 9, kRowDualShift = 10,
-  kVariableBoundChange = 11, kRowImpliedBoundChange = 12, kDoubletonEquation = 13
+  kVariableBoundChange = 11, kRowImpliedBoundChange = 12, kDoubletonEquation = 13, kFmeCol = 14
 };
 
 // One thread per record; long supports are walked by the same thread (the
@@ -78,6 +78,19 @@ __global__ void globalize_kernel(int64_t count, const int32_t* __restrict__ type
           id[1] = map_idx(id[1], cols, n);
           id[2] = map_idx(id[2], rows, m);
           for (int r = 0; r < id[3] && 4 + r < sz; ++r) id[4 + r] = map_idx(id[4 + r], rows, m);
+        }
+        break;
+      case kFmeCol:
+        // [K, col, rows[K], terms, L, (orient, len)[L], cols[terms]].
+        if (sz >= 4) {
+          const int k_rows = id[0];
+          id[1] = map_idx(id[1], cols, n);
+          for (int r = 0; r < k_rows && 2 + r < sz; ++r) id[2 + r] = map_idx(id[2 + r], rows, m);
+          if (3 + k_rows < sz) {
+            const int terms = id[2 + k_rows], exprs = id[3 + k_rows];
+            const int64_t first = int64_t(4 + k_rows) + 2 * int64_t(exprs);
+            for (int t = 0; t < terms && first + t < sz; ++t) id[first + t] = map_idx(id[first + t], cols, n);
+          }
         }
         break;
       default:

@@ -391,11 +391,93 @@ def setcover_lp(m: int, n: int, seed: int = 0, witness: bool = True) -> HostLP:
     return HostLP(m, n, ptr, idx, val, c, AL, AU, np.zeros(n), np.ones(n)).ensure_transpose()
 
 
+def auxiliary_lp(m: int, n: int, seed: int = 0, pairs: float = 0.02, products: float = 0.02) -> HostLP:
+    """random_lp(m, n) plus blocks of new [0, 1] columns and rows that the
+    projected-auxiliary Startup rules accept, and decoys they must reject.
+
+    * two-row block (pairs * n of them): a zero-cost t with t >= x/4 and
+      t <= 1 - y/4, x and y new columns of nonzero cost;
+    * product block (products * n): a zero-cost z with z >= x + y - 1,
+      z <= x, z <= y (the McCormick envelope of x y);
+    * decoys, one per 16 blocks of each kind: two t sharing their lower row
+      (row conflict), a t whose rows leave no margin (t >= x, t <= 1 - y,
+      so max(x + y - 1) = 1 > 0), a product whose upper row has
+      coefficient -0.5, and a product whose endpoint is itself a product
+      variable (endpoint conflict)."""
+    base = random_lp(m, n, seed)
+    rng = np.random.default_rng(seed + 7919)
+    rows, cols, vals = [], [], []
+    AL, AU, c = [], [], []
+    next_col, next_row = n, m
+
+    def new_cols(k):
+        nonlocal next_col
+        first = next_col
+        next_col += k
+        c.extend(np.round(rng.uniform(-3.0, 3.0, size=k), 2).tolist())
+        return list(range(first, first + k))
+
+    def new_row(entries, lo, hi):
+        nonlocal next_row
+        for j, a in entries:
+            rows.append(next_row)
+            cols.append(j)
+            vals.append(a)
+        AL.append(lo)
+        AU.append(hi)
+        next_row += 1
+
+    def two_row(margin=True):
+        t, x, y = new_cols(3)
+        c[t - n] = 0.0
+        q = 0.25 if margin else 1.0
+        new_row([(t, 1.0), (x, -q)], 0.0, INF)
+        new_row([(t, 1.0), (y, q)], -INF, 1.0)
+
+    def product(upper_coeff=-1.0, endpoint=None):
+        z, x, y = new_cols(3)
+        c[z - n] = 0.0
+        if endpoint is not None:
+            x = endpoint
+        new_row([(z, 1.0), (x, -1.0), (y, -1.0)], -1.0, INF)
+        new_row([(z, 1.0), (x, upper_coeff)], -INF, 0.0)
+        new_row([(z, 1.0), (y, -1.0)], -INF, 0.0)
+        return z
+
+    for k in range(int(pairs * n)):
+        if k % 16 == 5:
+            t1, t2, x, y1, y2 = new_cols(5)
+            c[t1 - n] = c[t2 - n] = 0.0
+            new_row([(t1, 1.0), (t2, 1.0), (x, -0.25)], 0.0, INF)
+            new_row([(t1, 1.0), (y1, 0.25)], -INF, 1.0)
+            new_row([(t2, 1.0), (y2, 0.25)], -INF, 1.0)
+        elif k % 16 == 11:
+            two_row(margin=False)
+        else:
+            two_row()
+    for k in range(int(products * n)):
+        if k % 16 == 3:
+            product(upper_coeff=-0.5)
+        elif k % 16 == 9:
+            product(endpoint=product())
+        else:
+            product()
+    n_new, m_new = next_col, next_row
+    brows = np.repeat(np.arange(m, dtype=np.int64), np.diff(base.row_ptr))
+    ptr, idx, val = coo_to_csr(m_new, np.concatenate([brows, np.array(rows, np.int64)]),
+                               np.concatenate([base.col_idx.astype(np.int64), np.array(cols, np.int64)]),
+                               np.concatenate([base.values, np.array(vals)]))
+    k = n_new - n
+    return HostLP(m_new, n_new, ptr, idx, val, np.concatenate([base.c, c]), np.concatenate([base.AL, AL]),
+                  np.concatenate([base.AU, AU]), np.concatenate([base.l, np.zeros(k)]),
+                  np.concatenate([base.u, np.ones(k)])).ensure_transpose()
+
+
 def workload(name: str, seed: int = 0) -> HostLP:
     """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
     'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows),
     'replicated:MxN*K' (K identical copies plus a coupling row), 'setcover:MxN' (unit set covering),
-    'qap:N'."""
+    'auxiliary:MxN' (random family plus projected-auxiliary blocks), 'qap:N'."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -413,6 +495,9 @@ def workload(name: str, seed: int = 0) -> HostLP:
         mn, k = spec.split("*")
         m, n = (int(v) for v in mn.split("x"))
         return replicated_lp(m, n, int(k), seed)
+    if name.startswith("auxiliary:"):
+        m, n = (int(v) for v in name.split(":")[1].split("x"))
+        return auxiliary_lp(m, n, seed)
     if name.startswith("setcover:"):
         m, n = (int(v) for v in name.split(":")[1].split("x"))
         return setcover_lp(m, n, seed)

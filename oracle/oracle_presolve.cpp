@@ -67,6 +67,20 @@ void globalize(Tape& t, const std::vector<int>& rows, const std::vector<int>& co
           for (int r = 0; r < id[3] && 4 + r < sz; ++r) id[4 + r] = mr(id[4 + r]);
         }
         break;
+      case FmeCol:
+        // [K, col, rows[K], terms, L, (orient, len)[L], cols[terms]]
+        // (gpu_presolve.cu:1335-1356).
+        if (sz >= 4) {
+          const int k_rows = id[0];
+          id[1] = mc(id[1]);
+          for (int r = 0; r < k_rows && 2 + r < sz; ++r) id[2 + r] = mr(id[2 + r]);
+          if (3 + k_rows < sz) {
+            const int terms = id[2 + k_rows], exprs = id[3 + k_rows];
+            const int64_t first = int64_t(4 + k_rows) + 2 * int64_t(exprs);
+            for (int q = 0; q < terms && first + q < sz; ++q) id[first + q] = mc(id[first + q]);
+          }
+        }
+        break;
       default:
         throw std::runtime_error("oracle: unknown tape record type");
     }
@@ -267,13 +281,19 @@ Result presolve(const Lp& lp, const gpp_params& p) {
   const auto t0 = std::chrono::steady_clock::now();
 
   if (p.enable_startup && p.max_iters > 0) {
-    // Startup (gpu_presolve.cu:2361-2454): of the structure-specific rules,
-    // column domination, applied before Cleanup; the phase consumes one
-    // iteration (:2453).
-    if (p.enable_structure_specific_rules && p.enable_column_domination) {
-      if (e.deferred_rule(true, "column_domination", [&] { rule_column_domination(e.plan, e.cur, p); }))
-        e.materialize("startup");
-    }
+    // Startup (gpu_presolve.cu:2361-2454): column domination, two-row
+    // variable elimination and zero-cost product variables share one plan
+    // (each sees the deletions of those before it), applied once before
+    // Cleanup; the phase consumes one iteration (:2453).
+    const bool batch = p.enable_structure_specific_rules &&
+                       (p.enable_column_domination || p.enable_two_row_variable_elimination ||
+                        p.enable_zero_cost_product_variables);
+    if (batch && e.deferred_rule(true, "startup_projection_batch", [&] {
+          if (p.enable_column_domination) rule_column_domination(e.plan, e.cur, p);
+          if (p.enable_two_row_variable_elimination) rule_two_row_variable_elimination(e.plan, e.cur, p);
+          if (p.enable_zero_cost_product_variables) rule_zero_cost_product_variables(e.plan, e.cur, p);
+        }))
+      e.materialize("startup");
     ++S.iterations;
   }
   auto cleanup = [&]() {
@@ -538,6 +558,27 @@ void Replay::run(int64_t k, bool primal, bool dual) {
     fixed_variable(k, primal, dual);
   } else if (type == InfiniteBoundDualFix) {
     infinite_dual_fix(k, primal, dual);
+  } else if (type == FmeCol) {
+    // replay_projected_column (postsolve_projected_variables.cuh:10-66).
+    const int K = id[0], col = id[1], L = id[3 + K];
+    int64_t meta = 4 + K, at = 4 + K + 2 * int64_t(L), vp = 0;
+    if (primal) {
+      double lo = -INFINITY, hi = INFINITY;
+      bool has_lo = false, has_hi = false;
+      for (int e = 0; e < L; ++e) {
+        const int orient = id[meta++], len = id[meta++];
+        double cand = v[vp];
+        for (int q = 0; q < len; ++q) cand += v[vp + 1 + q] * x[id[at++]];
+        if (orient > 0) { lo = std::fmax(lo, cand); has_lo = true; } else { hi = std::fmin(hi, cand); has_hi = true; }
+        vp += 1 + len;
+      }
+      x[col] = has_lo ? lo : (has_hi ? hi : 0.0);
+    }
+    if (dual) {
+      z[col] = 0.0;
+      got[col] = 1;
+      for (int q = 0; q < K; ++q) y[id[2 + q]] = 0.0;
+    }
   } else if (dual && type == RowDualShift) {
     y[id[0]] += v[0];
   } else if (dual && type == ParallelRow && ni >= 2 && nv >= 5) {

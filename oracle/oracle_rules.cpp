@@ -1502,5 +1502,281 @@ void rule_column_domination(Plan& plan, const Lp& lp, const gpp_params& p) {
   plan.has_col_action = plan.has_change = true;
 }
 
+
+// ---- projected auxiliaries ------------------------------------------------
+// Two-row variable elimination (rule_two_row_variable_elimination.cu) and
+// zero-cost product variables (rule_zero_cost_product_variables.cu): the
+// detectors see the plan's masks (the deletions of earlier rules of the
+// Startup batch), selected columns leave with their rows, and each leaves a
+// projected-column record (the device layout of device_recovery.cu:433-476).
+namespace {
+
+constexpr int kMaxCertified = 8;
+
+struct Expr {
+  double constant = 0.0;
+  std::vector<int> cols;
+  std::vector<double> coeffs;
+};
+
+bool add_term(Expr& e, int col, double coeff, size_t capacity) {
+  if (!std::isfinite(coeff)) return false;
+  for (size_t k = 0; k < e.cols.size(); ++k)
+    if (e.cols[k] == col) { e.coeffs[k] += coeff; return std::isfinite(e.coeffs[k]); }
+  if (e.cols.size() >= capacity) return false;
+  e.cols.push_back(col);
+  e.coeffs.push_back(coeff);
+  return true;
+}
+
+bool margin_le(double lhs, double rhs, double tol) {
+  if (!std::isfinite(lhs) || !std::isfinite(rhs)) return false;
+  return rhs - lhs >= tol * (1.0 + std::fmax(std::fabs(lhs), std::fabs(rhs)));
+}
+
+// The K rows of column j that the plan keeps, or empty.
+std::vector<int> kept_rows(const Lp& lp, const Plan& plan, int j, size_t K) {
+  std::vector<int> out;
+  for (int q = lp.AT.ptr[size_t(j)]; q < lp.AT.ptr[size_t(j) + 1]; ++q) {
+    const int i = lp.AT.idx[size_t(q)];
+    if (!plan.keep_row[size_t(i)]) continue;
+    if (out.size() == K) return {};
+    out.push_back(i);
+  }
+  return out.size() == K ? out : std::vector<int>{};
+}
+
+int live_in_row(const Lp& lp, const Plan& plan, int i, int cap) {
+  int live = 0;
+  for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q)
+    if (plan.keep_col[size_t(lp.A.idx[size_t(q)])] && ++live > cap) return live;
+  return live;
+}
+
+// Lower/upper bound on column j from a one-sided row (build_row_affine,
+// rule_two_row_variable_elimination.cu:150-200).
+bool row_expression(const Lp& lp, const Plan& plan, int i, int j, int max_nnz, double zero_tol, Expr& e,
+                    bool& lower) {
+  const int live = live_in_row(lp, plan, i, max_nnz);
+  if (live < 2 || live > max_nnz || live > kMaxCertified) return false;
+  int pivots = 0;
+  double pivot = 0.0;
+  for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q)
+    if (plan.keep_col[size_t(lp.A.idx[size_t(q)])] && lp.A.idx[size_t(q)] == j) { ++pivots; pivot = lp.A.val[size_t(q)]; }
+  if (pivots != 1 || !std::isfinite(pivot) || std::fabs(pivot) <= zero_tol) return false;
+  const double al = plan.AL[size_t(i)], au = plan.AU[size_t(i)];
+  double side;
+  if (std::isfinite(al) && std::isinf(au) && au > 0.0) { lower = pivot > 0.0; side = al; }
+  else if (std::isinf(al) && al < 0.0 && std::isfinite(au)) { lower = pivot < 0.0; side = au; }
+  else return false;
+  e = Expr{};
+  e.constant = side / pivot;
+  if (!std::isfinite(e.constant)) return false;
+  for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q) {
+    const int k = lp.A.idx[size_t(q)];
+    if (!plan.keep_col[size_t(k)] || k == j) continue;
+    if (!add_term(e, k, -lp.A.val[size_t(q)] / pivot, kMaxCertified - 1)) return false;
+  }
+  return true;
+}
+
+bool expr_range(const Expr& e, const Plan& plan, double& lo, double& hi) {
+  lo = hi = e.constant;
+  for (size_t k = 0; k < e.cols.size(); ++k) {
+    const double l = plan.l[size_t(e.cols[k])], u = plan.u[size_t(e.cols[k])], q = e.coeffs[k];
+    if (!std::isfinite(l) || !std::isfinite(u) || l > u) return false;
+    lo += q >= 0.0 ? q * l : q * u;
+    hi += q >= 0.0 ? q * u : q * l;
+  }
+  return std::isfinite(lo) && std::isfinite(hi);
+}
+
+bool max_difference(const Expr& lo_e, const Expr& up_e, const Plan& plan, double& out) {
+  Expr d;
+  for (size_t k = 0; k < lo_e.cols.size(); ++k)
+    if (!add_term(d, lo_e.cols[k], lo_e.coeffs[k], 2 * (kMaxCertified - 1))) return false;
+  for (size_t k = 0; k < up_e.cols.size(); ++k)
+    if (!add_term(d, up_e.cols[k], -up_e.coeffs[k], 2 * (kMaxCertified - 1))) return false;
+  double v = lo_e.constant - up_e.constant;
+  for (size_t k = 0; k < d.cols.size(); ++k) {
+    const double l = plan.l[size_t(d.cols[k])], u = plan.u[size_t(d.cols[k])];
+    if (!std::isfinite(l) || !std::isfinite(u) || l > u) return false;
+    v += d.coeffs[k] >= 0.0 ? d.coeffs[k] * u : d.coeffs[k] * l;
+  }
+  if (!std::isfinite(v)) return false;
+  out = v;
+  return true;
+}
+
+// McCormick row pattern (match_mccormick_row, rule_zero_cost_product_variables.cu:75-150).
+bool mccormick_row(const Lp& lp, const Plan& plan, int i, int z, bool& lower, int& e0, int& e1) {
+  e0 = e1 = -1;
+  const int live = live_in_row(lp, plan, i, 3);
+  if (live != 2 && live != 3) return false;
+  int pivots = 0;
+  double pivot = 0.0;
+  for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q)
+    if (plan.keep_col[size_t(lp.A.idx[size_t(q)])] && lp.A.idx[size_t(q)] == z) { pivot = lp.A.val[size_t(q)]; ++pivots; }
+  if (pivots != 1 || !std::isfinite(pivot) || pivot == 0.0) return false;
+  const double al = plan.AL[size_t(i)], au = plan.AU[size_t(i)];
+  double side;
+  if (std::isfinite(al) && std::isinf(au) && au > 0.0) { lower = pivot > 0.0; side = al; }
+  else if (std::isinf(al) && al < 0.0 && std::isfinite(au)) { lower = pivot < 0.0; side = au; }
+  else return false;
+  if (live != (lower ? 3 : 2) || side != (lower ? -pivot : 0.0)) return false;
+  int ends = 0;
+  for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q) {
+    const int k = lp.A.idx[size_t(q)];
+    if (!plan.keep_col[size_t(k)] || k == z) continue;
+    if (lp.A.val[size_t(q)] != -pivot || ends >= 2) return false;
+    (ends == 0 ? e0 : e1) = k;
+    ++ends;
+  }
+  return ends == (lower ? 2 : 1) && !(lower && e0 == e1);
+}
+
+// Records (before the deletions) and deletions for the selected columns.
+void commit_projected(Plan& plan, const Lp& lp, const gpp_params& p, const std::vector<int>& chosen,
+                      const std::vector<std::vector<int>>& rows, int K) {
+  if (p.record_postsolve_tape) {
+    for (int j : chosen) {
+      const auto& rr = rows[size_t(j)];
+      int lrow = -1;
+      double pivot = 0.0, side = 0.0;
+      for (int i : rr) {
+        int seen = 0;
+        double v = 0.0;
+        for (int q = lp.A.ptr[size_t(i)]; q < lp.A.ptr[size_t(i) + 1]; ++q)
+          if (lp.A.idx[size_t(q)] == j) { v = lp.A.val[size_t(q)]; ++seen; }
+        if (seen != 1 || !std::isfinite(v) || v == 0.0) break;
+        const double al = plan.AL[size_t(i)], au = plan.AU[size_t(i)];
+        const bool lo = std::isfinite(al) && std::isinf(au) && au > 0.0 && v > 0.0;
+        const bool up = std::isinf(al) && al < 0.0 && std::isfinite(au) && v < 0.0;
+        if (lo || up) { lrow = i; pivot = v; side = lo ? al : au; break; }
+      }
+      if (lrow < 0) throw std::runtime_error("oracle: projection certificate changed before commit");
+      std::vector<int> sup;
+      std::vector<double> coef;
+      for (int q = lp.A.ptr[size_t(lrow)]; q < lp.A.ptr[size_t(lrow) + 1]; ++q) {
+        const int k = lp.A.idx[size_t(q)];
+        if (k != j && plan.keep_col[size_t(k)]) { sup.push_back(k); coef.push_back(-lp.A.val[size_t(q)] / pivot); }
+      }
+      if (K == 3 && sup.size() != 2) throw std::runtime_error("oracle: projection certificate changed before commit");
+      std::vector<int> ids{K, j};
+      ids.insert(ids.end(), rr.begin(), rr.end());
+      const int len = int(sup.size());
+      ids.insert(ids.end(), {len, 2, 1, 0, 1, len});
+      ids.insert(ids.end(), sup.begin(), sup.end());
+      std::vector<double> vals{K == 2 ? plan.l[size_t(j)] : 0.0, side / pivot};
+      vals.insert(vals.end(), coef.begin(), coef.end());
+      plan.tape.add(FmeCol, ids, vals);
+    }
+  }
+  for (int j : chosen) {
+    plan.keep_col[size_t(j)] = 0;
+    for (int i : rows[size_t(j)]) plan.keep_row[size_t(i)] = 0;
+  }
+  plan.has_change = plan.has_row_action = plan.has_col_action = true;
+}
+
+// Select candidates whose rows no other candidate uses; threshold on the
+// share of the live columns.
+template <class Extra>
+void select_and_commit(Plan& plan, const Lp& lp, const gpp_params& p, const std::vector<uint8_t>& cand,
+                       const std::vector<std::vector<int>>& rows, int K, int live, int min_count, double min_ratio,
+                       Extra extra_ok) {
+  const int n = lp.n();
+  std::vector<int> row_count(size_t(lp.m()), 0);
+  for (int j = 0; j < n; ++j)
+    if (cand[size_t(j)]) for (int i : rows[size_t(j)]) ++row_count[size_t(i)];
+  std::vector<int> chosen;
+  for (int j = 0; j < n; ++j) {
+    if (!cand[size_t(j)]) continue;
+    bool ok = true;
+    for (int i : rows[size_t(j)]) ok = ok && row_count[size_t(i)] == 1;
+    if (ok && extra_ok(j)) chosen.push_back(j);
+  }
+  const int count = int(chosen.size());
+  const double ratio = double(count) / double(std::max(1, live));
+  if (count < std::max(1, min_count) || !(ratio + 1.0e-15 >= min_ratio)) return;
+  commit_projected(plan, lp, p, chosen, rows, K);
+}
+
+}  // namespace
+
+void rule_two_row_variable_elimination(Plan& plan, const Lp& lp, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (m <= 0 || n <= 0 || lp.A.ptr[size_t(m)] <= 0) return;
+  const int max_nnz = std::max(2, std::min(kMaxCertified, p.two_row_variable_elimination_max_row_nnz));
+  const double tol = std::max(p.two_row_variable_elimination_safety_tol,
+                              std::max(10.0 * p.feasibility_tol, 100.0 * p.zero_tol));
+  std::vector<uint8_t> cand(size_t(n), 0);
+  std::vector<std::vector<int>> rows(static_cast<size_t>(n), std::vector<int>{});
+  int live = 0;
+  for (int j = 0; j < n; ++j) {
+    if (!plan.keep_col[size_t(j)]) continue;
+    ++live;
+    const double l = plan.l[size_t(j)], u = plan.u[size_t(j)];
+    if (plan.c[size_t(j)] != 0.0 || !std::isfinite(l) || !std::isfinite(u) || !margin_le(l, u, tol)) continue;
+    auto rr = kept_rows(lp, plan, j, 2);
+    if (rr.empty() || rr[0] == rr[1]) continue;
+    Expr e0, e1;
+    bool lo0 = false, lo1 = false;
+    if (!row_expression(lp, plan, rr[0], j, max_nnz, p.zero_tol, e0, lo0) ||
+        !row_expression(lp, plan, rr[1], j, max_nnz, p.zero_tol, e1, lo1) || lo0 == lo1)
+      continue;
+    const Expr& le = lo0 ? e0 : e1;
+    const Expr& ue = lo0 ? e1 : e0;
+    double lmin, lmax, umin, umax, diff;
+    if (!expr_range(le, plan, lmin, lmax) || !expr_range(ue, plan, umin, umax)) continue;
+    if (!margin_le(lmax, u, tol) || !margin_le(l, umin, tol)) continue;
+    if (!max_difference(le, ue, plan, diff) || !margin_le(diff, 0.0, tol)) continue;
+    cand[size_t(j)] = 1;
+    rows[size_t(j)] = rr;
+  }
+  select_and_commit(plan, lp, p, cand, rows, 2, live, p.two_row_variable_elimination_min_candidates,
+                    p.two_row_variable_elimination_min_candidate_ratio, [](int) { return true; });
+}
+
+void rule_zero_cost_product_variables(Plan& plan, const Lp& lp, const gpp_params& p) {
+  if (plan.has_infeasible || plan.has_unbounded) return;
+  const int m = lp.m(), n = lp.n();
+  if (m <= 0 || n <= 0 || lp.A.ptr[size_t(m)] <= 0) return;
+  std::vector<uint8_t> cand(size_t(n), 0);
+  std::vector<std::vector<int>> rows(static_cast<size_t>(n), std::vector<int>{});
+  std::vector<int> end0(size_t(n), -1), end1(size_t(n), -1);
+  int live = 0;
+  for (int z = 0; z < n; ++z) {
+    if (!plan.keep_col[size_t(z)]) continue;
+    ++live;
+    if (plan.c[size_t(z)] != 0.0 || plan.l[size_t(z)] != 0.0 || plan.u[size_t(z)] != 1.0) continue;
+    auto rr = kept_rows(lp, plan, z, 3);
+    if (rr.empty() || rr[0] == rr[1] || rr[0] == rr[2] || rr[1] == rr[2]) continue;
+    int lower_at = -1, nup = 0, ups[2] = {-1, -1};
+    bool ok = true;
+    int e0[3], e1[3];
+    for (int k = 0; k < 3 && ok; ++k) {
+      bool lower = false;
+      if (!mccormick_row(lp, plan, rr[size_t(k)], z, lower, e0[k], e1[k])) ok = false;
+      else if (lower) { if (lower_at >= 0) ok = false; else lower_at = k; }
+      else { if (nup >= 2) ok = false; else ups[nup++] = k; }
+    }
+    if (!ok || lower_at < 0 || nup != 2) continue;
+    const int x = e0[lower_at], y = e1[lower_at], ux = e0[ups[0]], uy = e0[ups[1]];
+    if (x < 0 || y < 0 || x == y || !((ux == x && uy == y) || (ux == y && uy == x))) continue;
+    if (plan.l[size_t(x)] != 0.0 || plan.u[size_t(x)] != 1.0 || plan.l[size_t(y)] != 0.0 || plan.u[size_t(y)] != 1.0)
+      continue;
+    cand[size_t(z)] = 1;
+    rows[size_t(z)] = rr;
+    end0[size_t(z)] = x;
+    end1[size_t(z)] = y;
+  }
+  select_and_commit(plan, lp, p, cand, rows, 3, live, p.zero_cost_product_variables_min_candidates,
+                    p.zero_cost_product_variables_min_candidate_ratio, [&](int z) {
+                      return !cand[size_t(end0[size_t(z)])] && !cand[size_t(end1[size_t(z)])];
+                    });
+}
+
 }  // namespace oracle
 
