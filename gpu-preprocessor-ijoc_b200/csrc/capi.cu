@@ -882,6 +882,71 @@ void gpp_lp_free(gpp_lp* lp) {
   *lp = gpp_lp{};
 }
 
+namespace {
+void require_reduced(const gpp_summary* summary, const char* who) {
+  if (!summary || !summary->record) throw std::invalid_argument(std::string(who) + ": null argument");
+  if (summary->has_infeasible || summary->has_unbounded)
+    throw std::invalid_argument(std::string(who) + ": presolve ended infeasible or unbounded; no reduced LP");
+}
+}  // namespace
+
+int gpp_reduced_to_device(const gpp_summary* summary, gpp_lp* out) {
+  return guarded([&] {
+    require_reduced(summary, "gpp_reduced_to_device");
+    if (!out) throw std::invalid_argument("gpp_reduced_to_device: null argument");
+    const gpp_lp& r = summary->reduced_lp;
+    if (r.A.rows <= 0 || r.A.cols <= 0 || r.A.nnz <= 0)
+      throw std::invalid_argument("gpp_reduced_to_device: the reduced LP is empty");
+    *out = gpp_lp{};
+    auto dup = [](const auto* src, size_t count, auto** dst) {
+      using T = std::remove_const_t<std::remove_pointer_t<decltype(src)>>;
+      check(cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * std::max<size_t>(count, 1)), "cudaMalloc");
+      if (count) check(cudaMemcpy(*dst, src, sizeof(T) * count, cudaMemcpyDeviceToDevice), "handoff copy");
+    };
+    try {
+      const size_t m = size_t(r.A.rows), n = size_t(r.A.cols), nnz = size_t(r.A.nnz);
+      out->A = {r.A.rows, r.A.cols, r.A.nnz, nullptr, nullptr, nullptr};
+      out->AT = {r.AT.rows, r.AT.cols, r.AT.nnz, nullptr, nullptr, nullptr};
+      dup(r.A.rowPtr, m + 1, &out->A.rowPtr); dup(r.A.colVal, nnz, &out->A.colVal);
+      dup(r.A.nzVal, nnz, &out->A.nzVal);
+      dup(r.AT.rowPtr, n + 1, &out->AT.rowPtr); dup(r.AT.colVal, nnz, &out->AT.colVal);
+      dup(r.AT.nzVal, nnz, &out->AT.nzVal);
+      dup(r.c, n, &out->c); dup(r.AL, m, &out->AL); dup(r.AU, m, &out->AU);
+      dup(r.l, n, &out->l); dup(r.u, n, &out->u);
+      out->obj_constant = r.obj_constant;
+    } catch (...) {
+      gpp_lp_free(out);
+      throw;
+    }
+  });
+}
+
+int gpp_reduced_to_host(const gpp_summary* summary, gpp_offset* row_ptr, int32_t* col_idx, double* val, double* c,
+                        double* AL, double* AU, double* l, double* u, double* obj_constant) {
+  return guarded([&] {
+    require_reduced(summary, "gpp_reduced_to_host");
+    const gpp_lp& r = summary->reduced_lp;
+    const size_t m = size_t(std::max(0, r.A.rows)), n = size_t(std::max(0, r.A.cols)),
+                 nnz = size_t(std::max<gpp_offset>(0, r.A.nnz));
+    auto get = [](void* dst, const void* src, size_t bytes) {
+      if (dst && bytes) check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "handoff copy");
+    };
+    if (row_ptr && !r.A.rowPtr) {
+      for (size_t i = 0; i <= m; ++i) row_ptr[i] = 0;
+    } else {
+      get(row_ptr, r.A.rowPtr, sizeof(gpp_offset) * (m + 1));
+    }
+    get(col_idx, r.A.colVal, sizeof(int32_t) * nnz);
+    get(val, r.A.nzVal, sizeof(double) * nnz);
+    get(c, r.c, sizeof(double) * n);
+    get(AL, r.AL, sizeof(double) * m);
+    get(AU, r.AU, sizeof(double) * m);
+    get(l, r.l, sizeof(double) * n);
+    get(u, r.u, sizeof(double) * n);
+    if (obj_constant) *obj_constant = r.obj_constant;
+  });
+}
+
 int gpp_export_reduced(const gpp_summary* summary, const char* out_dir, const char* model_name) {
   return guarded([&] {
     if (!summary || !summary->record || !out_dir) throw std::invalid_argument("gpp_export_reduced: null argument");

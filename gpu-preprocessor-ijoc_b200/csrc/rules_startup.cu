@@ -35,25 +35,33 @@ namespace {
 
 enum : int32_t { kBadRow = 1, kBadColumn = 2, kBadValue = 4, kNoWitness = 8 };
 
-// One launch checks rows (sides and a cost-1 witness), columns (box and
-// cost) and every stored coefficient of A and A^T, grid-stride over the
-// largest of the three ranges.
-__global__ void cd_validate(int m, int n, offset_t nnz, const offset_t* __restrict__ ptr,
-                            const int32_t* __restrict__ idx, const double* __restrict__ a,
-                            const double* __restrict__ at, const double* __restrict__ c,
-                            const double* __restrict__ AL, const double* __restrict__ AU,
-                            const double* __restrict__ l, const double* __restrict__ u,
-                            int32_t* __restrict__ failure) {
+// First the cheap checks (row sides, column boxes and costs: m + n reads),
+// which reject almost every model; only then the per-entry ones (every
+// coefficient of A and A^T, and a cost-1 witness in each row).
+__global__ void cd_validate_sides(int m, int n, const double* __restrict__ c, const double* __restrict__ AL,
+                                  const double* __restrict__ AU, const double* __restrict__ l,
+                                  const double* __restrict__ u, int32_t* __restrict__ failure) {
+  int32_t bad = 0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    const double cj = c[j];
+    if (l[j] != 0.0 || u[j] != 1.0 || !(isfinite(cj) && cj >= 1.0 && floor(cj) == cj)) bad |= kBadColumn;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+    if (AL[i] != 1.0 || !(isinf(AU[i]) && AU[i] > 0.0)) bad |= kBadRow;
+  bad = __reduce_or_sync(0xffffffffu, bad);
+  if (bad && (threadIdx.x & 31) == 0) atomicOr(failure, bad);
+}
+
+__global__ void cd_validate_entries(int m, offset_t nnz, const offset_t* __restrict__ ptr,
+                                    const int32_t* __restrict__ idx, const double* __restrict__ a,
+                                    const double* __restrict__ at, const double* __restrict__ c,
+                                    int32_t* __restrict__ failure) {
   int32_t bad = 0;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nnz; t += stride)
     if (a[t] != 1.0 || at[t] != 1.0) bad |= kBadValue;
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) {
-    const double cj = c[j];
-    if (l[j] != 0.0 || u[j] != 1.0 || !(isfinite(cj) && cj >= 1.0 && floor(cj) == cj)) bad |= kBadColumn;
-  }
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride) {
-    if (AL[i] != 1.0 || !(isinf(AU[i]) && AU[i] > 0.0)) bad |= kBadRow;
     bool witness = false;
     for (offset_t p = ptr[i]; p < ptr[i + 1] && !witness; ++p) witness = c[idx[p]] == 1.0;
     if (!witness) bad |= kNoWitness;
@@ -555,8 +563,11 @@ void rule_column_domination(Plan& plan, const WorkingLp& lp, const gpp_params& p
   auto s = ctx().stream;
   Status st;
   st.clear(2);
-  GPP_LAUNCH(cd_validate, grid_stride_blocks(std::max<int64_t>(nnz, std::max(m, n))), kThreads, 0, s, m, n, nnz,
-             lp.A.ptr, lp.A.idx, lp.A.val, lp.AT.val, plan.c.p, plan.AL.p, plan.AU.p, plan.l.p, plan.u.p, st.d);
+  GPP_LAUNCH(cd_validate_sides, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, m, n, plan.c.p, plan.AL.p,
+             plan.AU.p, plan.l.p, plan.u.p, st.d);
+  if (st.read(1)[0] != 0) return;
+  GPP_LAUNCH(cd_validate_entries, grid_stride_blocks(std::max<int64_t>(nnz, m)), kThreads, 0, s, m, nnz, lp.A.ptr,
+             lp.A.idx, lp.A.val, lp.AT.val, plan.c.p, st.d);
   if (st.read(1)[0] != 0) return;
   DBuf<uint8_t> dominated(size_t(n), s);
   GPP_LAUNCH(cd_mark, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, plan.c.p, dominated.p, st.d + 1);

@@ -16,10 +16,10 @@ namespace gpp {
 void radix_sort_pairs(uint64_t* keys, int32_t* vals, int64_t n, cudaStream_t s) {
   if (n <= 1) return;
   const int64_t tiles = (n + kTile - 1) / kTile;
-  DBuf<uint32_t> seen(64, s);
-  seen.zero();
-  GPP_LAUNCH(digit_presence, grid_stride_blocks(n), kThreads, 0, s, keys, n, seen.p);
-  const std::vector<uint32_t> present = to_host(seen.p, 64);
+  DBuf<unsigned long long> varies(1, s);
+  varies.zero();
+  GPP_LAUNCH(digit_variation, grid_stride_blocks(n), kThreads, 0, s, keys, n, varies.p);
+  const uint64_t variation = read_scalar(varies.p);
   DBuf<uint64_t> k2(size_t(n), s);
   DBuf<int32_t> v2(size_t(n), s), counts(size_t(256 * tiles) + 1, s);
   uint64_t* ka = keys;
@@ -27,9 +27,7 @@ void radix_sort_pairs(uint64_t* keys, int32_t* vals, int64_t n, cudaStream_t s) 
   uint64_t* kb = k2.p;
   int32_t* vb = v2.p;
   for (int pass = 0; pass < 8; ++pass) {
-    int digits = 0;
-    for (int w = 0; w < 8; ++w) digits += __builtin_popcount(present[size_t(pass * 8 + w)]);
-    if (digits <= 1) continue;  // every key has the same digit: the pass is the identity
+    if (((variation >> (8 * pass)) & 0xffu) == 0) continue;  // one digit for every key: the identity
     GPP_LAUNCH(digit_histogram, int(tiles), kThreads, 0, s, ka, n, 8 * pass, counts.p, tiles);
     exclusive_scan_i32(counts.p, counts.p, 256 * tiles, s);
     GPP_LAUNCH(digit_scatter, int(tiles), kThreads, 0, s, ka, va, n, 8 * pass, counts.p, tiles, kb, vb);

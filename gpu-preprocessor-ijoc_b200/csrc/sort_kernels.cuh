@@ -29,20 +29,18 @@ __global__ void digit_histogram(const uint64_t* __restrict__ keys, int64_t n, in
   counts[int64_t(threadIdx.x) * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Digit presence over all 8 digit positions at once (for pass skipping).
-__global__ void digit_presence(const uint64_t* __restrict__ keys, int64_t n, uint32_t* __restrict__ seen) {
-  __shared__ uint32_t local[8 * 8];  // 8 passes x 256 bits
-  if (threadIdx.x < 64) local[threadIdx.x] = 0;
-  __syncthreads();
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const uint64_t k = keys[i];
-    for (int pass = 0; pass < 8; ++pass) {
-      const int d = int((k >> (8 * pass)) & 0xff);
-      atomicOr(&local[pass * 8 + (d >> 5)], 1u << (d & 31));
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 64 && local[threadIdx.x]) atomicOr(&seen[threadIdx.x], local[threadIdx.x]);
+// Which digit positions vary (for pass skipping): the OR over all keys of
+// key ^ keys[0].  A byte of it is zero exactly when every key has the same
+// digit there, and that pass is the identity.  One register OR per thread,
+// a warp reduction, one atomic per warp per half.
+__global__ void digit_variation(const uint64_t* __restrict__ keys, int64_t n, unsigned long long* __restrict__ out) {
+  const uint64_t first = keys[0];
+  uint64_t acc = 0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    acc |= keys[i] ^ first;
+  const uint32_t lo = __reduce_or_sync(0xffffffffu, uint32_t(acc));
+  const uint32_t hi = __reduce_or_sync(0xffffffffu, uint32_t(acc >> 32));
+  if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(out, (uint64_t(hi) << 32) | lo);
 }
 
 // Stable scatter of one tile: the tile's keys are first ranked into a

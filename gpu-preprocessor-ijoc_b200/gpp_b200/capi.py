@@ -172,6 +172,8 @@ def load():
         "gpp_mps_upload": (C.c_int, [vp, P(Lp)]),
         "gpp_lp_free": (None, [P(Lp)]),
         "gpp_export_reduced": (C.c_int, [P(Summary), C.c_char_p, C.c_char_p]),
+        "gpp_reduced_to_device": (C.c_int, [P(Summary), P(Lp)]),
+        "gpp_reduced_to_host": (C.c_int, [P(Summary)] + [vp] * 9),
         "gpp_schedule_model_create": (C.c_int, [vp, C.c_double, C.c_double, P(vp)]),
         "gpp_schedule_model_free": (None, [vp]),
         "gpp_preprocess_scheduled": (C.c_int, [P(Lp), P(Params), vp, P(Summary)]),
@@ -200,7 +202,7 @@ EXPORTED = [
     "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
     "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
     "gpp_mps_read", "gpp_mps_read_string", "gpp_mps_info", "gpp_mps_arrays", "gpp_mps_free", "gpp_mps_upload",
-    "gpp_lp_free", "gpp_export_reduced",
+    "gpp_lp_free", "gpp_export_reduced", "gpp_reduced_to_device", "gpp_reduced_to_host",
     "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
 ]

@@ -41,6 +41,15 @@ def ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None and t.numel() else C.c_void_p(0)
 
 
+def f64ptr(t, name="solution vector"):
+    """ptr() of a contiguous CUDA float64 tensor (the C ABI reads doubles)."""
+    if t is not None and t.numel():
+        torch = _torch()
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+            raise TypeError(f"{name} must be a contiguous CUDA float64 tensor, got {t.dtype} on {t.device}")
+    return ptr(t)
+
+
 class DeviceLp:
     """A host LP uploaded to the GPU; keeps the tensors alive."""
 
@@ -167,7 +176,7 @@ def postprocess(x_red, y_red, z_red, summary: capi.Summary, original: DeviceLp, 
         out = (np.zeros(summary.original_cols), np.zeros(summary.original_rows), np.zeros(summary.original_cols))
     addr = [a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr() for a in out]
     lp = original.struct()
-    _raise(lib.gpp_postprocess(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
+    _raise(lib.gpp_postprocess(f64ptr(x_red), f64ptr(y_red), f64ptr(z_red), C.byref(summary), C.byref(lp),
                                *(C.c_void_p(v) for v in addr)))
     return out
 
@@ -184,7 +193,7 @@ def postsolve_device(x_red, y_red, z_red, summary: capi.Summary, original: Devic
                torch.empty(summary.original_rows, dtype=torch.float64, device="cuda"),
                torch.empty(summary.original_cols, dtype=torch.float64, device="cuda"))
     lp = original.struct()
-    _raise(capi.load().gpp_postsolve_device(ptr(x_red), ptr(y_red), ptr(z_red), C.byref(summary), C.byref(lp),
+    _raise(capi.load().gpp_postsolve_device(f64ptr(x_red), f64ptr(y_red), f64ptr(z_red), C.byref(summary), C.byref(lp),
                                             *(ptr(t) for t in out)))
     return out
 
@@ -247,7 +256,7 @@ def postprocess_batch(xs, ys, zs, summaries, dlps, workers: int = 0):
     outs = [(np.zeros(s.original_cols), np.zeros(s.original_rows), np.zeros(s.original_cols)) for s in summaries]
     sums = (capi.Summary * k)(*summaries)
     lps = (capi.Lp * k)(*[d.struct() for d in dlps])
-    dev = [_ptr_array([ptr(v[i]) if v is not None and v[i] is not None else None for i in range(k)])
+    dev = [_ptr_array([f64ptr(v[i]) if v is not None and v[i] is not None else None for i in range(k)])
            for v in (xs, ys, zs)]
     host = [_ptr_array([o[j].ctypes.data for o in outs]) for j in range(3)]
     status = np.zeros(k, np.int32)

@@ -65,3 +65,23 @@ def free_lp(lp: capi.Lp) -> None:
 def export_reduced(summary: capi.Summary, out_dir: str, model_name: str = "") -> None:
     """gpp_export_reduced: the reduced LP in the reference's export format."""
     _raise(capi.load().gpp_export_reduced(C.byref(summary), out_dir.encode(), model_name.encode()))
+
+
+def reduced_to_device(summary: capi.Summary) -> capi.Lp:
+    """gpp_reduced_to_device: a solver-owned device copy of the reduced LP
+    (A, its stable transpose, vectors); release with free_lp."""
+    lp = capi.Lp()
+    _raise(capi.load().gpp_reduced_to_device(C.byref(summary), C.byref(lp)))
+    return lp
+
+
+def reduced_to_host(summary: capi.Summary) -> dict:
+    """gpp_reduced_to_host: the reduced LP as host arrays."""
+    m, n, nnz = summary.reduced_rows, summary.reduced_cols, summary.reduced_nnz
+    out = {"row_ptr": np.zeros(m + 1, np.int32), "col_idx": np.zeros(nnz, np.int32), "val": np.zeros(nnz),
+           "c": np.zeros(n), "AL": np.zeros(m), "AU": np.zeros(m), "l": np.zeros(n), "u": np.zeros(n)}
+    obj = C.c_double()
+    _raise(capi.load().gpp_reduced_to_host(C.byref(summary), *(out[k].ctypes.data_as(C.c_void_p) for k in (
+        "row_ptr", "col_idx", "val", "c", "AL", "AU", "l", "u")), C.byref(obj)))
+    out["obj_constant"] = obj.value
+    return out

@@ -318,6 +318,25 @@ GPP_API void gpp_lp_free(gpp_lp* lp);
  * which this engine does not time separately. */
 GPP_API int gpp_export_reduced(const gpp_summary* summary, const char* out_dir, const char* model_name);
 
+/* Solver handoff of the reduced LP (the reference's HPR-LP adapter,
+ * solver_interface/adapters/gpu.cpp:354-400 and :466-500).
+ *
+ * gpp_reduced_to_device copies the reduced LP, device to device, into new
+ * arrays on the current device that the caller owns and releases with
+ * gpp_lp_free: A, its stable transpose AT (rows of AT list the rows of A in
+ * ascending order, as build_stable_device_transpose makes them), c, AL, AU,
+ * l, u and the objective constant.  It fails with GPP_ERR_INVALID when the
+ * reduced LP is empty (no rows, columns or nonzeros), where the reference's
+ * adapter reports that preprocessing failed.
+ *
+ * gpp_reduced_to_host copies the same arrays to host buffers of the sizes in
+ * the summary (row_ptr: reduced_rows + 1; col_idx, val: reduced_nnz; c, l, u:
+ * reduced_cols; AL, AU: reduced_rows); any pointer may be NULL to skip that
+ * array. */
+GPP_API int gpp_reduced_to_device(const gpp_summary* summary, gpp_lp* out);
+GPP_API int gpp_reduced_to_host(const gpp_summary* summary, gpp_offset* row_ptr, int32_t* col_idx, double* val,
+                                double* c, double* AL, double* AU, double* l, double* u, double* obj_constant);
+
 /* ---- Learned round schedule -------------------------------------------------
  * The plain phase machine (Cleanup, Propagation, Aggregation, Parallel) runs
  * one phase per round.  A schedule model may, per round, skip any of six gated

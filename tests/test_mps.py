@@ -5,7 +5,9 @@ CPU: the reference reader's known-answer cases
 the reference reader itself (built from its sources by oracle/mps_ref.mk) on
 generated files in free and fixed format and on inputs both must reject.
 GPU: the library's upload gives the same presolve as the same LP uploaded
-from numpy, and the export writes the reduced LP in the reference's format."""
+from numpy, the export writes the reduced LP in the reference's format, and
+the solver handoff (device and host copies of the reduced LP) returns the
+summary's reduced LP with a stable transpose."""
 import os
 import subprocess
 import tempfile
@@ -147,3 +149,37 @@ def test_upload_and_export_reduced(tmp_path):
         device.free_summary(s2)
     finally:
         mps.free_lp(lp_c)
+
+
+@pytest.mark.gpu
+def test_solver_handoff_device_and_host():
+    from gpp_b200 import lpgen
+    lp = lpgen.random_lp(3000, 7500, seed=5)
+    d = device.DeviceLp(lp)
+    s = device.preprocess(d, capi.Params.defaults())
+    try:
+        r = device.Result(s)
+        host = mps.reduced_to_host(s)
+        for k, key in (("row_ptr", "A_ptr"), ("col_idx", "A_idx"), ("val", "A_val"), ("c", "c"), ("AL", "AL"),
+                       ("AU", "AU"), ("l", "l"), ("u", "u")):
+            assert np.array_equal(host[k].view(np.uint8), getattr(r, key).view(np.uint8)), k
+        assert host["obj_constant"] == r.obj_constant
+        copy = mps.reduced_to_device(s)
+        try:
+            m, n, nnz = s.reduced_rows, s.reduced_cols, s.reduced_nnz
+            assert (copy.A.rows, copy.A.cols, copy.A.nnz, copy.AT.rows, copy.AT.cols) == (m, n, nnz, n, m)
+            got = {k: device._d2h(p, cnt, dt) for k, p, cnt, dt in (
+                ("A_ptr", copy.A.rowPtr, m + 1, np.int32), ("A_idx", copy.A.colVal, nnz, np.int32),
+                ("A_val", copy.A.nzVal, nnz, np.float64), ("AT_ptr", copy.AT.rowPtr, n + 1, np.int32),
+                ("AT_idx", copy.AT.colVal, nnz, np.int32), ("AT_val", copy.AT.nzVal, nnz, np.float64),
+                ("c", copy.c, n, np.float64), ("l", copy.l, n, np.float64), ("u", copy.u, n, np.float64))}
+            for k, v in got.items():
+                assert np.array_equal(v.view(np.uint8), getattr(r, k).view(np.uint8)), k
+            # The transpose is the stable one: rows of A^T list A's rows in ascending order.
+            t_ptr, t_idx, t_val = lpgen.csr_transpose(m, n, got["A_ptr"], got["A_idx"], got["A_val"])
+            assert np.array_equal(t_ptr, got["AT_ptr"]) and np.array_equal(t_idx, got["AT_idx"])
+            assert np.array_equal(t_val, got["AT_val"])
+        finally:
+            mps.free_lp(copy)
+    finally:
+        device.free_summary(s)

@@ -243,7 +243,7 @@ def test_gpu_known_answer_and_variants(variant):
         assert got == (3, 4, 6)
         r = device.Result(s)
         assert sorted(r.fixed_idx.tolist()) == [3, 5]
-        x, _, _ = device.postprocess(torch.tensor([1.0, 1.0, 1.0, 0.0], device="cuda"),
+        x, _, _ = device.postprocess(torch.tensor([1.0, 1.0, 1.0, 0.0], dtype=torch.float64, device="cuda"),
                                      torch.zeros(3, dtype=torch.float64, device="cuda"),
                                      torch.zeros(4, dtype=torch.float64, device="cuda"), s, d)
         assert np.asarray(x).tolist() == [1.0, 1.0, 1.0, 0.0, 0.0, 0.0]
