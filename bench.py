@@ -237,6 +237,7 @@ def main():
     ap.add_argument("--batch", type=int, default=512,
                     help="LPs in the batched-form measurement (0 skips it; N=1 only)")
     ap.add_argument("--batch-max-workers", type=int, default=32)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule measurement")
     ap.add_argument("--kernel-table-out", default=None,
                     help="write every kernel's launches, ms and bytes per step to this CSV file")
     ap.add_argument("--no-kernel-table", action="store_true",
@@ -395,7 +396,7 @@ def main():
     # plain run's nnz removal it keeps.
     learned = None
     from gpp_b200 import schedule
-    if rank == 0 and os.path.exists(schedule.MODEL_FILE):
+    if rank == 0 and not args.no_learned and os.path.exists(schedule.MODEL_FILE):
         w_sched, skip_below, stop_above = schedule.load_model()
         with schedule.Model(w_sched, skip_below, stop_above) as model:
             times, kept_nnz = [], None
