@@ -9,8 +9,8 @@ probability that presolve should stop.  Labels come from traces of the plain
 loop: a rule that ran is labelled by whether it changed the model; a round is
 a stop point when less than ``STOP_SHARE`` of the run's total nnz removal is
 still to come after it (half of the 2% that the 98% bar allows).  The plain
-loop stays the default and the judge: a scheduled run must keep at least 98%
-of the plain run's nnz removal.
+loop stays the default and the yardstick: a scheduled run must keep at least
+98% of the plain run's nnz removal.
 """
 from __future__ import annotations
 

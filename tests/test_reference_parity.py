@@ -3,7 +3,7 @@
 oracle/_ref/ref_driver is the reference GPU-Preprocessor library, compiled from
 its own sources by oracle/ref.mk, behind a small exporter (oracle/ref_driver.cpp).
 The test runs it and the CUDA engine on identical synthetic LPs with the same
-rule set and requires what the north star asks: the removed rows and columns,
+rule set and requires drop-in parity: the removed rows and columns,
 the row/column maps and the sparsity pattern bit-exact; coefficients, bounds
 and sides within 1e-12 relative.  Skipped when the reference build is absent
 (it needs the reference sources at build time).
