@@ -185,6 +185,39 @@ __global__ void histogram(const int32_t* __restrict__ idx, offset_t nnz, int32_t
   for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * blockDim.x)
     atomicAdd(counts + idx[p], 1);
 }
+// Longest column (the histogram's largest count), one atomic per warp.
+__global__ void longest_count(const int32_t* __restrict__ counts, int n, int32_t* __restrict__ out) {
+  int32_t best = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) best = max(best, counts[j]);
+  best = __reduce_max_sync(0xffffffffu, best);
+  if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(out, best);
+}
+// Short-column transpose: each stored position goes to a slot of its column
+// through an atomic cursor (slot order within a column is arbitrary), then
+// every column's positions are put back in ascending order, which is the
+// stored (row-major) order: the same result as the stable sort.
+constexpr int kShortColumn = 64;
+__global__ void place_positions(offset_t nnz, const int32_t* __restrict__ idx, int32_t* __restrict__ cursor,
+                                int32_t* __restrict__ pos) {
+  for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * blockDim.x)
+    pos[atomicAdd(cursor + idx[p], 1)] = int32_t(p);
+}
+__global__ void order_columns(int n, const offset_t* __restrict__ ptr, int32_t* __restrict__ pos) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const offset_t first = ptr[j];
+    const int len = int(ptr[j + 1] - first);
+    if (len < 2) continue;
+    int32_t a[kShortColumn];
+    for (int k = 0; k < len; ++k) a[k] = pos[first + k];
+    for (int k = 1; k < len; ++k) {   // insertion sort: columns hold at most kShortColumn entries
+      const int32_t v = a[k];
+      int q = k - 1;
+      while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
+      a[q + 1] = v;
+    }
+    for (int k = 0; k < len; ++k) pos[first + k] = a[k];
+  }
+}
 // Column keys and entry positions of M, in stored (row-major) order.
 __global__ void transpose_keys(offset_t nnz, const int32_t* __restrict__ idx, uint64_t* __restrict__ keys,
                                int32_t* __restrict__ pos) {
@@ -282,9 +315,10 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
 }
 
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
-  // A stable radix sort of the stored entries by column: entries of one
-  // column keep their row-major order, i.e. ascending rows (duplicates in
-  // stored order), which is the row-sorted CSR of M^T.
+  // Entries ordered by column, each column in stored (row-major) order,
+  // i.e. ascending rows (duplicates in stored order): the row-sorted CSR of
+  // M^T.  Short columns (all at most kShortColumn long) use atomic slots and
+  // a per-column sort of the positions; otherwise a stable radix sort.
   DevCsr t;
   t.rows = M.cols;
   t.cols = M.rows;
@@ -301,10 +335,21 @@ DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
   const int g = grid_stride_blocks(M.nnz);
   GPP_LAUNCH(histogram, g, kThreads, 0, s, M.idx, M.nnz, cnt.p);
   exclusive_scan_i32(cnt.p, t.ptr, t.rows, s);
-  DBuf<uint64_t> keys(size_t(M.nnz), s);
   DBuf<int32_t> pos(size_t(M.nnz), s), row(size_t(M.nnz), s);
-  GPP_LAUNCH(transpose_keys, g, kThreads, 0, s, M.nnz, M.idx, keys.p, pos.p);
-  radix_sort_pairs(keys.p, pos.p, M.nnz, s);
+  Status st;
+  st.clear(1);
+  GPP_LAUNCH(longest_count, grid_stride_blocks(t.rows), kThreads, 0, s, cnt.p, t.rows, st.d);
+  if (st.read(1)[0] <= kShortColumn) {
+    DBuf<int32_t> cursor(size_t(t.rows), s);
+    check(cudaMemcpyAsync(cursor.p, t.ptr, sizeof(int32_t) * size_t(t.rows), cudaMemcpyDeviceToDevice, s),
+          "transpose cursors");
+    GPP_LAUNCH(place_positions, g, kThreads, 0, s, M.nnz, M.idx, cursor.p, pos.p);
+    GPP_LAUNCH(order_columns, grid_stride_blocks(t.rows), kThreads, 0, s, t.rows, t.ptr, pos.p);
+  } else {
+    DBuf<uint64_t> keys(size_t(M.nnz), s);
+    GPP_LAUNCH(transpose_keys, g, kThreads, 0, s, M.nnz, M.idx, keys.p, pos.p);
+    radix_sort_pairs(keys.p, pos.p, M.nnz, s);
+  }
   GPP_LAUNCH(row_of_entry, std::max(1, std::min((M.rows + 7) / 8, kNumSMs * 16)), kThreads, 0, s, M.rows, M.ptr,
              row.p);
   GPP_LAUNCH(transpose_gather, g, kThreads, 0, s, M.nnz, pos.p, row.p, M.val, t.idx, t.val);

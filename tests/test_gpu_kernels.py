@@ -130,6 +130,17 @@ def compaction_case(name):
         keep_r = np.ones(m, np.uint8)
         keep_r[17] = 0
         return m, n, p_, i_, v_, keep_r, (rng.random(n) < 0.5).astype(np.uint8)
+    if name == "dense_columns":
+        # Five columns in every row (longer than the short-column transpose
+        # takes), the rest short: the transpose takes its sorting path.
+        m, n = 3000, 500
+        lengths = rng.integers(0, 8, size=m)
+        p0, i0, _ = sparse_rows(m, n - 5, lengths, 15)
+        rows = np.repeat(np.arange(m), np.diff(p0))
+        r = np.concatenate([rows, np.repeat(np.arange(m), 5)])
+        c = np.concatenate([i0.astype(np.int64) + 5, np.tile(np.arange(5), m)])
+        p_, i_, v_ = lpgen.coo_to_csr(m, r.astype(np.int64), c, rng.standard_normal(r.size))
+        return m, n, p_, i_, v_, (rng.random(m) < 0.9).astype(np.uint8), (rng.random(n) < 0.8).astype(np.uint8)
     if name == "nothing_left":
         # Kept rows, kept columns, but no kept entry: every new pointer is 0.
         m, n = 3000, 600
@@ -141,7 +152,7 @@ def compaction_case(name):
     raise ValueError(name)
 
 
-@pytest.mark.parametrize("case", ["random_hubs", "empty_runs", "long_rows", "nothing_left"])
+@pytest.mark.parametrize("case", ["random_hubs", "empty_runs", "long_rows", "dense_columns", "nothing_left"])
 def test_compaction_and_transpose_vs_numpy(case):
     m, n, row_ptr, col_idx, values, keep_r, keep_c = compaction_case(case)
     A, keep = dev_csr(m, n, row_ptr, col_idx, values)
