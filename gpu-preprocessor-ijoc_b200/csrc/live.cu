@@ -526,6 +526,15 @@ __global__ void inc_fix(int rows, const offset_t* __restrict__ ptr, const int32_
   }
 }
 
+// Any row or column dropped by the masks (one flag word).
+__global__ void any_dropped(const uint8_t* __restrict__ keep_row, int m, const uint8_t* __restrict__ keep_col, int n,
+                            int32_t* __restrict__ flag) {
+  bool dropped = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max(m, n); i += gridDim.x * blockDim.x)
+    dropped = dropped || (i < m && !keep_row[i]) || (i < n && !keep_col[i]);
+  if (__any_sync(0xffffffffu, dropped) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 }  // namespace
 
 void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
@@ -533,11 +542,21 @@ void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
   auto s = ctx().stream;
   const int m = lp.m(), n = lp.n();
   if (!st.valid) {
+    // A full recount normally follows a fresh plan, whose masks keep every
+    // row and column: then the counts are the stored lengths, and the sweeps
+    // run without masks (no index or mask reads), with the same results.
+    Status removed;
+    removed.clear(1);
+    GPP_LAUNCH(any_dropped, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, plan.keep_row.p, m, plan.keep_col.p,
+               n, removed.d);
+    const bool all_kept = removed.read(1)[0] == 0;
+    const uint8_t* keep_row = all_kept ? nullptr : plan.keep_row.p;
+    const uint8_t* keep_col = all_kept ? nullptr : plan.keep_col.p;
     st.live_nnz.zero();
-    live_stats_side(lp.A, plan.keep_row.p, plan.keep_col.p, st.row_nnz.p, st.empty_row.p, st.singleton_row.p,
-                    st.srow_col.p, st.srow_val.p, st.live_nnz.p, s);
-    live_stats_side(lp.AT, plan.keep_col.p, plan.keep_row.p, st.col_nnz.p, st.empty_col.p, st.singleton_col.p,
-                    st.scol_row.p, st.scol_val.p, nullptr, s);
+    live_stats_side(lp.A, keep_row, keep_col, st.row_nnz.p, st.empty_row.p, st.singleton_row.p, st.srow_col.p,
+                    st.srow_val.p, st.live_nnz.p, s);
+    live_stats_side(lp.AT, keep_col, keep_row, st.col_nnz.p, st.empty_col.p, st.singleton_col.p, st.scol_row.p,
+                    st.scol_val.p, nullptr, s);
   } else {
     st.counters.zero();
     GPP_LAUNCH(inc_deleted, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, m, n, st.seen_row.p, plan.keep_row.p,
