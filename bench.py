@@ -38,15 +38,49 @@ RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singl
          "parallel_rows", "parallel_columns", "doubleton_equations"]
 
 
-# DRAM bytes (read + write) per launch from one ncu --set full capture of the
-# full-size workload (summarised under profiles/): the mean over the captured
-# launches, which are the step's first (full-size) launches.
-MEASURED_TRAFFIC = {
-    "copy_kept": 673.1e6,
-    "activity_kernel<false>": 1312.5e6,
-    "activity_kernel<true>": 1165.2e6,
-    "candidates_entries": 1216.9e6,
+# Kernel -> the source files whose text fixes its code; a DRAM traffic
+# figure measured by ncu is used only while these files are unchanged.
+KERNEL_SOURCES = {
+    "activity_kernel<false>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
+    "activity_kernel<true>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
+    "candidates_entries": ["csrc/rules_bound.cu", "csrc/common.cuh"],
+    "copy_kept": ["csrc/compact.cu", "csrc/common.cuh"],
 }
+
+
+def source_digest(files):
+    import hashlib
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(ROOT, "gpu-preprocessor-ijoc_b200", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def measured_traffic(kernel):
+    """DRAM read + write bytes per full-size launch of `kernel` from the ncu
+    records under profiles/ (lines 'traffic-record: kernel=... digest=...
+    dram_bytes_per_launch=... file=...'), used only when the digest of the
+    kernel's sources matches the one recorded with the capture.  Returns
+    (bytes or None, the record's file or a reason)."""
+    import glob
+    files = KERNEL_SOURCES.get(kernel)
+    if not files:
+        return None, "no ncu record for this kernel"
+    digest = source_digest(files)
+    stale = None
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        for line in open(path):
+            if not line.startswith("traffic-record:"):
+                continue
+            rec = dict(kv.split("=", 1) for kv in line.split()[1:])
+            if rec.get("kernel") != kernel:
+                continue
+            if rec.get("digest") == digest:
+                return float(rec["dram_bytes_per_launch"]), os.path.relpath(path, ROOT)
+            stale = os.path.relpath(path, ROOT)
+    return None, (f"ncu record {stale} predates the kernel's current sources" if stale
+                  else "no ncu record for this kernel")
 
 
 def peaks():
@@ -120,13 +154,34 @@ def make_batch_lp(job):
     return lp
 
 
-def run_batched(lps, params, max_workers):
-    """Batched form against looping the plain form over the same LPs, inputs resident on the GPU.
+LEARNED_SEEDS = (1, 2, 3)
 
-    Returns the JSON object of the batched measurement."""
+
+def make_scale_lp(job):
+    """One draw of a named workload (runs in a spawned worker process)."""
+    from gpp_b200 import lpgen
+    name, seed = job
+    return lpgen.workload(name, seed=seed)
+
+
+def batch_nnz_estimate(job):
+    """Expected nnz of one batched-workload LP (n = 2.5 m columns of 1 +
+    Poisson(4) entries): the weight of the greedy partition across ranks,
+    known before any LP is generated."""
+    m, _ = job
+    return int(12.5 * m)
+
+
+def run_batched(indices, lps, params, max_workers, rank=0, world=1, group=None):
+    """Batched form against looping the plain form over the same LPs, inputs
+    resident on the GPU.  With world > 1 every rank runs its share (`indices`,
+    `lps`) of the batch on its own GPU; the per-LP records are gathered to
+    rank 0 over `group` (gloo) and the times are the max over ranks.
+
+    Returns the JSON object of the batched measurement on rank 0."""
     import numpy as np
     import torch
-    from gpp_b200 import device
+    from gpp_b200 import capi, device, shard
     dlps = [device.DeviceLp(lp) for lp in lps]
     torch.cuda.synchronize()
 
@@ -139,11 +194,17 @@ def run_batched(lps, params, max_workers):
         return (s.reduced_rows, s.reduced_cols, s.reduced_nnz, s.iterations, s.has_infeasible, s.has_unbounded,
                 s.obj_constant_delta)
 
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier(group=group)
+        torch.cuda.synchronize()
+
     # Looping the plain form: presolve + postsolve of one LP after another.
-    from gpp_b200 import capi
     lib = capi.load()
     lib.gpp_kernel_launches(1)
     lib.gpp_host_syncs(1)
+    barrier()
     t0 = time.perf_counter()
     plain_keys, plain_lat = [], []
     for d in dlps:
@@ -154,33 +215,53 @@ def run_batched(lps, params, max_workers):
         device.free_summary(s)
     torch.cuda.synchronize()
     t_loop = time.perf_counter() - t0
-    per_lp = {"launches": round(lib.gpp_kernel_launches(0) / len(dlps), 1),
-              "host_syncs": round(lib.gpp_host_syncs(0) / len(dlps), 1)}
+    launches, syncs = lib.gpp_kernel_launches(0), lib.gpp_host_syncs(0)
 
-    workers, curve = device.batch_autotune(dlps, params, max_workers=max_workers)
-    torch.cuda.synchronize()
+    workers, curve = device.batch_autotune(dlps, params, max_workers=max_workers) if dlps else (1, {})
+    barrier()
     t0 = time.perf_counter()
-    sums, _ = device.preprocess_batch(dlps, params, workers=workers)
-    reds = [zeros(s) for s in sums]
-    device.postprocess_batch([r[0] for r in reds], [r[1] for r in reds], [r[2] for r in reds], sums, dlps,
-                             workers=workers)
+    sums = []
+    if dlps:
+        sums, _ = device.preprocess_batch(dlps, params, workers=workers)
+        reds = [zeros(s) for s in sums]
+        device.postprocess_batch([r[0] for r in reds], [r[1] for r in reds], [r[2] for r in reds], sums, dlps,
+                                 workers=workers)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
-    match = sum(key(s) == k for s, k in zip(sums, plain_keys))
-    lat = [s.preprocessing_seconds for s in sums]
+    records = {k: {"match": key(s) == pk, "lat": s.preprocessing_seconds, "plain_lat": pl, "nnz": lp.nnz}
+               for k, s, pk, pl, lp in zip(indices, sums, plain_keys, plain_lat, lps)}
     for s in sums:
         device.free_summary(s)
-    nnz = sum(lp.nnz for lp in lps)
+    times = [t_loop, t_batch, float(launches), float(syncs)]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor(times[:2], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+        c = torch.tensor(times[2:], dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM, group=group)
+        times = t.tolist() + c.tolist()
+    recs = shard.gather_records(records, rank, world, group)
+    if rank != 0:
+        return None
+    t_loop, t_batch, launches, syncs = times
+    count = len(recs)
+    lat = [r["lat"] for r in recs]
+    plain_lat = [r["plain_lat"] for r in recs]
+    match = sum(r["match"] for r in recs)
     pct = lambda v, q: round(1e3 * float(np.percentile(v, q)), 3)
-    return {"lps": len(lps), "nnz_total": int(nnz), "workload": BATCH_DESC, "workers": workers,
-            "autotune_sample_lps_per_s": curve, "looped_per_lp": per_lp,
-            "lps_per_s": round(len(lps) / t_batch, 2), "looped_lps_per_s": round(len(lps) / t_loop, 2),
+    return {"lps": count, "nnz_total": int(sum(r["nnz"] for r in recs)), "workload": BATCH_DESC,
+            "workers": workers, "autotune_sample_lps_per_s": curve,
+            "looped_per_lp": {"launches": round(launches / count, 1), "host_syncs": round(syncs / count, 1)},
+            "lps_per_s": round(count / t_batch, 2), "looped_lps_per_s": round(count / t_loop, 2),
             "speedup_vs_looped": round(t_loop / t_batch, 2), "batch_s": round(t_batch, 3),
             "looped_s": round(t_loop, 3),
             "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "looped_p50": pct(plain_lat, 50),
                            "looped_p99": pct(plain_lat, 99),
                            "definition": "per-LP presolve wall time (preprocessing_seconds) inside each run"},
-            "match_plain": f"{match}/{len(lps)}",
+            "match_plain": f"{match}/{count}",
+            "sharding": ("one GPU" if world == 1 else
+                         f"{world} ranks, greedy expected-nnz partition, no device collective; per-LP records "
+                         f"gathered on the host (gloo); times are the max over ranks"),
             "timing": "wall clock around presolve + postsolve of all LPs, device inputs resident, "
                       "reduced solutions all-zero"}
 
@@ -235,14 +316,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) loop")
     ap.add_argument("--batch", type=int, default=512,
-                    help="LPs in the batched-form measurement (0 skips it; N=1 only)")
+                    help="LPs in the batched-form measurement (0 skips it); sharded over the ranks when N > 1")
     ap.add_argument("--batch-max-workers", type=int, default=32)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule measurement")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference GPU library on the same LP")
     ap.add_argument("--kernel-table-out", default=None,
                     help="write every kernel's launches, ms and bytes per step to this CSV file")
     ap.add_argument("--no-kernel-table", action="store_true",
                     help="skip the extra pass that times every kernel with CUDA events")
+    ap.add_argument("--source-digests", action="store_true",
+                    help="print the source digest of every kernel that has ncu traffic records, then exit")
     args = ap.parse_args()
+    if args.source_digests:
+        for k, files in KERNEL_SOURCES.items():
+            print(k, source_digest(files))
+        return
     world, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -290,12 +379,18 @@ def main():
     out = (torch.empty(lp.n, dtype=torch.float64, device="cuda"), torch.empty(lp.m, dtype=torch.float64, device="cuda"),
            torch.empty(lp.n, dtype=torch.float64, device="cuda"))
 
+    post_events = []
+
     def device_steps(k):
         pre = []
         for _ in range(k):
             s = device.preprocess(dlp, params)
             pre.append(1e3 * s.elapsed_seconds)
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record(stream)
             device.postsolve_device(*red, s, dlp, out)
+            ev[1].record(stream)
+            post_events.append(ev)
             device.free_summary(s)
         return pre
 
@@ -310,6 +405,7 @@ def main():
     barrier()
     clk = clocks.stop()
     step_ms = t0.elapsed_time(t1) / args.steps
+    post_ms = statistics.mean(a.elapsed_time(b) for a, b in post_events)
     launches = int(lib.gpp_kernel_launches(0)) // args.steps
     syncs = int(lib.gpp_host_syncs(0)) // args.steps
     # Per-kernel table for the roofline: the same steps again with every
@@ -352,11 +448,23 @@ def main():
     # The batched workload is generated by spawned processes (after the timed
     # loops, so they do not compete with them for host cores; they overlap the
     # single-core CPU baseline instead).
-    batch_pool = batch_result = None
-    if args.batch > 0 and world == 1:
+    learned_pool = learned_result = None
+    from gpp_b200 import schedule as _schedule
+    if rank == 0 and not args.no_learned and os.path.exists(_schedule.MODEL_FILE):
         import multiprocessing as mp
-        batch_pool = mp.get_context("spawn").Pool(max(1, min(32, (os.cpu_count() or 2) - 2)))
-        batch_result = batch_pool.map_async(make_batch_lp, batch_jobs(args.batch), chunksize=1)
+        learned_pool = mp.get_context("spawn").Pool(len(LEARNED_SEEDS))
+        learned_result = learned_pool.map_async(make_scale_lp, [(args.workload, sd) for sd in LEARNED_SEEDS],
+                                                chunksize=1)
+    batch_pool = batch_result = None
+    batch_mine = []
+    if args.batch > 0:
+        import multiprocessing as mp
+        from gpp_b200 import shard
+        jobs = batch_jobs(args.batch)
+        batch_mine = shard.greedy_nnz_partition([batch_nnz_estimate(j) for j in jobs], world)[rank]
+        procs = max(1, min(32, ((os.cpu_count() or 2) - 2) // world))
+        batch_pool = mp.get_context("spawn").Pool(procs)
+        batch_result = batch_pool.map_async(make_batch_lp, [jobs[k] for k in batch_mine], chunksize=1)
 
     if world > 1:
         t = torch.tensor([step_ms, e2e_ms or 0.0], device="cuda")
@@ -376,9 +484,25 @@ def main():
             roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                         "launches_per_step": nl // args.steps, "avg_launch_us": round(1e3 * ms / nl, 2),
-                        "bytes_per_launch": int(by / nl),
-                        "traffic": MEASURED_TRAFFIC.get(name)}
+                        "bytes_per_launch": int(by / nl)}
+            traffic, source = measured_traffic(name)
+            roofline["traffic"] = traffic
+            roofline["traffic_source"] = source
     kernels = sorted((r for r in prof if not r[0].startswith("sync:")), key=lambda r: -r[2])[:8]
+    # End-to-end algorithmic bandwidth: every launch's algorithmic bytes in
+    # one step over the step's device time.
+    step_bytes = sum(r[3] for r in prof) / args.steps if prof else 0
+    algorithmic = None
+    if prof:
+        algorithmic = {"bytes_per_step": int(step_bytes),
+                       "gbs_per_step": round(step_bytes / 1e9 / (step_ms / 1e3), 1),
+                       "frac_of_peak": round(step_bytes / 1e9 / (step_ms / 1e3) / peak, 4),
+                       "kernel_ms_per_step": round(sum(r[2] for r in prof if not r[0].startswith("sync:"))
+                                                   / args.steps, 3)}
+    ref_gpu = None
+    if rank == 0 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu(lp, [t.cpu().numpy() for t in red], args.steps, max(args.warmup, 3),
+                                statistics.mean(pre_ms), post_ms)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         driver = os.path.join(ROOT, "oracle", "_ref", "pslp_driver")
@@ -391,32 +515,61 @@ def main():
             if wall:
                 cpu = {"value": round(1e3 * wall[0], 1), "unit": "ms", "cores": 1, "kind": "reference",
                        "sample": f"one PSLP 0.0.11 presolve of the full workload ({WORKLOAD_DESC}) on 1 host core"}
-    # Learned round schedule on the same LP (held out: the schedule is trained
-    # on LPs of at most 500,000 rows): presolve time and the share of the
-    # plain run's nnz removal it keeps.
+    # Learned round schedule on held-out draws of the scale workload (the
+    # schedule is trained on LPs of at most 500,000 rows; seeds 1-3 here, the
+    # timed LP above is seed 0): presolve time against the plain loop on the
+    # same LP, and the share of the plain run's nnz removal it keeps.
     learned = None
-    from gpp_b200 import schedule
-    if rank == 0 and not args.no_learned and os.path.exists(schedule.MODEL_FILE):
-        w_sched, skip_below, stop_above = schedule.load_model()
+    if learned_result is not None:
+        from gpp_b200 import schedule
+        try:
+            w_sched, skip_below, stop_above = schedule.load_model()
+        except ValueError as e:   # a model trained for another feature layout
+            learned = {"unavailable": str(e)}
+            learned_result = None
+            learned_pool.terminate()
+    if learned_result is not None:
+        reps = max(3, min(args.steps, 5))
+        per_lp = []
         with schedule.Model(w_sched, skip_below, stop_above) as model:
-            times, kept_nnz = [], None
-            for it in range(max(args.warmup, 3) + args.steps):
-                s = schedule.scheduled_preprocess(dlp, params, model)
-                if it >= max(args.warmup, 3):
-                    times.append(1e3 * s.elapsed_seconds)
-                kept_nnz = s.reduced_nnz
-                device.free_summary(s)
-        plain_ms = statistics.mean(pre_ms)
-        removed_plain = lp.nnz - reduced[2]
-        learned = {"presolve_ms": round(statistics.mean(times), 3), "plain_presolve_ms": round(plain_ms, 3),
-                   "time_ratio": round(statistics.mean(times) / plain_ms, 4),
-                   "nnz_removal_kept": round((lp.nnz - kept_nnz) / removed_plain, 5) if removed_plain else 1.0,
+            for seed, hlp in zip(LEARNED_SEEDS, learned_result.get()):
+                hd = device.DeviceLp(hlp)
+                run = lambda: device.preprocess(hd, params)
+                sched = lambda: schedule.scheduled_preprocess(hd, params, model)
+                res = {}
+                for kind, fn in (("plain", run), ("scheduled", sched)):
+                    times = []
+                    for it in range(2 + reps):
+                        s = fn()
+                        if it >= 2:
+                            times.append(1e3 * s.elapsed_seconds)
+                        res[kind] = (s.reduced_nnz, s.iterations)
+                        device.free_summary(s)
+                    res[kind + "_ms"] = statistics.mean(times)
+                removed_plain = hlp.nnz - res["plain"][0]
+                per_lp.append({"seed": seed, "nnz": hlp.nnz, "plain_presolve_ms": round(res["plain_ms"], 3),
+                               "presolve_ms": round(res["scheduled_ms"], 3),
+                               "time_ratio": round(res["scheduled_ms"] / res["plain_ms"], 4),
+                               "rounds": res["scheduled"][1], "plain_rounds": res["plain"][1],
+                               "nnz_removal_kept": round((hlp.nnz - res["scheduled"][0]) / removed_plain, 5)
+                               if removed_plain else 1.0})
+                del hd, hlp
+        ratios = [r["time_ratio"] for r in per_lp]
+        kept = [r["nnz_removal_kept"] for r in per_lp]
+        learned = {"time_ratio_mean": round(statistics.mean(ratios), 4), "time_ratio_max": max(ratios),
+                   "speedup_mean": round(1.0 / statistics.mean(ratios), 3),
+                   "nnz_removal_kept_min": min(kept), "held_out": per_lp,
                    "skip_below": skip_below, "stop_above": stop_above,
+                   "workload": "held-out draws of the scale workload (seeds %s)" % LEARNED_SEEDS,
+                   "timing": f"presolve elapsed_seconds, mean of {reps} runs after 2 warm-up, per LP",
                    "model": "2x64 FP32 MLP, trained on plain-loop traces"}
+        learned_pool.close()
+        learned_pool.join()
 
     batched = None
     if batch_result is not None:
-        batched = run_batched(batch_result.get(), params, args.batch_max_workers)
+        gloo = dist.new_group(backend="gloo") if world > 1 else None
+        batched = run_batched(batch_mine, batch_result.get(), params, args.batch_max_workers, rank, world, gloo)
         batch_pool.close()
         batch_pool.join()
     if rank == 0:
@@ -428,6 +581,7 @@ def main():
                        "rules": RULES, "folding": True, "folding_applied": bool(folded),
                        "reduced": {"rows": reduced[0], "cols": reduced[1], "nnz": reduced[2], "iterations": reduced[3]},
                        "presolve_ms": round(statistics.mean(pre_ms), 3),
+                       "postsolve_ms": round(post_ms, 3),
                        "l2": "inputs (~1 GB) larger than L2; no flush",
                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "gpu_launches": launches,
@@ -435,6 +589,8 @@ def main():
             "e2e": None if e2e_ms is None else {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
                                                 "d2h_bytes_per_step": d2h},
             "roofline": roofline,
+            "algorithmic": algorithmic,
+            "reference_gpu": ref_gpu,
             "kernels": [{"name": n, "launches_per_step": l // args.steps, "ms_per_step": round(m / args.steps, 3)}
                         for n, l, m, b in kernels],
             "cpu_baseline": cpu,

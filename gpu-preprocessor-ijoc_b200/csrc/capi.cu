@@ -456,11 +456,9 @@ int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t* indice
   });
 }
 
-int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32_t* col_color, double* row_scale,
-                           double* col_scale) {
-  return guarded([&] {
-    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
-    const gpp::FoldingResult& f = summary->record->folding;
+namespace {
+void export_map(const gpp::FoldingResult& f, int32_t* row_color, int32_t* col_color, double* row_scale,
+                double* col_scale) {
     if (!f.applied) return;
     auto s = gpp::ctx().stream;
     const size_t m = size_t(f.original_rows), n = size_t(f.original_cols);
@@ -469,7 +467,73 @@ int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32
     if (row_scale && m) check(cudaMemcpyAsync(row_scale, f.row_scale.p, 8 * m, cudaMemcpyDeviceToHost, s), "fold map");
     if (col_scale && n) check(cudaMemcpyAsync(col_scale, f.col_scale.p, 8 * n, cudaMemcpyDeviceToHost, s), "fold map");
     gpp::ctx().sync("export folding map");
+}
+
+const gpp::FoldingResult& run_result(const gpp_folding_run* run) {
+  static const gpp::FoldingResult none{};
+  if (!run) throw std::invalid_argument("null folding run");
+  return run->handle ? *static_cast<const gpp::FoldingResult*>(run->handle) : none;
+}
+}  // namespace
+
+int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32_t* col_color, double* row_scale,
+                           double* col_scale) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    export_map(summary->record->folding, row_color, col_color, row_scale, col_scale);
   });
+}
+
+int gpp_folding_run_export_map(const gpp_folding_run* run, int32_t* row_color, int32_t* col_color,
+                               double* row_scale, double* col_scale) {
+  return guarded([&] { export_map(run_result(run), row_color, col_color, row_scale, col_scale); });
+}
+
+int gpp_folding_run_unfold(const gpp_folding_run* run, const double* x_folded, const double* y_folded,
+                           const double* z_folded, double* x_out, double* y_out, double* z_out) {
+  return guarded([&] {
+    const gpp::FoldingResult& f = run_result(run);
+    if (!f.applied) throw std::invalid_argument("folding did not apply to this model");
+    gpp::unfold_to_host(f, x_folded, y_folded, z_folded, x_out, y_out, z_out);
+  });
+}
+
+int gpp_run_folding(const gpp_lp* lp, double tolerance, gpp_folding_run* out) {
+  return guarded([&] {
+    if (!lp || !out) throw std::invalid_argument("gpp_run_folding: null argument");
+    *out = gpp_folding_run{};
+    auto res = std::make_unique<gpp::FoldingResult>();
+    out->original_rows = out->folded_rows = lp->A.rows;
+    out->original_cols = out->folded_cols = lp->A.cols;
+    const auto t0 = std::chrono::steady_clock::now();
+    gpp::run_folding(*lp, tolerance, *res);
+    gpp::ctx().sync("run_folding");
+    out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (!res->applied) return;
+    out->applied = 1;
+    out->folded_rows = res->folded_rows;
+    out->folded_cols = res->folded_cols;
+    out->folded_lp = res->folded;
+    out->owns_folded_lp = 1;
+    out->row_color_id = res->row_color.p;
+    out->col_color_id = res->col_color.p;
+    out->row_scale = res->row_scale.p;
+    out->col_scale = res->col_scale.p;
+    out->handle = res.release();
+  });
+}
+
+void gpp_free_folding_run(gpp_folding_run* run) {
+  if (!run) return;
+  auto* res = static_cast<gpp::FoldingResult*>(run->handle);
+  if (res) {
+    try {
+      gpp::free_folding(*res);
+    } catch (...) {
+    }
+    delete res;
+  }
+  *run = gpp_folding_run{};
 }
 
 int gpp_unfold_solution(const gpp_summary* summary, const double* x_folded, const double* y_folded,
@@ -587,6 +651,8 @@ int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n) {
 int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, void* stream) {
   return guarded([&] { gpp::radix_sort_pairs_static(keys, values, n, static_cast<cudaStream_t>(stream)); });
 }
+
+void gpp_inject_alloc_failure(int64_t after) { gpp::inject_alloc_failure(after); }
 
 int gpp_device_alloc(void** ptr, size_t bytes) {
   return guarded([&] {

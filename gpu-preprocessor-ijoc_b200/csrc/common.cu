@@ -1,6 +1,8 @@
 // Engine context, status block, scans and the canonical deterministic sum.
 #include "common.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 #include <chrono>
 #include <string>
@@ -67,9 +69,27 @@ Context& ctx() {
   return *(*per_device)[size_t(dev)];
 }
 
+namespace {
+std::atomic<int64_t> g_alloc_countdown{-1};   // < 0: no failure armed
+}  // namespace
+
+void inject_alloc_failure(int64_t after) { g_alloc_countdown.store(after < 0 ? -1 : after); }
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  if (g_alloc_countdown.load(std::memory_order_relaxed) >= 0) {
+    int64_t left = g_alloc_countdown.load();
+    while (left >= 0 && !g_alloc_countdown.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 0) {
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+  }
+  return cudaMallocFromPoolAsync(p, bytes, ctx().pool, s);
+}
+
 Status::Status() {
-  check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().pool,
-                                ctx().stream),
+  check(pool_alloc(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().stream),
         "status alloc");
 }
 Status::~Status() { if (d) cudaFreeAsync(d, ctx().stream); }

@@ -90,6 +90,41 @@ __device__ __forceinline__ bool removed_column(double2 b) {
   return static_cast<unsigned long long>(__double_as_longlong(b.x)) == kRemovedColumnBits;
 }
 
+// L2 residency hints for the row sweeps over A (activity summary, bound
+// candidates).  Each stored entry gathers the 16-byte bound record of its
+// column; a column's record is gathered once per entry of the column (about
+// six times on the random family), while the CSR arrays are read exactly
+// once.  At 25M nnz the records are 80 MB and the streamed CSR 360 MB, so
+// with plain loads the stream pushes the records out of the 126 MB L2 and
+// most gathers go to DRAM as 32-byte sectors.  Gathers therefore carry an
+// L2 evict_last policy and streamed loads an evict_first policy that also
+// skips L1 (PTX createpolicy + ld.global.nc.L2::cache_hint).  The hints only
+// order evictions; the loaded values are the same.
+struct L2Hints {
+  uint64_t keep, stream;
+};
+__device__ __forceinline__ L2Hints l2_hints() {
+  L2Hints h;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(h.keep));
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(h.stream));
+  return h;
+}
+__device__ __forceinline__ double2 ld_keep(const double2* a, uint64_t pol) {
+  double2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_stream(const int32_t* a, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* a, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+
 // Order-free max / min of doubles as single 64-bit integer reductions (RED,
 // no value returned, nothing for the thread to wait on).  A double whose sign
 // bit is clear orders like its bits read as a signed integer; one whose sign
@@ -181,6 +216,13 @@ struct Context {
 };
 Context& ctx();
 
+// Every engine device allocation: stream-ordered from the context's pool.
+// A test hook (gpp_inject_alloc_failure) can make the k-th allocation after
+// it was armed return cudaErrorMemoryAllocation instead, a host-side fake of
+// an out-of-memory failure that touches no device state.
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
+void inject_alloc_failure(int64_t after);
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -192,8 +234,7 @@ struct DBuf {
     release();
     s = stream ? stream : ctx().stream;
     n = count;
-    if (count) check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().pool, s),
-                     "cudaMallocFromPoolAsync");
+    if (count) check(pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), s), "cudaMallocFromPoolAsync");
   }
   void release() {
     if (p) cudaFreeAsync(p, s);
@@ -232,8 +273,7 @@ template <class T>
 T* dalloc(size_t count) {
   T* p = nullptr;
   if (count)
-    check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().pool, ctx().stream),
-          "cudaMallocFromPoolAsync");
+    check(pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), ctx().stream), "cudaMallocFromPoolAsync");
   return p;
 }
 inline void dfree(void* p) {

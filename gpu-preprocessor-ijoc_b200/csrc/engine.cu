@@ -49,6 +49,7 @@ struct Engine {
   bool stats_dirty = true;
   DBuf<uint8_t> entry_cols;
   DBuf<double> ref_bounds;
+  uint32_t* inf_hist = nullptr;   // histogram features (scheduled runs only)
   uint64_t deletion_serial = 0;
   Status status;
 
@@ -67,11 +68,13 @@ struct Engine {
     pl.u.alloc(size_t(n), s()); pl.u.copy_from(cur.u, size_t(n));
     pl.AL.alloc(size_t(m), s()); pl.AL.copy_from(cur.AL, size_t(m));
     pl.AU.alloc(size_t(m), s()); pl.AU.copy_from(cur.AU, size_t(m));
+    pl.all_kept = true;
   }
   void prepare() {
     if (active) return;
     plan = Plan{};
     init_plan(plan);
+    plan.inf_hist = inf_hist;
     allocate_stats(stats, cur.m(), cur.n());
     entry_cols.alloc(size_t(cur.n()), s());
     stats_dirty = true;
@@ -99,6 +102,7 @@ struct Engine {
     plan.has_change = plan.has_row_action = plan.has_col_action = false;
     plan.has_redundant_row_deletion = plan.has_row_deletion = false;
     plan.obj_delta = 0.0;
+    plan.all_kept = false;
     rule();
     out.has_infeasible = plan.has_infeasible;
     out.has_unbounded = plan.has_unbounded;
@@ -332,6 +336,13 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
   int last_ran[kGatedRules];
   for (int& r : last_ran) r = -1;
   const bool scheduled = policy || trace;
+  DBuf<uint32_t> inf_hist;
+  if (scheduled) {
+    inf_hist.alloc(8, ctx().stream);
+    inf_hist.zero();
+    e.inf_hist = inf_hist.p;
+    if (e.active) e.plan.inf_hist = inf_hist.p;
+  }
   while (p.max_iters > 0 && !e.terminal && !time_exceeded()) {
     if (phase != Cleanup) {
       if (out.iterations >= p.max_iters) { out.stopped_at_iteration_limit = true; break; }
@@ -355,6 +366,11 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       f[21] = float(std::log10(double(initial_nnz_all)) / 8.0);
       f[22] = float(1.0 - double(before) / double(initial_nnz_all));
       f[23] = float(double(cur.m()) / double(initial_rows));
+      const std::vector<uint32_t> h = to_host(inf_hist.p, 8);
+      for (int side = 0; side < 2; ++side) {
+        const double rows = double(h[4 * side] + h[4 * side + 1] + h[4 * side + 2] + h[4 * side + 3]);
+        for (int k = 0; k < 4; ++k) f[24 + 4 * side + k] = rows > 0 ? float(double(h[4 * side + k]) / rows) : 0.0f;
+      }
       rec.phase = int32_t(phase);
       rec.iteration = out.iterations;
       rec.nnz_before = before;

@@ -74,6 +74,13 @@ struct Plan {
   bool has_change = false, has_row_action = false, has_col_action = false;
   bool has_redundant_row_deletion = false, has_row_deletion = false;
   bool has_infeasible = false, has_unbounded = false;
+  // True from a fresh plan (both masks all ones) until the first rule runs
+  // on it: a full recount of the live statistics then needs no mask reads.
+  bool all_kept = false;
+  // When set (scheduled and traced runs), bound strengthening bins the live
+  // rows of its activity summary by infinite-term count here: words 0-3 the
+  // rows with 0, 1, 2, >= 3 in the minimum activity, 4-7 the maximum.
+  uint32_t* inf_hist = nullptr;
   const uint8_t* rule_entry_keep_col = nullptr;
   const double* ref_l = nullptr;
   const double* ref_u = nullptr;

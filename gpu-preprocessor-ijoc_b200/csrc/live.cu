@@ -71,9 +71,10 @@ struct ActivityTerm {
   const double* val;
   const double2* lu;
   double zero_tol;
+  L2Hints hint;
   // The term of live stored entry p whose column bounds are b.
   __device__ __forceinline__ void operator()(offset_t p, double2 b, double& lo, double& hi, int& ni, int& pi) const {
-    const double a = __ldcs(val + p);   // streamed once: keep L2 for the gathered bounds
+    const double a = ld_stream(val + p, hint.stream);   // streamed once: keep L2 for the gathered bounds
     if constexpr (Plain) {
       // Plain sums of the redundant-row test: infinities propagate.
       lo += a >= 0.0 ? a * b.x : a * b.y;
@@ -86,7 +87,9 @@ struct ActivityTerm {
     if (isfinite(tlo)) lo += tlo; else if (tlo < 0.0) ++ni;
     if (isfinite(thi)) hi += thi; else if (thi > 0.0) ++pi;
   }
-  __device__ __forceinline__ double2 bounds(offset_t p) const { return lu[__ldcs(idx + p)]; }
+  __device__ __forceinline__ double2 bounds(offset_t p) const {
+    return ld_keep(lu + ld_stream(idx + p, hint.stream), hint.keep);
+  }
 };
 
 template <bool Plain>
@@ -102,7 +105,7 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   __shared__ int warp_counts[8];
   __shared__ double dagg[8];
   __shared__ int iagg[8];
-  const ActivityTerm<Plain> term{idx, val, lu, zero_tol};
+  const ActivityTerm<Plain> term{idx, val, lu, zero_tol, l2_hints()};
   const auto live_at = [&](offset_t p) { return !removed_column(term.bounds(p)); };
   const int b = blockIdx.x;
   if (b < short_blocks) {
@@ -526,15 +529,6 @@ __global__ void inc_fix(int rows, const offset_t* __restrict__ ptr, const int32_
   }
 }
 
-// Any row or column dropped by the masks (one flag word).
-__global__ void any_dropped(const uint8_t* __restrict__ keep_row, int m, const uint8_t* __restrict__ keep_col, int n,
-                            int32_t* __restrict__ flag) {
-  bool dropped = false;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max(m, n); i += gridDim.x * blockDim.x)
-    dropped = dropped || (i < m && !keep_row[i]) || (i < n && !keep_col[i]);
-  if (__any_sync(0xffffffffu, dropped) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
-}
-
 }  // namespace
 
 void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
@@ -543,15 +537,11 @@ void refresh_stats(Stats& st, const WorkingLp& lp, const Plan& plan) {
   const int m = lp.m(), n = lp.n();
   if (!st.valid) {
     // A full recount normally follows a fresh plan, whose masks keep every
-    // row and column: then the counts are the stored lengths, and the sweeps
-    // run without masks (no index or mask reads), with the same results.
-    Status removed;
-    removed.clear(1);
-    GPP_LAUNCH(any_dropped, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, plan.keep_row.p, m, plan.keep_col.p,
-               n, removed.d);
-    const bool all_kept = removed.read(1)[0] == 0;
-    const uint8_t* keep_row = all_kept ? nullptr : plan.keep_row.p;
-    const uint8_t* keep_col = all_kept ? nullptr : plan.keep_col.p;
+    // row and column (the host knows: Plan::all_kept): then the counts are
+    // the stored lengths, and the sweeps run without masks (no index or mask
+    // reads), with the same results.
+    const uint8_t* keep_row = plan.all_kept ? nullptr : plan.keep_row.p;
+    const uint8_t* keep_col = plan.all_kept ? nullptr : plan.keep_col.p;
     st.live_nnz.zero();
     live_stats_side(lp.A, keep_row, keep_col, st.row_nnz.p, st.empty_row.p, st.singleton_row.p, st.srow_col.p,
                     st.srow_val.p, st.live_nnz.p, s);

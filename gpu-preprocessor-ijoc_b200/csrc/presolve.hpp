@@ -35,7 +35,7 @@ enum GatedRule : int {
   kGateParallelColumns = 5,
   kGatedRules = 6
 };
-constexpr int kScheduleFeatures = 24;
+constexpr int kScheduleFeatures = 32;
 
 // What the host knows at the start of a round, normalised to about [0, 1]:
 //  0-3   phase one-hot (Cleanup, Propagation, Aggregation, Parallel)
@@ -48,6 +48,10 @@ constexpr int kScheduleFeatures = 24;
 //  21    log10(initial nnz) / 8
 //  22    share of the initial nnz removed so far
 //  23    kept rows / initial rows (as of the last materialisation)
+//  24-27 share of the live rows whose latest activity summary (the last
+//        bound-strengthening sweep) counts 0, 1, 2 or >= 3 infinite terms
+//        in the minimum activity; all zero before the first sweep
+//  28-31 the same for the maximum activity
 struct RoundRecord {
   int32_t phase = 0;          // 0 Cleanup, 1 Propagation, 2 Aggregation, 3 Parallel
   int32_t iteration = 0;

@@ -68,11 +68,11 @@ __device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
   return RowCtx{g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i]};
 }
 
-__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p) {
-  const int j = __ldcs(g.idx + p);   // CSR streamed once: keep L2 for the gathered bounds
-  const double2 b = g.lu[j];
+__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p, const L2Hints& h) {
+  const int j = ld_stream(g.idx + p, h.stream);   // CSR streamed once: keep L2 for the gathered bounds
+  const double2 b = ld_keep(g.lu + j, h.keep);
   if (removed_column(b)) return;
-  const double a = __ldcs(g.val + p);
+  const double a = ld_stream(g.val + p, h.stream);
   if (fabs(a) <= g.zero_tol) return;
   const double ol = b.x, ou = b.y;
   double il, iu;
@@ -94,6 +94,7 @@ constexpr int kTileRows = 2048;
 __global__ void __launch_bounds__(kThreads)
 candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g) {
   __shared__ offset_t sptr[kTileRows + 1];
+  const L2Hints hint = l2_hints();
   for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
     const offset_t last = min(nnz, base + kEntryTile) - 1;
     const int2 span = tile_rows[base / kEntryTile];   // rows of the tile's first and last entry
@@ -107,7 +108,7 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
       if (p > last) break;
       const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
       if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-      candidate_entry(g, row_ctx(g, i), p);
+      candidate_entry(g, row_ctx(g, i), p, hint);
     }
     __syncthreads();
   }
@@ -301,6 +302,22 @@ __global__ void fixed_record_pack(int n, const uint8_t* __restrict__ fx, const o
   }
 }
 
+// Live rows binned by infinite-term count of their minimum and maximum
+// activity (0, 1, 2, >= 3): the learned schedule's histogram features.
+__global__ void inf_histogram(int m, const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ ni,
+                              const int32_t* __restrict__ pi, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t bins[8];
+  if (threadIdx.x < 8) bins[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    if (!keep_row[i]) continue;
+    atomicAdd(&bins[min(ni[i], 3)], 1u);
+    atomicAdd(&bins[4 + min(pi[i], 3)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && bins[threadIdx.x]) atomicAdd(hist + threadIdx.x, bins[threadIdx.x]);
+}
+
 }  // namespace
 
 void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p) {
@@ -319,6 +336,10 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
   pack_bounds(plan.l.p, plan.u.p, plan.keep_col.p, n, lu.p, s);
   row_activity_summary_packed(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p, s);
   const RowSummary rs{mn.p, mx.p, ni.p, pi.p};
+  if (plan.inf_hist) {
+    check(cudaMemsetAsync(plan.inf_hist, 0, 8 * sizeof(uint32_t), s), "inf_hist");
+    GPP_LAUNCH(inf_histogram, grid_stride_blocks(m), kThreads, 0, s, m, plan.keep_row.p, ni.p, pi.p, plan.inf_hist);
+  }
   {
     CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, stats.row_nnz.p, plan.AL.p, plan.AU.p, lu.p, rs,
                p.zero_tol, cl.p, cu.p};

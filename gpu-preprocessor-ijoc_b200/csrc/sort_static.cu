@@ -20,6 +20,16 @@
 // (different streams, or different host threads without ordering between
 // them) race on it and give wrong results.  Nothing in the array has to start
 // at zero: each pass writes every count it later reads.
+//
+// Set-up.  CUDA loads a library's device code lazily, so the first call on a
+// device loads this module, and with it the fixed array: that load is the one
+// device allocation this entry point ever causes.  The same first call looks
+// up the array's device address (cudaGetSymbolAddress) with the device
+// current and keeps it for the rest of the process.  Any call does this, even
+// one with n <= 1, so a caller can warm a device up with an empty sort before
+// its arena takes the device's memory and before any stream capture.  A
+// cudaDeviceReset unloads the module; the kept address is then stale, so this
+// entry point must not be used on a device after it has been reset.
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -103,9 +113,11 @@ void radix_sort_pairs_static(uint64_t* keys, int32_t* vals, int64_t n, cudaStrea
   if (n > kStaticPairs)
     throw std::length_error("sort_pairs_static: " + std::to_string(n) + " pairs exceed the fixed scratch capacity of " +
                             std::to_string(kStaticPairs) + " pairs; use gpp_sort_pairs");
+  // Set-up first, so that any call, even an empty one, loads the module and
+  // looks up the array's address.
+  unsigned char* scratch = scratch_for_current_device();
   if (n <= 1) return;
   if (!keys || !vals) throw std::invalid_argument("sort_pairs_static: null key or value pointer");
-  unsigned char* scratch = scratch_for_current_device();
   auto* kb = reinterpret_cast<uint64_t*>(scratch + kKeysOffset);
   auto* vb = reinterpret_cast<int32_t*>(scratch + kValsOffset);
   auto* counts = reinterpret_cast<int32_t*>(scratch + kCountsOffset);

@@ -184,6 +184,7 @@ def load():
         "gpp_batch_autotune": (C.c_int, [vp, C.c_int32, P(Params), C.c_int32, P(C.c_int32), vp]),
         "gpp_profile_enable": (None, [C.c_int]),
         "gpp_profile_read": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(i64), P(f64), P(f64)]),
+        "gpp_inject_alloc_failure": (None, [i64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -198,7 +199,8 @@ EXPORTED = [
     "gpp_postsolve_device", "gpp_free_summary", "gpp_export_maps", "gpp_tape_sizes",
     "gpp_export_tape", "gpp_row_activity_summary", "gpp_live_stats", "gpp_col_max_abs",
     "gpp_compact_and_transpose", "gpp_parallel_row_hashes", "gpp_sort_pairs", "gpp_sort_pairs_static", "gpp_device_alloc", "gpp_device_free",
-    "gpp_export_folding_map", "gpp_unfold_solution",
+    "gpp_export_folding_map", "gpp_unfold_solution", "gpp_run_folding", "gpp_free_folding_run",
+    "gpp_folding_run_export_map", "gpp_folding_run_unfold", "gpp_inject_alloc_failure",
     "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
     "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
     "gpp_mps_read", "gpp_mps_read_string", "gpp_mps_info", "gpp_mps_arrays", "gpp_mps_free", "gpp_mps_upload",

@@ -2,7 +2,7 @@
 schedule MLP (trained and run by the library's CUDA kernels) and presolve
 scheduled by it.
 
-A round is one step of the phase machine.  Per round the model sees 24
+A round is one step of the phase machine.  Per round the model sees 32
 features (see include/gpp.h) and outputs, for each of six gated rules, the
 probability that the rule will change the model this round, and the
 probability that presolve should stop.  Labels come from traces of the plain
@@ -22,7 +22,7 @@ import numpy as np
 from . import capi
 from .device import _raise
 
-FEATURES, HIDDEN, OUTPUTS = 24, 64, 7
+FEATURES, HIDDEN, OUTPUTS = 32, 64, 7
 GATED_RULES = ("singleton_columns", "bound_strengthening", "redundant_rows_dual_fix", "doubleton_equations",
                "parallel_rows", "parallel_columns")
 PARAMS = FEATURES * HIDDEN + HIDDEN + HIDDEN * HIDDEN + HIDDEN + HIDDEN * OUTPUTS + OUTPUTS

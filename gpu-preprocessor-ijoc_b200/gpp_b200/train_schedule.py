@@ -1,10 +1,13 @@
 """Trains the learned round schedule.
 
-    python -m gpp_b200.train_schedule --out schedule_model.npz [--lps 600] [--seed 0]
+    python -m gpp_b200.train_schedule --out schedule_model.npz [--lps 20000] [--seed 0]
 
-1. Draws training LPs from the plain-presolve generator (lpgen.random_lp) with
-   m log-uniform in [1,000, 500,000] and n = 2.5 m (generated by spawned
-   processes), and records a trace of the plain phase machine on each.
+1. Draws training LPs from the plain-presolve generator (lpgen.random_lp, the
+   generator of the 2,000 x 5,000 case and of the batched workload) with m
+   log-uniform in [1,000, 500,000] and n = 2.5 m, generated by spawned
+   processes while the GPU traces the ones already made, and records a trace
+   of the plain phase machine on each (one trace per LP, one sample per
+   round).
 2. Trains the schedule MLP on the rounds of all traces (the library's CUDA
    kernels; Adam, masked binary cross-entropy).
 3. Chooses the two decision thresholds on held-out LPs (skip a rule below
@@ -17,6 +20,7 @@
 from __future__ import annotations
 
 import argparse
+import itertools
 import json
 import multiprocessing as mp
 import os
@@ -44,6 +48,20 @@ def jobs(count, seed, lo=1000, hi=500000):
     return [(int(m), int(seed * 100000 + k)) for k, m in enumerate(ms)]
 
 
+def bounded_imap(pool, fn, items, window):
+    """pool.imap with at most `window` results pending: generated LPs wait in
+    host memory only until the GPU has traced the ones before them."""
+    from collections import deque
+    it = iter(items)
+    pending = deque(pool.apply_async(fn, (x,)) for x in itertools.islice(it, window))
+    while pending:
+        r = pending.popleft().get()
+        nxt = next(it, None)
+        if nxt is not None:
+            pending.append(pool.apply_async(fn, (nxt,)))
+        yield r
+
+
 def removal(lp, s):
     return lp.nnz - s.reduced_nnz
 
@@ -51,32 +69,48 @@ def removal(lp, s):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
-    ap.add_argument("--lps", type=int, default=600)
+    ap.add_argument("--lps", type=int, default=20000)
     ap.add_argument("--holdout", type=int, default=40)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--max-m", type=int, default=500000)
+    ap.add_argument("--max-trace-seconds", type=float, default=None,
+                    help="stop tracing new LPs after this long (the notes record how many were traced)")
     args = ap.parse_args(argv)
 
     ctx = mp.get_context("spawn")
-    with ctx.Pool(max(1, min(32, (os.cpu_count() or 2) - 1))) as pool:
-        train_lps = pool.map(_draw, jobs(args.lps, args.seed + 1, hi=args.max_m), chunksize=1)
-        hold_lps = pool.map(_draw, jobs(args.holdout, args.seed + 2, hi=args.max_m), chunksize=1)
-
-    from gpp_b200 import capi, device, schedule
-    params = capi.Params.defaults()
+    workers = max(1, min(48, (os.cpu_count() or 2) - 2))
     X, Y, M = [], [], []
     t0 = time.perf_counter()
-    for lp in train_lps:
-        d = device.DeviceLp(lp)
-        s, tr = schedule.traced_preprocess(d, params)
-        device.free_summary(s)
-        y, m = schedule.labels(tr)
-        X.append(tr["features"]); Y.append(y); M.append(m)
-        del d
+    train_nnz = 0
+    with ctx.Pool(workers) as pool:
+        hold = pool.map_async(_draw, jobs(args.holdout, args.seed + 2, hi=args.max_m), chunksize=1)
+        from gpp_b200 import capi, device, schedule
+        params = capi.Params.defaults()
+        # Traced as they arrive; each LP is dropped once traced.
+        traced = 0
+        for lp in bounded_imap(pool, _draw, jobs(args.lps, args.seed + 1, hi=args.max_m), 2 * workers):
+            if args.max_trace_seconds and time.perf_counter() - t0 > args.max_trace_seconds:
+                pool.terminate()
+                break
+            traced += 1
+            d = device.DeviceLp(lp)
+            s, tr = schedule.traced_preprocess(d, params)
+            device.free_summary(s)
+            y, m = schedule.labels(tr)
+            X.append(tr["features"]); Y.append(y); M.append(m)
+            train_nnz += lp.nnz
+            del d, lp
+        hold_lps = hold.get() if hold.ready() or traced == args.lps else None
+    if hold_lps is None:   # the pool was stopped early: draw the held-out LPs now
+        with ctx.Pool(workers) as pool:
+            hold_lps = pool.map(_draw, jobs(args.holdout, args.seed + 2, hi=args.max_m), chunksize=1)
     X, Y, M = (np.concatenate(a) for a in (X, Y, M))
     trace_s = time.perf_counter() - t0
-    w, loss = schedule.train(X, Y, M, epochs=args.epochs, seed=args.seed)
+    t1 = time.perf_counter()
+    w, loss = schedule.train(X, Y, M, epochs=args.epochs, batch=args.batch, seed=args.seed)
+    train_s = time.perf_counter() - t1
 
     # Threshold on held-out LPs: plain first, then each threshold.
     dlps = [device.DeviceLp(lp) for lp in hold_lps]
@@ -104,7 +138,9 @@ def main(argv=None):
                 "mean_kept": float(np.mean(kept))}
     ok = [v for v in table.values() if v["min_kept"] >= KEEP_SHARE]
     best = min(ok, key=lambda v: v["time_ratio"]) if ok else {"skip_below": 0.0, "stop_above": 1.0}
-    notes = {"samples": int(len(X)), "train_lps": args.lps, "holdout_lps": args.holdout, "trace_seconds": trace_s,
+    notes = {"samples": int(len(X)), "train_lps": traced, "train_nnz": int(train_nnz), "holdout_lps": args.holdout,
+             "m_range": [1000, args.max_m], "generator_workers": workers, "train_seconds": train_s,
+             "epochs": args.epochs, "batch": args.batch, "trace_seconds": trace_s,
              "final_loss": float(loss[-1]) if len(loss) else None, "thresholds": table, "chosen": best,
              "positive_rate": [float(x) for x in (Y * M).sum(0) / np.maximum(M.sum(0), 1)]}
     schedule.save_model(args.out, w, best["skip_below"], best["stop_above"], loss=loss, notes=json.dumps(notes))

@@ -241,6 +241,38 @@ GPP_API int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t*
 GPP_API int gpp_export_folding_map(const gpp_summary* summary, int32_t* row_color, int32_t* col_color,
                                    double* row_scale, double* col_scale);
 
+/* folding::run_folding / free_folded_lp (folding/folding.hpp:16-20): colour
+ * refinement and the quotient LP of `lp` alone, without presolve.  When
+ * folding applies, `folded_lp` is a device model owned by the run
+ * (owns_folded_lp = 1) and the four map arrays are device arrays of the
+ * original sizes (1-based colours, unfold scales 1/|colour|); otherwise
+ * `applied` = 0, folded sizes equal the original ones, `folded_lp` is zero
+ * and the map pointers are NULL, as the reference's summary is.  A negative
+ * or non-finite tolerance gives GPP_ERR_INVALID.
+ * gpp_free_folding_run releases everything the run owns; calling it twice
+ * is safe. */
+typedef struct gpp_folding_run {
+  uint8_t applied;
+  int32_t original_rows, original_cols, folded_rows, folded_cols;
+  double seconds;
+  gpp_lp folded_lp;
+  uint8_t owns_folded_lp;
+  int32_t* row_color_id;
+  int32_t* col_color_id;
+  double* row_scale;
+  double* col_scale;
+  void* handle;
+} gpp_folding_run;
+GPP_API int gpp_run_folding(const gpp_lp* lp, double tolerance, gpp_folding_run* out);
+GPP_API void gpp_free_folding_run(gpp_folding_run* run);
+/* gpp_export_folding_map and gpp_unfold_solution for the map of a
+ * gpp_run_folding result (same outputs; nothing written / an invalid
+ * argument when folding did not apply). */
+GPP_API int gpp_folding_run_export_map(const gpp_folding_run* run, int32_t* row_color, int32_t* col_color,
+                                       double* row_scale, double* col_scale);
+GPP_API int gpp_folding_run_unfold(const gpp_folding_run* run, const double* x_folded, const double* y_folded,
+                                   const double* z_folded, double* x_out, double* y_out, double* z_out);
+
 /* folding::unfold_solution_device_to_host (folding/folding.hpp:40-44): map a
  * solution of the folded model (DEVICE arrays of folded_cols, folded_rows,
  * folded_cols entries; any may be NULL) to the original model on the HOST:
@@ -346,11 +378,11 @@ GPP_API int gpp_reduced_to_host(const gpp_summary* summary, gpp_offset* row_ptr,
  * layers of GPP_SCHEDULE_HIDDEN units and GPP_SCHEDULE_OUTPUTS logits (one per
  * gated rule, "the rule will change the model this round", then "stop").
  * The reference has no counterpart; its plain loop stays the default here. */
-#define GPP_SCHEDULE_FEATURES 24
+#define GPP_SCHEDULE_FEATURES 32
 #define GPP_SCHEDULE_HIDDEN 64
 #define GPP_SCHEDULE_OUTPUTS 7
 /* W1[24][64], b1[64], W2[64][64], b2[64], W3[64][7], b3[7], row-major. */
-#define GPP_SCHEDULE_PARAMS (24 * 64 + 64 + 64 * 64 + 64 + 64 * 7 + 7)
+#define GPP_SCHEDULE_PARAMS (32 * 64 + 64 + 64 * 64 + 64 + 64 * 7 + 7)
 
 /* gpp_preprocess that also records every round: features[r * 24 + i],
  * round_info[4 r ..] = phase (0 Cleanup, 1 Propagation, 2 Aggregation,
@@ -374,7 +406,7 @@ GPP_API int gpp_preprocess_scheduled(const gpp_lp* lp, const gpp_params* params,
                                      gpp_summary* out);
 
 /* Training and inference of the schedule MLP on the GPU (host arrays in and
- * out).  X is n x 24, Y and M (labels and 0/1 masks) are n x 7; the loss is
+ * out).  X is n x 32, Y and M (labels and 0/1 masks) are n x 7; the loss is
  * the mean over samples of the masked binary cross-entropy of the logits.
  * gpp_mlp_train runs `epochs` epochs of Adam (minibatches of `batch`, order
  * shuffled by `seed`) from and into `params`; loss_per_epoch may be NULL. */
@@ -440,9 +472,13 @@ GPP_API int gpp_sort_pairs(uint64_t* keys, int32_t* values, int64_t n);
  * GPP_ERR_LENGTH without touching the data.  A call launches kernels on
  * `stream` (a cudaStream_t; NULL for the legacy default stream) and returns
  * without synchronizing; it calls no cudaMalloc, cudaFree or allocating
- * library routine.  The first call on each device looks up the array's
- * device address with that device current; make that first call before any
- * stream capture.  Every call shares the one array, so calls whose work
+ * library routine.  The first call on each device (any n, 0 included) loads
+ * the library's device code on that device, which places the fixed array in
+ * device memory, and looks up the array's device address with that device
+ * current: make that first call before an arena allocator takes the device's
+ * memory and before any stream capture.  The address is kept for the life of
+ * the process, so do not use this entry point on a device after
+ * cudaDeviceReset.  Every call shares the one array, so calls whose work
  * overlaps on the GPU race and give wrong results: order them on one stream
  * or synchronize between them.  Output equals gpp_sort_pairs'. */
 #define GPP_SORT_STATIC_MAX_PAIRS (1 << 20)
@@ -454,6 +490,14 @@ GPP_API int gpp_sort_pairs_static(uint64_t* keys, int32_t* values, int64_t n, vo
  * cudaFree.  bytes = 0 gives NULL. */
 GPP_API int gpp_device_alloc(void** device_ptr, size_t bytes);
 GPP_API void gpp_device_free(void* device_ptr);
+
+/* Test hook for failure handling: the device allocation made `after`
+ * allocations from now (0 = the next one, counted over all threads) by any
+ * engine entry point returns cudaErrorMemoryAllocation instead of memory,
+ * exactly once; `after` < 0 disarms it.  The failing call returns
+ * GPP_ERR_CUDA with its message and releases what it had allocated; the
+ * device is not touched, so later calls run normally. */
+GPP_API void gpp_inject_alloc_failure(int64_t after);
 
 /* Last error message of the calling thread ("" when none). */
 GPP_API const char* gpp_last_error(void);

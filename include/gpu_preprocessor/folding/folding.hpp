@@ -61,16 +61,63 @@ inline FoldingMapHost copy_map_to_host(const FoldingMapDevice& map) {
   h.original_cols = map.original_cols;
   h.reduced_rows = map.reduced_rows;
   h.reduced_cols = map.reduced_cols;
-  if (map.owner == nullptr) return h;
+  if (map.owner == nullptr && map.run.handle == nullptr) return h;
   h.row_color_id.resize(static_cast<std::size_t>(map.original_rows));
   h.col_color_id.resize(static_cast<std::size_t>(map.original_cols));
   h.row_scale.resize(static_cast<std::size_t>(map.original_rows));
   h.col_scale.resize(static_cast<std::size_t>(map.original_cols));
   gpu_preprocessor::detail::throw_on_status(
-      gpp_export_folding_map(map.owner, h.row_color_id.data(), h.col_color_id.data(), h.row_scale.data(),
-                             h.col_scale.data()),
+      map.owner ? gpp_export_folding_map(map.owner, h.row_color_id.data(), h.col_color_id.data(),
+                                         h.row_scale.data(), h.col_scale.data())
+                : gpp_folding_run_export_map(&map.run, h.row_color_id.data(), h.col_color_id.data(),
+                                             h.row_scale.data(), h.col_scale.data()),
       "copy_map_to_host");
   return h;
+}
+
+// run_folding (folding/folding.hpp:16-18): folding alone.  When it applies,
+// the folded model and the map are device arrays owned by the summary until
+// free_folded_lp; otherwise the summary carries the original sizes only.
+// `verbose` is accepted for source compatibility and prints nothing.
+inline FoldingRunSummary run_folding(const presolve::LPInfoGpu& original_model, double tolerance,
+                                     bool verbose = false) {
+  (void)verbose;
+  gpp_folding_run r{};
+  gpu_preprocessor::detail::throw_on_status(gpp_run_folding(presolve::detail::as_c(&original_model), tolerance, &r),
+                                            "run_folding");
+  FoldingRunSummary s;
+  s.applied = r.applied != 0;
+  s.original_rows = r.original_rows;
+  s.original_cols = r.original_cols;
+  s.folded_rows = r.folded_rows;
+  s.folded_cols = r.folded_cols;
+  s.profile.total_seconds = r.seconds;
+  s.map.original_rows = r.original_rows;
+  s.map.original_cols = r.original_cols;
+  s.map.reduced_rows = r.folded_rows;
+  s.map.reduced_cols = r.folded_cols;
+  if (s.applied) {
+    s.map.row_color_id = r.row_color_id;
+    s.map.col_color_id = r.col_color_id;
+    s.map.row_scale = r.row_scale;
+    s.map.col_scale = r.col_scale;
+    s.map.owns_buffers = true;
+    s.map.run = r;
+    s.folded_lp = presolve::detail::from_c(r.folded_lp);
+    s.owns_folded_lp = true;
+  }
+  return s;
+}
+
+// free_folded_lp (folding/folding.hpp:20): releases the folded model and the
+// map of a run_folding summary; safe to call twice.
+inline void free_folded_lp(FoldingRunSummary& summary) {
+  gpp_free_folding_run(&summary.map.run);
+  summary.map.row_color_id = summary.map.col_color_id = nullptr;
+  summary.map.row_scale = summary.map.col_scale = nullptr;
+  summary.map.owns_buffers = false;
+  summary.folded_lp = presolve::LPInfoGpu{};
+  summary.owns_folded_lp = false;
 }
 
 // x_j = x_f[C(j)], z_j = z_f[C(j)] / |C(j)|, y_i = y_f[R(i)] / |R(i)|.
@@ -105,10 +152,14 @@ inline UnfoldedSolutionHost unfold_solution_device_to_host(const FoldingMapDevic
   if (x_red) out.x.resize(static_cast<std::size_t>(map.original_cols));
   if (y_red) out.y.resize(static_cast<std::size_t>(map.original_rows));
   if (z_red) out.z.resize(static_cast<std::size_t>(map.original_cols));
-  if (map.owner == nullptr) throw std::invalid_argument("unfold_solution_device_to_host: folding did not apply");
+  if (map.owner == nullptr && map.run.handle == nullptr)
+    throw std::invalid_argument("unfold_solution_device_to_host: folding did not apply");
+  double* xo = x_red ? out.x.data() : nullptr;
+  double* yo = y_red ? out.y.data() : nullptr;
+  double* zo = z_red ? out.z.data() : nullptr;
   gpu_preprocessor::detail::throw_on_status(
-      gpp_unfold_solution(map.owner, x_red, y_red, z_red, x_red ? out.x.data() : nullptr,
-                          y_red ? out.y.data() : nullptr, z_red ? out.z.data() : nullptr),
+      map.owner ? gpp_unfold_solution(map.owner, x_red, y_red, z_red, xo, yo, zo)
+                : gpp_folding_run_unfold(&map.run, x_red, y_red, z_red, xo, yo, zo),
       "unfold_solution_device_to_host");
   return out;
 }

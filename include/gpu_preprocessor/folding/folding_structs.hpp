@@ -1,10 +1,12 @@
 // Folding / pipeline structs of the C++ layer (GPU-Preprocessor's
 // cpp/include/gpu_preprocessor/folding/folding_structs.hpp:59-115).
 //
-// The folding map stays on the device inside the summary; FoldingMapDevice is
-// its sizes plus a view of the owning summary (not raw device pointers), and
-// copy_map_to_host / unfold_solution_device_to_host read it through the C ABI.
-// The folded model itself is internal to the engine and is not exported.
+// In the pipeline (run_gpu_presolve_with_folding / preprocess) the folding map
+// stays on the device inside the summary, and FoldingMapDevice is its sizes
+// plus a view of the owning summary.  A standalone run_folding exports what
+// the reference's does: the folded model and the map as device arrays (owned
+// by the run until free_folded_lp).  copy_map_to_host and
+// unfold_solution_device_to_host read either kind through the C ABI.
 #pragma once
 
 #include <cstdint>
@@ -25,12 +27,66 @@ struct FoldingMapHost {
   std::vector<double> col_scale;           // 1 / |colour of the column|
 };
 
+// Timings of a folding run.  This engine times the run as a whole
+// (total_seconds); the stage fields are kept for source compatibility and
+// stay zero.
+struct FoldingRefinementProfile {
+  double total_seconds = 0.0;
+  double init_color_seconds = 0.0;
+  double spmv_at_seconds = 0.0;
+  double refine_col_seconds = 0.0;
+  double spmv_a_seconds = 0.0;
+  double refine_row_seconds = 0.0;
+  std::int32_t rounds = 0;
+  bool refinement_ok = false;
+  std::int32_t final_row_colors = 0;
+  std::int32_t final_col_colors = 0;
+};
+
+struct FoldingReduceProfile {
+  double total_seconds = 0.0;
+  double count_color_seconds = 0.0;
+  double emit_triplet_seconds = 0.0;
+  double sort_reduce_seconds = 0.0;
+  double copy_unique_to_host_seconds = 0.0;
+  double host_filter_rebuild_seconds = 0.0;
+  double host_csr_build_seconds = 0.0;
+  double copy_reduced_matrix_to_device_seconds = 0.0;
+  double transpose_seconds = 0.0;
+  double sum_cost_seconds = 0.0;
+  double row_bounds_seconds = 0.0;
+  double col_bounds_seconds = 0.0;
+  NnzOffset unique_entries = 0;
+  NnzOffset kept_entries = 0;
+};
+
+struct FoldingMapProfile {
+  double total_seconds = 0.0;
+  double copy_color_ids_seconds = 0.0;
+  double count_color_seconds = 0.0;
+  double scale_seconds = 0.0;
+};
+
+struct FoldingProfile {
+  double total_seconds = 0.0;
+  FoldingRefinementProfile refinement;
+  FoldingReduceProfile reduce;
+  FoldingMapProfile map;
+};
+
 struct FoldingMapDevice {
   std::int32_t original_rows = 0;
   std::int32_t original_cols = 0;
   std::int32_t reduced_rows = 0;
   std::int32_t reduced_cols = 0;
-  const gpp_summary* owner = nullptr;  // the summary holding the map on the device
+  // Device arrays of a standalone run_folding (NULL in the pipeline's view).
+  std::int32_t* row_color_id = nullptr;
+  std::int32_t* col_color_id = nullptr;
+  double* row_scale = nullptr;
+  double* col_scale = nullptr;
+  bool owns_buffers = false;
+  const gpp_summary* owner = nullptr;  // pipeline: the summary holding the map on the device
+  gpp_folding_run run{};               // run_folding: the run holding the map
 };
 
 struct FoldingRunSummary {
@@ -39,7 +95,10 @@ struct FoldingRunSummary {
   std::int32_t original_cols = 0;
   std::int32_t folded_rows = 0;
   std::int32_t folded_cols = 0;
+  FoldingProfile profile;
   FoldingMapDevice map;
+  presolve::LPInfoGpu folded_lp;
+  bool owns_folded_lp = false;
 };
 
 // Move-only, like the reference's (its record cannot be copied).  After a

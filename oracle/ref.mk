@@ -1,8 +1,14 @@
 # Builds the reference GPU-Preprocessor library (the bit-exact structure
 # oracle, run only on a CUDA machine) straight from its sources with nvcc.
 # Usage: make -f oracle/ref.mk -j8   (from the repository root)
-# Inputs: REFERENCE (default /root/reference); outputs only under oracle/_ref/.
-REFERENCE ?= /root/reference
+# Input: the reference checkout, from GPP_REFERENCE (environment) or
+# REFERENCE=... on the command line; without one the recipe does nothing.
+# Outputs only under oracle/_ref/.
+REFERENCE ?= $(GPP_REFERENCE)
+ifeq ($(wildcard $(REFERENCE)/cpp/src),)
+all:
+	@echo "$(lastword $(MAKEFILE_LIST)): no reference checkout (set GPP_REFERENCE); skipped"
+else
 OUT := oracle/_ref
 OBJ := $(OUT)/obj
 NVCC ?= nvcc
@@ -47,3 +53,4 @@ $(OUT)/ref_driver: oracle/ref_driver.cpp $(OUT)/libgpp_ref.so
 	  oracle/ref_driver.cpp -L$(OUT) -lgpp_ref -lcusparse -Xlinker -rpath,'$$ORIGIN' -o $@
 
 .PHONY: all
+endif

@@ -89,6 +89,7 @@ int main(int argc, char** argv) {
       else if (k == "column_domination_min_fixed_cols") p.column_domination_min_fixed_cols = v;
       else if (k == "column_domination_min_candidate_ratio") p.column_domination_min_candidate_ratio = dv;
       else if (k == "max_iters") p.max_iters = v;
+      else if (k == "max_time") p.max_time = dv;
       else if (k == "folding_tolerance") p.folding_tolerance = dv;
       else if (k == "doubleton_equations_scan") p.doubleton_equations_scan = v != 0;
       else if (k == "doubleton_equations_max_fill_in_proxy") p.doubleton_equations_max_fill_in_proxy = v;

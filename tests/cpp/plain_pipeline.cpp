@@ -6,6 +6,7 @@
 //
 // usage: plain_pipeline defaults
 //        plain_pipeline run <lp.bin> <out_dir> [field=value ...]
+//        plain_pipeline fold <lp.bin> <out_dir>
 // `defaults` checks PresolveParams{} against gpp_default_params (no GPU).
 // `run` writes meta.txt, the recovery maps and tape, the folding map (when
 // folding applied), the reduced solution it fed to postprocess (xr, yr, zr)
@@ -217,9 +218,59 @@ static int run(const std::string& in, const std::string& out, const ps::Presolve
   return 0;
 }
 
+// folding::run_folding alone: sizes, the map (host copy and the device
+// arrays of the summary), the folded model, and the unfold of a folded point.
+static int fold(const std::string& in, const std::string& out) {
+  const HostLp h = read_lp(in);
+  gpp::DeviceLp lp;
+  lp.A = {int(h.m), int(h.n), checked_nnz_offset(h.nnz), upload(h.ptr), upload(h.idx), upload(h.val)};
+  lp.AT = {int(h.n), int(h.m), checked_nnz_offset(h.nnz), upload(h.tptr), upload(h.tidx), upload(h.tval)};
+  lp.c = upload(h.c); lp.l = upload(h.l); lp.u = upload(h.u); lp.AL = upload(h.AL); lp.AU = upload(h.AU);
+  lp.obj_constant = h.obj;
+  gpp::folding::FoldingRunSummary f = gpp::folding::run_folding(lp, 1e-9);
+  std::ofstream meta(out + "/meta.txt");
+  meta << "applied " << f.applied << "\noriginal_rows " << f.original_rows << "\noriginal_cols " << f.original_cols
+       << "\nfolded_rows " << f.folded_rows << "\nfolded_cols " << f.folded_cols << "\nowns_folded_lp "
+       << f.owns_folded_lp << "\nfolded_nnz " << f.folded_lp.A.nnz << "\n";
+  if (f.applied) {
+    const auto map = gpp::folding::copy_map_to_host(f.map);
+    save(out, "row_color", map.row_color_id);
+    save(out, "col_color", map.col_color_id);
+    save(out, "row_scale", map.row_scale);
+    save(out, "col_scale", map.col_scale);
+    const auto m0 = static_cast<std::size_t>(f.original_rows), n0 = static_cast<std::size_t>(f.original_cols);
+    save(out, "dev_row_color", download(f.map.row_color_id, m0));
+    save(out, "dev_col_scale", download(f.map.col_scale, n0));
+    const auto mf = static_cast<std::size_t>(f.folded_rows), nf = static_cast<std::size_t>(f.folded_cols);
+    save(out, "F_ptr", download(f.folded_lp.A.rowPtr, mf + 1));
+    save(out, "F_idx", download(f.folded_lp.A.colVal, static_cast<std::size_t>(f.folded_lp.A.nnz)));
+    save(out, "F_val", download(f.folded_lp.A.nzVal, static_cast<std::size_t>(f.folded_lp.A.nnz)));
+    save(out, "F_c", download(f.folded_lp.c, nf));
+    std::vector<double> xf(nf), yf(mf), zf(nf);
+    for (std::size_t j = 0; j < nf; ++j) { xf[j] = double(j % 5); zf[j] = 0.5 * double(j % 3); }
+    for (std::size_t i = 0; i < mf; ++i) yf[i] = double(i % 4) - 1.0;
+    double *dx = upload(xf), *dy = upload(yf), *dz = upload(zf);
+    const auto u = gpp::folding::unfold_solution_device_to_host(f.map, dx, dy, dz);
+    save(out, "ux", u.x);
+    save(out, "uy", u.y);
+    save(out, "uz", u.z);
+    for (double* q : {dx, dy, dz}) ck(cudaFree(q), "cudaFree");
+  }
+  gpp::folding::free_folded_lp(f);
+  gpp::folding::free_folded_lp(f);  // a second call is a no-op
+  if (f.owns_folded_lp || f.map.row_color_id != nullptr) throw std::runtime_error("free_folded_lp left state");
+  for (void* q : {static_cast<void*>(lp.A.rowPtr), static_cast<void*>(lp.A.colVal), static_cast<void*>(lp.A.nzVal),
+                  static_cast<void*>(lp.AT.rowPtr), static_cast<void*>(lp.AT.colVal),
+                  static_cast<void*>(lp.AT.nzVal), static_cast<void*>(lp.c), static_cast<void*>(lp.l),
+                  static_cast<void*>(lp.u), static_cast<void*>(lp.AL), static_cast<void*>(lp.AU)})
+    ck(cudaFree(q), "cudaFree");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   try {
     if (argc >= 2 && std::string(argv[1]) == "defaults") return check_defaults();
+    if (argc == 4 && std::string(argv[1]) == "fold") return fold(argv[2], argv[3]);
     if (argc < 4 || std::string(argv[1]) != "run") {
       std::cerr << "usage: plain_pipeline defaults | run <lp.bin> <out_dir> [field=value ...]\n";
       return 2;

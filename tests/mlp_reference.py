@@ -4,7 +4,7 @@ over samples of the masked binary cross-entropy of the logits, and its
 analytic gradient, in the library's flat parameter layout."""
 import numpy as np
 
-F, H, O = 24, 64, 7
+F, H, O = 32, 64, 7
 
 
 def unpack(w):

@@ -141,3 +141,48 @@ def test_plain_pipeline_matches_ctypes_path(program, tmp_path, workload, extra):
                 assert np.array_equal(read(out / key, np.float64).view(np.uint64), want.view(np.uint64)), key
     finally:
         device.free_summary(s)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("workload", ["replicated:100x250*4", "random:300x800"])
+def test_run_folding_matches_the_pipeline_map(program, tmp_path, workload):
+    """folding::run_folding / free_folded_lp of the layer: the same fold
+    decision, sizes and colour map as the pipeline's folding stage (presolve
+    off), a folded model of the folded sizes, and an unfold through the run's
+    own map equal to the pipeline's unfold of the same folded point."""
+    import torch
+    from gpp_b200 import capi, device, lpgen
+    lp = lpgen.workload(workload, seed=0)
+    lp_path = str(tmp_path / "lp.bin")
+    lpgen.save_lp(lp_path, lp)
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([program, "fold", lp_path, str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = meta(out / "meta.txt")
+    dlp = device.DeviceLp(lp)
+    s = device.preprocess(dlp, capi.Params.defaults(enable_folding=1, enable_presolve=0, folding_tolerance=1e-9))
+    try:
+        assert got["applied"] == s.folding_applied
+        assert (got["folded_rows"], got["folded_cols"]) == (s.folded_rows, s.folded_cols)
+        assert got["owns_folded_lp"] == s.folding_applied
+        if not s.folding_applied:
+            return
+        rc, cc, rs, cs = device.fold_map(s)
+        assert np.array_equal(read(out / "row_color", np.int32), rc)
+        assert np.array_equal(read(out / "col_color", np.int32), cc)
+        assert np.array_equal(read(out / "row_scale", np.float64), rs)
+        assert np.array_equal(read(out / "col_scale", np.float64), cs)
+        assert np.array_equal(read(out / "dev_row_color", np.int32), rc)
+        assert np.array_equal(read(out / "dev_col_scale", np.float64), cs)
+        assert len(read(out / "F_ptr", np.int32)) == s.folded_rows + 1
+        assert len(read(out / "F_c", np.float64)) == s.folded_cols
+        nf, mf = s.folded_cols, s.folded_rows
+        xf = torch.tensor([float(j % 5) for j in range(nf)], dtype=torch.float64).cuda()
+        yf = torch.tensor([float(i % 4) - 1.0 for i in range(mf)], dtype=torch.float64).cuda()
+        zf = torch.tensor([0.5 * float(j % 3) for j in range(nf)], dtype=torch.float64).cuda()
+        ux, uy, uz = device.unfold(xf, yf, zf, s)
+        for key, want in (("ux", ux), ("uy", uy), ("uz", uz)):
+            assert np.array_equal(read(out / key, np.float64), want), key
+    finally:
+        device.free_summary(s)

@@ -33,7 +33,11 @@ ALL = FULL + ["doubleton_equations"]
 SMALL_BATCH = dict(doubleton_equations_min_selected_per_batch=1, doubleton_equations_min_selected_ratio=0.0)
 
 
-def run_reference(lp, rules, extra=None):
+def run_reference(lp, rules, extra=None, point=None):
+    """Runs the reference library on `lp` and reads back what it exported.
+
+    `point` = (x, y, z) in reduced order also runs the reference's
+    postprocess on that point; its x_org, y_org, z_org are returned."""
     d = tempfile.mkdtemp()
     path = os.path.join(d, "lp.bin")
     lpgen.save_lp(path, lp)
@@ -41,6 +45,12 @@ def run_reference(lp, rules, extra=None):
     for f in RULE_FLAGS:
         args.append(f"{f}={1 if f[len('enable_'):] in rules else 0}")
     args += extra or []
+    if point is not None:
+        files = []
+        for name, v in zip(("x_red", "y_red", "z_red"), point):
+            files.append(os.path.join(d, name))
+            np.ascontiguousarray(v, dtype=np.float64).tofile(files[-1])
+        args += ["--postsolve", *files]
     r = subprocess.run(args, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     meta = {}
@@ -53,7 +63,8 @@ def run_reference(lp, rules, extra=None):
             "AU": np.float64, "row_map": np.int32, "col_map": np.int32, "fixed_idx": np.int32,
             "fixed_val": np.float64, "tape_types": np.int32, "tape_is": np.int32, "tape_vs": np.int32,
             "tape_idx": np.int32, "tape_val": np.float64, "row_color": np.int32, "col_color": np.int32,
-            "row_scale": np.float64, "col_scale": np.float64}
+            "row_scale": np.float64, "col_scale": np.float64, "x_org": np.float64, "y_org": np.float64,
+            "z_org": np.float64}
     for k, dt in spec.items():
         p = os.path.join(d, k)
         out[k] = np.fromfile(p, dtype=dt) if os.path.exists(p) else None
@@ -72,9 +83,24 @@ def close(a, b, rel=1e-12):
 needs_reference = pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference build (oracle/_ref) not present")
 
 
-def check_against_reference(lp, rules, extra=None):
+def reduced_point(got, rows, cols, seed=1):
+    """A seeded reduced primal/dual point: x inside the reduced bounds (finite
+    boxes of width 20 where a bound is infinite), y and z standard normal."""
+    rng = np.random.default_rng(seed)
+    lo = np.where(np.isfinite(got.l), got.l, np.where(np.isfinite(got.u), got.u - 20.0, -10.0))
+    hi = np.where(np.isfinite(got.u), got.u, lo + 20.0)
+    return lo + rng.random(cols) * (hi - lo), rng.standard_normal(rows), rng.standard_normal(cols)
+
+
+def check_against_reference(lp, rules, extra=None, oracle=True, postsolve=False):
+    """Presolves `lp` with the engine and with the reference library and
+    requires drop-in parity.  With `postsolve`, both also postprocess the same
+    reduced point, and the recovered x, y, z must agree within 1e-12 relative
+    and give the same objective within 1e-9 relative.  `postsolve` is True for
+    a seeded point inside the reduced bounds, or a function (result, summary)
+    -> (x, y, z) giving the point."""
+    import torch
     extra = {"enable_structure_specific_rules": 0, **(extra or {})}
-    ref = run_reference(lp, rules, [f"{k}={v}" for k, v in extra.items()])
     params = params_with_rules(rules, **{"enable_folding": 0, **extra})
     dlp = device.DeviceLp(lp)
     s = device.preprocess(dlp, params)
@@ -82,6 +108,13 @@ def check_against_reference(lp, rules, extra=None):
         got = device.Result(s)
         got.fold = device.fold_map(s)
         got.summary = type(s).from_buffer_copy(s)
+        point = None
+        if callable(postsolve):
+            point = postsolve(got, s)
+        elif postsolve:
+            point = reduced_point(got, s.reduced_rows, s.reduced_cols)
+        ref = run_reference(lp, rules, [f"{k}={v}" for k, v in extra.items()], point)
+        got.ref = ref
         m = ref["meta"]
         assert (s.reduced_rows, s.reduced_cols, s.reduced_nnz) == (
             int(m["reduced_rows"]), int(m["reduced_cols"]), int(m["reduced_nnz"]))
@@ -95,9 +128,17 @@ def check_against_reference(lp, rules, extra=None):
         assert np.array_equal(got.tape_types, ref["tape_types"])
         assert np.array_equal(got.tape_idx, ref["tape_idx"])
         assert close(got.tape_val, ref["tape_val"], 1e-9)
-        # The oracle agrees with both.
-        orc = pyoracle.presolve(lp, params)
-        assert np.array_equal(orc.row_map, ref["row_map"]) and np.array_equal(orc.col_map, ref["col_map"])
+        if postsolve:
+            x, y, z = device.postprocess(*(torch.from_numpy(v).cuda() for v in point), s, dlp)
+            for k, v in (("x_org", x), ("y_org", y), ("z_org", z)):
+                assert close(v, ref[k]), k
+            obj, obj_ref = float(lp.c @ x), float(lp.c @ ref["x_org"])
+            assert abs(obj - obj_ref) <= 1e-9 * max(1.0, abs(obj_ref))
+            got.solution = (x, y, z)
+        if oracle:
+            # The oracle agrees with both.
+            orc = pyoracle.presolve(lp, params)
+            assert np.array_equal(orc.row_map, ref["row_map"]) and np.array_equal(orc.col_map, ref["col_map"])
         return got
     finally:
         device.free_summary(s)
@@ -148,3 +189,36 @@ def test_reference_startup_rules_do_not_fire(workload):
     for k in ("row_map", "col_map", "A_idx", "tape_types"):
         assert np.array_equal(on[k], off[k]), k
     assert on["meta"]["iterations"] == off["meta"]["iterations"]
+
+
+@needs_reference
+@pytest.mark.parametrize("rules", [PROPAGATION, FULL, ALL])
+@pytest.mark.parametrize("workload", ["random:400x1000", "slack:2000x5000", "random:20000x50000"])
+def test_postsolve_matches_reference(rules, workload):
+    """The reference's postprocess and the engine's recover the same original
+    x, y, z from one seeded reduced point (tapes up to ~10^4 records, so the
+    engine's component-parallel replay is compared with the reference's)."""
+    extra = SMALL_BATCH if rules is ALL and workload != "random:20000x50000" else {}
+    got = check_against_reference(lpgen.workload(workload, seed=0), rules, extra, oracle=False, postsolve=True)
+    if rules is ALL:
+        assert 13 in got.tape_types.tolist()
+
+
+@needs_reference
+@pytest.mark.parametrize("workload,seed", [("random:400x1000", 0), ("random:400x1000", 3), ("slack:400x1000", 0)])
+def test_postsolve_of_optimum_matches_reference(workload, seed):
+    """The reduced LP's optimum (HiGHS) postsolved by the reference and by the
+    engine: same x, y, z, and the original objective within 1e-9 relative of
+    HiGHS on the unreduced LP."""
+    import lpsolve
+    lp = lpgen.workload(workload, seed=seed)
+
+    def optimum(got, s):
+        rr, yr, zr = lpsolve.solve(s.reduced_rows, s.reduced_cols, got.A_ptr, got.A_idx, got.A_val, got.c, got.AL,
+                                   got.AU, got.l, got.u)
+        return rr.x, yr, zr
+
+    got = check_against_reference(lp, ALL, SMALL_BATCH, oracle=False, postsolve=optimum)
+    res0, _, _ = lpsolve.solve(lp.m, lp.n, lp.row_ptr, lp.col_idx, lp.values, lp.c, lp.AL, lp.AU, lp.l, lp.u)
+    for x in (got.solution[0], got.ref["x_org"]):
+        assert abs(lp.c @ x - res0.fun) <= 1e-9 * max(1.0, abs(res0.fun))

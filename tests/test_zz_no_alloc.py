@@ -40,6 +40,8 @@ def test_static_sort_matches_pooled_sort_on_two_calls_in_a_row():
     lib = capi.load()
     rng = np.random.default_rng(7)
     stream = torch.cuda.current_stream()
+    # An empty sort is the set-up call: it loads the array and looks up its address.
+    assert lib.gpp_sort_pairs_static(None, None, 0, C.c_void_p(stream.cuda_stream)) == 0, lib.gpp_last_error()
     for call, n in enumerate((max_pairs(), 100_003)):
         keys, vals = make_pairs(rng, n)
         pk = torch.from_numpy(keys.view(np.int64)).cuda()
