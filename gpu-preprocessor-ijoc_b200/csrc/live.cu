@@ -74,7 +74,9 @@ struct ActivityTerm {
   L2Hints hint;
   // The term of live stored entry p whose column bounds are b.
   __device__ __forceinline__ void operator()(offset_t p, double2 b, double& lo, double& hi, int& ni, int& pi) const {
-    const double a = ld_stream(val + p, hint.stream);   // streamed once: keep L2 for the gathered bounds
+    add(ld_stream(val + p, hint.stream), b, lo, hi, ni, pi);   // streamed once: keep L2 for the gathered bounds
+  }
+  __device__ __forceinline__ void add(double a, double2 b, double& lo, double& hi, int& ni, int& pi) const {
     if constexpr (Plain) {
       // Plain sums of the redundant-row test: infinities propagate.
       lo += a >= 0.0 ? a * b.x : a * b.y;
@@ -90,7 +92,36 @@ struct ActivityTerm {
   __device__ __forceinline__ double2 bounds(offset_t p) const {
     return ld_keep(lu + ld_stream(idx + p, hint.stream), hint.keep);
   }
+  // One live entry as the reference's lane partial holds it when the lane
+  // sees no other entry: 0.0 + term (or 0.0 when the term is skipped), plus
+  // the infinite-term counts.
+  __device__ __forceinline__ void slot(double a, double2 b, double& plo, double& phi, int& ni, int& pi) const {
+    plo = 0.0;
+    phi = 0.0;
+    if constexpr (Plain) {
+      plo = plo + (a >= 0.0 ? a * b.x : a * b.y);
+      phi = phi + (a >= 0.0 ? a * b.y : a * b.x);
+      return;
+    }
+    if (fabs(a) <= zero_tol) return;
+    const double tlo = a >= 0.0 ? a * b.x : a * b.y;
+    const double thi = a >= 0.0 ? a * b.y : a * b.x;
+    if (isfinite(tlo)) plo = plo + tlo; else if (tlo < 0.0) ++ni;
+    if (isfinite(thi)) phi = phi + thi; else if (thi > 0.0) ++pi;
+  }
 };
+
+// Medium rows of at most 32 stored entries (most rows of the random family
+// hold 9-32) take eight lanes each, four rows per warp.  For such a row the
+// reference's warp association is fixed by live rank k alone: lane k holds
+// p[k] = 0.0 + term k (0.0 past the live length), and the shfl_down tree
+// 16,8,4,2,1 leaves in lane l < 8, after its first two steps,
+// (p[l] + p[l+16]) + (p[l+8] + p[l+24]); the tree 4,2,1 over those eight
+// lanes finishes the sum with the same roundings.  So lane l of a group forms
+// exactly that value and the group runs the last three steps.  Terms are
+// staged in shared memory at their live rank, so masked rows give the same
+// sums.
+constexpr int kGroupRowMax = 32;
 
 template <bool Plain>
 __global__ void __launch_bounds__(kThreads)
@@ -105,6 +136,8 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   __shared__ int warp_counts[8];
   __shared__ double dagg[8];
   __shared__ int iagg[8];
+  __shared__ double group_lo[(kThreads / 32) * 4 * kGroupRowMax];
+  __shared__ double group_hi[(kThreads / 32) * 4 * kGroupRowMax];
   const ActivityTerm<Plain> term{idx, val, lu, zero_tol, l2_hints()};
   const auto live_at = [&](offset_t p) { return !removed_column(term.bounds(p)); };
   const int b = blockIdx.x;
@@ -113,11 +146,30 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
       if (row_len(ptr, live_deg, i) > kShortRow) continue;
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
-      if (!keep_row || keep_row[i])
-        for (offset_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+      const offset_t first = ptr[i], last = ptr[i + 1];
+      if (keep_row && !keep_row[i]) {
+      } else if (last - first <= kShortRow) {
+        // All loads of the (at most 8) entries first, then the sequential sum.
+        int col[kShortRow];
+        double a[kShortRow];
+        double2 bnd[kShortRow];
+#pragma unroll
+        for (int k = 0; k < kShortRow; ++k) {
+          col[k] = first + k < last ? ld_stream(idx + first + k, term.hint.stream) : -1;
+          a[k] = first + k < last ? ld_stream(val + first + k, term.hint.stream) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < kShortRow; ++k)
+          bnd[k] = col[k] >= 0 ? ld_keep(lu + col[k], term.hint.keep) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int k = 0; k < kShortRow; ++k)
+          if (col[k] >= 0 && !removed_column(bnd[k])) term.add(a[k], bnd[k], lo, hi, ni, pi);
+      } else {
+        for (offset_t p = first; p < last; ++p) {
           const double2 bnd = term.bounds(p);
           if (!removed_column(bnd)) term(p, bnd, lo, hi, ni, pi);
         }
+      }
       min_fin[i] = lo; max_fin[i] = hi;
       if (min_inf) { min_inf[i] = ni; max_inf[i] = pi; }
     }
@@ -125,10 +177,12 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   }
   if (b < short_blocks + medium_blocks) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane >> 3, gl = lane & 7;
     const int nwarps = medium_blocks * (kThreads / 32);
     const int count = counts[0];
-    for (int q = (b - short_blocks) * (kThreads / 32) + warp; q < count; q += nwarps) {
-      const int row = medium[q];
+    double* glo = group_lo + (warp * 4 + grp) * kGroupRowMax;
+    double* ghi = group_hi + (warp * 4 + grp) * kGroupRowMax;
+    const auto full_row = [&](int row) {
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
       const offset_t first = ptr[row], last = ptr[row + 1];
@@ -140,6 +194,71 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
       if (lane == 0) {
         min_fin[row] = lo; max_fin[row] = hi;
         if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
+      }
+    };
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + warp) * 4; q0 < count; q0 += nwarps * 4) {
+      const int q = q0 + grp;
+      const bool have = q < count;
+      const int row = have ? medium[q] : 0;
+      const bool kept = have && (!keep_row || keep_row[row]);
+      const offset_t first = have ? ptr[row] : 0, last = have ? ptr[row + 1] : 0;
+      const bool grouped = have && (!kept || last - first <= kGroupRowMax);
+      const offset_t end = grouped && kept ? last : first;
+      // Every load of the row's (up to) four entries per lane first.
+      int col[4];
+      double a[4];
+      double2 bnd[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const offset_t p = first + gl + 8 * j;
+        col[j] = p < end ? ld_stream(idx + p, term.hint.stream) : -1;
+        a[j] = p < end ? ld_stream(val + p, term.hint.stream) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        bnd[j] = col[j] >= 0 ? ld_keep(lu + col[j], term.hint.keep) : make_double2(0.0, 0.0);
+      // Live mask over the group's 32 stored positions: bit (8j + gl) is
+      // stored entry gl + 8j.
+      unsigned live_mask = 0;
+      bool live[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        live[j] = col[j] >= 0 && !removed_column(bnd[j]);
+        live_mask |= ((__ballot_sync(0xffffffffu, live[j]) >> (grp * 8)) & 0xffu) << (8 * j);
+      }
+      int ni = 0, pi = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!live[j]) continue;
+        double plo, phi;
+        term.slot(a[j], bnd[j], plo, phi, ni, pi);
+        const int rank = __popc(live_mask & ((1u << (gl + 8 * j)) - 1u));
+        glo[rank] = plo;
+        ghi[rank] = phi;
+      }
+      __syncwarp();
+      const int nlive = __popc(live_mask);
+      const auto at = [&](const double* v, int r) { return r < nlive ? v[r] : 0.0; };
+      double lo = (at(glo, gl) + at(glo, gl + 16)) + (at(glo, gl + 8) + at(glo, gl + 24));
+      double hi = (at(ghi, gl) + at(ghi, gl + 16)) + (at(ghi, gl + 8) + at(ghi, gl + 24));
+      __syncwarp();
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) {
+        lo = lo + __shfl_down_sync(0xffffffffu, lo, off, 8);
+        hi = hi + __shfl_down_sync(0xffffffffu, hi, off, 8);
+        ni = ni + __shfl_down_sync(0xffffffffu, ni, off, 8);
+        pi = pi + __shfl_down_sync(0xffffffffu, pi, off, 8);
+      }
+      if (grouped && gl == 0) {
+        min_fin[row] = lo; max_fin[row] = hi;
+        if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
+      }
+      // Longer medium rows: one warp each, as before.
+      unsigned rest = __ballot_sync(0xffffffffu, have && !grouped && gl == 0);
+      while (rest) {
+        const int src = __ffs(rest) - 1;
+        rest &= rest - 1;
+        full_row(__shfl_sync(0xffffffffu, row, src));
       }
     }
     return;

@@ -68,12 +68,9 @@ __device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
   return RowCtx{g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i]};
 }
 
-__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p, const L2Hints& h) {
-  const int j = ld_stream(g.idx + p, h.stream);   // CSR streamed once: keep L2 for the gathered bounds
-  const double2 b = ld_keep(g.lu + j, h.keep);
-  if (removed_column(b)) return;
-  const double a = ld_stream(g.val + p, h.stream);
-  if (fabs(a) <= g.zero_tol) return;
+// Candidate bounds of column j from one entry a of a row (reference
+// :373-430); b holds the column's current bounds.
+__device__ __forceinline__ void candidate_update(const CandArgs& g, const RowCtx& rc, int j, double a, double2 b) {
   const double ol = b.x, ou = b.y;
   double il, iu;
   implied_bounds(a, ol, ou, rc.al, rc.au, rc.mn, rc.mx, rc.ni, rc.pi, il, iu);
@@ -95,6 +92,7 @@ __global__ void __launch_bounds__(kThreads)
 candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g) {
   __shared__ offset_t sptr[kTileRows + 1];
   const L2Hints hint = l2_hints();
+  constexpr int K = kEntryTile / kThreads;   // entries per thread and tile
   for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
     const offset_t last = min(nnz, base + kEntryTile) - 1;
     const int2 span = tile_rows[base / kEntryTile];   // rows of the tile's first and last entry
@@ -103,12 +101,31 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
     if (staged)
       for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
     __syncthreads();
-    for (int k = 0; k < kEntryTile / kThreads; ++k) {
+    // The thread's K entries are independent: issue every load of all K
+    // before using any (streamed index and value, the row of each entry,
+    // then the gathered column record and the row's sides and summary), so
+    // up to K dependent-load chains are in flight per thread instead of one.
+    int col[K], row[K];
+    double a[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
       const offset_t p = base + offset_t(k) * kThreads + threadIdx.x;
-      if (p > last) break;
-      const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
-      if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-      candidate_entry(g, row_ctx(g, i), p, hint);
+      const bool in = p <= last;
+      col[k] = in ? ld_stream(g.idx + p, hint.stream) : -1;
+      a[k] = in ? ld_stream(g.val + p, hint.stream) : 0.0;
+      row[k] = !in ? -1 : staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
+    }
+    double2 b[K];
+    bool use[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      use[k] = col[k] >= 0 && g.keep_row[row[k]] && g.row_nnz[row[k]] > 1;
+      b[k] = use[k] ? ld_keep(g.lu + col[k], hint.keep) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!use[k] || removed_column(b[k]) || fabs(a[k]) <= g.zero_tol) continue;
+      candidate_update(g, row_ctx(g, row[k]), col[k], a[k], b[k]);
     }
     __syncthreads();
   }
