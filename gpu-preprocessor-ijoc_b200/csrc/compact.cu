@@ -49,11 +49,17 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
   const int b = blockIdx.x;
   if (b < short_blocks) {
     for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
+      const offset_t first = ptr[r], last = ptr[r + 1];
+      if (last - first > kShortRow) continue;
       const int nr = outer_map[r];
       if (nr < 0) continue;
+      // All (at most 8) index loads, then all map gathers, in flight together.
+      int col[kShortRow];
+#pragma unroll
+      for (int k = 0; k < kShortRow; ++k) col[k] = first + k < last ? __ldcs(idx + first + k) : -1;
       int c = 0;
-      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p) c += inner_map[__ldcs(idx + p)] >= 0;
+#pragma unroll
+      for (int k = 0; k < kShortRow; ++k) c += col[k] >= 0 && inner_map[col[k]] >= 0;
       out_counts[nr] = c;
     }
     return;

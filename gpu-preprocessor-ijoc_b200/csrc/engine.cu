@@ -40,8 +40,6 @@ struct Engine {
   const gpp_params& p;
   PresolveOutput& out;
   WorkingLp cur;
-  bool at_sorted = false;     // rows of cur.AT strictly sorted (checked once for the input)
-  bool at_checked = false;
   bool terminal = false;
   bool active = false, pending = false;
   Plan plan;
@@ -154,13 +152,10 @@ struct Engine {
       next.AT = transpose_csr(next.A, s());
     } else {
       next.A = compact_csr(cur.A, rmap.p, m_new, cmap.p, n_new, s());
-      if (!at_checked) {
-        at_sorted = rows_strictly_sorted(cur.AT, s());
-        at_checked = true;
-      }
-      next.AT = at_sorted ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s()) : transpose_csr(next.A, s());
+      next.AT = cur.AT_sorted() ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s()) : transpose_csr(next.A, s());
+      next.a_sorted = cur.a_sorted;
     }
-    at_sorted = at_checked = true;
+    next.at_sorted = 1;
     next.c = dalloc<double>(size_t(n_new)); gather_by_map(next.c, pl.c.p, cmap.p, n, s());
     next.l = dalloc<double>(size_t(n_new)); gather_by_map(next.l, pl.l.p, cmap.p, n, s());
     next.u = dalloc<double>(size_t(n_new)); gather_by_map(next.u, pl.u.p, cmap.p, n, s());

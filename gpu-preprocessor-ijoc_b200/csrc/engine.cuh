@@ -101,11 +101,25 @@ struct Stats {
   DBuf<int32_t> deleted, counters;
 };
 
+bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s);
+
 struct WorkingLp {
   DevCsr A, AT;
   double *c = nullptr, *AL = nullptr, *AU = nullptr, *l = nullptr, *u = nullptr;
   double obj = 0.0;
   bool owns = false;
+  // Rows of A / AT strictly ascending: 1 yes, 0 no, -1 not checked yet.
+  // Compaction keeps a subsequence of every row, so it keeps the property;
+  // the transpose builds AT row-sorted.  Checked at most once per matrix.
+  mutable int a_sorted = -1, at_sorted = -1;
+  bool A_sorted() const {
+    if (a_sorted < 0) a_sorted = rows_strictly_sorted(A, ctx().stream) ? 1 : 0;
+    return a_sorted != 0;
+  }
+  bool AT_sorted() const {
+    if (at_sorted < 0) at_sorted = rows_strictly_sorted(AT, ctx().stream) ? 1 : 0;
+    return at_sorted != 0;
+  }
   int32_t m() const { return A.rows; }
   int32_t n() const { return A.cols; }
   void free_owned();

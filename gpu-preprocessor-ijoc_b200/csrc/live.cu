@@ -404,10 +404,20 @@ col_max_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __rest
   const int b = blockIdx.x;
   if (b < short_blocks) {
     for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      if (ptr[r + 1] - ptr[r] > kShortRow) continue;
+      const offset_t first = ptr[r], last = ptr[r + 1];
+      if (last - first > kShortRow) continue;
+      // All (at most 8) loads first; the max is order-free.
+      int row[kShortRow];
+      double a[kShortRow];
+#pragma unroll
+      for (int k = 0; k < kShortRow; ++k) {
+        row[k] = first + k < last ? __ldcs(idx + first + k) : -1;
+        a[k] = first + k < last ? __ldcs(val + first + k) : 0.0;
+      }
       double v = 0.0;
-      for (offset_t p = ptr[r]; p < ptr[r + 1]; ++p)
-        if (!keep_row || keep_row[idx[p]]) v = fmax(v, fabs(val[p]));
+#pragma unroll
+      for (int k = 0; k < kShortRow; ++k)
+        if (row[k] >= 0 && (!keep_row || keep_row[row[k]])) v = fmax(v, fabs(a[k]));
       out[r] = v;
     }
     return;

@@ -191,6 +191,9 @@ __global__ void finalize_kernel(int n, const uint8_t* __restrict__ keep_col, con
 }
 
 // Support rows and per-column tape sizes (reference :815-960, :970-1008).
+// Four columns per warp, eight lanes each: the lanes split a changed
+// column's entries; the support row is the smallest qualifying row, an
+// order-free minimum over the lanes.
 __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
                                const double* __restrict__ at_val, const uint8_t* __restrict__ keep_row,
                                const int32_t* __restrict__ row_nnz, const double* __restrict__ AL,
@@ -200,21 +203,33 @@ __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const
                                const double* __restrict__ fu, double zero_tol, double tol, double support_tol,
                                int32_t* __restrict__ sup_l, int32_t* __restrict__ sup_u,
                                int64_t* __restrict__ rec_count, int64_t* __restrict__ idx_count) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, g = lane & 7;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  for (int j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; j0 < n; j0 += nwarps * 4) {
+    const int j = j0 + (lane >> 3);
     int sl = INT_MAX, su = INT_MAX;
-    const bool nl = lch[j], nu = uch[j];
+    const bool nl = j < n && lch[j], nu = j < n && uch[j];
     if (nl || nu) {
-      for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) {
-        const int i = at_idx[p];
-        if (!keep_row[i] || row_nnz[i] <= 1) continue;
-        const double a = at_val[p];
-        if (fabs(a) <= zero_tol) continue;
-        double il, iu;
-        implied_bounds(a, l[j], u[j], AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
-        if (nl && fl[j] > l[j] + tol && isfinite(il) && fabs(il - fl[j]) <= support_tol) sl = min(sl, i);
-        if (nu && fu[j] < u[j] - tol && isfinite(iu) && fabs(iu - fu[j]) <= support_tol) su = min(su, i);
-      }
+      const double lj = l[j], uj = u[j], flj = fl[j], fuj = fu[j];
+      const bool want_l = nl && flj > lj + tol, want_u = nu && fuj < uj - tol;
+      if (want_l || want_u)
+        for (offset_t p = at_ptr[j] + g; p < at_ptr[j + 1]; p += 8) {
+          const int i = at_idx[p];
+          if (!keep_row[i] || row_nnz[i] <= 1) continue;
+          const double a = at_val[p];
+          if (fabs(a) <= zero_tol) continue;
+          double il, iu;
+          implied_bounds(a, lj, uj, AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
+          if (want_l && isfinite(il) && fabs(il - flj) <= support_tol) sl = min(sl, i);
+          if (want_u && isfinite(iu) && fabs(iu - fuj) <= support_tol) su = min(su, i);
+        }
     }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+      sl = min(sl, __shfl_down_sync(0xffffffffu, sl, off, 8));
+      su = min(su, __shfl_down_sync(0xffffffffu, su, off, 8));
+    }
+    if (g != 0 || j >= n) continue;
     sup_l[j] = sl;
     sup_u[j] = su;
     rec_count[j] = int64_t(nl) + int64_t(nu);
@@ -383,7 +398,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
     DBuf<int32_t> sl(size_t(n), s), su(size_t(n), s);
     DBuf<int64_t> rc(size_t(n) + 1, s), ic(size_t(n) + 1, s), rpos(size_t(n) + 1, s), ipos(size_t(n) + 1, s);
     const double support_tol = std::fmax(10.0 * p.bound_tol, 1.0e-10);
-    GPP_LAUNCH(support_kernel, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val,
+    GPP_LAUNCH(support_kernel, std::max(1, std::min((n + 31) / 32, kNumSMs * 16)), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val,
                plan.keep_row.p, stats.row_nnz.p, plan.AL.p, plan.AU.p, plan.l.p, plan.u.p, rs, lch.p, uch.p, fl.p,
                fu.p, p.zero_tol, p.bound_tol, support_tol, sl.p, su.p, rc.p, ic.p);
     exclusive_scan_i64(rc.p, rpos.p, n, s);

@@ -787,7 +787,7 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
   // The fill-in proxy walks columns in ascending row order (the reference
   // sorts AT in place when it is not, rule_doubleton_equations.cu:126-148).
   DevCsr sorted_at;
-  const bool at_sorted = rows_strictly_sorted(lp.AT, s);
+  const bool at_sorted = lp.AT_sorted();
   if (!at_sorted) sorted_at = transpose_csr(lp.A, s);
   const DevCsr& AT = at_sorted ? lp.AT : sorted_at;
   struct Release {
@@ -896,7 +896,7 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
                  dcol.p, dv.p, row_cnt.p);
     }
     exclusive_scan_i32(row_cnt.p, dptr.p, m, s);
-    const bool a_sorted = rows_strictly_sorted(lp.A, s);
+    const bool a_sorted = lp.A_sorted();
     DBuf<int32_t> cnt(size_t(m) + 1, s), long_rows(size_t(m), s), long_count(1, s);
     long_count.zero();
     if (a_sorted)

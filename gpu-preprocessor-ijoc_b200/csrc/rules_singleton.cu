@@ -114,24 +114,25 @@ struct CacheOut {
 };
 
 // _kernel_singleton_row_activity_cache (:555-614) for rows of live length
-// <= 1024: one warp per row loads 32 entries at a time.  The reference's
-// sequential loop skips a NaN term entirely, counts an infinite term and adds
-// a finite one; the counts and the NaN flag are order-free, so they come from
-// ballots, and the finite sums are formed in stored order by the same
-// shuffle-add chain on every lane.  A skipped term enters the chain as +0.0,
-// which is exact: a sum that starts at +0.0 never becomes -0.0 in
-// round-to-nearest, and x + (+0.0) == x for every other x.
+// <= 1024.  The reference's sequential loop skips a NaN term entirely, counts
+// an infinite term and adds a finite one; the counts and the NaN flag are
+// order-free, so they come from ballots, and the finite sums are formed in
+// stored order by the same shuffle-add chain on every lane of the row.  A
+// skipped term enters the chain as +0.0, which is exact: a sum that starts at
+// +0.0 never becomes -0.0 in round-to-nearest, and x + (+0.0) == x for every
+// other x.  Rows of at most 32 stored entries (nearly all) take eight lanes
+// each, four rows per warp, with all of a row's loads issued before its
+// chain; longer rows take a whole warp, 32 entries at a time.
 __global__ void sc_cache_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ st,
                               const int32_t* __restrict__ row_nnz, const offset_t* __restrict__ ptr,
                               const int32_t* __restrict__ idx, const double* __restrict__ val,
                               const uint8_t* __restrict__ keep_col, const double* __restrict__ l,
                               const double* __restrict__ u, CacheOut out) {
   const int count = st[kStRows];
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, grp = lane >> 3, gl = lane & 7;
   const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < count; w += warps) {
-    const int row = rows[w];
-    if (row_nnz[row] > kLongRow) continue;
+  const auto group_bits = [&](bool v) { return (__ballot_sync(0xffffffffu, v) >> (grp * 8)) & 0xffu; };
+  const auto whole_row = [&](int row) {
     RowCache r{0.0, 0.0, 0, 0, 0, 0, 0};
     const offset_t end = ptr[row + 1];
     for (offset_t chunk = ptr[row]; chunk < end; chunk += 32) {
@@ -163,6 +164,57 @@ __global__ void sc_cache_rows(const int32_t* __restrict__ rows, const int32_t* _
       }
     }
     if (lane == 0) out.store(row, r);
+  };
+  for (int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; w0 < count; w0 += warps * 4) {
+    const int w = w0 + grp;
+    const int row = w < count ? rows[w] : 0;
+    const bool take = w < count && row_nnz[row] <= kLongRow;
+    const offset_t first = take ? ptr[row] : 0, end = take ? ptr[row + 1] : 0;
+    const bool grouped = take && end - first <= 32;
+    const offset_t stop = grouped ? end : first;
+    int col[4];
+    double a[4], lj[4], uj[4];
+    bool live[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const offset_t p = first + gl + 8 * j;
+      col[j] = p < stop ? __ldcs(idx + p) : -1;
+      a[j] = p < stop ? __ldcs(val + p) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) live[j] = col[j] >= 0 && keep_col[col[j]];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      lj[j] = live[j] ? l[col[j]] : 0.0;
+      uj[j] = live[j] ? u[col[j]] : 0.0;
+    }
+    RowCache r{0.0, 0.0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double tmin = live[j] ? (a[j] >= 0.0 ? a[j] * lj[j] : a[j] * uj[j]) : 0.0;
+      const double tmax = live[j] ? (a[j] >= 0.0 ? a[j] * uj[j] : a[j] * lj[j]) : 0.0;
+      const bool nan = live[j] && (isnan(tmin) || isnan(tmax));
+      const bool counted = live[j] && !nan;
+      r.invalid |= group_bits(nan) != 0;
+      r.min_neg += __popc(group_bits(counted && isinf(tmin) && tmin < 0.0));
+      r.min_pos += __popc(group_bits(counted && isinf(tmin) && tmin > 0.0));
+      r.max_neg += __popc(group_bits(counted && isinf(tmax) && tmax < 0.0));
+      r.max_pos += __popc(group_bits(counted && isinf(tmax) && tmax > 0.0));
+      const double fmin_term = counted && isfinite(tmin) ? tmin : 0.0;
+      const double fmax_term = counted && isfinite(tmax) ? tmax : 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        r.fmin += __shfl_sync(0xffffffffu, fmin_term, k, 8);
+        r.fmax += __shfl_sync(0xffffffffu, fmax_term, k, 8);
+      }
+    }
+    if (grouped && gl == 0) out.store(row, r);
+    unsigned rest = __ballot_sync(0xffffffffu, take && !grouped && gl == 0);
+    while (rest) {
+      const int src = __ffs(rest) - 1;
+      rest &= rest - 1;
+      whole_row(__shfl_sync(0xffffffffu, row, src));
+    }
   }
 }
 
@@ -568,7 +620,7 @@ void rule_singleton_columns(Plan& plan, const WorkingLp& lp, const Stats& stats,
   DBuf<int4> counts(size_t(m), s);
   DBuf<uint8_t> invalid(size_t(m), s);
   const CacheOut cache{fmin.p, fmax.p, counts.p, invalid.p};
-  const int warp_blocks = std::max(1, std::min((nrows + 7) / 8, kNumSMs * 16));
+  const int warp_blocks = std::max(1, std::min((nrows + 31) / 32, kNumSMs * 16));
   GPP_LAUNCH(sc_cache_rows, warp_blocks, kThreads, 0, s, rows.p, st.d, stats.row_nnz.p, lp.A.ptr, lp.A.idx,
              lp.A.val, plan.keep_col.p, plan.l.p, plan.u.p, cache);
   if (f[kStLong])

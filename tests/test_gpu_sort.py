@@ -12,11 +12,13 @@ def test_radix_sort_pairs_matches_numpy():
     from gpp_b200 import capi
     lib = capi.load()
     rng = np.random.default_rng(0)
-    for n in (1, 7, 2048, 2049, 100_003):
+    # Up to 4096 pairs one block sorts them; above, the radix passes do.
+    for n in (1, 3, 7, 2048, 2049, 4096, 4097, 100_003):
         keys = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
         keys[rng.random(n) < 0.3] = keys[0]        # many duplicates: stability matters
         keys[: n // 10] &= np.uint64(0xFFFF)        # some small keys: skipped passes
-        vals = np.arange(n, dtype=np.int32)
+        keys[rng.random(n) < 0.05] |= np.uint64(1 << 63)   # unsigned order
+        vals = (np.arange(n, dtype=np.int32) * 7919) % max(n, 1)
         dk = torch.from_numpy(keys.view(np.int64)).cuda()
         dv = torch.from_numpy(vals).cuda()
         assert lib.gpp_sort_pairs(C.c_void_p(dk.data_ptr()), C.c_void_p(dv.data_ptr()), n) == 0
