@@ -13,6 +13,7 @@
 #include "sort.hpp"
 
 #include <algorithm>
+#include <utility>
 
 namespace gpp {
 
@@ -278,6 +279,83 @@ __global__ void compose_kernel(int32_t* __restrict__ next, const int32_t* __rest
 
 int roles_long(int rows) { return std::min<int>(kNumSMs * 4, rows); }
 
+// Old -> new maps of the row and the column masks together, straight from
+// the byte masks: one launch counts the kept items of every tile of
+// kMapTile items (row tiles first, then column tiles), a second gives each
+// kept item its rank (earlier tiles' counts plus a block scan) and writes -1
+// for a dropped one; the last tile of each mask writes its total.
+constexpr int kMapTile = 8 * kThreads;
+
+__device__ __forceinline__ int block_sum_i32(int v, int* sh) {
+  for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+  __syncthreads();
+  return t;
+}
+
+struct MaskPair {
+  const uint8_t* keep[2];
+  int32_t n[2];
+  int32_t tiles0;          // tiles of the first mask; the second's follow
+  int32_t* map[2];
+};
+
+__global__ void __launch_bounds__(kThreads) map_tile_counts(MaskPair mp, int32_t* __restrict__ tile_counts) {
+  __shared__ int sh[kThreads / 32];
+  const int side = int(blockIdx.x) < mp.tiles0 ? 0 : 1;
+  const int tile = side ? int(blockIdx.x) - mp.tiles0 : int(blockIdx.x);
+  const int64_t base = int64_t(tile) * kMapTile + int64_t(threadIdx.x) * 8;
+  int c = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c += base + k < mp.n[side] && mp.keep[side][base + k] != 0;
+  c = block_sum_i32(c, sh);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = c;
+}
+
+__global__ void __launch_bounds__(kThreads) map_tile_ranks(MaskPair mp, const int32_t* __restrict__ tile_counts,
+                                                           int32_t* __restrict__ totals) {
+  __shared__ int sh[kThreads / 32];
+  __shared__ int warp_incl[kThreads / 32];
+  const int side = int(blockIdx.x) < mp.tiles0 ? 0 : 1;
+  const int first_tile = side ? mp.tiles0 : 0;
+  const int tile = int(blockIdx.x) - first_tile;
+  int offset = 0;
+  for (int k = first_tile + int(threadIdx.x); k < int(blockIdx.x); k += kThreads) offset += tile_counts[k];
+  offset = block_sum_i32(offset, sh);
+  const int64_t base = int64_t(tile) * kMapTile + int64_t(threadIdx.x) * 8;
+  const uint8_t* keep = mp.keep[side];
+  const int32_t n = mp.n[side];
+  uint8_t kept[8];
+  int local = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    kept[k] = base + k < n && keep[base + k] != 0;
+    local += kept[k];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = local;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int peer = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += peer;
+  }
+  if (lane == 31) warp_incl[warp] = incl;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_incl[w];
+  int run = offset + before + incl - local;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (base + k < n) {
+      mp.map[side][base + k] = kept[k] ? run : -1;
+      run += kept[k];
+    }
+  const int tiles_side = side ? int(gridDim.x) - mp.tiles0 : mp.tiles0;
+  if (tile == tiles_side - 1 && threadIdx.x == kThreads - 1) totals[side] = run;
+}
+
 }  // namespace
 
 int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cudaStream_t s) {
@@ -289,8 +367,23 @@ int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cu
   return read_scalar(prefix.p + n);
 }
 
+std::pair<int32_t, int32_t> build_old_to_new_pair(const uint8_t* keep_row, int32_t m, int32_t* row_map,
+                                                  const uint8_t* keep_col, int32_t n, int32_t* col_map,
+                                                  cudaStream_t s) {
+  const int32_t tr = (m + kMapTile - 1) / kMapTile, tc = (n + kMapTile - 1) / kMapTile;
+  if (tr + tc == 0) return {0, 0};
+  MaskPair mp{{keep_row, keep_col}, {m, n}, tr, {row_map, col_map}};
+  DBuf<int32_t> counts(size_t(tr + tc), s);
+  Status st;
+  st.clear(2);   // a mask of no items keeps its total at 0
+  GPP_LAUNCH(map_tile_counts, tr + tc, kThreads, 0, s, mp, counts.p);
+  GPP_LAUNCH(map_tile_ranks, tr + tc, kThreads, 0, s, mp, counts.p, st.d);
+  const int32_t* t = st.read(2);
+  return {t[0], t[1]};
+}
+
 DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
-                   int32_t inner_new, cudaStream_t s) {
+                   int32_t inner_new, cudaStream_t s, int64_t known_nnz) {
   DevCsr out;
   out.rows = outer_new;
   out.cols = inner_new;
@@ -310,7 +403,7 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
   GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map,
                    sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
   exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
-  out.nnz = read_scalar(out.ptr + outer_new);
+  out.nnz = known_nnz >= 0 ? offset_t(known_nnz) : read_scalar(out.ptr + outer_new);
   out.idx = dalloc<int32_t>(size_t(out.nnz));
   out.val = dalloc<double>(size_t(out.nnz));
   const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +

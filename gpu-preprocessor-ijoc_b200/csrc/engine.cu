@@ -144,15 +144,15 @@ struct Engine {
       return;
     }
     DBuf<int32_t> rmap(size_t(std::max(m, 1)), s()), cmap(size_t(std::max(n, 1)), s());
-    const int m_new = build_old_to_new(pl.keep_row.p, m, rmap.p, s());
-    const int n_new = build_old_to_new(pl.keep_col.p, n, cmap.p, s());
+    const auto [m_new, n_new] = build_old_to_new_pair(pl.keep_row.p, m, rmap.p, pl.keep_col.p, n, cmap.p, s());
     WorkingLp next;
     if (pl.has_new_A) {
       next.A = compact_csr(pl.new_A, rmap.p, m_new, cmap.p, n_new, s());
       next.AT = transpose_csr(next.A, s());
     } else {
       next.A = compact_csr(cur.A, rmap.p, m_new, cmap.p, n_new, s());
-      next.AT = cur.AT_sorted() ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s()) : transpose_csr(next.A, s());
+      next.AT = cur.AT_sorted() ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s(), next.A.nnz)
+                                : transpose_csr(next.A, s());
       next.a_sorted = cur.a_sorted;
     }
     next.at_sorted = 1;

@@ -149,9 +149,17 @@ void col_max_abs(const DevCsr& AT, const uint8_t* keep_row, double* out, cudaStr
 
 // compact.cu
 int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cudaStream_t s);
+// Both maps of a materialisation at once (two launches, one readback); returns
+// the kept row and column counts.
+std::pair<int32_t, int32_t> build_old_to_new_pair(const uint8_t* keep_row, int32_t m, int32_t* row_map,
+                                                  const uint8_t* keep_col, int32_t n, int32_t* col_map,
+                                                  cudaStream_t s);
 // Stable compaction of M's kept rows (outer map) and kept entries (inner map).
+// `known_nnz` >= 0 is the compacted nnz when the caller knows it (the
+// transpose side of a materialisation keeps exactly the entries A keeps),
+// which saves the readback.
 DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
-                   const int32_t* inner_map, int32_t inner_new, cudaStream_t s);
+                   const int32_t* inner_map, int32_t inner_new, cudaStream_t s, int64_t known_nnz = -1);
 // General transpose (histogram, scan, scatter, per-row sort): rows of the
 // result list source rows in ascending order.
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s);
