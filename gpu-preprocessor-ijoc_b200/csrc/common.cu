@@ -37,6 +37,7 @@ Context::Context() {
   check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool threshold");
   check(cudaMallocHost(reinterpret_cast<void**>(&host_status), sizeof(int32_t) * kStatusWords),
         "cudaMallocHost status");
+  check(cudaMallocHost(reinterpret_cast<void**>(&host_scalar), 16), "cudaMallocHost scalar");
 }
 
 void Context::sync(const char* label) {
@@ -52,6 +53,7 @@ void Context::sync(const char* label) {
 
 Context::~Context() {
   if (host_status) cudaFreeHost(host_status);
+  if (host_scalar) cudaFreeHost(host_scalar);
   if (stream) cudaStreamDestroy(stream);
 }
 

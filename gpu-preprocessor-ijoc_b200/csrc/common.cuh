@@ -205,6 +205,7 @@ struct Context {
   int device = -1;
   cudaMemPool_t pool = nullptr;   // this context's own stream-ordered pool
   int32_t* host_status = nullptr;   // pinned, kStatusWords ints
+  unsigned char* host_scalar = nullptr;   // pinned, 16 bytes for scalar readbacks
   static constexpr int kStatusWords = 64;
   Context();
   ~Context();
@@ -291,10 +292,30 @@ std::vector<T> to_host(const T* d, size_t count) {
 }
 template <class T>
 T read_scalar(const T* d) {
-  T v{};
-  check(cudaMemcpyAsync(&v, d, sizeof(T), cudaMemcpyDeviceToHost, ctx().stream), "d2h scalar");
-  ctx().sync("d2h scalar sync");
+  // Through the context's pinned block: a pageable destination would make
+  // the copy go through a staging buffer.
+  static_assert(sizeof(T) <= 8, "scalar");
+  auto& c = ctx();
+  check(cudaMemcpyAsync(c.host_scalar, d, sizeof(T), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
+  c.sync("d2h scalar sync");
+  T v;
+  std::memcpy(&v, c.host_scalar, sizeof(T));
   return v;
+}
+// Two scalars (say the totals of two scans) with one wait.
+template <class T, class U>
+std::pair<T, U> read_scalars(const T* a, const U* b) {
+  static_assert(sizeof(T) <= 8 && sizeof(U) <= 8, "scalar");
+  auto& c = ctx();
+  unsigned char* h = c.host_scalar;
+  check(cudaMemcpyAsync(h, a, sizeof(T), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
+  check(cudaMemcpyAsync(h + 8, b, sizeof(U), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
+  c.sync("d2h scalar sync");
+  T va;
+  U vb;
+  std::memcpy(&va, h, sizeof(T));
+  std::memcpy(&vb, h + 8, sizeof(U));
+  return {va, vb};
 }
 
 // Status block: device ints zeroed per use, read back with one copy.

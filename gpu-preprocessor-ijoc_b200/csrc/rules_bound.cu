@@ -403,7 +403,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                fu.p, p.zero_tol, p.bound_tol, support_tol, sl.p, su.p, rc.p, ic.p);
     exclusive_scan_i64(rc.p, rpos.p, n, s);
     exclusive_scan_i64(ic.p, ipos.p, n, s);
-    const int64_t recs = read_scalar(rpos.p + n), nidx = read_scalar(ipos.p + n);
+    const auto [recs, nidx] = read_scalars(rpos.p + n, ipos.p + n);
     if (recs) {
       PostsolveSegment seg = make_segment(recs, nidx, 4 * recs);
       GPP_LAUNCH(pack_bound_records, grid_stride_blocks(n), kThreads, 0, s, n, lch.p, uch.p, sl.p, su.p, plan.l.p,
@@ -426,7 +426,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                plan.keep_row.p, rc.p, nz.p);
     exclusive_scan_i64(rc.p, rpos.p, n, s);
     exclusive_scan_i64(nz.p, npos.p, n, s);
-    const int64_t recs = read_scalar(rpos.p + n), nnz = read_scalar(npos.p + n);
+    const auto [recs, nnz] = read_scalars(rpos.p + n, npos.p + n);
     PostsolveSegment seg = make_segment(recs, recs + nnz, 2 * recs + nnz);
     DBuf<double> oc(size_t(recs), s), ov(size_t(recs), s);
     GPP_LAUNCH(fixed_record_pack, grid_stride_blocks(n), kThreads, 0, s, n, fx.p, lp.AT.ptr, lp.AT.idx, lp.AT.val,

@@ -673,7 +673,7 @@ void rule_parallel_columns(Plan& plan, const WorkingLp& lp, const Stats&, const 
                  rc.p, nz.p);
       exclusive_scan_i64(rc.p, rpos.p, n, s);
       exclusive_scan_i64(nz.p, npos.p, n, s);
-      const int64_t recs = read_scalar(rpos.p + n), nnz = read_scalar(npos.p + n);
+      const auto [recs, nnz] = read_scalars(rpos.p + n, npos.p + n);
       PostsolveSegment seg = make_segment(recs, recs + nnz, 2 * recs + nnz);
       GPP_LAUNCH(fixed_pack, grid_stride_blocks(n), kThreads, 0, s, n, fixed.p, lp.AT.ptr, lp.AT.idx, lp.AT.val,
                  plan.keep_row.p, fval.p, plan.c.p, rpos.p, npos.p, seg.types.p, seg.is.p, seg.vs.p, seg.idx.p,

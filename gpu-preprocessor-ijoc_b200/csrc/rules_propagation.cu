@@ -249,7 +249,7 @@ void rule_dual_fix(Plan& plan, const WorkingLp& lp, const Stats& stats, const gp
                plan.rule_entry_keep_col, lp.A.ptr, lp.A.idx, lp.AT.ptr, lp.AT.idx, rc.p, sz.p);
     exclusive_scan_i64(rc.p, rpos.p, n, s);
     exclusive_scan_i64(sz.p, spos.p, n, s);
-    const int64_t recs = read_scalar(rpos.p + n), size = read_scalar(spos.p + n);
+    const auto [recs, size] = read_scalars(rpos.p + n, spos.p + n);
     if (recs) {
       PostsolveSegment seg = make_segment(recs, size + 3 * recs, size + recs);
       GPP_LAUNCH(infinite_pack, grid_stride_blocks(n), kThreads, 0, s, n, fixed.p, inf_fix.p, fval.p, plan.keep_row.p,

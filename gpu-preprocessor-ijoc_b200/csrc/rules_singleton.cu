@@ -671,7 +671,8 @@ void rule_singleton_columns(Plan& plan, const WorkingLp& lp, const Stats& stats,
                  plan.keep_col.p, p.zero_tol, sel.p, sup.p);
       exclusive_scan_i32(sel.p, rec.p, nelim, s);
       exclusive_scan_i64(sup.p, spos.p, nelim, s);
-      const int64_t recs = read_scalar(rec.p + nelim), support = read_scalar(spos.p + nelim);
+      const auto [recs32, support] = read_scalars(rec.p + nelim, spos.p + nelim);
+      const int64_t recs = recs32;
       if (recs) {
         PostsolveSegment seg = make_segment(recs, 3 * recs + support, 6 * recs + support);
         GPP_LAUNCH(sc_sub_pack, blocks, kThreads, 0, s, sorted.p, nelim, owner.p, kind.p, sel.p, rec.p, spos.p,

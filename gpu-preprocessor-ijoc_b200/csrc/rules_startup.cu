@@ -499,7 +499,7 @@ void commit_projection(Plan& plan, const WorkingLp& lp, const gpp_params& p, con
     exclusive_scan_i64(rc.p, rpos.p, n, s);
     exclusive_scan_i64(sc.p, spos.p, n, s);
     if (st.read(1)[0]) throw std::runtime_error("projection tape certificate changed before commit");
-    const int64_t recs = read_scalar(rpos.p + n), support = read_scalar(spos.p + n);
+    const auto [recs, support] = read_scalars(rpos.p + n, spos.p + n);
     if (recs) {
       PostsolveSegment seg = make_segment(recs, int64_t(K + 8) * recs + support, 2 * recs + support);
       GPP_LAUNCH(projection_pack<K>, grid_stride_blocks(n), kThreads, 0, s, n, in, selected.p, incident, rpos.p,
