@@ -270,6 +270,48 @@ def run_batched(indices, lps, params, max_workers, rank=0, world=1, group=None):
                       "reduced solutions all-zero"}
 
 
+def reference_gpu(lp, point, steps, warmup, presolve_ms, postsolve_ms):
+    """The reference GPU library (built from its sources into
+    oracle/_ref/ref_driver) on the same LP, B200 and parameters: `warmup` +
+    `steps` presolves (device sync before and after each; the mean over the
+    timed ones), then one postprocess of the same reduced point."""
+    from gpp_b200 import lpgen
+    from gpp_b200.capi import RULE_FLAGS
+    driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(driver):
+        return {"unavailable": "oracle/_ref/ref_driver was not built (needs the reference sources at build time)"}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "lp.bin")
+        lpgen.save_lp(path, lp)
+        files = []
+        for name, v in zip(("x", "y", "z"), point):
+            files.append(os.path.join(d, name))
+            v.astype("float64").tofile(files[-1])
+        args = [driver, path, d, "enable_folding=1"]
+        args += [f"{f}={1 if f[len('enable_'):] in RULES else 0}" for f in RULE_FLAGS]
+        args += ["--repeat", str(warmup + steps), "--postsolve", *files]
+        r = subprocess.run(args, capture_output=True, text=True)
+        if r.returncode != 0:
+            return {"unavailable": "ref_driver failed: " + (r.stderr.strip().splitlines() or ["?"])[-1]}
+        meta = {}
+        for line in open(os.path.join(d, "meta.txt")):
+            k, *v = line.split()
+            meta[k] = v
+    wall = [float(v) for v in meta["wall_seconds"]][warmup:]
+    ref_pre = 1e3 * statistics.mean(wall)
+    ref_post = 1e3 * float(meta["postsolve_seconds"][0])
+    return {"presolve_ms": round(ref_pre, 3), "postsolve_ms": round(ref_post, 3),
+            "preprocessing_seconds_last": float(meta["preprocessing_seconds"][0]),
+            "reduced": {"rows": int(meta["reduced_rows"][0]), "cols": int(meta["reduced_cols"][0]),
+                        "nnz": int(meta["reduced_nnz"][0]), "iterations": int(meta["iterations"][0])},
+            "presolve_speedup": round(ref_pre / presolve_ms, 2),
+            "postsolve_speedup": round(ref_post / postsolve_ms, 2),
+            "timing": f"wall time of gpu_preprocessor::preprocess with device syncs, mean of {len(wall)} after "
+                      f"{warmup} warm-up; one postprocess (host outputs, first call) of the bench's reduced point; "
+                      f"this engine's postsolve_ms is device outputs",
+            "build": "reference library compiled from its sources with nvcc 12.9 -O3 for sm_100 (oracle/ref.mk)"}
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -92,10 +92,19 @@ def reduced_point(got, rows, cols, seed=1):
     return lo + rng.random(cols) * (hi - lo), rng.standard_normal(rows), rng.standard_normal(cols)
 
 
+# Recovered solutions are compared at 1e-9 relative (the objective too).  The
+# reference is compiled with floating-point contraction on (nvcc's default),
+# so its doubleton replay x_elim = beta + alpha * x_keep is one fused rounding
+# where this engine (and its oracle) round twice; where the two terms nearly
+# cancel the difference grows past 1e-12: on the 29.8M-nnz LP, 2 of 5,000,000
+# entries differ by 1.7e-12 and 1.5e-12 relative, with the objective equal.
+POSTSOLVE_REL = 1e-9
+
+
 def check_against_reference(lp, rules, extra=None, oracle=True, postsolve=False):
     """Presolves `lp` with the engine and with the reference library and
     requires drop-in parity.  With `postsolve`, both also postprocess the same
-    reduced point, and the recovered x, y, z must agree within 1e-12 relative
+    reduced point, and the recovered x, y, z must agree within POSTSOLVE_REL
     and give the same objective within 1e-9 relative.  `postsolve` is True for
     a seeded point inside the reduced bounds, or a function (result, summary)
     -> (x, y, z) giving the point."""
@@ -131,7 +140,7 @@ def check_against_reference(lp, rules, extra=None, oracle=True, postsolve=False)
         if postsolve:
             x, y, z = device.postprocess(*(torch.from_numpy(v).cuda() for v in point), s, dlp)
             for k, v in (("x_org", x), ("y_org", y), ("z_org", z)):
-                assert close(v, ref[k]), k
+                assert close(v, ref[k], POSTSOLVE_REL), k
             obj, obj_ref = float(lp.c @ x), float(lp.c @ ref["x_org"])
             assert abs(obj - obj_ref) <= 1e-9 * max(1.0, abs(obj_ref))
             got.solution = (x, y, z)
