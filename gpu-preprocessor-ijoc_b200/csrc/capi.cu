@@ -803,15 +803,25 @@ int gpp_preprocess_traced(const gpp_lp* lp, const gpp_params* params, gpp_summar
   });
 }
 
-int gpp_schedule_model_create(const float* params, double skip_below, double stop_above,
-                              gpp_schedule_model** out) {
+int gpp_schedule_model_create_per_rule(const float* params, const double* skip_below, double stop_above,
+                                       gpp_schedule_model** out) {
   return guarded([&] {
-    if (!params || !out || !(skip_below >= 0.0 && skip_below <= 1.0) || !(stop_above >= 0.0))
+    if (!params || !out || !skip_below || !(stop_above >= 0.0))
       throw std::invalid_argument("gpp_schedule_model_create: null argument or threshold out of range");
+    for (int g = 0; g < gpp::kGatedRules; ++g)
+      if (!(skip_below[g] >= 0.0 && skip_below[g] <= 1.0))
+        throw std::invalid_argument("gpp_schedule_model_create: skip threshold out of range");
     auto m = std::make_unique<gpp_schedule_model>();
     m->policy = std::make_unique<gpp::MlpSchedule>(params, skip_below, stop_above);
     *out = m.release();
   });
+}
+
+int gpp_schedule_model_create(const float* params, double skip_below, double stop_above,
+                              gpp_schedule_model** out) {
+  double each[gpp::kGatedRules];
+  std::fill(each, each + gpp::kGatedRules, skip_below);
+  return gpp_schedule_model_create_per_rule(params, each, stop_above, out);
 }
 
 void gpp_schedule_model_free(gpp_schedule_model* model) { delete model; }

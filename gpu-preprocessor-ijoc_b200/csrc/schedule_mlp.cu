@@ -263,8 +263,8 @@ void mlp_train(float* params, const float* X, const float* Y, const float* M, in
 
 // ---- the policy ---------------------------------------------------------------
 
-MlpSchedule::MlpSchedule(const float* params, double skip_below, double stop_above)
-    : skip_below_(skip_below), stop_above_(stop_above) {
+MlpSchedule::MlpSchedule(const float* params, const double* skip_below, double stop_above) : stop_above_(stop_above) {
+  std::copy(skip_below, skip_below + kGatedRules, skip_below_);
   auto s = ctx().stream;
   weights_.alloc(size_t(kScheduleParams), s);
   check(cudaMemcpyAsync(weights_.p, params, sizeof(float) * kScheduleParams, cudaMemcpyHostToDevice, s), "weights");
@@ -288,7 +288,7 @@ uint32_t MlpSchedule::decide(const float* features, bool* stop) {
   const float* p = host + kScheduleFeatures;
   uint32_t skip = 0;
   for (int g = 0; g < kGatedRules; ++g)
-    if (double(p[g]) < skip_below_) skip |= 1u << g;
+    if (double(p[g]) < skip_below_[g]) skip |= 1u << g;
   *stop = stop_above_ < 1.0 && double(p[kGatedRules]) > stop_above_;
   ++decisions_;
   return skip;

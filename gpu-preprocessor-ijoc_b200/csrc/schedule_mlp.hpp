@@ -22,17 +22,18 @@ void mlp_forward(const float* params, const float* X, int64_t n, float* probs);
 void mlp_gradients(const float* params, const float* X, const float* Y, const float* M, int64_t n, float* grads,
                    float* loss);
 
-// Skips gated rule g when its probability is below `skip_below`; stops when
-// the stop probability is above `stop_above` (never when stop_above >= 1).
+// Skips gated rule g when its probability is below `skip_below[g]`; stops
+// when the stop probability is above `stop_above` (never when stop_above >= 1).
 class MlpSchedule final : public SchedulePolicy {
  public:
-  MlpSchedule(const float* params, double skip_below, double stop_above);
+  MlpSchedule(const float* params, const double* skip_below, double stop_above);
   uint32_t decide(const float* features, bool* stop) override;
   int64_t decisions() const { return decisions_; }
 
  private:
   DBuf<float> weights_;
-  double skip_below_, stop_above_;
+  double skip_below_[kGatedRules];
+  double stop_above_;
   int64_t decisions_ = 0;
 };
 

@@ -176,6 +176,7 @@ def load():
         "gpp_reduced_to_host": (C.c_int, [P(Summary)] + [vp] * 9),
         "gpp_schedule_model_create": (C.c_int, [vp, C.c_double, C.c_double, P(vp)]),
         "gpp_schedule_model_free": (None, [vp]),
+        "gpp_schedule_model_create_per_rule": (C.c_int, [vp, vp, C.c_double, P(vp)]),
         "gpp_preprocess_scheduled": (C.c_int, [P(Lp), P(Params), vp, P(Summary)]),
         "gpp_mlp_train": (C.c_int, [vp, vp, vp, vp, i64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, vp]),
         "gpp_mlp_forward": (C.c_int, [vp, vp, i64, vp]),
@@ -205,7 +206,8 @@ EXPORTED = [
     "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
     "gpp_mps_read", "gpp_mps_read_string", "gpp_mps_info", "gpp_mps_arrays", "gpp_mps_free", "gpp_mps_upload",
     "gpp_lp_free", "gpp_export_reduced", "gpp_reduced_to_device", "gpp_reduced_to_host",
-    "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free", "gpp_preprocess_scheduled",
+    "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free",
+    "gpp_schedule_model_create_per_rule", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
 ]
 

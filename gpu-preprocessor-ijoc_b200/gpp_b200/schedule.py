@@ -121,29 +121,36 @@ def keep_all_params():
 
 
 def save_model(path, params, skip_below, stop_above, **info):
-    """Parameters, the two decision thresholds and training notes in one .npz."""
-    np.savez(path, params=np.asarray(params, np.float32), skip_below=np.float64(skip_below),
+    """Parameters, the decision thresholds (skip: one value, or one per gated
+    rule) and training notes in one .npz."""
+    np.savez(path, params=np.asarray(params, np.float32), skip_below=np.asarray(skip_below, np.float64),
              stop_above=np.float64(stop_above), **{k: np.asarray(v) for k, v in info.items()})
 
 
 def load_model(path=MODEL_FILE):
-    """(parameters, skip_below, stop_above) of a saved schedule model."""
+    """(parameters, skip_below, stop_above) of a saved schedule model;
+    skip_below is a float or a list of one threshold per gated rule."""
     with np.load(path) as z:
         w = z["params"].astype(np.float32)
-        skip_below, stop_above = float(z["skip_below"]), float(z["stop_above"])
+        sb = np.asarray(z["skip_below"], np.float64)
+        skip_below = float(sb) if sb.ndim == 0 else [float(v) for v in sb]
+        stop_above = float(z["stop_above"])
     if w.size != PARAMS:
         raise ValueError(f"{path}: {w.size} parameters, expected {PARAMS}")
     return w, skip_below, stop_above
 
 
 class Model:
-    """gpp_schedule_model_create / gpp_schedule_model_free."""
+    """gpp_schedule_model_create(_per_rule) / gpp_schedule_model_free.
+    skip_below: one threshold for every gated rule, or one per rule."""
 
     def __init__(self, params, skip_below=0.5, stop_above=0.5):
         self.w = np.ascontiguousarray(params, np.float32)
         self.h = C.c_void_p()
-        _raise(capi.load().gpp_schedule_model_create(_p(self.w), float(skip_below), float(stop_above),
-                                                     C.byref(self.h)))
+        sb = np.ascontiguousarray(np.broadcast_to(np.asarray(skip_below, np.float64), (len(GATED_RULES),)))
+        self.skip_below = sb
+        _raise(capi.load().gpp_schedule_model_create_per_rule(_p(self.w), _p(sb), float(stop_above),
+                                                              C.byref(self.h)))
 
     def close(self):
         if self.h:

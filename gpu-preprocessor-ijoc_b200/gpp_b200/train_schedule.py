@@ -10,11 +10,11 @@
    round).
 2. Trains the schedule MLP on the rounds of all traces (the library's CUDA
    kernels; Adam, masked binary cross-entropy).
-3. Chooses the two decision thresholds on held-out LPs (skip a rule below
-   one probability, stop above another): the pair with the least total
-   presolve time among those that keep at least 98% of the plain run's nnz
-   removal on every held-out LP (the plain loop -- skip nothing, never stop
-   -- if none does).
+3. Chooses the decision thresholds on held-out LPs (skip a gated rule below
+   its own probability threshold, stop above another), searching greedily
+   for the least total presolve time that keeps at least 98% of the plain
+   run's nnz removal on every held-out LP (the plain loop -- skip nothing,
+   never stop -- if nothing does).
 4. Writes parameters, thresholds and training notes to --out.
 """
 from __future__ import annotations
@@ -66,6 +66,42 @@ def removal(lp, s):
     return lp.nnz - s.reduced_nnz
 
 
+def choose_thresholds(evaluate, rules):
+    """Decision thresholds on held-out LPs.  `evaluate(skip, stop)` gives
+    (time ratio, smallest kept share) for one skip threshold per gated rule.
+    First the stop threshold with no rule skipped; then, rule by rule, the
+    skip threshold that lowers the time most while every held-out LP keeps at
+    least KEEP_SHARE of its plain removal; then the stop threshold again for
+    the chosen skips.  Returns (skip per rule, stop, table of every try)."""
+    table = []
+
+    def run(skip, stop):
+        ratio, kept = evaluate(list(skip), stop)
+        table.append({"skip_below": list(skip), "stop_above": stop, "time_ratio": ratio, "min_kept": kept})
+        return ratio, kept
+
+    skip = [0.0] * rules
+    best_stop, best_ratio = 1.0, run(skip, 1.0)[0]
+    for stop in STOP_ABOVE[:-1]:
+        ratio, kept = run(skip, stop)
+        if kept >= KEEP_SHARE and ratio < best_ratio:
+            best_stop, best_ratio = stop, ratio
+    for g in range(rules):
+        for t in SKIP_BELOW[:-1]:
+            trial = list(skip)
+            trial[g] = t
+            ratio, kept = run(trial, best_stop)
+            if kept >= KEEP_SHARE and ratio < best_ratio:
+                skip, best_ratio = trial, ratio
+    for stop in STOP_ABOVE:
+        if stop == best_stop:
+            continue
+        ratio, kept = run(skip, stop)
+        if kept >= KEEP_SHARE and ratio < best_ratio:
+            best_stop, best_ratio = stop, ratio
+    return skip, best_stop, best_ratio, table
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
@@ -77,6 +113,7 @@ def main(argv=None):
     ap.add_argument("--max-m", type=int, default=500000)
     ap.add_argument("--max-trace-seconds", type=float, default=None,
                     help="stop tracing new LPs after this long (the notes record how many were traced)")
+    ap.add_argument("--traces-out", default=None, help="save the traced rounds (compressed .npz)")
     args = ap.parse_args(argv)
 
     ctx = mp.get_context("spawn")
@@ -108,11 +145,13 @@ def main(argv=None):
             hold_lps = pool.map(_draw, jobs(args.holdout, args.seed + 2, hi=args.max_m), chunksize=1)
     X, Y, M = (np.concatenate(a) for a in (X, Y, M))
     trace_s = time.perf_counter() - t0
+    if args.traces_out:
+        np.savez_compressed(args.traces_out, X=X, Y=Y, M=M, train_lps=traced, train_nnz=train_nnz)
     t1 = time.perf_counter()
     w, loss = schedule.train(X, Y, M, epochs=args.epochs, batch=args.batch, seed=args.seed)
     train_s = time.perf_counter() - t1
 
-    # Threshold on held-out LPs: plain first, then each threshold.
+    # Thresholds on held-out LPs, against their plain runs.
     dlps = [device.DeviceLp(lp) for lp in hold_lps]
     plain_t, plain_r = [], []
     for lp, d in zip(hold_lps, dlps):
@@ -122,28 +161,25 @@ def main(argv=None):
         plain_t.append(s.preprocessing_seconds)
         plain_r.append(removal(lp, s))
         device.free_summary(s)
-    table = {}
-    for skip_below in SKIP_BELOW:
-        for stop_above in STOP_ABOVE:
-            times, kept = [], []
-            with schedule.Model(w, skip_below, stop_above) as model:
-                for lp, d, pr in zip(hold_lps, dlps, plain_r):
-                    s = schedule.scheduled_preprocess(d, params, model)
-                    times.append(s.preprocessing_seconds)
-                    kept.append(removal(lp, s) / pr if pr > 0 else 1.0)
-                    device.free_summary(s)
-            table[f"{skip_below}/{stop_above}"] = {
-                "skip_below": skip_below, "stop_above": stop_above,
-                "time_ratio": float(np.sum(times) / np.sum(plain_t)), "min_kept": float(np.min(kept)),
-                "mean_kept": float(np.mean(kept))}
-    ok = [v for v in table.values() if v["min_kept"] >= KEEP_SHARE]
-    best = min(ok, key=lambda v: v["time_ratio"]) if ok else {"skip_below": 0.0, "stop_above": 1.0}
+
+    def evaluate(skip, stop):
+        times, kept = [], []
+        with schedule.Model(w, skip, stop) as model:
+            for lp, d, pr in zip(hold_lps, dlps, plain_r):
+                s = schedule.scheduled_preprocess(d, params, model)
+                times.append(s.preprocessing_seconds)
+                kept.append(removal(lp, s) / pr if pr > 0 else 1.0)
+                device.free_summary(s)
+        return float(np.sum(times) / np.sum(plain_t)), float(np.min(kept))
+
+    skip, stop, ratio, table = choose_thresholds(evaluate, len(schedule.GATED_RULES))
     notes = {"samples": int(len(X)), "train_lps": traced, "train_nnz": int(train_nnz), "holdout_lps": args.holdout,
              "m_range": [1000, args.max_m], "generator_workers": workers, "train_seconds": train_s,
              "epochs": args.epochs, "batch": args.batch, "trace_seconds": trace_s,
-             "final_loss": float(loss[-1]) if len(loss) else None, "thresholds": table, "chosen": best,
+             "final_loss": float(loss[-1]) if len(loss) else None, "thresholds": table,
+             "chosen": {"skip_below": skip, "stop_above": stop, "time_ratio": ratio},
              "positive_rate": [float(x) for x in (Y * M).sum(0) / np.maximum(M.sum(0), 1)]}
-    schedule.save_model(args.out, w, best["skip_below"], best["stop_above"], loss=loss, notes=json.dumps(notes))
+    schedule.save_model(args.out, w, skip, stop, loss=loss, notes=json.dumps(notes))
     print(json.dumps(notes, indent=1))
 
 

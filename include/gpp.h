@@ -400,6 +400,12 @@ typedef struct gpp_schedule_model gpp_schedule_model;
  * One model may be used by one host thread at a time. */
 GPP_API int gpp_schedule_model_create(const float* params, double skip_below, double stop_above,
                                       gpp_schedule_model** out);
+/* The same with one skip threshold per gated rule (GPP_SCHEDULE_GATED_RULES
+ * values, in the order singleton columns, bound strengthening, redundant rows
+ * + dual fix, doubleton equations, parallel rows, parallel columns). */
+#define GPP_SCHEDULE_GATED_RULES 6
+GPP_API int gpp_schedule_model_create_per_rule(const float* params, const double* skip_below, double stop_above,
+                                               gpp_schedule_model** out);
 GPP_API void gpp_schedule_model_free(gpp_schedule_model* model);
 /* gpp_preprocess with the rounds scheduled by `model`. */
 GPP_API int gpp_preprocess_scheduled(const gpp_lp* lp, const gpp_params* params, gpp_schedule_model* model,

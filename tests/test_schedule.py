@@ -171,3 +171,21 @@ def test_shipped_schedule_gains_over_plain(m, seed):
     assert lp.nnz - nnz_sched >= 0.98 * (lp.nnz - nnz_plain)
     assert it_sched < it_plain
     assert t_sched < t_plain
+
+
+def test_threshold_search_keeps_the_removal_bar():
+    """The held-out threshold search on a synthetic cost model: skipping rule
+    2 is free of loss and saves time, skipping rule 0 loses removal; stopping
+    early saves time but loses removal below 0.8."""
+    from gpp_b200.train_schedule import KEEP_SHARE, choose_thresholds
+
+    def evaluate(skip, stop):
+        ratio = 1.0 - 0.3 * (skip[2] > 0) - 0.2 * (skip[0] > 0) - 0.1 * (stop < 1.0)
+        kept = 1.0 - (0.05 if skip[0] > 0 else 0.0) - (0.03 if stop < 0.8 else 0.0)
+        return ratio, kept
+
+    skip, stop, ratio, table = choose_thresholds(evaluate, 6)
+    assert skip[0] == 0.0 and skip[2] > 0.0
+    assert 0.8 <= stop < 1.0
+    assert abs(ratio - 0.6) < 1e-12
+    assert all(t["min_kept"] >= KEEP_SHARE or t["time_ratio"] >= ratio for t in table)
