@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kThreads)
 candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g) {
   __shared__ offset_t sptr[kTileRows + 1];
   const L2Hints hint = l2_hints();
-  constexpr int K = kEntryTile / kThreads;   // entries per thread and tile
+  constexpr int K = 4;   // entries whose loads are all issued before any is used
   for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
     const offset_t last = min(nnz, base + kEntryTile) - 1;
     const int2 span = tile_rows[base / kEntryTile];   // rows of the tile's first and last entry
@@ -101,31 +101,36 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
     if (staged)
       for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
     __syncthreads();
-    // The thread's K entries are independent: issue every load of all K
-    // before using any (streamed index and value, the row of each entry,
-    // then the gathered column record and the row's sides and summary), so
-    // up to K dependent-load chains are in flight per thread instead of one.
-    int col[K], row[K];
-    double a[K];
+    // Each round takes K of the thread's entries and issues every load they
+    // need (index, value and row; then the column record, the row's masks,
+    // sides and summary) before the first candidate update, whose atomics
+    // would otherwise keep later loads from being hoisted above them.
+    for (int k0 = 0; k0 < kEntryTile / kThreads; k0 += K) {
+      int col[K], row[K];
+      double a[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const offset_t p = base + offset_t(k) * kThreads + threadIdx.x;
-      const bool in = p <= last;
-      col[k] = in ? ld_stream(g.idx + p, hint.stream) : -1;
-      a[k] = in ? ld_stream(g.val + p, hint.stream) : 0.0;
-      row[k] = !in ? -1 : staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
-    }
-    double2 b[K];
-    bool use[K];
+      for (int k = 0; k < K; ++k) {
+        const offset_t p = base + offset_t(k0 + k) * kThreads + threadIdx.x;
+        const bool in = p <= last;
+        col[k] = in ? ld_stream(g.idx + p, hint.stream) : -1;
+        a[k] = in ? ld_stream(g.val + p, hint.stream) : 0.0;
+        row[k] = !in ? -1 : staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
+      }
+      double2 b[K];
+      RowCtx rc[K];
+      bool use[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      use[k] = col[k] >= 0 && g.keep_row[row[k]] && g.row_nnz[row[k]] > 1;
-      b[k] = use[k] ? ld_keep(g.lu + col[k], hint.keep) : make_double2(0.0, 0.0);
-    }
+      for (int k = 0; k < K; ++k) {
+        const int i = row[k] >= 0 ? row[k] : 0;
+        use[k] = row[k] >= 0 && g.keep_row[i] && g.row_nnz[i] > 1;
+        b[k] = ld_keep(g.lu + (col[k] >= 0 ? col[k] : 0), hint.keep);
+        rc[k] = row_ctx(g, i);
+      }
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (!use[k] || removed_column(b[k]) || fabs(a[k]) <= g.zero_tol) continue;
-      candidate_update(g, row_ctx(g, row[k]), col[k], a[k], b[k]);
+      for (int k = 0; k < K; ++k) {
+        if (!use[k] || removed_column(b[k]) || fabs(a[k]) <= g.zero_tol) continue;
+        candidate_update(g, rc[k], col[k], a[k], b[k]);
+      }
     }
     __syncthreads();
   }
@@ -191,9 +196,9 @@ __global__ void finalize_kernel(int n, const uint8_t* __restrict__ keep_col, con
 }
 
 // Support rows and per-column tape sizes (reference :815-960, :970-1008).
-// Four columns per warp, eight lanes each: the lanes split a changed
-// column's entries; the support row is the smallest qualifying row, an
-// order-free minimum over the lanes.
+// One thread per column; only changed columns read their entries.  The
+// support row is the smallest qualifying row (order-free).  Columns of at most
+// 8 entries run an unrolled loop, so their independent loads overlap.
 __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
                                const double* __restrict__ at_val, const uint8_t* __restrict__ keep_row,
                                const int32_t* __restrict__ row_nnz, const double* __restrict__ AL,
@@ -203,33 +208,29 @@ __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const
                                const double* __restrict__ fu, double zero_tol, double tol, double support_tol,
                                int32_t* __restrict__ sup_l, int32_t* __restrict__ sup_u,
                                int64_t* __restrict__ rec_count, int64_t* __restrict__ idx_count) {
-  const int lane = threadIdx.x & 31, g = lane & 7;
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
-  for (int j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; j0 < n; j0 += nwarps * 4) {
-    const int j = j0 + (lane >> 3);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     int sl = INT_MAX, su = INT_MAX;
-    const bool nl = j < n && lch[j], nu = j < n && uch[j];
+    const bool nl = lch[j], nu = uch[j];
     if (nl || nu) {
       const double lj = l[j], uj = u[j], flj = fl[j], fuj = fu[j];
       const bool want_l = nl && flj > lj + tol, want_u = nu && fuj < uj - tol;
-      if (want_l || want_u)
-        for (offset_t p = at_ptr[j] + g; p < at_ptr[j + 1]; p += 8) {
-          const int i = at_idx[p];
-          if (!keep_row[i] || row_nnz[i] <= 1) continue;
-          const double a = at_val[p];
-          if (fabs(a) <= zero_tol) continue;
-          double il, iu;
-          implied_bounds(a, lj, uj, AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
-          if (want_l && isfinite(il) && fabs(il - flj) <= support_tol) sl = min(sl, i);
-          if (want_u && isfinite(iu) && fabs(iu - fuj) <= support_tol) su = min(su, i);
-        }
-    }
+      const auto visit = [&](int i, double a) {
+        if (!keep_row[i] || row_nnz[i] <= 1 || fabs(a) <= zero_tol) return;
+        double il, iu;
+        implied_bounds(a, lj, uj, AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
+        if (want_l && isfinite(il) && fabs(il - flj) <= support_tol) sl = min(sl, i);
+        if (want_u && isfinite(iu) && fabs(iu - fuj) <= support_tol) su = min(su, i);
+      };
+      const offset_t first = at_ptr[j], last = at_ptr[j + 1];
+      if (!(want_l || want_u)) {
+      } else if (last - first <= 8) {
 #pragma unroll
-    for (int off = 4; off > 0; off >>= 1) {
-      sl = min(sl, __shfl_down_sync(0xffffffffu, sl, off, 8));
-      su = min(su, __shfl_down_sync(0xffffffffu, su, off, 8));
+        for (int k = 0; k < 8; ++k)
+          if (first + k < last) visit(at_idx[first + k], at_val[first + k]);
+      } else {
+        for (offset_t p = first; p < last; ++p) visit(at_idx[p], at_val[p]);
+      }
     }
-    if (g != 0 || j >= n) continue;
     sup_l[j] = sl;
     sup_u[j] = su;
     rec_count[j] = int64_t(nl) + int64_t(nu);
@@ -398,7 +399,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
     DBuf<int32_t> sl(size_t(n), s), su(size_t(n), s);
     DBuf<int64_t> rc(size_t(n) + 1, s), ic(size_t(n) + 1, s), rpos(size_t(n) + 1, s), ipos(size_t(n) + 1, s);
     const double support_tol = std::fmax(10.0 * p.bound_tol, 1.0e-10);
-    GPP_LAUNCH(support_kernel, std::max(1, std::min((n + 31) / 32, kNumSMs * 16)), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val,
+    GPP_LAUNCH(support_kernel, grid_stride_blocks(n), kThreads, 0, s, n, lp.AT.ptr, lp.AT.idx, lp.AT.val,
                plan.keep_row.p, stats.row_nnz.p, plan.AL.p, plan.AU.p, plan.l.p, plan.u.p, rs, lch.p, uch.p, fl.p,
                fu.p, p.zero_tol, p.bound_tol, support_tol, sl.p, su.p, rc.p, ic.p);
     exclusive_scan_i64(rc.p, rpos.p, n, s);

@@ -45,8 +45,9 @@ __global__ void redundant_apply(int m, const uint8_t* __restrict__ action, uint8
 }
 
 // _kernel_dual_fix_candidates (rule_dual_fix.cu:205-309).
-// Four columns per warp, eight lanes each: the lanes split the column's
-// entries and OR their lock flags (order-free), lane 0 of the group decides.
+// One thread per column.  A column of at most 8 entries runs an unrolled
+// pass without the early exit, so its independent loads overlap; the lock
+// flags only ever turn on, so the result is the same.
 __global__ void dual_fix_candidates(int n, const uint8_t* __restrict__ keep_col, const uint8_t* __restrict__ keep_row,
                                     const double* __restrict__ c, const double* __restrict__ l,
                                     const double* __restrict__ u, const double* __restrict__ AL,
@@ -56,30 +57,27 @@ __global__ void dual_fix_candidates(int n, const uint8_t* __restrict__ keep_col,
                                     uint8_t* __restrict__ fixed, uint8_t* __restrict__ inf_fix,
                                     double* __restrict__ fval, double* __restrict__ contrib,
                                     int32_t* __restrict__ status) {
-  const int lane = threadIdx.x & 31, g = lane & 7, grp = lane >> 3;
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
-  for (int j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; j0 < n; j0 += nwarps * 4) {
-    const int j = j0 + grp;
-    const bool kept = j < n && keep_col[j];
-    const double lj = kept ? l[j] : 0.0, uj = kept ? u[j] : 0.0, cj = kept ? c[j] : 0.0;
-    const bool infeasible = kept && lj > uj + bound_tol;
-    const bool scan = kept && !infeasible && !(fabs(cj) > zt && col_nnz[j] > max_degree);
-    bool down = false, up = false;
-    if (scan)
-      for (offset_t p = at_ptr[j] + g; p < at_ptr[j + 1]; p += 8) {
-        const int row = at_idx[p];
-        if (!keep_row[row]) continue;
-        const double a = at_val[p];
-        if (a > zt) { down = down || isfinite(AL[row]); up = up || isfinite(AU[row]); }
-        else if (a < -zt) { down = down || isfinite(AU[row]); up = up || isfinite(AL[row]); }
-        if (down && up) break;
-      }
-    down = ((__ballot_sync(0xffffffffu, down) >> (grp * 8)) & 0xffu) != 0;
-    up = ((__ballot_sync(0xffffffffu, up) >> (grp * 8)) & 0xffu) != 0;
-    if (g != 0 || j >= n) continue;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     fixed[j] = 0; inf_fix[j] = 0; fval[j] = 0.0; contrib[j] = 0.0;
-    if (infeasible) { atomicMax(status + 0, 1); continue; }
-    if (!scan) continue;
+    if (!keep_col[j]) continue;
+    const double lj = l[j], uj = u[j];
+    if (lj > uj + bound_tol) { atomicMax(status + 0, 1); continue; }
+    const double cj = c[j];
+    if (fabs(cj) > zt && col_nnz[j] > max_degree) continue;
+    bool down = false, up = false;
+    const auto visit = [&](int row, double a) {
+      if (!keep_row[row]) return;
+      if (a > zt) { down = down || isfinite(AL[row]); up = up || isfinite(AU[row]); }
+      else if (a < -zt) { down = down || isfinite(AU[row]); up = up || isfinite(AL[row]); }
+    };
+    const offset_t first = at_ptr[j], last = at_ptr[j + 1];
+    if (last - first <= 8) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (first + k < last) visit(at_idx[first + k], at_val[first + k]);
+    } else {
+      for (offset_t p = first; p < last && !(down && up); ++p) visit(at_idx[p], at_val[p]);
+    }
     bool f = false, fi = false;
     double v = 0.0;
     if (cj > zt) {
@@ -226,7 +224,7 @@ void rule_dual_fix(Plan& plan, const WorkingLp& lp, const Stats& stats, const gp
   DBuf<double> fval(size_t(n), s), contrib(size_t(n), s), shift(size_t(std::max(m, 1)), s);
   Status st;
   st.clear(4);
-  GPP_LAUNCH(dual_fix_candidates, std::max(1, std::min((n + 31) / 32, kNumSMs * 16)), kThreads, 0, s, n, plan.keep_col.p, plan.keep_row.p,
+  GPP_LAUNCH(dual_fix_candidates, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, plan.keep_row.p,
              plan.c.p, plan.l.p, plan.u.p, plan.AL.p, plan.AU.p, lp.AT.ptr, lp.AT.idx, lp.AT.val, p.zero_tol,
              p.bound_tol, p.dual_fix_max_nonzero_cost_col_degree, stats.col_nnz.p, fixed.p, inf_fix.p, fval.p,
              contrib.p, st.d);
