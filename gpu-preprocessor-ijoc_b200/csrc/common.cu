@@ -98,11 +98,11 @@ Status::~Status() { if (d) cudaFreeAsync(d, ctx().stream); }
 void Status::clear(int words) {
   check(cudaMemsetAsync(d, 0, sizeof(int32_t) * size_t(words), ctx().stream), "status clear");
 }
-const int32_t* Status::read(int words) {
+const int32_t* Status::read(int words, const char* where) {
   auto& c = ctx();
   check(cudaMemcpyAsync(c.host_status, d, sizeof(int32_t) * size_t(words), cudaMemcpyDeviceToHost, c.stream),
         "status read");
-  c.sync("status sync");
+  c.sync(where);
   return c.host_status;
 }
 

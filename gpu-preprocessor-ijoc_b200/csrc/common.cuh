@@ -290,26 +290,26 @@ std::vector<T> to_host(const T* d, size_t count) {
   return h;
 }
 template <class T>
-T read_scalar(const T* d) {
+T read_scalar(const T* d, const char* where = __builtin_FUNCTION()) {
   // Through the context's pinned block: a pageable destination would make
   // the copy go through a staging buffer.
   static_assert(sizeof(T) <= 8, "scalar");
   auto& c = ctx();
   check(cudaMemcpyAsync(c.host_scalar, d, sizeof(T), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
-  c.sync("d2h scalar sync");
+  c.sync(where);
   T v;
   std::memcpy(&v, c.host_scalar, sizeof(T));
   return v;
 }
 // Two scalars (say the totals of two scans) with one wait.
 template <class T, class U>
-std::pair<T, U> read_scalars(const T* a, const U* b) {
+std::pair<T, U> read_scalars(const T* a, const U* b, const char* where = __builtin_FUNCTION()) {
   static_assert(sizeof(T) <= 8 && sizeof(U) <= 8, "scalar");
   auto& c = ctx();
   unsigned char* h = c.host_scalar;
   check(cudaMemcpyAsync(h, a, sizeof(T), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
   check(cudaMemcpyAsync(h + 8, b, sizeof(U), cudaMemcpyDeviceToHost, c.stream), "d2h scalar");
-  c.sync("d2h scalar sync");
+  c.sync(where);
   T va;
   U vb;
   std::memcpy(&va, h, sizeof(T));
@@ -323,7 +323,8 @@ struct Status {
   Status();
   ~Status();
   void clear(int words = Context::kStatusWords);
-  const int32_t* read(int words = Context::kStatusWords);
+  // `where` (the calling function) labels the wait in the benchmark's profile.
+  const int32_t* read(int words = Context::kStatusWords, const char* where = __builtin_FUNCTION());
 };
 
 // ---------------------------------------------------------------------------
