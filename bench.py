@@ -313,6 +313,15 @@ def reference_gpu(lp, point, steps, warmup, presolve_ms, postsolve_ms):
             "build": "reference library compiled from its sources with nvcc 12.9 -O3 for sm_100 (oracle/ref.mk)"}
 
 
+def optional(measure):
+    """Runs one of the bench line's optional measurements; a failure there
+    becomes {"error": ...} in the line instead of losing the line."""
+    try:
+        return measure()
+    except Exception as e:  # reported, not hidden: the line carries the message
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -545,15 +554,16 @@ def main():
     step_bytes = sum(r[3] for r in prof) / args.steps if prof else 0
     algorithmic = None
     if prof:
-        algorithmic = {"bytes_per_step": int(step_bytes),
+        algorithmic = {"kernels_counted": sorted({r[0] for r in prof if r[3] > 0}),
+                       "bytes_per_step": int(step_bytes),
                        "gbs_per_step": round(step_bytes / 1e9 / (step_ms / 1e3), 1),
                        "frac_of_peak": round(step_bytes / 1e9 / (step_ms / 1e3) / peak, 4),
                        "kernel_ms_per_step": round(sum(r[2] for r in prof if not r[0].startswith("sync:"))
                                                    / args.steps, 3)}
     ref_gpu = None
     if rank == 0 and not args.no_reference_gpu:
-        ref_gpu = reference_gpu(lp, [t.cpu().numpy() for t in red], args.steps, max(args.warmup, 3),
-                                statistics.mean(pre_ms), post_ms)
+        ref_gpu = optional(lambda: reference_gpu(lp, [t.cpu().numpy() for t in red], args.steps, max(args.warmup, 3),
+                                                 statistics.mean(pre_ms), post_ms))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         driver = os.path.join(ROOT, "oracle", "_ref", "pslp_driver")
@@ -582,7 +592,7 @@ def main():
             learned = {"unavailable": str(e)}
             learned_result = None
             learned_pool.terminate()
-    if learned_result is not None:
+    def learned_measurement():
         reps = max(3, min(args.steps, 5))
         per_lp = []
         with schedule.Model(w_sched, skip_below, stop_above) as model:
@@ -610,20 +620,24 @@ def main():
                 del hd, hlp
         ratios = [r["time_ratio"] for r in per_lp]
         kept = [r["nnz_removal_kept"] for r in per_lp]
-        learned = {"time_ratio_mean": round(statistics.mean(ratios), 4), "time_ratio_max": max(ratios),
+        return {"time_ratio_mean": round(statistics.mean(ratios), 4), "time_ratio_max": max(ratios),
                    "speedup_mean": round(1.0 / statistics.mean(ratios), 3),
                    "nnz_removal_kept_min": min(kept), "held_out": per_lp,
                    "skip_below": skip_below, "stop_above": stop_above,
-                   "workload": "held-out draws of the scale workload (seeds %s)" % LEARNED_SEEDS,
+                   "workload": f"held-out draws of the scale workload (seeds {list(LEARNED_SEEDS)})",
                    "timing": f"presolve elapsed_seconds, mean of {reps} runs after 2 warm-up, per LP",
                    "model": "2x64 FP32 MLP, trained on plain-loop traces"}
+
+    if learned_result is not None:
+        learned = optional(learned_measurement)
         learned_pool.close()
         learned_pool.join()
 
     batched = None
     if batch_result is not None:
         gloo = dist.new_group(backend="gloo") if world > 1 else None
-        batched = run_batched(batch_mine, batch_result.get(), params, args.batch_max_workers, rank, world, gloo)
+        batched = optional(lambda: run_batched(batch_mine, batch_result.get(), params, args.batch_max_workers, rank,
+                                               world, gloo))
         batch_pool.close()
         batch_pool.join()
     if rank == 0:
