@@ -40,58 +40,6 @@ Context::Context() {
   check(cudaMallocHost(reinterpret_cast<void**>(&host_scalar), 16), "cudaMallocHost scalar");
 }
 
-namespace {
-struct L2Limits {
-  size_t max_persist = 0, max_window = 0;
-  bool set_aside = false;
-};
-std::mutex g_l2_mutex;
-L2Limits& l2_limits(int device) {
-  static std::vector<L2Limits> per_device;
-  if (size_t(device) >= per_device.size()) per_device.resize(size_t(device) + 1);
-  return per_device[size_t(device)];
-}
-}  // namespace
-
-L2Residency::L2Residency(const void* base, size_t bytes, cudaStream_t s) : s_(s) {
-  if (!base || bytes < (size_t(16) << 20)) return;
-  const int device = ctx().device;
-  size_t persist = 0, window = 0;
-  {
-    std::lock_guard<std::mutex> lock(g_l2_mutex);
-    L2Limits& lim = l2_limits(device);
-    if (!lim.set_aside) {
-      int mp = 0, mw = 0;
-      check(cudaDeviceGetAttribute(&mp, cudaDevAttrMaxPersistingL2CacheSize, device), "L2 persisting size");
-      check(cudaDeviceGetAttribute(&mw, cudaDevAttrMaxAccessPolicyWindowSize, device), "L2 window size");
-      lim.max_persist = size_t(mp);
-      lim.max_window = size_t(mw);
-      if (lim.max_persist > 0) check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim.max_persist), "L2 set-aside");
-      lim.set_aside = true;
-    }
-    persist = lim.max_persist;
-    window = lim.max_window;
-  }
-  if (persist == 0 || window == 0) return;
-  check(cudaCtxResetPersistingL2Cache(), "L2 reset persisting");
-  cudaStreamAttrValue attr{};
-  attr.accessPolicyWindow.base_ptr = const_cast<void*>(base);
-  attr.accessPolicyWindow.num_bytes = std::min(bytes, window);
-  attr.accessPolicyWindow.hitRatio =
-      float(std::min(1.0, double(persist) / double(attr.accessPolicyWindow.num_bytes)));
-  attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-  attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-  check(cudaStreamSetAttribute(s_, cudaStreamAttributeAccessPolicyWindow, &attr), "L2 window");
-  active_ = true;
-}
-
-L2Residency::~L2Residency() {
-  if (!active_) return;
-  cudaStreamAttrValue attr{};
-  attr.accessPolicyWindow.num_bytes = 0;
-  cudaStreamSetAttribute(s_, cudaStreamAttributeAccessPolicyWindow, &attr);
-}
-
 void Context::sync(const char* label) {
   ++sync_counter();
   if (!profiling()) {

@@ -216,26 +216,6 @@ struct Context {
 };
 Context& ctx();
 
-// Keeps a gathered table resident in L2 for the kernels queued on `s` while
-// the object lives: an access-policy window marks `bytes` from `base`
-// persisting (hit) / streaming (miss) on the stream, and the first use in the
-// process sets aside L2 for persisting lines in this process's context (the
-// device's largest set-aside; normal accesses still use the space while no
-// persisting line holds it).  Lines left persisting by an earlier table are
-// demoted first.  Tables under 16 MB fit L2 anyway and get no window.  The
-// window is removed again on destruction.
-class L2Residency {
- public:
-  L2Residency(const void* base, size_t bytes, cudaStream_t s);
-  ~L2Residency();
-  L2Residency(const L2Residency&) = delete;
-  L2Residency& operator=(const L2Residency&) = delete;
-
- private:
-  cudaStream_t s_ = nullptr;
-  bool active_ = false;
-};
-
 // Every engine device allocation: stream-ordered from the context's pool.
 // A test hook (gpp_inject_alloc_failure) can make the k-th allocation after
 // it was armed return cudaErrorMemoryAllocation instead, a host-side fake of

@@ -842,7 +842,6 @@ void row_plain_minmax(const DevCsr& A, const double* l, const double* u, const u
   if (!A.rows) return;
   DBuf<double2> lu(size_t(std::max(A.cols, 1)), s);
   pack_bounds(l, u, keep_col, A.cols, lu.p, s);
-  const L2Residency resident_bounds(lu.p, sizeof(double2) * size_t(A.cols), s);
   launch_activity<true>(A, lu.p, 0.0, keep_row, live_deg, row_min, row_max, nullptr, nullptr, 16.0, s);
 }
 

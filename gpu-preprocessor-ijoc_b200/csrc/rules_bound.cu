@@ -255,11 +255,8 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
   DBuf<double2> lu(size_t(n), s);
   pack_bounds(plan.l.p, plan.u.p, plan.keep_col.p, n, lu.p, s);
   const CandSink sink{plan.AL.p, plan.AU.p, stats.row_nnz.p, cl.p, cu.p};
-  {
-    const L2Residency resident_bounds(lu.p, sizeof(double2) * size_t(n), s);
-    row_activity_and_candidates(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p,
-                                sink, s);
-  }
+  row_activity_and_candidates(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p, sink,
+                              s);
   const RowSummary rs{mn.p, mx.p, ni.p, pi.p};
   if (plan.inf_hist) {
     check(cudaMemsetAsync(plan.inf_hist, 0, 8 * sizeof(uint32_t), s), "inf_hist");
