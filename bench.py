@@ -47,8 +47,7 @@ RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singl
 KERNEL_SOURCES = {
     "activity_kernel<false>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
     "activity_kernel<true>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
-    "activity_candidates_kernel": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/bound_candidates.cuh",
-                                   "csrc/common.cuh"],
+    "candidates_entries": ["csrc/rules_bound.cu", "csrc/common.cuh"],
     "copy_kept": ["csrc/compact.cu", "csrc/common.cuh"],
 }
 

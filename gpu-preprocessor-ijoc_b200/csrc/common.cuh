@@ -18,6 +18,7 @@ namespace gpp {
 
 using offset_t = gpp_offset;
 constexpr int kThreads = 256;
+constexpr int kEntryTile = 2048;    // stored entries per tile of the entry-parallel sweeps
 constexpr int kShortRow = 8;      // rows of live length <= 8: one thread per row
 constexpr int kLongRow = 1024;    // rows of live length > 1024: one block per row
 constexpr int kNumSMs = 148;      // B200

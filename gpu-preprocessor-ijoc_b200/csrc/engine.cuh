@@ -23,6 +23,10 @@ struct DevCsr {
 // and long queues list the remaining rows for warp- and block-per-row work.
 struct RowSchedule {
   DBuf<int32_t> medium, long_rows, counts;  // counts[0] medium, counts[1] long
+  // Stored schedules only: for every tile of kEntryTile stored entries, the
+  // rows that hold its first (x) and last (y) entry.
+  DBuf<int2> tile_rows;
+  int64_t tiles = 0;
   mutable int sorted = -1;  // rows strictly ascending: -1 not yet checked, else 0 / 1
   const offset_t* ptr = nullptr;
   int32_t rows = -1;
@@ -131,13 +135,6 @@ void allocate_stats(Stats& st, int32_t m, int32_t n);
 // Packs {l_j, u_j} of every column (a removed one as the reserved NaN pair).
 void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int32_t n, double2* lu,
                  cudaStream_t s);
-struct CandSink;
-// The activity summary with the bound-strengthening candidates of every entry
-// formed in the same sweep (live.cu; the candidate arrays hold the current
-// bounds on entry and receive RED max / min).
-void row_activity_and_candidates(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
-                                 const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,
-                                 int32_t* max_inf, const CandSink& cand, cudaStream_t s);
 void row_activity_summary_packed(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
                                  const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,
                                  int32_t* max_inf, cudaStream_t s);

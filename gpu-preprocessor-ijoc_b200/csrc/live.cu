@@ -12,7 +12,6 @@
 //   medium : 32 lane partials, shfl_down tree 16,8,4,2,1 (own + peer),
 //   long   : 256 lane partials, per-warp shfl tree 1,2,4,8,16 then warp
 //            aggregates added in warp order (cub::BlockReduce default).
-#include "bound_candidates.cuh"
 #include "engine.cuh"
 #include "live_visit.cuh"
 
@@ -124,19 +123,15 @@ struct ActivityTerm {
 // sums.
 constexpr int kGroupRowMax = 32;
 
-// With Cand, the sweep also forms the bound-strengthening candidates of every
-// entry of a row once the row's summary is complete (rows kept, of more than
-// one live entry): the row's entries are still in registers for short and
-// grouped rows, and are read a second time only for the few longer rows.
-template <bool Plain, bool Cand>
-__device__ __forceinline__ void
-activity_body(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+template <bool Plain>
+__global__ void __launch_bounds__(kThreads)
+activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                 const double* __restrict__ val, const double2* __restrict__ lu, double zero_tol,
                 const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ live_deg,
                 const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
                 const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
                 double* __restrict__ min_fin, double* __restrict__ max_fin, int32_t* __restrict__ min_inf,
-                int32_t* __restrict__ max_inf, CandSink cand) {
+                int32_t* __restrict__ max_inf) {
   __shared__ int slots[256];
   __shared__ int warp_counts[8];
   __shared__ double dagg[8];
@@ -169,30 +164,10 @@ activity_body(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict
 #pragma unroll
         for (int k = 0; k < kShortRow; ++k)
           if (col[k] >= 0 && !removed_column(bnd[k])) term.add(a[k], bnd[k], lo, hi, ni, pi);
-        if constexpr (Cand) {
-          if (cand.row_nnz[i] > 1) {
-            const double al = cand.AL[i], au = cand.AU[i];
-#pragma unroll
-            for (int k = 0; k < kShortRow; ++k)
-              if (col[k] >= 0 && !removed_column(bnd[k]) && !(fabs(a[k]) <= zero_tol))
-                cand.entry(col[k], a[k], bnd[k], al, au, lo, hi, ni, pi);
-          }
-        }
       } else {
         for (offset_t p = first; p < last; ++p) {
           const double2 bnd = term.bounds(p);
           if (!removed_column(bnd)) term(p, bnd, lo, hi, ni, pi);
-        }
-        if constexpr (Cand) {
-          if (cand.row_nnz[i] > 1) {
-            const double al = cand.AL[i], au = cand.AU[i];
-            for (offset_t p = first; p < last; ++p) {
-              const int j = ld_stream(idx + p, term.hint.stream);
-              const double2 b = ld_keep(lu + j, term.hint.keep);
-              const double av = ld_stream(val + p, term.hint.stream);
-              if (!removed_column(b) && !(fabs(av) <= zero_tol)) cand.entry(j, av, b, al, au, lo, hi, ni, pi);
-            }
-          }
         }
       }
       min_fin[i] = lo; max_fin[i] = hi;
@@ -219,19 +194,6 @@ activity_body(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict
       if (lane == 0) {
         min_fin[row] = lo; max_fin[row] = hi;
         if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
-      }
-      if constexpr (Cand) {
-        lo = __shfl_sync(0xffffffffu, lo, 0); hi = __shfl_sync(0xffffffffu, hi, 0);
-        ni = __shfl_sync(0xffffffffu, ni, 0); pi = __shfl_sync(0xffffffffu, pi, 0);
-        if ((!keep_row || keep_row[row]) && cand.row_nnz[row] > 1) {
-          const double al = cand.AL[row], au = cand.AU[row];
-          for (offset_t p = first + lane; p < last; p += 32) {
-            const int j = ld_stream(idx + p, term.hint.stream);
-            const double2 b = ld_keep(lu + j, term.hint.keep);
-            const double av = ld_stream(val + p, term.hint.stream);
-            if (!removed_column(b) && !(fabs(av) <= zero_tol)) cand.entry(j, av, b, al, au, lo, hi, ni, pi);
-          }
-        }
       }
     };
     for (int q0 = ((b - short_blocks) * (kThreads / 32) + warp) * 4; q0 < count; q0 += nwarps * 4) {
@@ -291,18 +253,6 @@ activity_body(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict
         min_fin[row] = lo; max_fin[row] = hi;
         if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
       }
-      if constexpr (Cand) {
-        // The group's totals (lane 0 of the group) to all eight lanes; the
-        // entries are still in registers.
-        lo = __shfl_sync(0xffffffffu, lo, grp * 8); hi = __shfl_sync(0xffffffffu, hi, grp * 8);
-        ni = __shfl_sync(0xffffffffu, ni, grp * 8); pi = __shfl_sync(0xffffffffu, pi, grp * 8);
-        if (grouped && kept && cand.row_nnz[row] > 1) {
-          const double al = cand.AL[row], au = cand.AU[row];
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (live[j] && !(fabs(a[j]) <= zero_tol)) cand.entry(col[j], a[j], bnd[j], al, au, lo, hi, ni, pi);
-        }
-      }
       // Longer medium rows: one warp each, as before.
       unsigned rest = __ballot_sync(0xffffffffu, have && !grouped && gl == 0);
       while (rest) {
@@ -332,47 +282,9 @@ activity_body(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict
     if (threadIdx.x == 0) {
       min_fin[row] = lo; max_fin[row] = hi;
       if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
-      if constexpr (Cand) { dagg[0] = lo; dagg[1] = hi; iagg[0] = ni; iagg[1] = pi; }
     }
     __syncthreads();
-    if constexpr (Cand) {
-      lo = dagg[0]; hi = dagg[1]; ni = iagg[0]; pi = iagg[1];
-      if ((!keep_row || keep_row[row]) && cand.row_nnz[row] > 1) {
-        const double al = cand.AL[row], au = cand.AU[row];
-        for (offset_t p = first + threadIdx.x; p < last; p += kThreads) {
-          const int j = ld_stream(idx + p, term.hint.stream);
-          const double2 b = ld_keep(lu + j, term.hint.keep);
-          const double av = ld_stream(val + p, term.hint.stream);
-          if (!removed_column(b) && !(fabs(av) <= zero_tol)) cand.entry(j, av, b, al, au, lo, hi, ni, pi);
-        }
-      }
-      __syncthreads();
-    }
   }
-}
-
-template <bool Plain>
-__global__ void __launch_bounds__(kThreads) activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                const double* __restrict__ val, const double2* __restrict__ lu, double zero_tol,
-                const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ live_deg,
-                const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
-                const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
-                double* __restrict__ min_fin, double* __restrict__ max_fin, int32_t* __restrict__ min_inf,
-                int32_t* __restrict__ max_inf, CandSink cand) {
-  activity_body<Plain, false>(m, ptr, idx, val, lu, zero_tol, keep_row, live_deg, medium, longq, counts, short_blocks, medium_blocks,
-                            min_fin, max_fin, min_inf, max_inf, cand);
-}
-
-// The fused activity + candidate sweep, under its own name in launch lists.
-__global__ void __launch_bounds__(kThreads) activity_candidates_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                const double* __restrict__ val, const double2* __restrict__ lu, double zero_tol,
-                const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ live_deg,
-                const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
-                const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
-                double* __restrict__ min_fin, double* __restrict__ max_fin, int32_t* __restrict__ min_inf,
-                int32_t* __restrict__ max_inf, CandSink cand) {
-  activity_body<false, true>(m, ptr, idx, val, lu, zero_tol, keep_row, live_deg, medium, longq, counts, short_blocks, medium_blocks,
-                            min_fin, max_fin, min_inf, max_inf, cand);
 }
 
 __global__ void pack_bounds_kernel(int n, const double* __restrict__ l, const double* __restrict__ u,
@@ -576,6 +488,22 @@ ScheduleCache& schedule_cache() {
 
 }  // namespace
 
+namespace {
+// Row r writes the tiles whose first stored position, or last one (the last
+// tile ends at nnz - 1), falls in [ptr[r], ptr[r+1]): every tile gets both
+// rows with no search, in one pass over the row pointers.
+__global__ void tile_rows_kernel(int rows, offset_t nnz, const offset_t* __restrict__ ptr, int2* __restrict__ tile_rows) {
+  constexpr int64_t T = kEntryTile;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const int64_t a = ptr[r], b = ptr[r + 1];
+    if (a == b) continue;
+    for (int64_t t = (a + T - 1) / T; t * T < b; ++t) tile_rows[t].x = r;
+    for (int64_t t = (a + T) / T - 1; (t + 1) * T <= b; ++t) tile_rows[t].y = r;
+    if (b == nnz) tile_rows[(nnz - 1) / T].y = r;
+  }
+}
+}  // namespace
+
 void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees, cudaStream_t st) {
   const size_t rows = size_t(std::max(M.rows, 1));
   if (s.medium.n < rows) s.medium.alloc(rows, st);
@@ -584,7 +512,13 @@ void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees
   check(cudaMemsetAsync(s.counts.p, 0, 2 * sizeof(int32_t), st), "schedule counts");
   GPP_LAUNCH(classify_rows, blocks_for(M.rows), kThreads, 0, st, M.ptr, M.rows, live_degrees, s.medium.p,
              s.long_rows.p, s.counts.p);
+  s.tiles = 0;
   s.sorted = -1;
+  if (!live_degrees && M.rows > 0 && M.nnz > 0) {
+    s.tiles = (int64_t(M.nnz) + kEntryTile - 1) / kEntryTile;
+    if (s.tile_rows.n < size_t(s.tiles)) s.tile_rows.alloc(size_t(s.tiles), st);
+    GPP_LAUNCH(tile_rows_kernel, grid_stride_blocks(M.rows), kThreads, 0, st, M.rows, M.nnz, M.ptr, s.tile_rows.p);
+  }
   s.ptr = M.ptr;
   s.rows = M.rows;
   s.nnz = M.nnz;
@@ -772,10 +706,10 @@ void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int3
 }
 
 namespace {
-template <bool Plain, bool Cand = false>
+template <bool Plain>
 void launch_activity(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
                      const int32_t* live_deg, double* lo, double* hi, int32_t* ni, int32_t* pi, double out_bytes,
-                     cudaStream_t s, CandSink cand = CandSink{}) {
+                     cudaStream_t s) {
   static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
   const RowSchedule* sch;
   if (live_deg) {
@@ -787,35 +721,19 @@ void launch_activity(const DevCsr& A, const double2* lu, double zero_tol, const 
   const Roles r = roles_for(A.rows);
   // Algorithmic bytes (each array charged once): row pointers, column indices
   // and values, packed column bounds, row mask, live degrees, the outputs.
-  // With the candidates: the row sides (16 B per row) and the two candidate
-  // bound arrays (16 B per column, charged once).
   const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
-                       (live_deg ? 4.0 * A.rows : 0) + out_bytes * A.rows + (Cand ? 16.0 * A.rows + 16.0 * A.cols : 0);
+                       (live_deg ? 4.0 * A.rows : 0) + out_bytes * A.rows;
   const int grid = r.short_blocks + r.medium_blocks + r.long_blocks;
   if constexpr (Plain)
-    GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu,
-                     zero_tol, keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
-                     r.medium_blocks, lo, hi, ni, pi, cand);
-  else if constexpr (Cand)
-    GPP_LAUNCH_BYTES(activity_candidates_kernel, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu,
-                     zero_tol, keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
-                     r.medium_blocks, lo, hi, ni, pi, cand);
+    GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
   else
-    GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu,
-                     zero_tol, keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
-                     r.medium_blocks, lo, hi, ni, pi, cand);
+    GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
 }
 }  // namespace
-
-void row_activity_and_candidates(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
-                                 const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,
-                                 int32_t* max_inf, const CandSink& cand, cudaStream_t s) {
-  // compute_row_activity_summary (gpu_presolve_kernels.cu:744-787) with the
-  // candidate pass of apply_rule_bound_strengthening (:373-430) fused in.
-  if (!A.rows) return;
-  launch_activity<false, true>(A, lu, zero_tol, keep_row, live_deg, min_fin, max_fin, min_inf, max_inf, 24.0, s,
-                               cand);
-}
 
 void row_activity_summary_packed(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
                                  const int32_t* live_deg, double* min_fin, double* max_fin, int32_t* min_inf,

@@ -3,12 +3,10 @@
 // rows for the postsolve tape, and the fixed-column row shift.
 //
 // Reference: rules/rule_bound_strengthening.cu:336-813 (kernels) and
-// :1176-1557 (driver).  Candidate bounds are combined with order-free RED
-// max / min; they are formed inside the activity sweep (live.cu), which holds
-// each row's finished summary and entries in registers.
+// :1176-1557 (driver).  Candidate bounds are combined with CAS max/min, whose
+// result does not depend on the order of the updates.
 #include <climits>
 
-#include "bound_candidates.cuh"
 #include "engine.cuh"
 
 namespace gpp {
@@ -22,6 +20,99 @@ struct RowSummary {
   const int32_t* ni;
   const int32_t* pi;
 };
+
+// Implied bounds of the column of entry a from its row (reference :349-430).
+__device__ __forceinline__ void implied_bounds(double a, double lj, double uj, double al, double au, double mn,
+                                               double mx, int ni, int pi, double& il, double& iu) {
+  double tmin, tmax;
+  if (a >= 0.0) { tmin = a * lj; tmax = a * uj; } else { tmin = a * uj; tmax = a * lj; }
+  double rmin, rmax;
+  if (isfinite(tmin)) rmin = ni == 0 ? mn - tmin : -INFINITY;
+  else if (tmin < 0.0) rmin = ni > 1 ? -INFINITY : mn;
+  else rmin = mn;
+  if (isfinite(tmax)) rmax = pi == 0 ? mx - tmax : INFINITY;
+  else if (tmax > 0.0) rmax = pi > 1 ? INFINITY : mx;
+  else rmax = mx;
+  il = -INFINITY;
+  iu = INFINITY;
+  if (a > 0.0) {
+    if (isfinite(al) && isfinite(rmax)) il = (al - rmax) / a;
+    if (isfinite(au) && isfinite(rmin)) iu = (au - rmin) / a;
+  } else {
+    if (isfinite(au) && isfinite(rmin)) il = (au - rmin) / a;
+    if (isfinite(al) && isfinite(rmax)) iu = (al - rmax) / a;
+  }
+}
+
+struct CandArgs {
+  const offset_t* ptr;
+  const int32_t* idx;
+  const double* val;
+  const uint8_t* keep_row;
+  const int32_t* row_nnz;
+  const double* AL;
+  const double* AU;
+  const double2* lu;   // packed column bounds, removed columns marked
+  RowSummary rs;
+  double zero_tol;
+  double* cand_l;
+  double* cand_u;
+};
+
+// The row's sides and activity summary, loaded once per row.
+struct RowCtx {
+  double al, au, mn, mx;
+  int ni, pi;
+};
+__device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
+  return RowCtx{g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i]};
+}
+
+__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p, const L2Hints& h) {
+  const int j = ld_stream(g.idx + p, h.stream);   // CSR streamed once: keep L2 for the gathered bounds
+  const double2 b = ld_keep(g.lu + j, h.keep);
+  if (removed_column(b)) return;
+  const double a = ld_stream(g.val + p, h.stream);
+  if (fabs(a) <= g.zero_tol) return;
+  const double ol = b.x, ou = b.y;
+  double il, iu;
+  implied_bounds(a, ol, ou, rc.al, rc.au, rc.mn, rc.mx, rc.ni, rc.pi, il, iu);
+  double nl = ol, nu = ou;
+  if (isfinite(il)) nl = fmax(nl, il);
+  if (isfinite(iu)) nu = fmin(nu, iu);
+  if (nl > ol) red_max_f64(&g.cand_l[j], nl);
+  if (nu < ou) red_min_f64(&g.cand_u[j], nu);
+}
+
+// Entry-parallel form of the candidate sweep: the candidates are combined by
+// atomic max / min, which is order-free, so instead of row roles every thread
+// takes consecutive stored entries (coalesced loads, full memory-level
+// parallelism) and finds their row by a binary search over the tile's row
+// pointers, staged in shared memory.
+constexpr int kTileRows = 2048;
+
+__global__ void __launch_bounds__(kThreads)
+candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g) {
+  __shared__ offset_t sptr[kTileRows + 1];
+  const L2Hints hint = l2_hints();
+  for (offset_t base = offset_t(blockIdx.x) * kEntryTile; base < nnz; base += offset_t(gridDim.x) * kEntryTile) {
+    const offset_t last = min(nnz, base + kEntryTile) - 1;
+    const int2 span = tile_rows[base / kEntryTile];   // rows of the tile's first and last entry
+    const int r0 = span.x, r1 = span.y;
+    const bool staged = r1 - r0 + 1 <= kTileRows;
+    if (staged)
+      for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
+    __syncthreads();
+    for (int k = 0; k < kEntryTile / kThreads; ++k) {
+      const offset_t p = base + offset_t(k) * kThreads + threadIdx.x;
+      if (p > last) break;
+      const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
+      if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
+      candidate_entry(g, row_ctx(g, i), p, hint);
+    }
+    __syncthreads();
+  }
+}
 
 // _kernel_finalize_bound_strengthening (reference :646-796).
 __global__ void finalize_kernel(int n, const uint8_t* __restrict__ keep_col, const double* __restrict__ l,
@@ -83,9 +174,6 @@ __global__ void finalize_kernel(int n, const uint8_t* __restrict__ keep_col, con
 }
 
 // Support rows and per-column tape sizes (reference :815-960, :970-1008).
-// One thread per column; only changed columns read their entries.  The
-// support row is the smallest qualifying row (order-free).  Columns of at most
-// 8 entries run an unrolled loop, so their independent loads overlap.
 __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const int32_t* __restrict__ at_idx,
                                const double* __restrict__ at_val, const uint8_t* __restrict__ keep_row,
                                const int32_t* __restrict__ row_nnz, const double* __restrict__ AL,
@@ -99,23 +187,15 @@ __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const
     int sl = INT_MAX, su = INT_MAX;
     const bool nl = lch[j], nu = uch[j];
     if (nl || nu) {
-      const double lj = l[j], uj = u[j], flj = fl[j], fuj = fu[j];
-      const bool want_l = nl && flj > lj + tol, want_u = nu && fuj < uj - tol;
-      const auto visit = [&](int i, double a) {
-        if (!keep_row[i] || row_nnz[i] <= 1 || fabs(a) <= zero_tol) return;
+      for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) {
+        const int i = at_idx[p];
+        if (!keep_row[i] || row_nnz[i] <= 1) continue;
+        const double a = at_val[p];
+        if (fabs(a) <= zero_tol) continue;
         double il, iu;
-        implied_bounds(a, lj, uj, AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
-        if (want_l && isfinite(il) && fabs(il - flj) <= support_tol) sl = min(sl, i);
-        if (want_u && isfinite(iu) && fabs(iu - fuj) <= support_tol) su = min(su, i);
-      };
-      const offset_t first = at_ptr[j], last = at_ptr[j + 1];
-      if (!(want_l || want_u)) {
-      } else if (last - first <= 8) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (first + k < last) visit(at_idx[first + k], at_val[first + k]);
-      } else {
-        for (offset_t p = first; p < last; ++p) visit(at_idx[p], at_val[p]);
+        implied_bounds(a, l[j], u[j], AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
+        if (nl && fl[j] > l[j] + tol && isfinite(il) && fabs(il - fl[j]) <= support_tol) sl = min(sl, i);
+        if (nu && fu[j] < u[j] - tol && isfinite(iu) && fabs(iu - fu[j]) <= support_tol) su = min(su, i);
       }
     }
     sup_l[j] = sl;
@@ -254,13 +334,20 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
   // One packed bounds array serves the activity sweep and the candidate sweep.
   DBuf<double2> lu(size_t(n), s);
   pack_bounds(plan.l.p, plan.u.p, plan.keep_col.p, n, lu.p, s);
-  const CandSink sink{plan.AL.p, plan.AU.p, stats.row_nnz.p, cl.p, cu.p};
-  row_activity_and_candidates(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p, sink,
-                              s);
+  row_activity_summary_packed(lp.A, lu.p, p.zero_tol, plan.keep_row.p, stats.row_nnz.p, mn.p, mx.p, ni.p, pi.p, s);
   const RowSummary rs{mn.p, mx.p, ni.p, pi.p};
   if (plan.inf_hist) {
     check(cudaMemsetAsync(plan.inf_hist, 0, 8 * sizeof(uint32_t), s), "inf_hist");
     GPP_LAUNCH(inf_histogram, grid_stride_blocks(m), kThreads, 0, s, m, plan.keep_row.p, ni.p, pi.p, plan.inf_hist);
+  }
+  {
+    CandArgs g{lp.A.ptr, lp.A.idx, lp.A.val, plan.keep_row.p, stats.row_nnz.p, plan.AL.p, plan.AU.p, lu.p, rs,
+               p.zero_tol, cl.p, cu.p};
+    const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + 4.0 * m + 16.0 * m + 24.0 * m + 16.0 * n +
+                         16.0 * n;
+    const RowSchedule& sch = stored_schedule(lp.A);
+    GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(sch.tiles, kNumSMs * 8))),
+                     kThreads, 0, s, lp.A.nnz, sch.tile_rows.p, g);
   }
   col_max_abs(lp.AT, plan.keep_row.p, vmax.p, s);
   DBuf<double> fl(size_t(n), s), fu(size_t(n), s), fixv(size_t(n), s);

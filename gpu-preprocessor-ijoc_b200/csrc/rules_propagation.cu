@@ -45,9 +45,6 @@ __global__ void redundant_apply(int m, const uint8_t* __restrict__ action, uint8
 }
 
 // _kernel_dual_fix_candidates (rule_dual_fix.cu:205-309).
-// One thread per column.  A column of at most 8 entries runs an unrolled
-// pass without the early exit, so its independent loads overlap; the lock
-// flags only ever turn on, so the result is the same.
 __global__ void dual_fix_candidates(int n, const uint8_t* __restrict__ keep_col, const uint8_t* __restrict__ keep_row,
                                     const double* __restrict__ c, const double* __restrict__ l,
                                     const double* __restrict__ u, const double* __restrict__ AL,
@@ -65,18 +62,13 @@ __global__ void dual_fix_candidates(int n, const uint8_t* __restrict__ keep_col,
     const double cj = c[j];
     if (fabs(cj) > zt && col_nnz[j] > max_degree) continue;
     bool down = false, up = false;
-    const auto visit = [&](int row, double a) {
-      if (!keep_row[row]) return;
+    for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) {
+      const int row = at_idx[p];
+      if (!keep_row[row]) continue;
+      const double a = at_val[p];
       if (a > zt) { down = down || isfinite(AL[row]); up = up || isfinite(AU[row]); }
       else if (a < -zt) { down = down || isfinite(AU[row]); up = up || isfinite(AL[row]); }
-    };
-    const offset_t first = at_ptr[j], last = at_ptr[j + 1];
-    if (last - first <= 8) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if (first + k < last) visit(at_idx[first + k], at_val[first + k]);
-    } else {
-      for (offset_t p = first; p < last && !(down && up); ++p) visit(at_idx[p], at_val[p]);
+      if (down && up) break;
     }
     bool f = false, fi = false;
     double v = 0.0;
