@@ -196,12 +196,24 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
         if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
       }
     };
-    for (int q0 = ((b - short_blocks) * (kThreads / 32) + warp) * 4; q0 < count; q0 += nwarps * 4) {
+    // The row ids and row pointers of later iterations are loaded ahead (the
+    // queue entry two iterations ahead, the pointers one ahead), so each
+    // iteration's critical path starts at its entries instead of at the queue.
+    const int step = nwarps * 4;
+    const int q_first = ((b - short_blocks) * (kThreads / 32) + warp) * 4 + grp;
+    int row_next = q_first < count ? medium[q_first] : 0;
+    int row_after = q_first + step < count ? medium[q_first + step] : 0;
+    offset_t first_next = q_first < count ? ptr[row_next] : 0, last_next = q_first < count ? ptr[row_next + 1] : 0;
+    for (int q0 = ((b - short_blocks) * (kThreads / 32) + warp) * 4; q0 < count; q0 += step) {
       const int q = q0 + grp;
       const bool have = q < count;
-      const int row = have ? medium[q] : 0;
+      const int row = row_next;
+      const offset_t first = first_next, last = last_next;
+      row_next = row_after;
+      first_next = q + step < count ? ptr[row_next] : 0;
+      last_next = q + step < count ? ptr[row_next + 1] : 0;
+      row_after = q + 2 * step < count ? medium[q + 2 * step] : 0;
       const bool kept = have && (!keep_row || keep_row[row]);
-      const offset_t first = have ? ptr[row] : 0, last = have ? ptr[row + 1] : 0;
       const bool grouped = have && (!kept || last - first <= kGroupRowMax);
       const offset_t end = grouped && kept ? last : first;
       // Every load of the row's (up to) four entries per lane first.
