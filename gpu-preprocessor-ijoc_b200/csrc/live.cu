@@ -142,11 +142,21 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   const auto live_at = [&](offset_t p) { return !removed_column(term.bounds(p)); };
   const int b = blockIdx.x;
   if (b < short_blocks) {
-    for (int i = b * blockDim.x + threadIdx.x; i < m; i += short_blocks * blockDim.x) {
-      if (row_len(ptr, live_deg, i) > kShortRow) continue;
+    // The next row's pointers and live length are loaded one iteration ahead.
+    const int stride = short_blocks * blockDim.x;
+    int i_next = b * blockDim.x + threadIdx.x;
+    offset_t first_next = i_next < m ? ptr[i_next] : 0, last_next = i_next < m ? ptr[i_next + 1] : 0;
+    int len_next = i_next < m && live_deg ? live_deg[i_next] : int(last_next - first_next);
+    for (int i = i_next; i < m; i += stride) {
+      const offset_t first = first_next, last = last_next;
+      const int len = len_next;
+      i_next = i + stride;
+      first_next = i_next < m ? ptr[i_next] : 0;
+      last_next = i_next < m ? ptr[i_next + 1] : 0;
+      len_next = i_next < m && live_deg ? live_deg[i_next] : int(last_next - first_next);
+      if (len > kShortRow) continue;
       double lo = 0.0, hi = 0.0;
       int ni = 0, pi = 0;
-      const offset_t first = ptr[i], last = ptr[i + 1];
       if (keep_row && !keep_row[i]) {
       } else if (last - first <= kShortRow) {
         // All loads of the (at most 8) entries first, then the sequential sum.

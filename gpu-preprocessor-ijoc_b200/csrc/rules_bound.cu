@@ -68,12 +68,9 @@ __device__ __forceinline__ RowCtx row_ctx(const CandArgs& g, int i) {
   return RowCtx{g.AL[i], g.AU[i], g.rs.mn[i], g.rs.mx[i], g.rs.ni[i], g.rs.pi[i]};
 }
 
-__device__ __forceinline__ void candidate_entry(const CandArgs& g, const RowCtx& rc, offset_t p, const L2Hints& h) {
-  const int j = ld_stream(g.idx + p, h.stream);   // CSR streamed once: keep L2 for the gathered bounds
-  const double2 b = ld_keep(g.lu + j, h.keep);
-  if (removed_column(b)) return;
-  const double a = ld_stream(g.val + p, h.stream);
-  if (fabs(a) <= g.zero_tol) return;
+// Candidate bounds of column j from one entry a of a row (reference
+// :373-430); b holds the column's current bounds.
+__device__ __forceinline__ void candidate_update(const CandArgs& g, const RowCtx& rc, int j, double a, double2 b) {
   const double ol = b.x, ou = b.y;
   double il, iu;
   implied_bounds(a, ol, ou, rc.al, rc.au, rc.mn, rc.mx, rc.ni, rc.pi, il, iu);
@@ -103,12 +100,24 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
     if (staged)
       for (int k = threadIdx.x; k <= r1 - r0 + 1; k += kThreads) sptr[k] = g.ptr[r0 + k];
     __syncthreads();
-    for (int k = 0; k < kEntryTile / kThreads; ++k) {
-      const offset_t p = base + offset_t(k) * kThreads + threadIdx.x;
-      if (p > last) break;
+    // The next entry's index and value are loaded one iteration ahead, so an
+    // entry's critical path starts at its gather.
+    constexpr int K = kEntryTile / kThreads;
+    offset_t p = base + threadIdx.x;
+    int j = p <= last ? ld_stream(g.idx + p, hint.stream) : -1;
+    double a = p <= last ? ld_stream(g.val + p, hint.stream) : 0.0;
+    for (int k = 0; k < K && p <= last; ++k, p += kThreads) {
+      const offset_t pn = p + kThreads;
+      const bool next = k + 1 < K && pn <= last;
+      const int jn = next ? ld_stream(g.idx + pn, hint.stream) : -1;
+      const double an = next ? ld_stream(g.val + pn, hint.stream) : 0.0;
       const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
-      if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;
-      candidate_entry(g, row_ctx(g, i), p, hint);
+      if (g.keep_row[i] && g.row_nnz[i] > 1) {
+        const double2 b = ld_keep(g.lu + j, hint.keep);
+        if (!removed_column(b) && !(fabs(a) <= g.zero_tol)) candidate_update(g, row_ctx(g, i), j, a, b);
+      }
+      j = jn;
+      a = an;
     }
     __syncthreads();
   }
