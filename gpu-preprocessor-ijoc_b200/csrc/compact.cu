@@ -49,8 +49,14 @@ count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict
   __shared__ int scount[8];
   const int b = blockIdx.x;
   if (b < short_blocks) {
-    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      const offset_t first = ptr[r], last = ptr[r + 1];
+    const int stride_ = short_blocks * blockDim.x;
+    int r_next = b * blockDim.x + threadIdx.x;
+    offset_t first_next = r_next < rows ? ptr[r_next] : 0, last_next = r_next < rows ? ptr[r_next + 1] : 0;
+    for (int r = r_next; r < rows; r += stride_) {
+      const offset_t first = first_next, last = last_next;
+      r_next = r + stride_;   // the next row's pointers, one iteration ahead
+      first_next = r_next < rows ? ptr[r_next] : 0;
+      last_next = r_next < rows ? ptr[r_next + 1] : 0;
       if (last - first > kShortRow) continue;
       const int nr = outer_map[r];
       if (nr < 0) continue;

@@ -343,8 +343,14 @@ live_stats_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __r
   const int b = blockIdx.x;
   unsigned long long acc = 0;  // live entries seen by this thread, added once per block
   if (b < short_blocks) {
-    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      const offset_t first = ptr[r], last = ptr[r + 1];
+    const int stride_ = short_blocks * blockDim.x;
+    int r_next = b * blockDim.x + threadIdx.x;
+    offset_t first_next = r_next < rows ? ptr[r_next] : 0, last_next = r_next < rows ? ptr[r_next + 1] : 0;
+    for (int r = r_next; r < rows; r += stride_) {
+      const offset_t first = first_next, last = last_next;
+      r_next = r + stride_;   // the next row's pointers, one iteration ahead
+      first_next = r_next < rows ? ptr[r_next] : 0;
+      last_next = r_next < rows ? ptr[r_next + 1] : 0;
       if (last - first > kShortRow) continue;
       const bool active = !keep_outer || keep_outer[r];
       int count = 0;
@@ -425,8 +431,14 @@ col_max_kernel(int rows, const offset_t* __restrict__ ptr, const int32_t* __rest
   __shared__ double smax[8];
   const int b = blockIdx.x;
   if (b < short_blocks) {
-    for (int r = b * blockDim.x + threadIdx.x; r < rows; r += short_blocks * blockDim.x) {
-      const offset_t first = ptr[r], last = ptr[r + 1];
+    const int stride_ = short_blocks * blockDim.x;
+    int r_next = b * blockDim.x + threadIdx.x;
+    offset_t first_next = r_next < rows ? ptr[r_next] : 0, last_next = r_next < rows ? ptr[r_next + 1] : 0;
+    for (int r = r_next; r < rows; r += stride_) {
+      const offset_t first = first_next, last = last_next;
+      r_next = r + stride_;   // the next row's pointers, one iteration ahead
+      first_next = r_next < rows ? ptr[r_next] : 0;
+      last_next = r_next < rows ? ptr[r_next + 1] : 0;
       if (last - first > kShortRow) continue;
       // All (at most 8) loads first; the max is order-free.
       int row[kShortRow];
