@@ -165,11 +165,25 @@ __global__ void sc_cache_rows(const int32_t* __restrict__ rows, const int32_t* _
     }
     if (lane == 0) out.store(row, r);
   };
-  for (int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; w0 < count; w0 += warps * 4) {
+  // Row ids two iterations ahead and row pointers and lengths one ahead, so
+  // an iteration's critical path starts at its entries.
+  const int step = warps * 4;
+  const int w_first = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4 + grp;
+  int row_next = w_first < count ? rows[w_first] : 0;
+  int row_after = w_first + step < count ? rows[w_first + step] : 0;
+  int len_next = w_first < count ? row_nnz[row_next] : 0;
+  offset_t first_next = w_first < count ? ptr[row_next] : 0, end_next = w_first < count ? ptr[row_next + 1] : 0;
+  for (int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; w0 < count; w0 += step) {
     const int w = w0 + grp;
-    const int row = w < count ? rows[w] : 0;
-    const bool take = w < count && row_nnz[row] <= kLongRow;
-    const offset_t first = take ? ptr[row] : 0, end = take ? ptr[row + 1] : 0;
+    const int row = row_next;
+    const bool take = w < count && len_next <= kLongRow;
+    const offset_t first = take ? first_next : 0, end = take ? end_next : 0;
+    row_next = row_after;
+    const bool more = w + step < count;
+    len_next = more ? row_nnz[row_next] : 0;
+    first_next = more ? ptr[row_next] : 0;
+    end_next = more ? ptr[row_next + 1] : 0;
+    row_after = w + 2 * step < count ? rows[w + 2 * step] : 0;
     const bool grouped = take && end - first <= 32;
     const offset_t stop = grouped ? end : first;
     int col[4];
