@@ -400,14 +400,20 @@ int gpp_preprocess(const gpp_lp* lp, const gpp_params* params, gpp_summary* out)
   return guarded([&] { preprocess_into(lp, params, out, true); });
 }
 
-int gpp_postsolve_device(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
-                         const gpp_lp* original, double* x_org, double* y_org, double* z_org) {
+int gpp_postsolve_device_lower(const double* x_red, const double* y_red, const double* z_red,
+                               const gpp_summary* summary, const gpp_lp* original, const double* original_l,
+                               double* x_org, double* y_org, double* z_org) {
   return guarded([&] {
     if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
     const gpp_record* rec = summary->record;
     if (rec->folding.applied) throw std::invalid_argument("folded summaries postsolve through gpp_postprocess");
-    gpp::run_postsolve(rec->out, x_red, y_red, z_red, original, x_org, y_org, z_org);
+    gpp::run_postsolve(rec->out, x_red, y_red, z_red, original, x_org, y_org, z_org, original_l);
   });
+}
+
+int gpp_postsolve_device(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
+                         const gpp_lp* original, double* x_org, double* y_org, double* z_org) {
+  return gpp_postsolve_device_lower(x_red, y_red, z_red, summary, original, nullptr, x_org, y_org, z_org);
 }
 
 int gpp_postprocess(const double* x_red, const double* y_red, const double* z_red, const gpp_summary* summary,
@@ -577,6 +583,125 @@ int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t* index_s
       if (fixed_val) std::copy(b.begin(), b.end(), fixed_val + fk);
       fk += seg.count;
     }
+  });
+}
+
+int gpp_recovery_checkpoints(const gpp_summary* summary, int32_t* count, int32_t* kinds, int32_t* payloads,
+                             int64_t* tape_positions) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const gpp::Record& r = summary->record->out.record;
+    if (count) *count = int32_t(r.timeline.size());
+    for (size_t k = 0; k < r.timeline.size(); ++k) {
+      if (kinds) kinds[k] = r.timeline[k].kind;
+      if (payloads) payloads[k] = r.timeline[k].payload;
+      if (tape_positions) tape_positions[k] = r.timeline[k].tape_position;
+    }
+  });
+}
+
+extern "C++" {
+namespace {
+const gpp::AbsValueRecovery& absolute_value_at(const gpp_summary* summary, int32_t index) {
+  if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+  const auto& v = summary->record->out.record.absval;
+  if (index < 0 || size_t(index) >= v.size()) throw std::invalid_argument("no absolute-value recovery at that index");
+  return v[size_t(index)];
+}
+template <class T>
+void copy_out(T* dst, const gpp::DBuf<T>& src, int64_t n) {
+  if (dst && n > 0)
+    check(cudaMemcpyAsync(dst, src.p, sizeof(T) * size_t(n), cudaMemcpyDeviceToHost, gpp::ctx().stream), "export");
+}
+template <class T>
+void copy_in(gpp::DBuf<T>& dst, const T* src, int64_t n, const char* what) {
+  if (n < 0) throw std::invalid_argument(std::string("negative count in ") + what);
+  if (n > 0 && !src) throw std::invalid_argument(std::string("missing array ") + what);
+  dst.alloc(size_t(n));
+  if (n > 0)
+    check(cudaMemcpyAsync(dst.p, src, sizeof(T) * size_t(n), cudaMemcpyHostToDevice, gpp::ctx().stream), what);
+}
+}  // namespace
+}
+
+int gpp_absolute_value_sizes(const gpp_summary* summary, int32_t index, int32_t sizes[6]) {
+  return guarded([&] {
+    const auto& a = absolute_value_at(summary, index);
+    if (!sizes) throw std::invalid_argument("sizes is null");
+    sizes[0] = a.pattern;
+    sizes[1] = a.splits;
+    sizes[2] = a.pairs;
+    sizes[3] = a.links;
+    sizes[4] = a.max_groups;
+    sizes[5] = a.max_entries;
+  });
+}
+
+int gpp_export_absolute_value(const gpp_summary* summary, int32_t index, int32_t* split_t, int32_t* split_e,
+                              double* split_rho, int32_t* pair_bound, int32_t* pair_free, int32_t* linked_slack,
+                              int32_t* linked_t, double* linked_factor, int32_t* max_slack, int32_t* max_starts,
+                              int32_t* max_t, double* max_factor) {
+  return guarded([&] {
+    const auto& a = absolute_value_at(summary, index);
+    copy_out(split_t, a.split_t, a.splits);
+    copy_out(split_e, a.split_e, a.splits);
+    copy_out(split_rho, a.split_rho, a.splits);
+    copy_out(pair_bound, a.pair_bound, a.pairs);
+    copy_out(pair_free, a.pair_free, a.pairs);
+    copy_out(linked_slack, a.link_slack, a.links);
+    copy_out(linked_t, a.link_t, a.links);
+    copy_out(linked_factor, a.link_factor, a.links);
+    copy_out(max_slack, a.max_slack, a.max_groups);
+    copy_out(max_starts, a.max_start, a.max_groups ? a.max_groups + 1 : 0);
+    copy_out(max_t, a.max_t, a.max_entries);
+    copy_out(max_factor, a.max_factor, a.max_entries);
+    if (max_starts && !a.max_groups) max_starts[0] = 0;
+    gpp::ctx().sync("export absolute-value recovery");
+  });
+}
+
+int gpp_restore_absolute_value(double* x_org, const gpp_absolute_value_recovery* steps, int32_t count,
+                               const double* original_l) {
+  return guarded([&] {
+    if (count < 0 || (count > 0 && (!steps || !x_org))) throw std::invalid_argument("invalid recovery steps");
+    for (int32_t k = count - 1; k >= 0; --k) {
+      const gpp_absolute_value_recovery& h = steps[k];
+      gpp::AbsValueRecovery d;
+      d.pattern = h.pattern;
+      d.splits = h.split_count;
+      d.pairs = h.pair_count;
+      d.links = h.linked_count;
+      d.max_groups = h.max_group_count;
+      if (d.max_groups < 0) throw std::invalid_argument("negative max-slack group count");
+      if (d.max_groups > 0 && !h.max_starts) throw std::invalid_argument("missing array max_starts");
+      d.max_entries = d.max_groups ? h.max_starts[d.max_groups] : 0;
+      for (int32_t g = 0; g < d.max_groups; ++g)
+        if (h.max_starts[g] < 0 || h.max_starts[g] > h.max_starts[g + 1])
+          throw std::invalid_argument("max_starts is not ascending");
+      auto ids_ok = [](const int32_t* v, int32_t n) {
+        for (int32_t i = 0; i < n; ++i)
+          if (v[i] < 0) return false;
+        return true;
+      };
+      copy_in(d.split_t, h.split_t, d.splits, "split_t");
+      copy_in(d.split_e, h.split_e, d.splits, "split_e");
+      copy_in(d.split_rho, h.split_rho, d.splits, "split_rho");
+      copy_in(d.pair_bound, h.pair_bound, d.pairs, "pair_bound");
+      copy_in(d.pair_free, h.pair_free, d.pairs, "pair_free");
+      copy_in(d.link_slack, h.linked_slack, d.links, "linked_slack");
+      copy_in(d.link_t, h.linked_t, d.links, "linked_t");
+      copy_in(d.link_factor, h.linked_factor, d.links, "linked_factor");
+      copy_in(d.max_slack, h.max_slack, d.max_groups, "max_slack");
+      copy_in(d.max_start, h.max_starts, d.max_groups ? d.max_groups + 1 : 0, "max_starts");
+      copy_in(d.max_t, h.max_t, d.max_entries, "max_t");
+      copy_in(d.max_factor, h.max_factor, d.max_entries, "max_factor");
+      if (!ids_ok(h.split_t, d.splits) || !ids_ok(h.split_e, d.splits) || !ids_ok(h.pair_bound, d.pairs) ||
+          !ids_ok(h.pair_free, d.pairs) || !ids_ok(h.linked_slack, d.links) || !ids_ok(h.linked_t, d.links) ||
+          !ids_ok(h.max_slack, d.max_groups) || !ids_ok(h.max_t, d.max_entries))
+        throw std::invalid_argument("negative column id in a recovery step");
+      gpp::restore_absolute_value(x_org, d, original_l, gpp::ctx().stream);
+    }
+    gpp::ctx().sync("restore absolute value");
   });
 }
 

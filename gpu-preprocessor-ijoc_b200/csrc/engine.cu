@@ -164,6 +164,10 @@ struct Engine {
     next.obj = cur.obj + pl.obj_delta;
     // update_device_recovery (device_recovery.cu:892-975).
     capture_tape(r, pl.tape);
+    if (pl.absval) {
+      capture_absolute_value(r, std::move(*pl.absval));
+      pl.absval.reset();
+    }
     if (!cleanup_captured && n_new != n) append_fixed(r, pl.keep_col.p, nullptr, pl.l.p, pl.u.p, n);
     if (m_new != r.m) {
       DBuf<int32_t> rows(size_t(m_new), s());
@@ -242,8 +246,10 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
     // off when enable_structure_specific_rules is (:2088-2094).  Column
     // domination, two-row variable elimination and zero-cost product
     // variables share one plan, each seeing the deletions of those before it,
-    // and the plan is applied once before Cleanup.  The piecewise-linear
-    // reformulations are not run.  The phase consumes one iteration (:2453).
+    // and the plan is applied once; then the absolute-value reformulation,
+    // gated by its prefix screen, runs on its own materialised plan (:2447).
+    // The variable-pair reformulation is not run.  The phase consumes one
+    // iteration (:2453).
     const bool batch = p.enable_structure_specific_rules &&
                        (p.enable_column_domination || p.enable_two_row_variable_elimination ||
                         p.enable_zero_cost_product_variables);
@@ -255,6 +261,10 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
             rule_zero_cost_product_variables(e.plan, cur, p);
         }))
       e.materialize("startup");
+    if (p.enable_structure_specific_rules && p.enable_piecewise_linear_reformulation_absolute_value &&
+        !e.terminal && !time_exceeded() && absolute_value_prefix_screen(cur))
+      e.materialized_rule(true, "startup_piecewise_linear_reformulation_absolute_value",
+                          [&](Plan& pl) { rule_absolute_value(pl, cur, p); });
     ++out.iterations;
   }
   auto deferred = [&](bool enabled, const char* name, auto rule) {

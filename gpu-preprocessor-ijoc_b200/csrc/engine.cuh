@@ -75,12 +75,42 @@ struct FixedSegment {
   int64_t count = 0;
 };
 
+// Primal recovery of one absolute-value reformulation (reference
+// PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep,
+// presolve_structs.hpp:207-236), on the device.  Column ids are the working
+// model's until captured into the record, original ids after.  Restored in
+// this order: splits (t, e) <- (t + e, (t - e) / rho); outer pairs
+// free <- bound; linked slacks slack <- factor * t; max slacks
+// slack <- max(l_slack, max_k factor_k * t_k) per group.
+struct AbsValueRecovery {
+  int32_t pattern = 0;   // gpp_absolute_value_pattern
+  DBuf<int32_t> split_t, split_e;
+  DBuf<double> split_rho;
+  DBuf<int32_t> pair_bound, pair_free;
+  DBuf<int32_t> link_slack, link_t;
+  DBuf<double> link_factor;
+  DBuf<int32_t> max_slack, max_start, max_t;   // groups; groups + 1; entries
+  DBuf<double> max_factor;
+  int32_t splits = 0, pairs = 0, links = 0, max_groups = 0, max_entries = 0;
+};
+
+// Where a primal recovery sits in the tape (reference PrimalRecoveryCheckpoint,
+// presolve_structs.hpp:256-266): records at or after `tape_position` are
+// replayed (primal pass) before it is applied.
+struct RecoveryCheckpoint {
+  int32_t kind = 0;        // 0 absolute value
+  int32_t payload = 0;     // index into Record::absval
+  int64_t tape_position = 0;
+};
+
 struct Record {
   int32_t m0 = 0, n0 = 0;
   DBuf<int32_t> rows, cols;   // current index -> original index
   int32_t m = 0, n = 0;
   std::vector<PostsolveSegment> segments;
   std::vector<FixedSegment> fixed;
+  std::vector<AbsValueRecovery> absval;
+  std::vector<RecoveryCheckpoint> timeline;
   int64_t records = 0, indices = 0, values = 0;
 };
 
@@ -104,6 +134,7 @@ struct Plan {
   bool has_new_A = false;
   DevCsr new_A;                  // owned when has_new_A
   std::vector<PostsolveSegment> tape;   // local indices until captured
+  std::unique_ptr<AbsValueRecovery> absval;   // set by the absolute-value reformulation
 };
 
 struct Stats {
@@ -196,6 +227,9 @@ void append_fixed(Record& r, const uint8_t* keep_col, const uint8_t* prior, cons
 // Builds a device segment from host-side packed arrays (records laid out
 // contiguously); used by rules that pack on the device and know the counts.
 PostsolveSegment make_segment(int64_t count, int64_t n_idx, int64_t n_val);
+// Moves an absolute-value recovery into the record (column ids made
+// original through r.cols) with a checkpoint at the current tape length.
+void capture_absolute_value(Record& r, AbsValueRecovery&& step);
 
 // rules_*.cu
 void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p);
@@ -213,6 +247,11 @@ void rule_zero_cost_product_variables(Plan& plan, const WorkingLp& lp, const gpp
 void rule_parallel_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_parallel_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+// rules_pwl_abs.cu: piecewise-linear reformulation of absolute values.
+// The prefix screen (rows 0-3 look like one of the three layouts) gates the
+// rule as the reference's does.
+bool absolute_value_prefix_screen(const WorkingLp& lp);
+void rule_absolute_value(Plan& plan, const WorkingLp& lp, const gpp_params& p);
 
 // Row-wise shift sum_j a_ij * v_j over kept rows and selected columns, in
 // ascending column order (deterministic replacement of atomicAdd shifts).

@@ -304,10 +304,11 @@ struct SegView {
   int64_t count;
 };
 
-// The reference's serial interpreter: one thread walks a segment backwards.
-__global__ void replay_serial(SegView t, Sol s, Model M, int primal, int dual) {
+// The reference's serial interpreter: one thread walks records [lo, hi) of a
+// segment backwards.
+__global__ void replay_serial(SegView t, Sol s, Model M, int primal, int dual, int64_t lo, int64_t hi) {
   if (blockIdx.x || threadIdx.x) return;
-  for (int64_t k = t.count - 1; k >= 0; --k)
+  for (int64_t k = hi - 1; k >= lo; --k)
     replay_record(t.types[k], t.idx + t.is[k], t.is[k + 1] - t.is[k], t.val + t.vs[k], t.vs[k + 1] - t.vs[k], s, M,
                   primal != 0, dual != 0);
 }
@@ -480,14 +481,14 @@ __device__ void record_resources(int type, const int32_t* id, int64_t ni, int64_
   }
 }
 
-__global__ void cp_active(TapeView t, int dual, int32_t* __restrict__ flag) {
+__global__ void cp_active(TapeView t, int dual, int64_t lo, int64_t hi, int32_t* __restrict__ flag) {
   for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < t.total; g += int64_t(gridDim.x) * blockDim.x) {
     int type;
     const int32_t* id;
     int64_t ni, nv;
     const double* v;
     t.at(g, type, id, ni, v, nv);
-    flag[g] = replays_in(type, dual != 0) ? 1 : 0;
+    flag[g] = g >= lo && g < hi && replays_in(type, dual != 0) ? 1 : 0;
   }
 }
 
@@ -585,8 +586,9 @@ __global__ void cp_replay(TapeView t, const int64_t* __restrict__ act, const uin
   }
 }
 
+// Replays the records [lo, hi) of the whole tape (global indices).
 void replay_parallel(const std::vector<PostsolveSegment>& segments, int m0, int n0, const Sol& s, const Model& M,
-                     bool dual, cudaStream_t st) {
+                     bool dual, cudaStream_t st, int64_t lo, int64_t hi) {
   std::vector<SegView> hv;
   std::vector<int64_t> hs{0};
   for (const auto& seg : segments) {
@@ -602,7 +604,7 @@ void replay_parallel(const std::vector<PostsolveSegment>& segments, int m0, int 
   check(cudaMemcpyAsync(starts.p, hs.data(), sizeof(int64_t) * hs.size(), cudaMemcpyHostToDevice, st), "tape starts");
   const TapeView t{segs.p, starts.p, int(hv.size()), total};
   DBuf<int32_t> flag(size_t(total) + 1, st), pos(size_t(total) + 1, st);
-  GPP_LAUNCH(cp_active, grid_stride_blocks(total), kThreads, 0, st, t, int(dual), flag.p);
+  GPP_LAUNCH(cp_active, grid_stride_blocks(total), kThreads, 0, st, t, int(dual), lo, hi, flag.p);
   exclusive_scan_i32(flag.p, pos.p, total, st);
   const int count = read_scalar(pos.p + total);
   if (!count) return;
@@ -626,10 +628,58 @@ void replay_parallel(const std::vector<PostsolveSegment>& segments, int m0, int 
              int(!dual), int(dual));
 }
 
+// ---- piecewise-linear primal recoveries ---------------------------------------
+// postsolve_piecewise_linear_reformulation_absolute_value.cu:9-105.
+
+__global__ void restore_splits(double* __restrict__ x, const int32_t* __restrict__ t, const int32_t* __restrict__ e,
+                               const double* __restrict__ rho, int k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    const double tv = x[t[i]], ev = x[e[i]];
+    x[t[i]] = tv + ev;
+    x[e[i]] = (tv - ev) / rho[i];
+  }
+}
+__global__ void restore_pairs(double* __restrict__ x, const int32_t* __restrict__ bound,
+                              const int32_t* __restrict__ free_col, int k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) x[free_col[i]] = x[bound[i]];
+}
+__global__ void restore_links(double* __restrict__ x, const int32_t* __restrict__ slack, const int32_t* __restrict__ t,
+                              const double* __restrict__ f, int k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) x[slack[i]] = f[i] * x[t[i]];
+}
+// One warp per group: slack = max(l_slack (0 when absent or not finite),
+// max_k factor_k t_k).  fmax ignores NaN and is exact, so any order of the
+// maximum gives the reference's value.
+__global__ void restore_max_slacks(double* __restrict__ x, const int32_t* __restrict__ slack,
+                                   const int32_t* __restrict__ start, const int32_t* __restrict__ t,
+                                   const double* __restrict__ f, int groups, const double* __restrict__ lower) {
+  const int lane = threadIdx.x & 31;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < groups; g += (gridDim.x * blockDim.x) >> 5) {
+    const int32_t sc = slack[g];
+    double lb = lower ? lower[sc] : 0.0;
+    if (!isfinite(lb)) lb = 0.0;
+    double v = lb;
+    for (int q = start[g] + lane; q < start[g + 1]; q += 32) v = fmax(v, f[q] * x[t[q]]);
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) x[sc] = v;
+  }
+}
+
 }  // namespace
 
+void restore_absolute_value(double* x, const AbsValueRecovery& r, const double* lower, cudaStream_t st) {
+  GPP_LAUNCH(restore_splits, grid_stride_blocks(r.splits), kThreads, 0, st, x, r.split_t.p, r.split_e.p,
+             r.split_rho.p, r.splits);
+  GPP_LAUNCH(restore_pairs, grid_stride_blocks(r.pairs), kThreads, 0, st, x, r.pair_bound.p, r.pair_free.p, r.pairs);
+  GPP_LAUNCH(restore_links, grid_stride_blocks(r.links), kThreads, 0, st, x, r.link_slack.p, r.link_t.p,
+             r.link_factor.p, r.links);
+  GPP_LAUNCH(restore_max_slacks, grid_stride_blocks(int64_t(r.max_groups) * 32), kThreads, 0, st, x, r.max_slack.p,
+             r.max_start.p, r.max_t.p, r.max_factor.p, r.max_groups, lower);
+}
+
 void run_postsolve(const PresolveOutput& out, const double* x_red, const double* y_red, const double* z_red,
-                   const gpp_lp* original, double* x, double* y, double* z) {
+                   const gpp_lp* original, double* x, double* y, double* z, const double* lower) {
+  if (!lower && original) lower = original->l;
   auto st = ctx().stream;
   const Record& r = out.record;
   const int m0 = r.m0, n0 = r.n0;
@@ -650,14 +700,32 @@ void run_postsolve(const PresolveOutput& out, const double* x_red, const double*
               original->AT.nzVal, original->c, original->l, original->u, true};
   }
   const Sol s{x, y, z, got.p};
-  if (r.records < kParallelMinRecords) {
-    for (int pass = 0; pass < 2; ++pass)
-      for (auto it = r.segments.rbegin(); it != r.segments.rend(); ++it)
-        GPP_LAUNCH(replay_serial, 1, 1, 0, st, view(*it), s, M, pass == 0, pass == 1);
-  } else {
-    replay_parallel(r.segments, m0, n0, s, M, false, st);
-    replay_parallel(r.segments, m0, n0, s, M, true, st);
+  // Records [lo, hi) of the tape (global indices), newest first.
+  auto replay = [&](int64_t lo, int64_t hi, bool dual) {
+    if (lo >= hi) return;
+    if (r.records < kParallelMinRecords) {
+      int64_t end = r.records;
+      for (auto it = r.segments.rbegin(); it != r.segments.rend(); ++it) {
+        const int64_t begin = end - it->count;
+        const int64_t a = std::max(lo, begin), b = std::min(hi, end);
+        if (a < b) GPP_LAUNCH(replay_serial, 1, 1, 0, st, view(*it), s, M, !dual, dual, a - begin, b - begin);
+        end = begin;
+      }
+    } else {
+      replay_parallel(r.segments, m0, n0, s, M, dual, st, lo, hi);
+    }
+  };
+  // Primal pass split at the piecewise-linear checkpoints, newest first: the
+  // records after a checkpoint, then its recovery (postsolve_gpu,
+  // gpu_postsolve.cu:637-663); the dual pass over the whole tape.
+  int64_t range_end = r.records;
+  for (auto it = r.timeline.rbegin(); it != r.timeline.rend(); ++it) {
+    replay(it->tape_position, range_end, false);
+    restore_absolute_value(x, r.absval[size_t(it->payload)], lower, st);
+    range_end = it->tape_position;
   }
+  replay(0, range_end, false);
+  replay(0, r.records, true);
   if (original && y && z && n0) {
     DBuf<uint8_t> prot(size_t(n0), st);
     prot.zero();

@@ -74,7 +74,12 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
 
 // postsolve_gpu (cpp/src/presolve/gpu_postsolve.cu:535-670): device arrays
 // x_org (n0), y_org (m0), z_org (n0) receive the original-space solution.
+// Applies one absolute-value primal recovery to the device vector x
+// (original order); `lower` (device, may be null) bounds the max slacks.
+void restore_absolute_value(double* x, const AbsValueRecovery& r, const double* lower, cudaStream_t st);
+// `lower` bounds the absolute-value max slacks (original->l when null).
 void run_postsolve(const PresolveOutput& out, const double* x_red, const double* y_red, const double* z_red,
-                   const gpp_lp* original, double* x_org, double* y_org, double* z_org);
+                   const gpp_lp* original, double* x_org, double* y_org, double* z_org,
+                   const double* lower = nullptr);
 
 }  // namespace gpp

@@ -114,7 +114,31 @@ __global__ void fixed_pack(int32_t n, const int32_t* __restrict__ flag, const in
     }
 }
 
+__global__ void globalize_ids(int32_t* __restrict__ ids, int64_t n, const int32_t* __restrict__ cols) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    ids[i] = cols[ids[i]];
+}
+
 }  // namespace
+
+void capture_absolute_value(Record& r, AbsValueRecovery&& step) {
+  // update_device_recovery (device_recovery.cu:912-928): column ids through
+  // the record's current map, a checkpoint at the current tape length.
+  auto s = ctx().stream;
+  auto glob = [&](DBuf<int32_t>& ids, int64_t n) {
+    GPP_LAUNCH(globalize_ids, grid_stride_blocks(n), kThreads, 0, s, ids.p, n, r.cols.p);
+  };
+  glob(step.split_t, step.splits);
+  glob(step.split_e, step.splits);
+  glob(step.pair_bound, step.pairs);
+  glob(step.pair_free, step.pairs);
+  glob(step.link_slack, step.links);
+  glob(step.link_t, step.links);
+  glob(step.max_slack, step.max_groups);
+  glob(step.max_t, step.max_entries);
+  r.timeline.push_back(RecoveryCheckpoint{0, int32_t(r.absval.size()), r.records});
+  r.absval.push_back(std::move(step));
+}
 
 void init_record(Record& r, int32_t m, int32_t n) {
   auto s = ctx().stream;

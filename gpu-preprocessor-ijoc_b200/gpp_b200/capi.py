@@ -126,6 +126,16 @@ class Summary(C.Structure):
                 ("folded_rows", i32), ("folded_cols", i32)]
 
 
+class AbsoluteValueRecovery(C.Structure):
+    """gpp_absolute_value_recovery: one step as host arrays (pointers)."""
+    _fields_ = [("pattern", i32), ("split_count", i32), ("split_t", C.c_void_p), ("split_e", C.c_void_p),
+                ("split_rho", C.c_void_p), ("pair_count", i32), ("pair_bound", C.c_void_p),
+                ("pair_free", C.c_void_p), ("linked_count", i32), ("linked_slack", C.c_void_p),
+                ("linked_t", C.c_void_p), ("linked_factor", C.c_void_p), ("max_group_count", i32),
+                ("max_slack", C.c_void_p), ("max_starts", C.c_void_p), ("max_t", C.c_void_p),
+                ("max_factor", C.c_void_p)]
+
+
 _lib = None
 
 
@@ -144,6 +154,7 @@ def load():
         "gpp_run_presolve": (C.c_int, [P(Lp), P(Params), C.c_int, P(Summary)]),
         "gpp_postprocess": (C.c_int, [vp, vp, vp, P(Summary), P(Lp), vp, vp, vp]),
         "gpp_postsolve_device": (C.c_int, [vp, vp, vp, P(Summary), P(Lp), vp, vp, vp]),
+        "gpp_postsolve_device_lower": (C.c_int, [vp, vp, vp, P(Summary), P(Lp), vp, vp, vp, vp]),
         "gpp_free_summary": (None, [P(Summary)]),
         "gpp_export_maps": (C.c_int, [P(Summary), vp, vp]),
         "gpp_tape_sizes": (C.c_int, [P(Summary), P(i64), P(i64), P(i64), P(i64)]),
@@ -186,6 +197,10 @@ def load():
         "gpp_profile_enable": (None, [C.c_int]),
         "gpp_profile_read": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(i64), P(f64), P(f64)]),
         "gpp_inject_alloc_failure": (None, [i64]),
+        "gpp_recovery_checkpoints": (C.c_int, [P(Summary), P(i32), vp, vp, vp]),
+        "gpp_absolute_value_sizes": (C.c_int, [P(Summary), i32, vp]),
+        "gpp_export_absolute_value": (C.c_int, [P(Summary), i32] + [vp] * 12),
+        "gpp_restore_absolute_value": (C.c_int, [vp, P(AbsoluteValueRecovery), i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -209,7 +224,12 @@ EXPORTED = [
     "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free",
     "gpp_schedule_model_create_per_rule", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
+    "gpp_recovery_checkpoints", "gpp_absolute_value_sizes", "gpp_export_absolute_value", "gpp_postsolve_device_lower",
+    "gpp_restore_absolute_value",
 ]
+
+# Absolute-value recovery patterns (include/gpp.h GPP_ABS_*).
+ABS_L1_SPLIT, ABS_GRAPH_L1, ABS_OUTER_PAIR = 1, 2, 3
 
 
 def check(status: int) -> None:

@@ -155,6 +155,60 @@ class Result:
             _raise(lib.gpp_export_tape(C.byref(s), *(a.ctypes.data_as(C.c_void_p) for a in (
                 self.tape_types, self.tape_is, self.tape_vs, self.tape_idx, self.tape_val, self.fixed_idx,
                 self.fixed_val))))
+            self.checkpoints, self.absolute_value = export_recoveries(s)
+
+
+def export_recoveries(s):
+    """The record's primal-recovery checkpoints [(kind, payload, tape
+    position)] and its absolute-value recoveries as dicts of host arrays."""
+    lib = capi.load()
+    k = C.c_int32()
+    _raise(lib.gpp_recovery_checkpoints(C.byref(s), C.byref(k), None, None, None))
+    kinds, payloads = np.zeros(k.value, np.int32), np.zeros(k.value, np.int32)
+    pos = np.zeros(k.value, np.int64)
+    _raise(lib.gpp_recovery_checkpoints(C.byref(s), C.byref(k), *(a.ctypes.data_as(C.c_void_p)
+                                                                   for a in (kinds, payloads, pos))))
+    steps = []
+    for i in range(int((kinds == 0).sum())):
+        z = np.zeros(6, np.int32)
+        _raise(lib.gpp_absolute_value_sizes(C.byref(s), i, z.ctypes.data_as(C.c_void_p)))
+        pattern, ns, npairs, nl, ng, ne = (int(v) for v in z)
+        a = dict(pattern=pattern, split_t=np.zeros(ns, np.int32), split_e=np.zeros(ns, np.int32),
+                 split_rho=np.zeros(ns), pair_bound=np.zeros(npairs, np.int32), pair_free=np.zeros(npairs, np.int32),
+                 link_slack=np.zeros(nl, np.int32), link_t=np.zeros(nl, np.int32), link_factor=np.zeros(nl),
+                 max_slack=np.zeros(ng, np.int32), max_start=np.zeros(ng + 1, np.int32),
+                 max_t=np.zeros(ne, np.int32), max_factor=np.zeros(ne))
+        keys = ("split_t", "split_e", "split_rho", "pair_bound", "pair_free", "link_slack", "link_t", "link_factor",
+                "max_slack", "max_start", "max_t", "max_factor")
+        _raise(lib.gpp_export_absolute_value(C.byref(s), i, *(a[q].ctypes.data_as(C.c_void_p) for q in keys)))
+        steps.append(a)
+    return list(zip(kinds.tolist(), payloads.tolist(), pos.tolist())), steps
+
+
+def restore_absolute_value(x, steps, original_l=None):
+    """postsolve_restore_piecewise_linear_reformulation_absolute_value_gpu on
+    the device vector `x` (torch, float64) with host steps (dicts as
+    export_recoveries returns)."""
+    lib = capi.load()
+    keep = []
+
+    def ptr(v, dt):
+        v = np.ascontiguousarray(v, dtype=dt)
+        keep.append(v)
+        return v.ctypes.data_as(C.c_void_p)
+
+    arr = (capi.AbsoluteValueRecovery * max(1, len(steps)))()
+    for i, a in enumerate(steps):
+        ng = len(a["max_slack"])
+        arr[i] = capi.AbsoluteValueRecovery(
+            a["pattern"], len(a["split_t"]), ptr(a["split_t"], np.int32), ptr(a["split_e"], np.int32),
+            ptr(a["split_rho"], np.float64), len(a["pair_bound"]), ptr(a["pair_bound"], np.int32),
+            ptr(a["pair_free"], np.int32), len(a["link_slack"]), ptr(a["link_slack"], np.int32),
+            ptr(a["link_t"], np.int32), ptr(a["link_factor"], np.float64), ng, ptr(a["max_slack"], np.int32),
+            ptr(a["max_start"] if ng else np.zeros(1), np.int32), ptr(a["max_t"], np.int32),
+            ptr(a["max_factor"], np.float64))
+    lp = C.c_void_p(original_l.data_ptr()) if original_l is not None else None
+    _raise(lib.gpp_restore_absolute_value(C.c_void_p(x.data_ptr()), arr, len(steps), lp))
 
 
 def preprocess(dlp: DeviceLp, params=None) -> capi.Summary:

@@ -473,11 +473,195 @@ def auxiliary_lp(m: int, n: int, seed: int = 0, pairs: float = 0.02, products: f
                   np.concatenate([base.u, np.ones(k)])).ensure_transpose()
 
 
+def _build(m, n, entries, c, AL, AU, l, u) -> HostLP:
+    rows = np.array([r for r, _, _ in entries], np.int64)
+    cols = np.array([j for _, j, _ in entries], np.int64)
+    vals = np.array([a for _, _, a in entries], np.float64)
+    ptr, idx, val = coo_to_csr(m, rows, cols, vals)
+    return HostLP(m, n, ptr, idx, val, np.asarray(c, np.float64), np.asarray(AL, np.float64),
+                  np.asarray(AU, np.float64), np.asarray(l, np.float64), np.asarray(u, np.float64)).ensure_transpose()
+
+
+def _epigraph_pair(rng, t, e, r1, r2, entries, AL, AU, scale=None, mirror=None):
+    """Rows r1, r2 reading  a t - a e >= 0  and  a t + a e >= 0  (a > 0), each
+    row at random in its [0, inf) form or as its (-inf, 0] negation."""
+    a = float(rng.choice([1.0, 2.0, 0.5])) if scale is None else scale
+    for r, se in ((r1, -1.0), (r2, 1.0)):
+        neg = bool(rng.random() < 0.5) if mirror is None else mirror
+        k = -1.0 if neg else 1.0
+        entries += [(r, t, k * a), (r, e, k * se * a)]
+        AL[r], AU[r] = (-INF, 0.0) if neg else (0.0, INF)
+
+
+def l1_split_lp(blocks: int, features: int, seed: int = 0, e_bounds: str = "free", decoy: str = "") -> HostLP:
+    """L1 regression  min sum_i |r_i|,  r_i = b_i - a_i x, in the 3-row block
+    layout the absolute-value reformulation's l1 split accepts: block i is the
+    equality  a_i x + w_i e_i = b_i  and the pair  t_i >= |e_i|  (rows 3i,
+    3i+1, 3i+2).  Feature columns x are free; every e_i is free
+    (e_bounds="free"), in a finite box ("finite") or bounded below only
+    ("lower").  Columns are shuffled so t and e come in both orders.
+    `decoy` breaks one block: "coef" (an epigraph coefficient off by one
+    ulp), "incidence" (t_0 also in block 1's equality), "shared" (block 1's
+    pair reuses block 0's t)."""
+    rng = np.random.default_rng(seed)
+    n = features + 2 * blocks
+    perm = rng.permutation(n)
+    X = perm[:features]
+    T = perm[features:features + blocks]
+    E = perm[features + blocks:]
+    m = 3 * blocks
+    entries = []
+    AL = np.zeros(m)
+    AU = np.zeros(m)
+    c = np.zeros(n)
+    c[X] = np.round(rng.uniform(-0.1, 0.1, features), 3)
+    c[T] = 1.0
+    l = np.full(n, -INF)
+    u = np.full(n, INF)
+    l[T] = 0.0
+    if e_bounds == "finite":
+        l[E], u[E] = -50.0, 50.0
+    elif e_bounds == "lower":
+        l[E] = -50.0
+    for i in range(blocks):
+        k = int(rng.integers(1, min(features, 6) + 1))
+        cols = rng.choice(X, size=k, replace=False)
+        for j in cols:
+            entries.append((3 * i, int(j), float(np.round(rng.uniform(-5, 5), 2) or 1.0)))
+        entries.append((3 * i, int(E[i]), float(rng.choice([1.0, -1.0, 2.0]))))
+        AL[3 * i] = AU[3 * i] = float(np.round(rng.uniform(-10, 10), 2))
+        _epigraph_pair(rng, int(T[i]), int(E[i]), 3 * i + 1, 3 * i + 2, entries, AL, AU)
+    if decoy == "coef":
+        r, j, a = entries[-1]
+        entries[-1] = (r, j, float(np.nextafter(a, 2 * a)))
+    elif decoy == "incidence":
+        entries.append((3, int(T[0]), 1.0))
+    elif decoy == "shared":
+        entries = [(r, int(T[0]) if (r in (4, 5) and j == int(T[1])) else j, a) for r, j, a in entries]
+    return _build(m, n, entries, c, AL, AU, l, u)
+
+
+def graph_l1_lp(blocks: int, features: int, seed: int = 0, group: int = 4, decoy: str = "") -> HostLP:
+    """L1 model in the 4-row block layout of the graph variant: block i is the
+    equality  a_i x + e_i = b_i,  the pair  t_i >= |e_i|  and  s - beta t_i >= 0
+    for an auxiliary s shared by `group` consecutive blocks (zero cost,
+    [0, inf)), so postsolve recovers s = max beta t.  `decoy`: "aux_cost"
+    (one auxiliary has a cost), "extra_row" (block 0's fourth row has a
+    third entry), "r3_sign" (a fourth row with the wrong sign)."""
+    rng = np.random.default_rng(seed)
+    aux = (blocks + group - 1) // group
+    n = features + 2 * blocks + aux
+    perm = rng.permutation(n)
+    X = perm[:features]
+    T = perm[features:features + blocks]
+    E = perm[features + blocks:features + 2 * blocks]
+    S = perm[features + 2 * blocks:]
+    m = 4 * blocks
+    entries = []
+    AL = np.zeros(m)
+    AU = np.zeros(m)
+    c = np.zeros(n)
+    c[X] = np.round(rng.uniform(-0.1, 0.1, features), 3)
+    c[T] = np.round(rng.uniform(0.5, 2.0, blocks), 2)
+    l = np.full(n, -INF)
+    u = np.full(n, INF)
+    l[T] = 0.0
+    l[S] = 0.0
+    for i in range(blocks):
+        k = int(rng.integers(1, min(features, 6) + 1))
+        for j in rng.choice(X, size=k, replace=False):
+            entries.append((4 * i, int(j), float(np.round(rng.uniform(-5, 5), 2) or 1.0)))
+        entries.append((4 * i, int(E[i]), float(rng.choice([1.0, -1.0, 3.0]))))
+        AL[4 * i] = AU[4 * i] = float(np.round(rng.uniform(-10, 10), 2))
+        _epigraph_pair(rng, int(T[i]), int(E[i]), 4 * i + 1, 4 * i + 2, entries, AL, AU, scale=1.0)
+        beta = float(rng.choice([1.0, 0.5, 2.0, 1.5]))
+        sgn = -1.0 if (decoy == "r3_sign" and i == blocks - 1) else 1.0
+        entries += [(4 * i + 3, int(S[i // group]), sgn * 1.0), (4 * i + 3, int(T[i]), -beta)]
+        AL[4 * i + 3], AU[4 * i + 3] = 0.0, INF
+    if decoy == "aux_cost":
+        c[S[0]] = 0.25
+    elif decoy == "extra_row":
+        entries.append((3, int(X[0]), 1.0))
+    return _build(m, n, entries, c, AL, AU, l, u)
+
+
+def outer_l1_lp(pairs: int, blocks: int, features: int = 6, seed: int = 0, share: bool = True,
+                decoy: str = "") -> HostLP:
+    """The outer-pair + linked-l1 layout: `pairs` 3-row groups forcing a free
+    column f equal to a column b in [0, 10] (with `share`, every second pair
+    reuses the previous b), then `blocks` 8-row blocks: an equality holding e
+    and a few features (sometimes an outer free column), the pair q >= |e|
+    on (e, q) with e's column before q's, the link alpha q - s = 0 and four
+    rows x - s >= 0 on positive-cost columns x in [0, inf).  `decoy`:
+    "dup_free" (two pairs share a free column), "role" (a block's q appears
+    in another block's equality), "x_cost" (a zero-cost x)."""
+    rng = np.random.default_rng(seed)
+    entries = []
+    AL, AU = [], []
+    c, l, u = [], [], []
+
+    def col(cost, lo, hi):
+        c.append(cost)
+        l.append(lo)
+        u.append(hi)
+        return len(c) - 1
+
+    def row(ent, lo, hi):
+        r = len(AL)
+        entries.extend((r, j, a) for j, a in ent)
+        AL.append(lo)
+        AU.append(hi)
+
+    bounds, frees = [], []
+    for p in range(pairs):
+        b = bounds[-1] if (share and p % 2 == 1) else col(float(np.round(rng.uniform(0.5, 3), 2)), 0.0, 10.0)
+        f = col(float(np.round(rng.uniform(-1, 1), 2)), -INF, INF)
+        if decoy == "dup_free" and p == 1:
+            c.pop(); l.pop(); u.pop()
+            f = frees[0]
+        bounds.append(b)
+        frees.append(f)
+    feats = [col(float(np.round(rng.uniform(-0.1, 0.1), 3)), -INF, INF) for _ in range(features)]
+    # Pair rows come after all columns exist so (b, f) is in column order.
+    for b, f in zip(bounds, frees):
+        assert b < f
+        row([(b, 1.0), (f, -1.0)], 0.0, INF)
+        row([(b, 1.0), (f, 1.0)], 0.0, INF)
+        row([(b, -1.0), (f, 1.0)], 0.0, INF)
+    qs = []
+    for i in range(blocks):
+        e = col(0.0, -INF, INF)
+        q = col(float(np.round(rng.uniform(0.0, 1.0), 2)), 0.0, INF)
+        s = col(0.0, 0.0, INF)
+        xs = [col(0.0 if (decoy == "x_cost" and i == 0 and k == 0) else float(np.round(rng.uniform(0.1, 2), 2)),
+                  0.0, INF) for k in range(4)]
+        qs.append(q)
+        dense = [(j, float(np.round(rng.uniform(-5, 5), 2) or 1.0))
+                 for j in rng.choice(feats, size=min(3, features), replace=False)]
+        if frees and rng.random() < 0.5:
+            dense.append((int(rng.choice(frees)), 1.5))
+        dense.append((e, float(rng.choice([1.0, -2.0]))))
+        if decoy == "role" and i == 1:
+            dense.append((qs[0], 1.0))
+        rhs = float(np.round(rng.uniform(-10, 10), 2))
+        row(dense, rhs, rhs)
+        row([(e, -1.0), (q, 1.0)], 0.0, INF)
+        row([(e, 1.0), (q, 1.0)], 0.0, INF)
+        alpha = float(rng.choice([1.0, 0.5, 2.0]))
+        row([(q, alpha), (s, -1.0)], 0.0, 0.0)
+        for x in xs:
+            row([(s, -1.0), (x, 1.0)], 0.0, INF)
+    n = len(c)
+    return _build(len(AL), n, entries, c, AL, AU, l, u)
+
+
 def workload(name: str, seed: int = 0) -> HostLP:
     """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
     'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows),
     'replicated:MxN*K' (K identical copies plus a coupling row), 'setcover:MxN' (unit set covering),
-    'auxiliary:MxN' (random family plus projected-auxiliary blocks), 'qap:N'."""
+    'auxiliary:MxN' (random family plus projected-auxiliary blocks), 'qap:N', and the
+    absolute-value layouts 'l1split:KxP' (K blocks, P features), 'graphl1:KxP' and
+    'outerl1:PAIRSxBLOCKS'."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -503,6 +687,15 @@ def workload(name: str, seed: int = 0) -> HostLP:
         return setcover_lp(m, n, seed)
     if name.startswith("qap:"):
         return qap_lp(int(name.split(":")[1]), seed)
+    if name.startswith("l1split:"):
+        k, p = (int(v) for v in name.split(":")[1].split("x"))
+        return l1_split_lp(k, p, seed)
+    if name.startswith("graphl1:"):
+        k, p = (int(v) for v in name.split(":")[1].split("x"))
+        return graph_l1_lp(k, p, seed)
+    if name.startswith("outerl1:"):
+        pairs, blocks = (int(v) for v in name.split(":")[1].split("x"))
+        return outer_l1_lp(pairs, blocks, seed=seed)
     raise ValueError(f"unknown workload {name!r}")
 
 

@@ -108,11 +108,11 @@ typedef struct gpp_params {
   double parallel_columns_max_abs_ratio;
   int32_t parallel_columns_scale_guard_max_group_size;
   int32_t parallel_columns_scale_guard_min_groups;
-  /* The structure-specific startup rules (column domination, two-row
-   * variable elimination, zero-cost product variables, the piecewise-linear
-   * reformulations) and their settings are carried for layout parity with
-   * PresolveParams; this engine does not run those rules, so the Startup
-   * phase only consumes its iteration. */
+  /* The structure-specific startup rules: column domination, two-row
+   * variable elimination, zero-cost product variables and the
+   * absolute-value piecewise-linear reformulation run as in the reference;
+   * the variable-pair reformulation's settings are carried for layout
+   * parity with PresolveParams but that rule is not run. */
   uint8_t enable_structure_specific_rules;
   uint8_t enable_two_row_variable_elimination;
   int32_t two_row_variable_elimination_max_row_nnz;
@@ -147,6 +147,13 @@ typedef struct gpp_params {
   uint8_t enable_startup;
   int64_t bound_strengthening_bound_only_nnz_round_budget;
 } gpp_params;
+
+/* piecewise_linear_reformulation_absolute_value_residual_bound_mode values
+ * (PiecewiseLinearReformulationAbsoluteValueResidualBoundMode,
+ * presolve_structs.hpp:15-26). */
+#define GPP_RESIDUAL_PRESERVE_FINITE 0
+#define GPP_RESIDUAL_STRICT_FREE_ONLY 1
+#define GPP_RESIDUAL_LEGACY_WIDE_AS_FREE 2
 
 /* Reference defaults (presolve_structs.hpp:28-158). */
 GPP_API void gpp_default_params(gpp_params* params);
@@ -212,6 +219,14 @@ GPP_API int gpp_postsolve_device(const double* x_red, const double* y_red, const
                          const gpp_summary* summary, const gpp_lp* original,
                          double* x_org, double* y_org, double* z_org);
 
+/* postsolve_gpu with its original_l argument (gpu_postsolve.hpp:26-31):
+ * original_l (DEVICE, n0 entries, may be NULL) bounds the absolute-value
+ * reformulation's max slacks below; when NULL, original->l is used (0 when
+ * `original` is NULL too).  gpp_postsolve_device is this with NULL. */
+GPP_API int gpp_postsolve_device_lower(const double* x_red, const double* y_red, const double* z_red,
+                                       const gpp_summary* summary, const gpp_lp* original,
+                                       const double* original_l, double* x_org, double* y_org, double* z_org);
+
 /* gpu_preprocessor::free_summary (gpu_preprocessor.hpp:35-39) /
  * presolve::free_gpu_presolve_reduced_lp (gpu_presolve.hpp:38).
  * Idempotent: a second call is a no-op. */
@@ -233,6 +248,72 @@ GPP_API int gpp_tape_sizes(const gpp_summary* summary, int64_t* records, int64_t
 GPP_API int gpp_export_tape(const gpp_summary* summary, int32_t* types, int64_t* index_starts,
                     int64_t* value_starts, int32_t* indices, double* vals,
                     int32_t* fixed_idx, double* fixed_val);
+
+/* ---- Piecewise-linear primal recoveries ---------------------------------- */
+
+/* Layout an absolute-value reformulation matched: the reference's recovery
+ * `pattern` strings (rule_piecewise_linear_reformulation_absolute_value.cu:
+ * "l1_split_3row" :1998, "graph_l1_substitution" :2235,
+ * "outer_pair_linked_l1" :2683). */
+#define GPP_ABS_L1_SPLIT 1
+#define GPP_ABS_GRAPH_L1 2
+#define GPP_ABS_OUTER_PAIR 3
+
+/* One absolute-value primal recovery step
+ * (PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep,
+ * presolve_structs.hpp:207-236) as HOST arrays of original column ids.
+ * Applied as: splits (t, e) <- (t + e, (t - e) / rho); outer pairs
+ * free <- bound; linked slacks slack <- factor * t; max-slack group g
+ * (entries [max_starts[g], max_starts[g + 1])) slack <- max(l_slack,
+ * max factor * t). */
+typedef struct gpp_absolute_value_recovery {
+  int32_t pattern;
+  int32_t split_count;
+  const int32_t* split_t;
+  const int32_t* split_e;
+  const double* split_rho;
+  int32_t pair_count;
+  const int32_t* pair_bound;
+  const int32_t* pair_free;
+  int32_t linked_count;
+  const int32_t* linked_slack;
+  const int32_t* linked_t;
+  const double* linked_factor;
+  int32_t max_group_count;
+  const int32_t* max_slack;
+  const int32_t* max_starts;    /* max_group_count + 1 entries */
+  const int32_t* max_t;
+  const double* max_factor;
+} gpp_absolute_value_recovery;
+
+/* The record's primal-recovery checkpoints (primal_recovery_timeline,
+ * presolve_structs.hpp:256-266, 362).  *count is always written; kinds
+ * (0 = absolute value), payloads (index of the recovery of that kind) and
+ * tape_positions (records replayed before the recovery is applied), when not
+ * NULL, receive *count entries. */
+GPP_API int gpp_recovery_checkpoints(const gpp_summary* summary, int32_t* count, int32_t* kinds,
+                                     int32_t* payloads, int64_t* tape_positions);
+
+/* Sizes of absolute-value recovery `index`: sizes[0] pattern, [1] splits,
+ * [2] outer pairs, [3] linked slacks, [4] max-slack groups, [5] max-slack
+ * entries. */
+GPP_API int gpp_absolute_value_sizes(const gpp_summary* summary, int32_t index, int32_t sizes[6]);
+
+/* Copies absolute-value recovery `index` to HOST arrays sized by
+ * gpp_absolute_value_sizes (max_starts: groups + 1); any pointer may be NULL. */
+GPP_API int gpp_export_absolute_value(const gpp_summary* summary, int32_t index, int32_t* split_t,
+                                      int32_t* split_e, double* split_rho, int32_t* pair_bound,
+                                      int32_t* pair_free, int32_t* linked_slack, int32_t* linked_t,
+                                      double* linked_factor, int32_t* max_slack, int32_t* max_starts,
+                                      int32_t* max_t, double* max_factor);
+
+/* postsolve_restore_piecewise_linear_reformulation_absolute_value_gpu
+ * (presolve/gpu_postsolve.hpp:15-18): applies `count` steps to the DEVICE
+ * vector x_org, the last step first.  original_l (DEVICE, may be NULL) gives
+ * the max slacks' lower bounds (0 when NULL or not finite).  Column ids must
+ * be below the length of x_org; they are not checked against it. */
+GPP_API int gpp_restore_absolute_value(double* x_org, const gpp_absolute_value_recovery* steps,
+                                       int32_t count, const double* original_l);
 
 /* folding::copy_map_to_host (folding/folding.hpp:22): the 1-based colour of
  * every original row / column and the unfold scales 1/|colour|, as HOST

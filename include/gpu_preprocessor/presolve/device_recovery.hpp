@@ -1,7 +1,8 @@
 // Diagnostic export of the recovery record (GPU-Preprocessor's
 // cpp/include/gpu_preprocessor/presolve/device_recovery.hpp:84,
 // export_recovery_record), over gpp_export_maps / gpp_tape_sizes /
-// gpp_export_tape.  Postsolve never needs it.
+// gpp_export_tape / gpp_recovery_checkpoints / gpp_export_absolute_value.
+// Postsolve never needs it.
 #pragma once
 
 #include <cstdint>
@@ -38,6 +39,46 @@ inline void export_recovery_record(PresolveRecordGpu& record) {
   for (std::size_t k = 0; k < is.size(); ++k) {
     t.index_starts[k] = checked_nnz_offset(is[k]);
     t.value_starts[k] = checked_nnz_offset(vs[k]);
+  }
+  // Primal-recovery checkpoints and the absolute-value payloads.
+  std::int32_t count = 0;
+  throw_on_status(gpp_recovery_checkpoints(s, &count, nullptr, nullptr, nullptr), "export_recovery_record checkpoints");
+  std::vector<std::int32_t> kinds(static_cast<std::size_t>(count)), payloads(static_cast<std::size_t>(count));
+  std::vector<std::int64_t> positions(static_cast<std::size_t>(count));
+  throw_on_status(gpp_recovery_checkpoints(s, &count, kinds.data(), payloads.data(), positions.data()),
+                  "export_recovery_record checkpoints");
+  record.primal_recovery_timeline.clear();
+  record.piecewise_linear_reformulation_absolute_value_recoveries.clear();
+  for (std::int32_t k = 0; k < count; ++k) {
+    record.primal_recovery_timeline.push_back({static_cast<PrimalRecoveryKind>(kinds[std::size_t(k)]),
+                                               checked_nnz_offset(payloads[std::size_t(k)]),
+                                               checked_nnz_offset(positions[std::size_t(k)])});
+    if (kinds[std::size_t(k)] != 0) continue;
+    std::int32_t z[6];
+    throw_on_status(gpp_absolute_value_sizes(s, payloads[std::size_t(k)], z), "export_recovery_record sizes");
+    std::vector<std::int32_t> st(z[1]), se(z[1]), pb(z[2]), pf(z[2]), ls(z[3]), lt(z[3]), ms(z[4]),
+        mstart(std::size_t(z[4]) + 1), mt(z[5]);
+    std::vector<double> sr(z[1]), lf(z[3]), mf(z[5]);
+    throw_on_status(gpp_export_absolute_value(s, payloads[std::size_t(k)], st.data(), se.data(), sr.data(), pb.data(),
+                                              pf.data(), ls.data(), lt.data(), lf.data(), ms.data(), mstart.data(),
+                                              mt.data(), mf.data()),
+                    "export_recovery_record absolute value");
+    PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep step;
+    step.pattern = z[0] == GPP_ABS_L1_SPLIT ? "l1_split_3row"
+                   : z[0] == GPP_ABS_GRAPH_L1 ? "graph_l1_substitution"
+                                              : "outer_pair_linked_l1";
+    for (std::int32_t i = 0; i < z[1]; ++i) step.splits.push_back({st[std::size_t(i)], se[std::size_t(i)], sr[std::size_t(i)]});
+    for (std::int32_t i = 0; i < z[2]; ++i) step.outer_pairs.push_back({pb[std::size_t(i)], pf[std::size_t(i)]});
+    for (std::int32_t i = 0; i < z[3]; ++i)
+      step.linked_slacks.push_back({ls[std::size_t(i)], lt[std::size_t(i)], lf[std::size_t(i)]});
+    for (std::int32_t g = 0; g < z[4]; ++g) {
+      AbsoluteValueMaxSlackRecovery m;
+      m.slack_col = ms[std::size_t(g)];
+      m.t_cols.assign(mt.begin() + mstart[std::size_t(g)], mt.begin() + mstart[std::size_t(g) + 1]);
+      m.factors.assign(mf.begin() + mstart[std::size_t(g)], mf.begin() + mstart[std::size_t(g) + 1]);
+      step.max_slacks.push_back(std::move(m));
+    }
+    record.piecewise_linear_reformulation_absolute_value_recoveries.push_back(std::move(step));
   }
 }
 

@@ -12,6 +12,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <limits>
+#include <string>
 #include <vector>
 
 #include "gpp.h"
@@ -190,6 +191,52 @@ enum class PostsolveReductionType : std::int32_t {
   FmeCol = 14,
 };
 
+// Primal recovery of the absolute-value reformulation (the reference's
+// presolve_structs.hpp:207-236): host views filled by export_recovery_record
+// and the input of postsolve_restore_piecewise_linear_reformulation_absolute_value_gpu.
+struct PiecewiseLinearReformulationAbsoluteValueSplitRecovery {
+  std::int32_t t_col = -1;
+  std::int32_t e_col = -1;
+  double rho = 1.0;
+};
+
+struct AbsoluteValueOuterPairRecovery {
+  std::int32_t bound_col = -1;
+  std::int32_t free_col = -1;
+};
+
+struct AbsoluteValueLinkedSlackRecovery {
+  std::int32_t slack_col = -1;
+  std::int32_t t_col = -1;
+  double factor = 0.0;
+};
+
+struct AbsoluteValueMaxSlackRecovery {
+  std::int32_t slack_col = -1;
+  std::vector<std::int32_t> t_cols;
+  std::vector<double> factors;
+};
+
+struct PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep {
+  std::string pattern;
+  std::vector<PiecewiseLinearReformulationAbsoluteValueSplitRecovery> splits;
+  std::vector<AbsoluteValueOuterPairRecovery> outer_pairs;
+  std::vector<AbsoluteValueLinkedSlackRecovery> linked_slacks;
+  std::vector<AbsoluteValueMaxSlackRecovery> max_slacks;
+};
+
+// Where a primal recovery sits among the tape records (presolve_structs.hpp:252-266).
+enum class PrimalRecoveryKind : std::uint8_t {
+  PiecewiseLinearReformulationAbsoluteValue = 0,
+  PiecewiseLinearReformulationVariablePair = 1,
+};
+
+struct PrimalRecoveryCheckpoint {
+  PrimalRecoveryKind kind = PrimalRecoveryKind::PiecewiseLinearReformulationAbsoluteValue;
+  NnzOffset payload_index = -1;
+  NnzOffset tape_position = 0;
+};
+
 // Host view of the recovery tape, filled only by export_recovery_record.
 // Postsolve never needs it: the tape stays on the device.
 struct PostsolveTape {
@@ -219,6 +266,9 @@ struct PresolveRecordGpu {
       tape.types.swap(o.tape.types); tape.index_starts.swap(o.tape.index_starts);
       tape.value_starts.swap(o.tape.value_starts); tape.indices.swap(o.tape.indices);
       tape.vals.swap(o.tape.vals);
+      piecewise_linear_reformulation_absolute_value_recoveries.swap(
+          o.piecewise_linear_reformulation_absolute_value_recoveries);
+      primal_recovery_timeline.swap(o.primal_recovery_timeline);
       handle = o.handle;
       o.handle = gpp_summary{};
     }
@@ -236,6 +286,9 @@ struct PresolveRecordGpu {
   double obj_constant_old = 0.0;
   double obj_constant_new = 0.0;
   PostsolveTape tape;
+  std::vector<PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep>
+      piecewise_linear_reformulation_absolute_value_recoveries;
+  std::vector<PrimalRecoveryCheckpoint> primal_recovery_timeline;
   gpp_summary handle{};  // the C-ABI summary whose record this is
 };
 

@@ -8,7 +8,9 @@
 // LP file format: see gpp_b200/lpgen.py save_lp.  Outputs (raw little-endian):
 // meta.txt, A_ptr/A_idx/A_val, AT_ptr/AT_idx/AT_val, c/l/u/AL/AU, row_map,
 // col_map, fixed_idx/fixed_val, tape_types/tape_is/tape_vs/tape_idx/tape_val,
-// and (with --postsolve) x_org/y_org/z_org.
+// ckpt_kind/ckpt_payload/ckpt_position (primal-recovery checkpoints),
+// abs<k>_* (absolute-value recoveries; pattern in meta.txt), and (with
+// --postsolve) x_org/y_org/z_org.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -95,6 +97,11 @@ int main(int argc, char** argv) {
       else if (k == "doubleton_equations_max_fill_in_proxy") p.doubleton_equations_max_fill_in_proxy = v;
       else if (k == "doubleton_equations_min_selected_per_batch") p.doubleton_equations_min_selected_per_batch = v;
       else if (k == "doubleton_equations_min_selected_ratio") p.doubleton_equations_min_selected_ratio = dv;
+      else if (k == "piecewise_linear_reformulation_absolute_value_residual_bound_mode")
+        p.piecewise_linear_reformulation_absolute_value_residual_bound_mode =
+            static_cast<gp::presolve::PiecewiseLinearReformulationAbsoluteValueResidualBoundMode>(v);
+      else if (k == "piecewise_linear_reformulation_absolute_value_residual_bound_as_free_min")
+        p.piecewise_linear_reformulation_absolute_value_residual_bound_as_free_min = dv;
       else throw std::invalid_argument("unknown parameter " + k);
 #undef FLAG
     }
@@ -190,6 +197,44 @@ int main(int argc, char** argv) {
     save(out, "tape_vs", record.tape.value_starts);
     save(out, "tape_idx", record.tape.indices);
     save(out, "tape_val", record.tape.vals);
+    // Primal-recovery checkpoints and the absolute-value recoveries.
+    {
+      std::vector<int> kinds, payloads;
+      std::vector<long long> positions;
+      for (const auto& c : record.primal_recovery_timeline) {
+        kinds.push_back(int(c.kind));
+        payloads.push_back(int(c.payload_index));
+        positions.push_back((long long)c.tape_position);
+      }
+      save(out, "ckpt_kind", kinds);
+      save(out, "ckpt_payload", payloads);
+      save(out, "ckpt_position", positions);
+      meta << "absolute_value_steps " << record.piecewise_linear_reformulation_absolute_value_recoveries.size()
+           << "\n";
+      int k = 0;
+      for (const auto& a : record.piecewise_linear_reformulation_absolute_value_recoveries) {
+        const std::string p = "abs" + std::to_string(k++) + "_";
+        meta << p << "pattern " << a.pattern << "\n";
+        std::vector<int> st, se, pb, pf, ls, lt, ms, mstart{0}, mt;
+        std::vector<double> sr, lf, mf;
+        for (const auto& x : a.splits) { st.push_back(x.t_col); se.push_back(x.e_col); sr.push_back(x.rho); }
+        for (const auto& x : a.outer_pairs) { pb.push_back(x.bound_col); pf.push_back(x.free_col); }
+        for (const auto& x : a.linked_slacks) { ls.push_back(x.slack_col); lt.push_back(x.t_col); lf.push_back(x.factor); }
+        for (const auto& g : a.max_slacks) {
+          ms.push_back(g.slack_col);
+          mt.insert(mt.end(), g.t_cols.begin(), g.t_cols.end());
+          mf.insert(mf.end(), g.factors.begin(), g.factors.end());
+          mstart.push_back(int(mt.size()));
+        }
+        save(out, (p + "split_t").c_str(), st); save(out, (p + "split_e").c_str(), se);
+        save(out, (p + "split_rho").c_str(), sr);
+        save(out, (p + "pair_bound").c_str(), pb); save(out, (p + "pair_free").c_str(), pf);
+        save(out, (p + "link_slack").c_str(), ls); save(out, (p + "link_t").c_str(), lt);
+        save(out, (p + "link_factor").c_str(), lf);
+        save(out, (p + "max_slack").c_str(), ms); save(out, (p + "max_start").c_str(), mstart);
+        save(out, (p + "max_t").c_str(), mt); save(out, (p + "max_factor").c_str(), mf);
+      }
+    }
     if (!xs.empty()) {
       auto x = load<double>(xs), y = load<double>(ys), z = load<double>(zs);
       double *dx = up(x), *dy = up(y), *dz = up(z);

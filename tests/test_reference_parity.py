@@ -57,7 +57,7 @@ def run_reference(lp, rules, extra=None, point=None):
     for line in open(os.path.join(d, "meta.txt")):
         k, *v = line.split()
         meta[k] = v[0] if len(v) == 1 else v
-    out = {"meta": meta}
+    out = {"meta": meta, "dir": d}
     spec = {"A_ptr": np.int32, "A_idx": np.int32, "A_val": np.float64, "AT_ptr": np.int32, "AT_idx": np.int32,
             "AT_val": np.float64, "c": np.float64, "l": np.float64, "u": np.float64, "AL": np.float64,
             "AU": np.float64, "row_map": np.int32, "col_map": np.int32, "fixed_idx": np.int32,
