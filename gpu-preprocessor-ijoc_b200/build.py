@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "--fmad=false",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
          "--extended-lambda", "-I", os.path.join(HERE, "..", "include")]
-UNITS = ["common.cu", "live.cu", "compact.cu", "recovery.cu", "rules_cleanup.cu", "rules_bound.cu", "rules_propagation.cu", "sort.cu", "sort_static.cu", "rules_parallel.cu", "rules_singleton.cu", "rules_doubleton.cu", "rules_startup.cu", "rules_pwl_abs.cu",
+UNITS = ["common.cu", "live.cu", "compact.cu", "recovery.cu", "rules_cleanup.cu", "rules_bound.cu", "rules_propagation.cu", "sort.cu", "sort_static.cu", "rules_parallel.cu", "rules_singleton.cu", "rules_doubleton.cu", "rules_startup.cu", "rules_pwl_abs.cu", "rules_pwl_pair.cu",
          "engine.cu", "postsolve.cu", "folding.cu", "schedule_mlp.cu", "mps_reader.cpp", "capi.cu"]
 
 

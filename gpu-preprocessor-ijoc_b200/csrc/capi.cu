@@ -660,6 +660,34 @@ int gpp_export_absolute_value(const gpp_summary* summary, int32_t index, int32_t
   });
 }
 
+int gpp_variable_pair_size(const gpp_summary* summary, int32_t index, int32_t* count) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const auto& v = summary->record->out.record.varpair;
+    if (index < 0 || size_t(index) >= v.size()) throw std::invalid_argument("no variable-pair recovery at that index");
+    if (!count) throw std::invalid_argument("count is null");
+    *count = v[size_t(index)].count;
+  });
+}
+
+int gpp_export_variable_pair(const gpp_summary* summary, int32_t index, int32_t* plus_cols, int32_t* minus_cols,
+                             int32_t* root_plus_cols, int32_t* root_minus_cols, double* plus_shift,
+                             double* minus_shift) {
+  return guarded([&] {
+    if (!summary || !summary->record) throw std::invalid_argument("summary has no recovery record");
+    const auto& v = summary->record->out.record.varpair;
+    if (index < 0 || size_t(index) >= v.size()) throw std::invalid_argument("no variable-pair recovery at that index");
+    const auto& r = v[size_t(index)];
+    copy_out(plus_cols, r.plus, r.count);
+    copy_out(minus_cols, r.minus, r.count);
+    copy_out(root_plus_cols, r.root_plus, r.count);
+    copy_out(root_minus_cols, r.root_minus, r.count);
+    copy_out(plus_shift, r.plus_shift, r.count);
+    copy_out(minus_shift, r.minus_shift, r.count);
+    gpp::ctx().sync("export variable-pair recovery");
+  });
+}
+
 int gpp_restore_absolute_value(double* x_org, const gpp_absolute_value_recovery* steps, int32_t count,
                                const double* original_l) {
   return guarded([&] {

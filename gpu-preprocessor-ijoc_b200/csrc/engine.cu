@@ -168,6 +168,10 @@ struct Engine {
       capture_absolute_value(r, std::move(*pl.absval));
       pl.absval.reset();
     }
+    if (pl.varpair) {
+      capture_variable_pair(r, std::move(*pl.varpair));
+      pl.varpair.reset();
+    }
     if (!cleanup_captured && n_new != n) append_fixed(r, pl.keep_col.p, nullptr, pl.l.p, pl.u.p, n);
     if (m_new != r.m) {
       DBuf<int32_t> rows(size_t(m_new), s());
@@ -246,10 +250,10 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
     // off when enable_structure_specific_rules is (:2088-2094).  Column
     // domination, two-row variable elimination and zero-cost product
     // variables share one plan, each seeing the deletions of those before it,
-    // and the plan is applied once; then the absolute-value reformulation,
-    // gated by its prefix screen, runs on its own materialised plan (:2447).
-    // The variable-pair reformulation is not run.  The phase consumes one
-    // iteration (:2453).
+    // and the plan is applied once; then the variable-pair reformulation
+    // (:2416-2445) and the absolute-value reformulation, gated by its prefix
+    // screen (:2447), each on its own materialised plan.  The phase consumes
+    // one iteration (:2453).
     const bool batch = p.enable_structure_specific_rules &&
                        (p.enable_column_domination || p.enable_two_row_variable_elimination ||
                         p.enable_zero_cost_product_variables);
@@ -261,6 +265,10 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
             rule_zero_cost_product_variables(e.plan, cur, p);
         }))
       e.materialize("startup");
+    if (p.enable_structure_specific_rules && p.enable_piecewise_linear_reformulation_variable_pair && !e.terminal &&
+        !time_exceeded())
+      e.materialized_rule(true, "startup_piecewise_linear_reformulation_variable_pair",
+                          [&](Plan& pl) { rule_variable_pair(pl, cur, p); });
     if (p.enable_structure_specific_rules && p.enable_piecewise_linear_reformulation_absolute_value &&
         !e.terminal && !time_exceeded() && absolute_value_prefix_screen(cur))
       e.materialized_rule(true, "startup_piecewise_linear_reformulation_absolute_value",

@@ -94,12 +94,22 @@ struct AbsValueRecovery {
   int32_t splits = 0, pairs = 0, links = 0, max_groups = 0, max_entries = 0;
 };
 
+// Primal recovery of one variable-pair reformulation (reference
+// PiecewiseLinearReformulationVariablePairRecoveryStep, presolve_structs.hpp:243-250):
+// x[plus_k] = plus_shift_k + x[root_plus_k], x[minus_k] = minus_shift_k +
+// x[root_minus_k], every root value read before any member is written.
+struct VarPairRecovery {
+  DBuf<int32_t> plus, minus, root_plus, root_minus;
+  DBuf<double> plus_shift, minus_shift;
+  int32_t count = 0;
+};
+
 // Where a primal recovery sits in the tape (reference PrimalRecoveryCheckpoint,
 // presolve_structs.hpp:256-266): records at or after `tape_position` are
 // replayed (primal pass) before it is applied.
 struct RecoveryCheckpoint {
-  int32_t kind = 0;        // 0 absolute value
-  int32_t payload = 0;     // index into Record::absval
+  int32_t kind = 0;        // 0 absolute value, 1 variable pair
+  int32_t payload = 0;     // index into Record::absval / Record::varpair
   int64_t tape_position = 0;
 };
 
@@ -110,6 +120,7 @@ struct Record {
   std::vector<PostsolveSegment> segments;
   std::vector<FixedSegment> fixed;
   std::vector<AbsValueRecovery> absval;
+  std::vector<VarPairRecovery> varpair;
   std::vector<RecoveryCheckpoint> timeline;
   int64_t records = 0, indices = 0, values = 0;
 };
@@ -135,6 +146,7 @@ struct Plan {
   DevCsr new_A;                  // owned when has_new_A
   std::vector<PostsolveSegment> tape;   // local indices until captured
   std::unique_ptr<AbsValueRecovery> absval;   // set by the absolute-value reformulation
+  std::unique_ptr<VarPairRecovery> varpair;   // set by the variable-pair reformulation
 };
 
 struct Stats {
@@ -230,6 +242,7 @@ PostsolveSegment make_segment(int64_t count, int64_t n_idx, int64_t n_val);
 // Moves an absolute-value recovery into the record (column ids made
 // original through r.cols) with a checkpoint at the current tape length.
 void capture_absolute_value(Record& r, AbsValueRecovery&& step);
+void capture_variable_pair(Record& r, VarPairRecovery&& step);
 
 // rules_*.cu
 void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p);
@@ -252,6 +265,9 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
 // rule as the reference's does.
 bool absolute_value_prefix_screen(const WorkingLp& lp);
 void rule_absolute_value(Plan& plan, const WorkingLp& lp, const gpp_params& p);
+// rules_pwl_pair.cu: piecewise-linear reformulation of variable pairs
+// (epigraph, else shifted antipodal).
+void rule_variable_pair(Plan& plan, const WorkingLp& lp, const gpp_params& p);
 
 // Row-wise shift sum_j a_ij * v_j over kept rows and selected columns, in
 // ascending column order (deterministic replacement of atomicAdd shifts).

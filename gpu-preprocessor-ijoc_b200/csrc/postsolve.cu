@@ -665,7 +665,35 @@ __global__ void restore_max_slacks(double* __restrict__ x, const int32_t* __rest
   }
 }
 
+// Roots' values first, then every member (restore_piecewise_linear_reformulation_variable_pair,
+// postsolve_piecewise_linear_reformulation_variable_pair.cu:9-95).
+__global__ void cache_pair_roots(double* __restrict__ pc, double* __restrict__ mc, const double* __restrict__ x,
+                                 const int32_t* __restrict__ rp, const int32_t* __restrict__ rm, int k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    pc[i] = x[rp[i]];
+    mc[i] = x[rm[i]];
+  }
+}
+__global__ void restore_pair_members(double* __restrict__ x, const int32_t* __restrict__ plus,
+                                     const int32_t* __restrict__ minus, const double* __restrict__ ps,
+                                     const double* __restrict__ ms, const double* __restrict__ pc,
+                                     const double* __restrict__ mc, int k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    x[plus[i]] = ps[i] + pc[i];
+    x[minus[i]] = ms[i] + mc[i];
+  }
+}
+
 }  // namespace
+
+void restore_variable_pair(double* x, const VarPairRecovery& r, cudaStream_t st) {
+  if (!r.count) return;
+  DBuf<double> pc(size_t(r.count), st), mc(size_t(r.count), st);
+  GPP_LAUNCH(cache_pair_roots, grid_stride_blocks(r.count), kThreads, 0, st, pc.p, mc.p, x, r.root_plus.p,
+             r.root_minus.p, r.count);
+  GPP_LAUNCH(restore_pair_members, grid_stride_blocks(r.count), kThreads, 0, st, x, r.plus.p, r.minus.p,
+             r.plus_shift.p, r.minus_shift.p, pc.p, mc.p, r.count);
+}
 
 void restore_absolute_value(double* x, const AbsValueRecovery& r, const double* lower, cudaStream_t st) {
   GPP_LAUNCH(restore_splits, grid_stride_blocks(r.splits), kThreads, 0, st, x, r.split_t.p, r.split_e.p,
@@ -721,7 +749,8 @@ void run_postsolve(const PresolveOutput& out, const double* x_red, const double*
   int64_t range_end = r.records;
   for (auto it = r.timeline.rbegin(); it != r.timeline.rend(); ++it) {
     replay(it->tape_position, range_end, false);
-    restore_absolute_value(x, r.absval[size_t(it->payload)], lower, st);
+    if (it->kind == 0) restore_absolute_value(x, r.absval[size_t(it->payload)], lower, st);
+    else restore_variable_pair(x, r.varpair[size_t(it->payload)], st);
     range_end = it->tape_position;
   }
   replay(0, range_end, false);

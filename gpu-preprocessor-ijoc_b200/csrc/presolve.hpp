@@ -77,6 +77,8 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
 // Applies one absolute-value primal recovery to the device vector x
 // (original order); `lower` (device, may be null) bounds the max slacks.
 void restore_absolute_value(double* x, const AbsValueRecovery& r, const double* lower, cudaStream_t st);
+// Applies one variable-pair primal recovery to x.
+void restore_variable_pair(double* x, const VarPairRecovery& r, cudaStream_t st);
 // `lower` bounds the absolute-value max slacks (original->l when null).
 void run_postsolve(const PresolveOutput& out, const double* x_red, const double* y_red, const double* z_red,
                    const gpp_lp* original, double* x_org, double* y_org, double* z_org,

@@ -140,6 +140,15 @@ void capture_absolute_value(Record& r, AbsValueRecovery&& step) {
   r.absval.push_back(std::move(step));
 }
 
+void capture_variable_pair(Record& r, VarPairRecovery&& step) {
+  // update_device_recovery (device_recovery.cu:929-941).
+  auto s = ctx().stream;
+  for (DBuf<int32_t>* ids : {&step.plus, &step.minus, &step.root_plus, &step.root_minus})
+    GPP_LAUNCH(globalize_ids, grid_stride_blocks(step.count), kThreads, 0, s, ids->p, step.count, r.cols.p);
+  r.timeline.push_back(RecoveryCheckpoint{1, int32_t(r.varpair.size()), r.records});
+  r.varpair.push_back(std::move(step));
+}
+
 void init_record(Record& r, int32_t m, int32_t n) {
   auto s = ctx().stream;
   r.m0 = r.m = m;

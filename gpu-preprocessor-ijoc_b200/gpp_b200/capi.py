@@ -201,6 +201,8 @@ def load():
         "gpp_absolute_value_sizes": (C.c_int, [P(Summary), i32, vp]),
         "gpp_export_absolute_value": (C.c_int, [P(Summary), i32] + [vp] * 12),
         "gpp_restore_absolute_value": (C.c_int, [vp, P(AbsoluteValueRecovery), i32, vp]),
+        "gpp_variable_pair_size": (C.c_int, [P(Summary), i32, P(i32)]),
+        "gpp_export_variable_pair": (C.c_int, [P(Summary), i32] + [vp] * 6),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -225,7 +227,7 @@ EXPORTED = [
     "gpp_schedule_model_create_per_rule", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",
     "gpp_recovery_checkpoints", "gpp_absolute_value_sizes", "gpp_export_absolute_value", "gpp_postsolve_device_lower",
-    "gpp_restore_absolute_value",
+    "gpp_restore_absolute_value", "gpp_variable_pair_size", "gpp_export_variable_pair",
 ]
 
 # Absolute-value recovery patterns (include/gpp.h GPP_ABS_*).

@@ -156,6 +156,22 @@ class Result:
                 self.tape_types, self.tape_is, self.tape_vs, self.tape_idx, self.tape_val, self.fixed_idx,
                 self.fixed_val))))
             self.checkpoints, self.absolute_value = export_recoveries(s)
+            self.variable_pair = export_variable_pairs(s, self.checkpoints)
+
+
+def export_variable_pairs(s, checkpoints):
+    """The record's variable-pair recoveries as dicts of host arrays."""
+    lib = capi.load()
+    out = []
+    for i in range(sum(1 for k, _, _ in checkpoints if k == 1)):
+        n = C.c_int32()
+        _raise(lib.gpp_variable_pair_size(C.byref(s), i, C.byref(n)))
+        a = {k: np.zeros(n.value, np.int32) for k in ("plus", "minus", "root_plus", "root_minus")}
+        a.update({k: np.zeros(n.value) for k in ("plus_shift", "minus_shift")})
+        _raise(lib.gpp_export_variable_pair(C.byref(s), i, *(a[k].ctypes.data_as(C.c_void_p) for k in (
+            "plus", "minus", "root_plus", "root_minus", "plus_shift", "minus_shift"))))
+        out.append(a)
+    return out
 
 
 def export_recoveries(s):

@@ -655,6 +655,144 @@ def outer_l1_lp(pairs: int, blocks: int, features: int = 6, seed: int = 0, share
     return _build(len(AL), n, entries, c, AL, AU, l, u)
 
 
+def _pair_components(rng, P, size):
+    """A random partition of P pairs into components of `size` pairs (the
+    last may be smaller) and a spanning tree of each, plus one extra edge
+    (a cycle) in every fourth component of three or more."""
+    perm = rng.permutation(P)
+    comps = [perm[i:i + size] for i in range(0, P, size)]
+    edges = []
+    for k, comp in enumerate(comps):
+        for j in range(1, len(comp)):
+            edges.append((int(comp[int(rng.integers(0, j))]), int(comp[j])))
+        if len(comp) >= 3 and k % 4 == 0:
+            edges.append((int(comp[0]), int(comp[-1])))
+    owner = np.empty(P, np.int64)
+    for k, comp in enumerate(comps):
+        owner[comp] = k
+    return comps, edges, owner
+
+
+def _pair_row(rng, P, pairs, d, eq):
+    """A row of pair terms  sum v_k (p_k - m_k)  with sides from the planted
+    differences d: an equality or a one-sided row with slack."""
+    v = np.round(rng.uniform(-4, 4, len(pairs)), 2)
+    v[v == 0] = 1.0
+    act = float(sum(vk * d[q] for vk, q in zip(v, pairs)))
+    ent = [(int(q), float(vk)) for q, vk in zip(pairs, v)] + [(int(q) + P, float(-vk)) for q, vk in zip(pairs, v)]
+    if eq:
+        return ent, act, act
+    return ent, act - float(rng.uniform(0.5, 2)), INF
+
+
+def epigraph_pair_lp(components: int, size: int, tails: int = 2, rows: int = 0, seed: int = 0,
+                     decoy: str = "") -> HostLP:
+    """The variable-pair epigraph layout: P = components * size pairs (p_i =
+    column i, m_i = column P + i, zero cost, [0, inf) or [0, u]), then `tails`
+    positive-cost columns T.  Pair i's epigraph row  -a (p_i + m_i) + b T >= L
+    shares (a, b, L, T) with its component; merge rows
+    v (p_a - m_a) - v (p_b - m_b) = 0  join each component (a spanning tree,
+    some with a cycle); `rows` (default P) further rows of 1-5 pair terms
+    with sides from planted per-component differences.  Rows are shuffled.
+    `decoy`: "epigraph_side" (one pair's L differs from its component's),
+    "stray" (a row with a tail column in it)."""
+    rng = np.random.default_rng(seed)
+    P = components * size
+    comps, edges, owner = _pair_components(rng, P, size)
+    rows = P if rows == 0 else rows
+    n = 2 * P + tails
+    c = np.zeros(n)
+    c[2 * P:] = np.round(rng.uniform(0.5, 2.0, tails), 2)
+    l = np.zeros(n)
+    u = np.full(n, INF)
+    for k, comp in enumerate(comps):
+        if k % 3 == 1:
+            u[comp] = np.round(rng.uniform(20, 40, len(comp)), 1)
+            u[comp + P] = np.round(rng.uniform(20, 40, len(comp)), 1)
+    d = np.round(rng.uniform(-5, 5, len(comps)), 2)[owner]
+    gdat = [(float(rng.choice([1.0, 2.0])), float(rng.choice([1.0, 0.5])), float(np.round(rng.uniform(-3, 0), 1)),
+             2 * P + int(rng.integers(0, tails))) for _ in comps]
+    body = []
+    for i in range(P):
+        a, b, L, t = gdat[owner[i]]
+        if decoy == "epigraph_side" and i == int(comps[0][-1]) and len(comps[0]) > 1:
+            L -= 1.0
+        body.append(([(i, -a), (i + P, -a), (t, b)], L, INF))
+    for x, y in edges:
+        lo_, hi_ = min(x, y), max(x, y)
+        v = float(rng.choice([1.0, -2.0, 0.5]))
+        body.append(([(lo_, v), (hi_, -v), (lo_ + P, -v), (hi_ + P, v)], 0.0, 0.0))
+    for r in range(rows):
+        k = int(rng.integers(1, 6))
+        pairs = rng.choice(P, size=k, replace=False)
+        ent, lo_, hi_ = _pair_row(rng, P, pairs, d, eq=(r % 3 == 0))
+        if decoy == "stray" and r == 0:
+            ent.append((2 * P, 1.0))
+            lo_, hi_ = -INF, INF
+        body.append((ent, lo_, hi_))
+    order = rng.permutation(len(body))
+    entries, AL, AU = [], [], []
+    for new, old in enumerate(order):
+        ent, lo_, hi_ = body[old]
+        entries += [(new, j, a) for j, a in ent]
+        AL.append(lo_)
+        AU.append(hi_)
+    return _build(len(body), n, entries, c, AL, AU, l, u)
+
+
+def antipodal_pair_lp(components: int, size: int, rows: int = 0, seed: int = 0, uniform_cost: bool = True,
+                      decoy: str = "") -> HostLP:
+    """The shifted-antipodal layout: P = components * size pairs, columns
+    p_i = i and m_i = P + i only, costs c_p = c_m = rho (one value per
+    component with `uniform_cost`, else per pair), lower bounds shared by a
+    component (some nonzero, so the shift and the objective constant are
+    exercised), finite or infinite uppers; merge rows joining each component
+    and `rows` (default P) rows of 1-6 pair terms with sides from planted
+    differences.  `decoy`: "shift" (a merge edge between components of
+    different shifts), "cost" (one pair with c_p != c_m)."""
+    rng = np.random.default_rng(seed)
+    P = components * size
+    comps, edges, owner = _pair_components(rng, P, size)
+    rows = P if rows == 0 else rows
+    n = 2 * P
+    rho = np.round(rng.uniform(0.5, 3.0, len(comps)), 2)[owner] if uniform_cost else \
+        np.round(rng.uniform(0.5, 3.0, P), 2)
+    c = np.concatenate([rho, rho])
+    lows = [(0.0, 0.0), (1.0, 1.0), (2.0, 0.5), (0.25, 0.75)]
+    lp_, lm_ = np.zeros(P), np.zeros(P)
+    for k, comp in enumerate(comps):
+        lp_[comp], lm_[comp] = lows[k % len(lows)]
+    l = np.concatenate([lp_, lm_])
+    u = np.full(n, INF)
+    for k, comp in enumerate(comps):
+        if k % 3 == 2:
+            u[comp] = l[comp] + 40.0
+            u[comp + P] = l[comp + P] + 40.0
+    if decoy == "cost":
+        c[P] += 0.5
+    d = np.round(rng.uniform(-5, 5, len(comps)), 2)[owner] + (lp_ - lm_)
+    body = []
+    if decoy == "shift":
+        a, b = int(comps[0][0]), int(comps[2][0])   # shifts 0 and 1.5
+        edges.append((a, b))
+    for x, y in edges:
+        lo_, hi_ = min(x, y), max(x, y)
+        v = float(rng.choice([1.0, -2.0, 0.5]))
+        body.append(([(lo_, v), (hi_, -v), (lo_ + P, -v), (hi_ + P, v)], 0.0, 0.0))
+    for r in range(rows):
+        k = int(rng.integers(1, 7))
+        pairs = rng.choice(P, size=k, replace=False)
+        body.append(_pair_row(rng, P, pairs, d, eq=(r % 3 == 0)))
+    order = rng.permutation(len(body))
+    entries, AL, AU = [], [], []
+    for new, old in enumerate(order):
+        ent, lo_, hi_ = body[old]
+        entries += [(new, j, a) for j, a in ent]
+        AL.append(lo_)
+        AU.append(hi_)
+    return _build(len(body), n, entries, c, AL, AU, l, u)
+
+
 def workload(name: str, seed: int = 0) -> HostLP:
     """Named workloads: 'small' (2,000 x 5,000), 'scale' (2M x 5M + hubs), 'qap30',
     'random:MxN', 'slack:MxN' (random family with singleton columns on 30% of rows),

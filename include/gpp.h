@@ -108,11 +108,10 @@ typedef struct gpp_params {
   double parallel_columns_max_abs_ratio;
   int32_t parallel_columns_scale_guard_max_group_size;
   int32_t parallel_columns_scale_guard_min_groups;
-  /* The structure-specific startup rules: column domination, two-row
-   * variable elimination, zero-cost product variables and the
-   * absolute-value piecewise-linear reformulation run as in the reference;
-   * the variable-pair reformulation's settings are carried for layout
-   * parity with PresolveParams but that rule is not run. */
+  /* The structure-specific startup rules (column domination, two-row
+   * variable elimination, zero-cost product variables, the variable-pair
+   * and absolute-value piecewise-linear reformulations) run as in the
+   * reference. */
   uint8_t enable_structure_specific_rules;
   uint8_t enable_two_row_variable_elimination;
   int32_t two_row_variable_elimination_max_row_nnz;
@@ -288,7 +287,7 @@ typedef struct gpp_absolute_value_recovery {
 
 /* The record's primal-recovery checkpoints (primal_recovery_timeline,
  * presolve_structs.hpp:256-266, 362).  *count is always written; kinds
- * (0 = absolute value), payloads (index of the recovery of that kind) and
+ * (0 = absolute value, 1 = variable pair), payloads (index of the recovery of that kind) and
  * tape_positions (records replayed before the recovery is applied), when not
  * NULL, receive *count entries. */
 GPP_API int gpp_recovery_checkpoints(const gpp_summary* summary, int32_t* count, int32_t* kinds,
@@ -306,6 +305,17 @@ GPP_API int gpp_export_absolute_value(const gpp_summary* summary, int32_t index,
                                       int32_t* pair_free, int32_t* linked_slack, int32_t* linked_t,
                                       double* linked_factor, int32_t* max_slack, int32_t* max_starts,
                                       int32_t* max_t, double* max_factor);
+
+/* Size (pairs) of variable-pair recovery `index`
+ * (PiecewiseLinearReformulationVariablePairRecoveryStep, presolve_structs.hpp:243-250). */
+GPP_API int gpp_variable_pair_size(const gpp_summary* summary, int32_t index, int32_t* count);
+
+/* Copies variable-pair recovery `index` to HOST arrays of *count entries
+ * (original column ids; x[plus] = plus_shift + x[root_plus], likewise for
+ * minus); any pointer may be NULL. */
+GPP_API int gpp_export_variable_pair(const gpp_summary* summary, int32_t index, int32_t* plus_cols,
+                                     int32_t* minus_cols, int32_t* root_plus_cols, int32_t* root_minus_cols,
+                                     double* plus_shift, double* minus_shift);
 
 /* postsolve_restore_piecewise_linear_reformulation_absolute_value_gpu
  * (presolve/gpu_postsolve.hpp:15-18): applies `count` steps to the DEVICE

@@ -49,10 +49,29 @@ inline void export_recovery_record(PresolveRecordGpu& record) {
                   "export_recovery_record checkpoints");
   record.primal_recovery_timeline.clear();
   record.piecewise_linear_reformulation_absolute_value_recoveries.clear();
+  record.piecewise_linear_reformulation_variable_pair_recoveries.clear();
   for (std::int32_t k = 0; k < count; ++k) {
     record.primal_recovery_timeline.push_back({static_cast<PrimalRecoveryKind>(kinds[std::size_t(k)]),
                                                checked_nnz_offset(payloads[std::size_t(k)]),
                                                checked_nnz_offset(positions[std::size_t(k)])});
+    if (kinds[std::size_t(k)] == 1) {
+      std::int32_t n = 0;
+      throw_on_status(gpp_variable_pair_size(s, payloads[std::size_t(k)], &n), "export_recovery_record sizes");
+      PiecewiseLinearReformulationVariablePairRecoveryStep step;
+      step.plus_cols.resize(std::size_t(n));
+      step.minus_cols.resize(std::size_t(n));
+      step.root_plus_cols.resize(std::size_t(n));
+      step.root_minus_cols.resize(std::size_t(n));
+      step.plus_shift.resize(std::size_t(n));
+      step.minus_shift.resize(std::size_t(n));
+      throw_on_status(gpp_export_variable_pair(s, payloads[std::size_t(k)], step.plus_cols.data(),
+                                               step.minus_cols.data(), step.root_plus_cols.data(),
+                                               step.root_minus_cols.data(), step.plus_shift.data(),
+                                               step.minus_shift.data()),
+                      "export_recovery_record variable pair");
+      record.piecewise_linear_reformulation_variable_pair_recoveries.push_back(std::move(step));
+      continue;
+    }
     if (kinds[std::size_t(k)] != 0) continue;
     std::int32_t z[6];
     throw_on_status(gpp_absolute_value_sizes(s, payloads[std::size_t(k)], z), "export_recovery_record sizes");

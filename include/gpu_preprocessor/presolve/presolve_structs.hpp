@@ -225,6 +225,16 @@ struct PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep {
   std::vector<AbsoluteValueMaxSlackRecovery> max_slacks;
 };
 
+// Primal recovery of the variable-pair reformulation (presolve_structs.hpp:243-250).
+struct PiecewiseLinearReformulationVariablePairRecoveryStep {
+  std::vector<std::int32_t> plus_cols;
+  std::vector<std::int32_t> minus_cols;
+  std::vector<std::int32_t> root_plus_cols;
+  std::vector<std::int32_t> root_minus_cols;
+  std::vector<double> plus_shift;
+  std::vector<double> minus_shift;
+};
+
 // Where a primal recovery sits among the tape records (presolve_structs.hpp:252-266).
 enum class PrimalRecoveryKind : std::uint8_t {
   PiecewiseLinearReformulationAbsoluteValue = 0,
@@ -268,6 +278,8 @@ struct PresolveRecordGpu {
       tape.vals.swap(o.tape.vals);
       piecewise_linear_reformulation_absolute_value_recoveries.swap(
           o.piecewise_linear_reformulation_absolute_value_recoveries);
+      piecewise_linear_reformulation_variable_pair_recoveries.swap(
+          o.piecewise_linear_reformulation_variable_pair_recoveries);
       primal_recovery_timeline.swap(o.primal_recovery_timeline);
       handle = o.handle;
       o.handle = gpp_summary{};
@@ -288,6 +300,8 @@ struct PresolveRecordGpu {
   PostsolveTape tape;
   std::vector<PiecewiseLinearReformulationAbsoluteValuePrimalRecoveryStep>
       piecewise_linear_reformulation_absolute_value_recoveries;
+  std::vector<PiecewiseLinearReformulationVariablePairRecoveryStep>
+      piecewise_linear_reformulation_variable_pair_recoveries;
   std::vector<PrimalRecoveryCheckpoint> primal_recovery_timeline;
   gpp_summary handle{};  // the C-ABI summary whose record this is
 };

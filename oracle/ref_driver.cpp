@@ -9,7 +9,8 @@
 // meta.txt, A_ptr/A_idx/A_val, AT_ptr/AT_idx/AT_val, c/l/u/AL/AU, row_map,
 // col_map, fixed_idx/fixed_val, tape_types/tape_is/tape_vs/tape_idx/tape_val,
 // ckpt_kind/ckpt_payload/ckpt_position (primal-recovery checkpoints),
-// abs<k>_* (absolute-value recoveries; pattern in meta.txt), and (with
+// abs<k>_* (absolute-value recoveries; pattern in meta.txt), vp<k>_*
+// (variable-pair recoveries), and (with
 // --postsolve) x_org/y_org/z_org.
 #include <cuda_runtime.h>
 
@@ -97,6 +98,20 @@ int main(int argc, char** argv) {
       else if (k == "doubleton_equations_max_fill_in_proxy") p.doubleton_equations_max_fill_in_proxy = v;
       else if (k == "doubleton_equations_min_selected_per_batch") p.doubleton_equations_min_selected_per_batch = v;
       else if (k == "doubleton_equations_min_selected_ratio") p.doubleton_equations_min_selected_ratio = dv;
+#define NUM(name) else if (k == #name) p.name = static_cast<decltype(p.name)>(dv)
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_probe_pairs);
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_min_pairs);
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_min_potential_gain);
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_min_actual_gain);
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_max_tail_cols);
+      NUM(piecewise_linear_reformulation_variable_pair_epigraph_max_quotient_terms_per_row);
+      NUM(piecewise_linear_reformulation_variable_pair_shifted_antipodal_probe_pairs);
+      NUM(piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_pairs);
+      NUM(piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_potential_gain);
+      NUM(piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_actual_gain);
+      NUM(piecewise_linear_reformulation_variable_pair_shifted_antipodal_max_quotient_terms_per_row);
+      NUM(feasibility_tol);
+#undef NUM
       else if (k == "piecewise_linear_reformulation_absolute_value_residual_bound_mode")
         p.piecewise_linear_reformulation_absolute_value_residual_bound_mode =
             static_cast<gp::presolve::PiecewiseLinearReformulationAbsoluteValueResidualBoundMode>(v);
@@ -211,6 +226,17 @@ int main(int argc, char** argv) {
       save(out, "ckpt_position", positions);
       meta << "absolute_value_steps " << record.piecewise_linear_reformulation_absolute_value_recoveries.size()
            << "\n";
+      meta << "variable_pair_steps " << record.piecewise_linear_reformulation_variable_pair_recoveries.size()
+           << "\n";
+      int v = 0;
+      for (const auto& a : record.piecewise_linear_reformulation_variable_pair_recoveries) {
+        const std::string p = "vp" + std::to_string(v++) + "_";
+        save(out, (p + "plus").c_str(), a.plus_cols); save(out, (p + "minus").c_str(), a.minus_cols);
+        save(out, (p + "root_plus").c_str(), a.root_plus_cols);
+        save(out, (p + "root_minus").c_str(), a.root_minus_cols);
+        save(out, (p + "plus_shift").c_str(), a.plus_shift);
+        save(out, (p + "minus_shift").c_str(), a.minus_shift);
+      }
       int k = 0;
       for (const auto& a : record.piecewise_linear_reformulation_absolute_value_recoveries) {
         const std::string p = "abs" + std::to_string(k++) + "_";

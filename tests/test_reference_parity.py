@@ -187,11 +187,10 @@ def test_folding_matches_reference(workload):
 @needs_reference
 @pytest.mark.parametrize("workload", ["random:400x1000", "small", "slack:2000x5000", "random:20000x50000"])
 def test_reference_startup_rules_do_not_fire(workload):
-    """Of the reference's structure-specific startup rules this engine runs
-    column domination only.  On these workloads the reference's own detectors
-    reject all of them: its output with the rules on equals its output with
-    them off, so the engine's parity holds for the reference's default
-    settings too."""
+    """On these workloads the reference's own structure-specific detectors
+    reject every structure-specific startup rule: its output with the rules on
+    equals its output with them off, so the parity tests above (rules off)
+    also hold for the reference's default settings."""
     lp = lpgen.workload(workload, seed=0)
     on = run_reference(lp, ALL, ["enable_structure_specific_rules=1"])
     off = run_reference(lp, ALL)
