@@ -45,11 +45,10 @@ RULES = ["infeasible_and_fixed_variables", "empty_columns", "empty_rows", "singl
 # Kernel -> the source files whose text fixes its code; a DRAM traffic
 # figure measured by ncu is used only while these files are unchanged.
 KERNEL_SOURCES = {
-    "activity_tiles<false>": ["csrc/live.cu", "csrc/common.cuh", "csrc/engine.cuh"],
-    "activity_tiles<true>": ["csrc/live.cu", "csrc/common.cuh", "csrc/engine.cuh"],
-    "candidates_tiles": ["csrc/rules_bound.cu", "csrc/common.cuh", "csrc/engine.cuh"],
-    "copy_tiles": ["csrc/compact.cu", "csrc/common.cuh", "csrc/engine.cuh"],
-    "count_tiles": ["csrc/compact.cu", "csrc/common.cuh", "csrc/engine.cuh"],
+    "activity_kernel<false>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
+    "activity_kernel<true>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
+    "candidates_entries": ["csrc/rules_bound.cu", "csrc/common.cuh"],
+    "copy_kept": ["csrc/compact.cu", "csrc/common.cuh"],
 }
 
 

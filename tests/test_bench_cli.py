@@ -41,7 +41,7 @@ def test_bench_uses_no_undefined_global():
 def test_source_digests_print():
     r = subprocess.run([sys.executable, BENCH, "--source-digests"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
-    assert "candidates_tiles" in r.stdout
+    assert "candidates_entries" in r.stdout
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "pslp_driver")),
