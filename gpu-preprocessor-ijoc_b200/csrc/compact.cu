@@ -13,7 +13,6 @@
 #include "sort.hpp"
 
 #include <algorithm>
-#include <climits>
 #include <utility>
 
 namespace gpp {
@@ -192,121 +191,6 @@ copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict_
       w += total;
       __syncthreads();
     }
-  }
-}
-
-// Tiled compaction over the row tiles (rows of up to kActRowMax entries;
-// longer rows keep the block-per-row roles above).  Both passes read a
-// tile's entries with coalesced loads and one map gather each.  The count
-// pass sums each kept row's kept entries from shared memory; the copy pass
-// ranks the tile's kept entries with one block scan (the kept entries of
-// consecutive kept rows are consecutive in the output, starting at the
-// output row pointer of the tile's first kept row), so its stores are
-// contiguous too.
-__global__ void __launch_bounds__(kThreads)
-count_tiles(const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx, const int32_t* __restrict__ outer_map,
-            const int32_t* __restrict__ inner_map, const int32_t* __restrict__ tile_first,
-            const int32_t* __restrict__ counts, int32_t* __restrict__ out_counts) {
-  __shared__ offset_t sptr[kActTileRows + 1];
-  __shared__ uint8_t kept[kActTileEntries];
-  const int tiles = counts[0];
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int r0 = tile_first[t], r1 = tile_first[t + 1], nr = r1 - r0;
-    for (int k = threadIdx.x; k <= nr; k += kThreads) sptr[k] = ptr[r0 + k];
-    __syncthreads();
-    const int r_end = nr > 0 && sptr[nr] - sptr[nr - 1] > kActRowMax ? nr - 1 : nr;
-    const offset_t e0 = sptr[0];
-    const int ne = int(sptr[r_end] - e0);
-    constexpr int K = kActTileEntries / kThreads;
-    int col[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      col[k] = e < ne ? __ldcs(idx + e0 + e) : -1;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      if (e < ne) kept[e] = inner_map[col[k]] >= 0;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < r_end; k += kThreads) {
-      const int nrow = outer_map[r0 + k];
-      if (nrow < 0) continue;
-      int c = 0;
-      for (int e = int(sptr[k] - e0); e < int(sptr[k + 1] - e0); ++e) c += kept[e];
-      out_counts[nrow] = c;
-    }
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(kThreads)
-copy_tiles(const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx, const double* __restrict__ val,
-           const int32_t* __restrict__ outer_map, const int32_t* __restrict__ inner_map,
-           const int32_t* __restrict__ tile_first, const int32_t* __restrict__ counts,
-           const offset_t* __restrict__ out_ptr, int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
-  __shared__ offset_t sptr[kActTileRows + 1];
-  __shared__ int32_t newcol[kActTileEntries];   // new column of a kept entry of a kept row, else -1
-  __shared__ int32_t warp_tot[kThreads / 32];
-  __shared__ int first_kept;
-  const int tiles = counts[0];
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int r0 = tile_first[t], r1 = tile_first[t + 1], nr = r1 - r0;
-    for (int k = threadIdx.x; k <= nr; k += kThreads) sptr[k] = ptr[r0 + k];
-    if (threadIdx.x == 0) first_kept = INT_MAX;
-    __syncthreads();
-    const int r_end = nr > 0 && sptr[nr] - sptr[nr - 1] > kActRowMax ? nr - 1 : nr;
-    const offset_t e0 = sptr[0];
-    const int ne = int(sptr[r_end] - e0);
-    // Row-kept flags onto the row's entries (dropped rows give -1), and the
-    // tile's first kept row.
-    for (int k = threadIdx.x; k < r_end; k += kThreads) {
-      const bool keep_r = outer_map[r0 + k] >= 0;
-      if (keep_r) atomicMin(&first_kept, k);
-      for (int e = int(sptr[k] - e0); e < int(sptr[k + 1] - e0); ++e) newcol[e] = keep_r ? 0 : -1;
-    }
-    __syncthreads();
-    constexpr int K = kActTileEntries / kThreads;
-    int col[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      col[k] = e < ne && newcol[e] == 0 ? __ldcs(idx + e0 + e) : -1;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      if (e < ne) newcol[e] = col[k] >= 0 ? inner_map[col[k]] : -1;
-    }
-    __syncthreads();
-    // Output slots: thread t owns the tile's entries [8t, 8t + 8).
-    const int b0 = int(threadIdx.x) * K;
-    int run = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) run += b0 + k < ne && newcol[b0 + k] >= 0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = run;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const int peer = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= off) incl += peer;
-    }
-    if (lane == 31) warp_tot[warp] = incl;
-    __syncthreads();
-    int before = 0;
-    for (int w = 0; w < warp; ++w) before += warp_tot[w];
-    offset_t o = first_kept < r_end ? out_ptr[outer_map[r0 + first_kept]] + before + incl - run : 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = b0 + k;
-      if (e < ne && newcol[e] >= 0) {
-        out_idx[o] = newcol[e];
-        out_val[o] = __ldcs(val + e0 + e);
-        ++o;
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -515,27 +399,23 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
     return out;
   }
   const RowSchedule& sch = stored_schedule(M);
-  const RowSchedule& tiles = row_tiles(M, s);
+  const int gb = std::max(1, std::min((M.rows + 31) / 32, kNumSMs * 16));
   const int lb = roles_long(M.rows);
-  const int tb = int(std::min<int64_t>(int64_t(kNumSMs) * 6, (2 * int64_t(M.nnz) + M.rows) / kActTileWeight + 2));
-  // Rows of up to kActRowMax entries by tiles; longer rows (the stored
-  // schedule's long queue) one block each.
+  // Counting reads only: short rows one per thread (more rows in flight),
+  // medium rows four per warp, long rows one per block.
+  const int sb = grid_stride_blocks(M.rows, kThreads, 16), mb = std::min<int>(kNumSMs * 8, (M.rows + 7) / 8);
   DBuf<int32_t> counts(size_t(outer_new) + 1, s);
   const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * outer_new;
-  GPP_LAUNCH_BYTES(count_tiles, count_bytes, tb, kThreads, 0, s, M.ptr, M.idx, outer_map, inner_map,
-                   tiles.act_first.p, tiles.act_counts.p, counts.p);
-  GPP_LAUNCH(count_kept, lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map, sch.medium.p,
-             sch.long_rows.p, sch.counts.p, 0, 0, counts.p);
+  GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map,
+                   sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
   exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
   out.nnz = known_nnz >= 0 ? offset_t(known_nnz) : read_scalar(out.ptr + outer_new);
   out.idx = dalloc<int32_t>(size_t(out.nnz));
   out.val = dalloc<double>(size_t(out.nnz));
   const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +
                             4.0 * (outer_new + 1) + 12.0 * out.nnz;
-  GPP_LAUNCH_BYTES(copy_tiles, copy_bytes, tb, kThreads, 0, s, M.ptr, M.idx, M.val, outer_map, inner_map,
-                   tiles.act_first.p, tiles.act_counts.p, out.ptr, out.idx, out.val);
-  GPP_LAUNCH(copy_kept, lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map, inner_map, sch.long_rows.p,
-             sch.counts.p, 0, out.ptr, out.idx, out.val);
+  GPP_LAUNCH_BYTES(copy_kept, copy_bytes, gb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map,
+                   inner_map, sch.long_rows.p, sch.counts.p, gb, out.ptr, out.idx, out.val);
   return out;
 }
 
