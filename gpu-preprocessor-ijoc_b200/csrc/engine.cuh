@@ -40,17 +40,6 @@ struct RowSchedule {
   uint64_t epoch = 0;
 };
 
-// Row tiles (see RowSchedule::act_*): rows of at most kActRowMax stored
-// entries, a new tile every kActTileWeight units of weight (a row weighs its
-// length + 1; a longer row weighs a whole tile), so a tile holds at most
-// kActTileEntries entries of at most kActTileRows rows.
-constexpr int kActRowMax = 1024;
-constexpr int kActTileWeight = 1024;
-constexpr int kActTileEntries = 2048;
-constexpr int kActTileRows = 1024;
-struct DevCsr;
-const RowSchedule& row_tiles(const DevCsr& A, cudaStream_t s);
-
 // Builds the schedule of `M` by stored length (live_degrees == nullptr) or by
 // the given per-row live degree.
 void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees, cudaStream_t st);

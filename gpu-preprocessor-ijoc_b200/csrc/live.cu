@@ -326,6 +326,10 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
 // is exact: a sum that starts at +0.0 never becomes -0.0.  Rows longer than
 // kActRowMax go to activity_long_rows, one block each, with the same
 // association as the untiled kernel.
+constexpr int kActRowMax = 1024;
+constexpr int kActTileWeight = 1024;
+constexpr int kActTileEntries = 2048;
+constexpr int kActTileRows = 2048;
 
 __global__ void act_tile_weights(int m, const offset_t* __restrict__ ptr, int64_t* __restrict__ w) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -970,7 +974,7 @@ void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int3
 
 namespace {
 // Row tiles of the activity sweep, built once per stored matrix.
-void ensure_row_tiles(const RowSchedule& sch, const DevCsr& A, cudaStream_t s) {
+void ensure_activity_tiles(const RowSchedule& sch, const DevCsr& A, cudaStream_t s) {
   if (sch.act_built) return;
   const int m = A.rows;
   const size_t max_tiles = size_t((2 * int64_t(A.nnz) + m) / kActTileWeight + 2);
@@ -985,21 +989,13 @@ void ensure_row_tiles(const RowSchedule& sch, const DevCsr& A, cudaStream_t s) {
              sch.act_counts.p);
   sch.act_built = true;
 }
-}  // namespace
-
-const RowSchedule& row_tiles(const DevCsr& A, cudaStream_t s) {
-  const RowSchedule& sch = stored_schedule(A);
-  ensure_row_tiles(sch, A, s);
-  return sch;
-}
-
-namespace {
 
 template <bool Plain>
 void launch_activity(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
                      const int32_t* live_deg, double* lo, double* hi, int32_t* ni, int32_t* pi, double out_bytes,
                      cudaStream_t s) {
-  const RowSchedule& sch = row_tiles(A, s);
+  const RowSchedule& sch = stored_schedule(A);
+  ensure_activity_tiles(sch, A, s);
   // Algorithmic bytes (each array charged once): row pointers, column indices
   // and values, packed column bounds, row mask, live degrees, the outputs.
   const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +

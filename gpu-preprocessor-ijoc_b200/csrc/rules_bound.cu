@@ -123,81 +123,6 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
   }
 }
 
-// Tiled form over the activity sweep's row tiles: a block stages the sides,
-// activity summary and eligibility of the tile's rows once (coalesced: the
-// rows are consecutive), then every thread takes 8 of the tile's entries,
-// finds their rows by a binary search over the staged row pointers, and
-// forms the candidates (RED max / min, order-free).  Rows longer than
-// kActRowMax: candidates_long_rows, one block per row.
-__global__ void __launch_bounds__(kThreads)
-candidates_tiles(const int32_t* __restrict__ tile_first, const int32_t* __restrict__ counts, CandArgs g) {
-  __shared__ offset_t sptr[kActTileRows + 1];
-  __shared__ double s_al[kActTileRows], s_au[kActTileRows], s_mn[kActTileRows], s_mx[kActTileRows];
-  __shared__ int16_t s_ni[kActTileRows], s_pi[kActTileRows];
-  __shared__ uint8_t s_ok[kActTileRows];
-  const L2Hints hint = l2_hints();
-  const int tiles = counts[0];
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int r0 = tile_first[t], r1 = tile_first[t + 1];
-    for (int k = threadIdx.x; k <= r1 - r0; k += kThreads) sptr[k] = g.ptr[r0 + k];
-    for (int k = threadIdx.x; k < r1 - r0; k += kThreads) {
-      const int i = r0 + k;
-      s_ok[k] = g.keep_row[i] && g.row_nnz[i] > 1;
-      s_al[k] = g.AL[i]; s_au[k] = g.AU[i];
-      s_mn[k] = g.rs.mn[i]; s_mx[k] = g.rs.mx[i];
-      s_ni[k] = int16_t(min(g.rs.ni[i], 2)); s_pi[k] = int16_t(min(g.rs.pi[i], 2));   // only 0, 1, > 1 matter
-    }
-    __syncthreads();
-    const int nr = r1 - r0;
-    const int r_end = nr > 0 && sptr[nr] - sptr[nr - 1] > kActRowMax ? nr - 1 : nr;
-    const offset_t e0 = sptr[0];
-    const int ne = int(sptr[r_end] - e0);
-    // Two rounds of 4 entries per thread, every load of a round in flight
-    // before its first use.
-    constexpr int K = 4;
-    for (int k0 = 0; k0 < kActTileEntries / kThreads; k0 += K) {
-      int col[K];
-      double a[K];
-      double2 b[K];
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int e = (k0 + k) * kThreads + threadIdx.x;
-        col[k] = e < ne ? ld_stream(g.idx + e0 + e, hint.stream) : -1;
-        a[k] = e < ne ? ld_stream(g.val + e0 + e, hint.stream) : 0.0;
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        b[k] = col[k] >= 0 ? ld_keep(g.lu + col[k], hint.keep) : make_double2(0.0, 0.0);
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int e = (k0 + k) * kThreads + threadIdx.x;
-        if (e >= ne) break;
-        const int lr = row_of(sptr, 0, r_end, e0 + e);
-        if (!s_ok[lr] || removed_column(b[k]) || fabs(a[k]) <= g.zero_tol) continue;
-        candidate_update(g, RowCtx{s_al[lr], s_au[lr], s_mn[lr], s_mx[lr], s_ni[lr], s_pi[lr]}, col[k], a[k], b[k]);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(kThreads)
-candidates_long_rows(const int32_t* __restrict__ big, const int32_t* __restrict__ counts, CandArgs g) {
-  const L2Hints hint = l2_hints();
-  const int nbig = counts[1];
-  for (int q = blockIdx.x; q < nbig; q += gridDim.x) {
-    const int i = big[q];
-    if (!g.keep_row[i] || g.row_nnz[i] <= 1) continue;   // block-uniform
-    const RowCtx rc = row_ctx(g, i);
-    for (offset_t p = g.ptr[i] + threadIdx.x; p < g.ptr[i + 1]; p += kThreads) {
-      const int j = ld_stream(g.idx + p, hint.stream);
-      const double2 bj = ld_keep(g.lu + j, hint.keep);
-      const double aj = ld_stream(g.val + p, hint.stream);
-      if (!removed_column(bj) && !(fabs(aj) <= g.zero_tol)) candidate_update(g, rc, j, aj, bj);
-    }
-  }
-}
-
 // _kernel_finalize_bound_strengthening (reference :646-796).
 __global__ void finalize_kernel(int n, const uint8_t* __restrict__ keep_col, const double* __restrict__ l,
                                 const double* __restrict__ u, const double* __restrict__ cand_l,
@@ -429,10 +354,9 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                p.zero_tol, cl.p, cu.p};
     const double bytes = 4.0 * (m + 1) + 12.0 * lp.A.nnz + double(m) + 4.0 * m + 16.0 * m + 24.0 * m + 16.0 * n +
                          16.0 * n;
-    const RowSchedule& sch = row_tiles(lp.A, s);
-    const int grid = int(std::min<int64_t>(int64_t(kNumSMs) * 4, (2 * int64_t(lp.A.nnz) + m) / kActTileWeight + 2));
-    GPP_LAUNCH_BYTES(candidates_tiles, bytes, grid, kThreads, 0, s, sch.act_first.p, sch.act_counts.p, g);
-    GPP_LAUNCH(candidates_long_rows, std::min(kNumSMs * 2, m), kThreads, 0, s, sch.act_big.p, sch.act_counts.p, g);
+    const RowSchedule& sch = stored_schedule(lp.A);
+    GPP_LAUNCH_BYTES(candidates_entries, bytes, int(std::max<int64_t>(1, std::min<int64_t>(sch.tiles, kNumSMs * 8))),
+                     kThreads, 0, s, lp.A.nnz, sch.tile_rows.p, g);
   }
   col_max_abs(lp.AT, plan.keep_row.p, vmax.p, s);
   DBuf<double> fl(size_t(n), s), fu(size_t(n), s), fixv(size_t(n), s);
