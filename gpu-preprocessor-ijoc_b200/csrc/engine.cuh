@@ -28,12 +28,6 @@ struct RowSchedule {
   DBuf<int2> tile_rows;
   int64_t tiles = 0;
   mutable int sorted = -1;  // rows strictly ascending: -1 not yet checked, else 0 / 1
-  // Row tiles of the activity sweep (stored schedules only, built on first
-  // use): tile t holds rows [act_first[t], act_first[t+1]), at most 2,048
-  // stored entries of rows of up to 1,024 entries; longer rows are listed in
-  // act_big.  act_counts: [0] tiles, [1] long rows (device only).
-  mutable bool act_built = false;
-  mutable DBuf<int32_t> act_first, act_big, act_counts;
   const offset_t* ptr = nullptr;
   int32_t rows = -1;
   offset_t nnz = -1;

@@ -309,238 +309,6 @@ activity_kernel(int m, const offset_t* __restrict__ ptr, const int32_t* __restri
   }
 }
 
-// ---- tiled activity sweep ------------------------------------------------------
-//
-// Rows of up to kActRowMax stored entries are cut into tiles of at most
-// kActTileEntries entries (weight of a row = its length + 1, a tile every
-// kActTileWeight units; a longer row weighs a full tile and so always ends
-// its tile).  A block loads a tile's entries with coalesced index / value
-// loads and one gather per entry, all in flight together, and stages each
-// entry's term in shared memory: the finite part of its minimum and maximum
-// term (+0.0 for a removed column, a |a| <= zero_tol entry or an infinite
-// term) and its live / infinite flags.  The row sums are then formed from
-// shared memory in the reference's association: rows of at most kShortRow
-// live entries sequentially by one thread, the others by a warp whose lane l
-// holds 0.0 + the terms of live ranks l, l+32, ... in rank order, finished by
-// the shfl_down tree 16,8,4,2,1.  Adding +0.0 for a skipped or removed entry
-// is exact: a sum that starts at +0.0 never becomes -0.0.  Rows longer than
-// kActRowMax go to activity_long_rows, one block each, with the same
-// association as the untiled kernel.
-constexpr int kActRowMax = 1024;
-constexpr int kActTileWeight = 1024;
-constexpr int kActTileEntries = 2048;
-constexpr int kActTileRows = 2048;
-
-__global__ void act_tile_weights(int m, const offset_t* __restrict__ ptr, int64_t* __restrict__ w) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const int len = int(ptr[i + 1] - ptr[i]);
-    w[i] = len <= kActRowMax ? len + 1 : kActTileWeight;
-  }
-}
-
-// Row i starts tile floor(W[i] / kActTileWeight) (W the exclusive prefix of
-// the weights); it writes the first row of every tile from the one after its
-// predecessor's up to its own, so tiles that no row starts in are empty.
-__global__ void act_tile_bounds(int m, const int64_t* __restrict__ W, const offset_t* __restrict__ ptr,
-                                int32_t* __restrict__ first, int32_t* __restrict__ big,
-                                int32_t* __restrict__ counts) {
-  const int stride = gridDim.x * blockDim.x;
-  const int top = (m + stride - 1) / stride * stride;   // every thread of a block runs the same trips
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < top; i += stride) {
-    bool is_big = false;
-    if (i < m) {
-      const int64_t t = W[i] / kActTileWeight;
-      const int64_t tp = i > 0 ? W[i - 1] / kActTileWeight : -1;
-      for (int64_t k = tp + 1; k <= t; ++k) first[k] = i;
-      is_big = ptr[i + 1] - ptr[i] > kActRowMax;
-      if (i == m - 1) {
-        const int64_t tiles = (W[m] + kActTileWeight - 1) / kActTileWeight;
-        for (int64_t k = t + 1; k <= tiles; ++k) first[k] = m;
-        counts[0] = int32_t(tiles);
-      }
-    }
-    const int at = block_append(counts + 1, is_big);
-    if (is_big) big[at] = i;
-  }
-}
-
-template <bool Plain>
-__global__ void __launch_bounds__(kThreads)
-activity_tiles(int m, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-               const double* __restrict__ val, const double2* __restrict__ lu, double zero_tol,
-               const uint8_t* __restrict__ keep_row, const int32_t* __restrict__ live_deg,
-               const int32_t* __restrict__ tile_first, const int32_t* __restrict__ counts,
-               double* __restrict__ min_fin, double* __restrict__ max_fin, int32_t* __restrict__ min_inf,
-               int32_t* __restrict__ max_inf) {
-  __shared__ double tl[kActTileEntries], th[kActTileEntries];
-  __shared__ uint8_t info[kActTileEntries];   // bit 0 live, bit 1 -inf in the minimum, bit 2 +inf in the maximum
-  __shared__ offset_t sptr[kActTileRows + 1];
-  __shared__ int slots[kThreads / 32][32];
-  const ActivityTerm<Plain> term{idx, val, lu, zero_tol, l2_hints()};
-  const int tiles = counts[0];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int r0 = tile_first[t], r1 = tile_first[t + 1];
-    for (int k = threadIdx.x; k <= r1 - r0; k += kThreads) sptr[k] = ptr[r0 + k];
-    __syncthreads();
-    // A long row can only be the tile's last one; its entries are not staged.
-    const int r_end = r1 > r0 && sptr[r1 - r0] - sptr[r1 - 1 - r0] > kActRowMax ? r1 - 1 : r1;
-    const offset_t e0 = sptr[0];
-    const int ne = int(sptr[r_end - r0] - e0);
-    // Stage the tile's terms: every load of the thread's (up to 8) entries
-    // first, then the gathers, then the terms.
-    constexpr int K = kActTileEntries / kThreads;
-    int col[K];
-    double a[K];
-    double2 bnd[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      col[k] = e < ne ? ld_stream(idx + e0 + e, term.hint.stream) : -1;
-      a[k] = e < ne ? ld_stream(val + e0 + e, term.hint.stream) : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      bnd[k] = col[k] >= 0 ? ld_keep(lu + col[k], term.hint.keep) : make_double2(0.0, 0.0);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = k * kThreads + threadIdx.x;
-      if (e >= ne) break;
-      double plo = 0.0, phi = 0.0;
-      int ni = 0, pi = 0;
-      const bool live = !removed_column(bnd[k]);
-      if (live) term.slot(a[k], bnd[k], plo, phi, ni, pi);
-      tl[e] = plo;
-      th[e] = phi;
-      info[e] = uint8_t(live) | uint8_t(ni << 1) | uint8_t(pi << 2);
-    }
-    __syncthreads();
-    // Short rows: one thread each, sequential over the stored entries.
-    for (int r = r0 + int(threadIdx.x); r < r_end; r += kThreads) {
-      const int o = int(sptr[r - r0] - e0), len = int(sptr[r + 1 - r0] - sptr[r - r0]);
-      const int live_len = live_deg ? live_deg[r] : len;
-      if (live_len > kShortRow) continue;
-      double lo = 0.0, hi = 0.0;
-      int ni = 0, pi = 0;
-      if (!keep_row || keep_row[r])
-        for (int k = 0; k < len; ++k) {
-          lo += tl[o + k];
-          hi += th[o + k];
-          ni += (info[o + k] >> 1) & 1;
-          pi += (info[o + k] >> 2) & 1;
-        }
-      min_fin[r] = lo; max_fin[r] = hi;
-      if (min_inf) { min_inf[r] = ni; max_inf[r] = pi; }
-    }
-    // The other rows: one warp each, lane l over live ranks l, l+32, ...
-    for (int r = r0 + warp; r < r_end; r += kThreads / 32) {
-      const int o = int(sptr[r - r0] - e0), len = int(sptr[r + 1 - r0] - sptr[r - r0]);
-      const int live_len = live_deg ? live_deg[r] : len;
-      if (live_len <= kShortRow) continue;   // warp-uniform
-      double lo = 0.0, hi = 0.0;
-      int ni = 0, pi = 0;
-      if (!keep_row || keep_row[r]) {
-        if (live_deg && live_len == len) {   // every entry live: rank = stored offset
-          for (int k = lane; k < len; k += 32) {
-            lo += tl[o + k];
-            hi += th[o + k];
-            ni += (info[o + k] >> 1) & 1;
-            pi += (info[o + k] >> 2) & 1;
-          }
-        } else {
-          int carry = 0;
-          for (int c = 0; c < len; c += 32) {
-            const int k = c + lane;
-            const bool live = k < len && (info[o + k] & 1);
-            const unsigned mask = __ballot_sync(0xffffffffu, live);
-            const int cnt = __popc(mask);
-            if (live) slots[warp][(carry + __popc(mask & ((1u << lane) - 1u))) & 31] = k;
-            __syncwarp();
-            if (((lane - carry) & 31) < cnt) {
-              const int q = o + slots[warp][lane];
-              lo += tl[q];
-              hi += th[q];
-              ni += (info[q] >> 1) & 1;
-              pi += (info[q] >> 2) & 1;
-            }
-            __syncwarp();
-            carry = (carry + cnt) & 31;
-          }
-        }
-      }
-      lo = warp_sum_down(lo); hi = warp_sum_down(hi); ni = warp_sum_down(ni); pi = warp_sum_down(pi);
-      if (lane == 0) {
-        min_fin[r] = lo; max_fin[r] = hi;
-        if (min_inf) { min_inf[r] = ni; max_inf[r] = pi; }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Rows longer than kActRowMax stored entries, one block each, in the class of
-// their live length (short: sequential; medium: warp 0, 32 lane partials;
-// long: 256 thread partials in the cub::BlockReduce order).
-template <bool Plain>
-__global__ void __launch_bounds__(kThreads)
-activity_long_rows(const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx, const double* __restrict__ val,
-                   const double2* __restrict__ lu, double zero_tol, const uint8_t* __restrict__ keep_row,
-                   const int32_t* __restrict__ live_deg, const int32_t* __restrict__ big,
-                   const int32_t* __restrict__ counts, double* __restrict__ min_fin, double* __restrict__ max_fin,
-                   int32_t* __restrict__ min_inf, int32_t* __restrict__ max_inf) {
-  __shared__ int slots[256];
-  __shared__ int warp_counts[8];
-  __shared__ double dagg[8];
-  __shared__ int iagg[8];
-  const ActivityTerm<Plain> term{idx, val, lu, zero_tol, l2_hints()};
-  const auto live_at = [&](offset_t p) { return !removed_column(term.bounds(p)); };
-  const int nbig = counts[1];
-  for (int q = blockIdx.x; q < nbig; q += gridDim.x) {
-    const int row = big[q];
-    const offset_t first = ptr[row], last = ptr[row + 1];
-    const int live_len = live_deg ? live_deg[row] : int(last - first);
-    const bool kept = !keep_row || keep_row[row];
-    const bool all_live = live_deg && live_len == int(last - first);
-    double lo = 0.0, hi = 0.0;
-    int ni = 0, pi = 0;
-    if (live_len <= kShortRow) {
-      if (threadIdx.x == 0) {
-        if (kept)
-          for (offset_t p = first; p < last; ++p) {
-            const double2 bnd = term.bounds(p);
-            if (!removed_column(bnd)) term(p, bnd, lo, hi, ni, pi);
-          }
-        min_fin[row] = lo; max_fin[row] = hi;
-        if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
-      }
-    } else if (live_len <= kLongRow) {
-      if (threadIdx.x < 32) {
-        if (kept)
-          live_visit_by<32>(first, last, all_live, live_at, slots, nullptr,
-                            [&](offset_t p) { term(p, term.bounds(p), lo, hi, ni, pi); });
-        lo = warp_sum_down(lo); hi = warp_sum_down(hi); ni = warp_sum_down(ni); pi = warp_sum_down(pi);
-        if (threadIdx.x == 0) {
-          min_fin[row] = lo; max_fin[row] = hi;
-          if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
-        }
-      }
-    } else {
-      if (kept)
-        live_visit_by<256>(first, last, all_live, live_at, slots, warp_counts,
-                           [&](offset_t p) { term(p, term.bounds(p), lo, hi, ni, pi); });
-      lo = block_sum_cub_order(lo, dagg);
-      hi = block_sum_cub_order(hi, dagg);
-      ni = block_sum_cub_order(ni, iagg);
-      pi = block_sum_cub_order(pi, iagg);
-      if (threadIdx.x == 0) {
-        min_fin[row] = lo; max_fin[row] = hi;
-        if (min_inf) { min_inf[row] = ni; max_inf[row] = pi; }
-      }
-    }
-    __syncthreads();
-  }
-}
-
 __global__ void pack_bounds_kernel(int n, const double* __restrict__ l, const double* __restrict__ u,
                                    const uint8_t* __restrict__ keep, double2* __restrict__ lu) {
   const double removed = __longlong_as_double(static_cast<long long>(kRemovedColumnBits));
@@ -780,7 +548,6 @@ void build_schedule(RowSchedule& s, const DevCsr& M, const int32_t* live_degrees
              s.long_rows.p, s.counts.p);
   s.tiles = 0;
   s.sorted = -1;
-  s.act_built = false;
   if (!live_degrees && M.rows > 0 && M.nnz > 0) {
     s.tiles = (int64_t(M.nnz) + kEntryTile - 1) / kEntryTile;
     if (s.tile_rows.n < size_t(s.tiles)) s.tile_rows.alloc(size_t(s.tiles), st);
@@ -973,46 +740,32 @@ void pack_bounds(const double* l, const double* u, const uint8_t* keep_col, int3
 }
 
 namespace {
-// Row tiles of the activity sweep, built once per stored matrix.
-void ensure_activity_tiles(const RowSchedule& sch, const DevCsr& A, cudaStream_t s) {
-  if (sch.act_built) return;
-  const int m = A.rows;
-  const size_t max_tiles = size_t((2 * int64_t(A.nnz) + m) / kActTileWeight + 2);
-  if (sch.act_first.n < max_tiles + 1) sch.act_first.alloc(max_tiles + 1, s);
-  if (sch.act_big.n < size_t(std::max(m, 1))) sch.act_big.alloc(size_t(std::max(m, 1)), s);
-  if (sch.act_counts.n < 2) sch.act_counts.alloc(2, s);
-  sch.act_counts.zero();
-  DBuf<int64_t> w(size_t(m) + 1, s), W(size_t(m) + 1, s);
-  GPP_LAUNCH(act_tile_weights, grid_stride_blocks(m), kThreads, 0, s, m, A.ptr, w.p);
-  exclusive_scan_i64(w.p, W.p, m, s);
-  GPP_LAUNCH(act_tile_bounds, grid_stride_blocks(m), kThreads, 0, s, m, W.p, A.ptr, sch.act_first.p, sch.act_big.p,
-             sch.act_counts.p);
-  sch.act_built = true;
-}
-
 template <bool Plain>
 void launch_activity(const DevCsr& A, const double2* lu, double zero_tol, const uint8_t* keep_row,
                      const int32_t* live_deg, double* lo, double* hi, int32_t* ni, int32_t* pi, double out_bytes,
                      cudaStream_t s) {
-  const RowSchedule& sch = stored_schedule(A);
-  ensure_activity_tiles(sch, A, s);
+  static thread_local RowSchedule* live_schedule = new RowSchedule;  // never destroyed (see schedule_cache)
+  const RowSchedule* sch;
+  if (live_deg) {
+    build_schedule(*live_schedule, A, live_deg, s);
+    sch = live_schedule;
+  } else {
+    sch = &stored_schedule(A);
+  }
+  const Roles r = roles_for(A.rows);
   // Algorithmic bytes (each array charged once): row pointers, column indices
   // and values, packed column bounds, row mask, live degrees, the outputs.
   const double bytes = 4.0 * (A.rows + 1) + 12.0 * A.nnz + 16.0 * A.cols + (keep_row ? A.rows : 0) +
                        (live_deg ? 4.0 * A.rows : 0) + out_bytes * A.rows;
-  const int tiles_grid = int(std::min<int64_t>(int64_t(kNumSMs) * 3, (2 * int64_t(A.nnz) + A.rows) / kActTileWeight + 2));
-  const int long_grid = std::min(kNumSMs * 2, std::max(1, A.rows));
-  if constexpr (Plain) {
-    GPP_LAUNCH_BYTES(activity_tiles<true>, bytes, tiles_grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu,
-                     zero_tol, keep_row, live_deg, sch.act_first.p, sch.act_counts.p, lo, hi, ni, pi);
-    GPP_LAUNCH(activity_long_rows<true>, long_grid, kThreads, 0, s, A.ptr, A.idx, A.val, lu, zero_tol, keep_row,
-               live_deg, sch.act_big.p, sch.act_counts.p, lo, hi, ni, pi);
-  } else {
-    GPP_LAUNCH_BYTES(activity_tiles<false>, bytes, tiles_grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu,
-                     zero_tol, keep_row, live_deg, sch.act_first.p, sch.act_counts.p, lo, hi, ni, pi);
-    GPP_LAUNCH(activity_long_rows<false>, long_grid, kThreads, 0, s, A.ptr, A.idx, A.val, lu, zero_tol, keep_row,
-               live_deg, sch.act_big.p, sch.act_counts.p, lo, hi, ni, pi);
-  }
+  const int grid = r.short_blocks + r.medium_blocks + r.long_blocks;
+  if constexpr (Plain)
+    GPP_LAUNCH_BYTES(activity_kernel<true>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
+  else
+    GPP_LAUNCH_BYTES(activity_kernel<false>, bytes, grid, kThreads, 0, s, A.rows, A.ptr, A.idx, A.val, lu, zero_tol,
+                     keep_row, live_deg, sch->medium.p, sch->long_rows.p, sch->counts.p, r.short_blocks,
+                     r.medium_blocks, lo, hi, ni, pi);
 }
 }  // namespace
 
