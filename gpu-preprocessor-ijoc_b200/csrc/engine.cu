@@ -263,8 +263,12 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
             rule_two_row_variable_elimination(e.plan, cur, p);
           if (p.enable_zero_cost_product_variables && !time_exceeded())
             rule_zero_cost_product_variables(e.plan, cur, p);
-        }))
-      e.materialize("startup");
+        })) {
+    }
+    // Applies the batch when it changed the model, and in any case retires
+    // its plan: the reformulations below replace the working model, and the
+    // main loop's first rule then starts a fresh plan on the model they leave.
+    e.materialize("startup");
     if (p.enable_structure_specific_rules && p.enable_piecewise_linear_reformulation_variable_pair && !e.terminal &&
         !time_exceeded())
       e.materialized_rule(true, "startup_piecewise_linear_reformulation_variable_pair",

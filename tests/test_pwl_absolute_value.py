@@ -194,7 +194,10 @@ def trp_file(ref, name, dt):
 
 
 def presolve_vs_reference(lp, extra, postsolve=False):
-    got = trp.check_against_reference(lp, trp.ALL, extra, oracle=False, postsolve=postsolve)
+    """Startup-only settings (max_iters in `extra`) also turn every other rule
+    off, so the reduced model is exactly the reformulation's rewrite."""
+    rules = [] if extra.get("max_iters") == 1 else trp.ALL
+    got = trp.check_against_reference(lp, rules, extra, oracle=False, postsolve=postsolve)
     check_recoveries(got)
     return got
 
