@@ -799,7 +799,8 @@ def workload(name: str, seed: int = 0) -> HostLP:
     'replicated:MxN*K' (K identical copies plus a coupling row), 'setcover:MxN' (unit set covering),
     'auxiliary:MxN' (random family plus projected-auxiliary blocks), 'qap:N', and the
     absolute-value layouts 'l1split:KxP' (K blocks, P features), 'graphl1:KxP' and
-    'outerl1:PAIRSxBLOCKS'."""
+    'outerl1:PAIRSxBLOCKS', and the variable-pair layouts 'epigraph:CxS' / 'antipodal:CxS'
+    (C components of S pairs)."""
     if name == "small":
         return random_lp(2000, 5000, seed)
     if name == "scale":
@@ -831,6 +832,12 @@ def workload(name: str, seed: int = 0) -> HostLP:
     if name.startswith("graphl1:"):
         k, p = (int(v) for v in name.split(":")[1].split("x"))
         return graph_l1_lp(k, p, seed)
+    if name.startswith("antipodal:"):
+        k, size = (int(v) for v in name.split(":")[1].split("x"))
+        return antipodal_pair_lp(k, size, seed=seed)
+    if name.startswith("epigraph:"):
+        k, size = (int(v) for v in name.split(":")[1].split("x"))
+        return epigraph_pair_lp(k, size, seed=seed)
     if name.startswith("outerl1:"):
         pairs, blocks = (int(v) for v in name.split(":")[1].split("x"))
         return outer_l1_lp(pairs, blocks, seed=seed)

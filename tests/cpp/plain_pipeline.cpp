@@ -161,6 +161,47 @@ static int run(const std::string& in, const std::string& out, const ps::Presolve
   save(out, "tape_vs", record.tape.value_starts);
   save(out, "tape_idx", record.tape.indices);
   save(out, "tape_val", record.tape.vals);
+  // The piecewise-linear reformulations' checkpoints and payloads, and the
+  // absolute-value steps applied to a fixed vector by the public restore.
+  {
+    std::vector<std::int32_t> kinds, payloads, st, se, vplus, vroot;
+    std::vector<long long> positions;
+    std::vector<double> sr, vshift;
+    for (const auto& c : record.primal_recovery_timeline) {
+      kinds.push_back(static_cast<std::int32_t>(c.kind));
+      payloads.push_back(c.payload_index);
+      positions.push_back(c.tape_position);
+    }
+    for (const auto& a : record.piecewise_linear_reformulation_absolute_value_recoveries)
+      for (const auto& x : a.splits) {
+        st.push_back(x.t_col);
+        se.push_back(x.e_col);
+        sr.push_back(x.rho);
+      }
+    for (const auto& a : record.piecewise_linear_reformulation_variable_pair_recoveries) {
+      vplus.insert(vplus.end(), a.plus_cols.begin(), a.plus_cols.end());
+      vroot.insert(vroot.end(), a.root_plus_cols.begin(), a.root_plus_cols.end());
+      vshift.insert(vshift.end(), a.plus_shift.begin(), a.plus_shift.end());
+    }
+    save(out, "ckpt_kind", kinds);
+    save(out, "ckpt_payload", payloads);
+    save(out, "ckpt_position", positions);
+    save(out, "abs_split_t", st);
+    save(out, "abs_split_e", se);
+    save(out, "abs_split_rho", sr);
+    save(out, "vp_plus", vplus);
+    save(out, "vp_root_plus", vroot);
+    save(out, "vp_plus_shift", vshift);
+    if (!record.piecewise_linear_reformulation_absolute_value_recoveries.empty()) {
+      std::vector<double> xv(static_cast<std::size_t>(h.n));
+      for (std::size_t j = 0; j < xv.size(); ++j) xv[j] = 0.5 * double(j % 9) - 1.0;
+      double* dxv = upload(xv);
+      ps::postsolve_restore_piecewise_linear_reformulation_absolute_value_gpu(
+          dxv, record.piecewise_linear_reformulation_absolute_value_recoveries, lp.l);
+      save(out, "restored", download(dxv, xv.size()));
+      ck(cudaFree(dxv), "cudaFree");
+    }
+  }
 
   if (summary.folding_applied) {
     const auto map = gpp::folding::copy_map_to_host(summary.folding.map);

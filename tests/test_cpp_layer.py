@@ -65,6 +65,11 @@ CASES = [
                             doubleton_equations_min_selected_ratio=0.0)),
     ("replicated:100x250*4", dict(enable_folding=1)),
     ("hub:300x800", dict()),  # the reference's defaults
+    # The piecewise-linear reformulations through the layer's record export and restore.
+    ("l1split:200x12", dict(enable_folding=0)),
+    ("graphl1:200x12", dict(enable_folding=0)),
+    ("antipodal:40x4", dict(enable_folding=0,
+                            piecewise_linear_reformulation_variable_pair_shifted_antipodal_min_pairs=16)),
 ]
 
 
@@ -86,7 +91,7 @@ def meta(path):
 def test_plain_pipeline_matches_ctypes_path(program, tmp_path, workload, extra):
     import torch
     from gpp_b200 import capi, device, lpgen
-    name = workload if workload.split(":")[0] in ("slack", "replicated") else None
+    name = workload if workload.split(":")[0] in ("slack", "replicated", "l1split", "graphl1", "antipodal") else None
     lp = lpgen.workload(name, seed=3) if name else lpgen.random_lp(300, 800, seed=3, hub_rows=4)
     lp_path = str(tmp_path / "lp.bin")
     lpgen.save_lp(lp_path, lp)
@@ -124,6 +129,26 @@ def test_plain_pipeline_matches_ctypes_path(program, tmp_path, workload, extra):
         assert np.array_equal(read(out / "tape_val", np.float64).view(np.uint64), ref.tape_val.view(np.uint64))
         assert np.array_equal(read(out / "fixed_idx", np.int32), ref.fixed_idx)
         assert np.array_equal(read(out / "fixed_val", np.float64).view(np.uint64), ref.fixed_val.view(np.uint64))
+        ck = list(zip(read(out / "ckpt_kind", np.int32).tolist(), read(out / "ckpt_payload", np.int32).tolist(),
+                      read(out / "ckpt_position", np.int64).tolist()))
+        assert ck == ref.checkpoints
+        if workload.split(":")[0] in ("l1split", "graphl1", "antipodal"):
+            assert len(ck) == 1
+        splits = [(a["split_t"], a["split_e"], a["split_rho"]) for a in ref.absolute_value]
+        if splits:
+            assert np.array_equal(read(out / "abs_split_t", np.int32), np.concatenate([t for t, _, _ in splits]))
+            assert np.array_equal(read(out / "abs_split_e", np.int32), np.concatenate([e for _, e, _ in splits]))
+            assert np.array_equal(read(out / "abs_split_rho", np.float64), np.concatenate([r for _, _, r in splits]))
+            xv = torch.tensor(0.5 * (np.arange(lp.n) % 9) - 1.0, dtype=torch.float64, device="cuda")
+            device.restore_absolute_value(xv, ref.absolute_value, dlp.t["l"])
+            assert np.array_equal(read(out / "restored", np.float64).view(np.uint64),
+                                  xv.cpu().numpy().view(np.uint64))
+        if ref.variable_pair:
+            assert np.array_equal(read(out / "vp_plus", np.int32), np.concatenate([a["plus"] for a in ref.variable_pair]))
+            assert np.array_equal(read(out / "vp_root_plus", np.int32),
+                                  np.concatenate([a["root_plus"] for a in ref.variable_pair]))
+            assert np.array_equal(read(out / "vp_plus_shift", np.float64),
+                                  np.concatenate([a["plus_shift"] for a in ref.variable_pair]))
         if s.folding_applied:
             rc, cc, rs, cs = device.fold_map(s)
             assert np.array_equal(read(out / "row_color", np.int32), rc)
