@@ -212,6 +212,15 @@ struct Engine {
     terminal = pl.has_infeasible || pl.has_unbounded;
     const bool changed = !terminal && pl.has_change;
     if (changed) {
+      // A deferred plan still open here (Startup's batch plan when the batch
+      // changed nothing) describes the model this rule replaces: retire it,
+      // so the next deferred rule starts a fresh plan on the new model.
+      if (active) {
+        if (pending) throw std::logic_error("materialized rule over a plan with unapplied changes");
+        active = false;
+        plan = Plan{};
+        stats = Stats{};
+      }
       apply(pl, false);
       out.trace.push_back(std::string("apply=") + name);
     }
@@ -263,12 +272,8 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
             rule_two_row_variable_elimination(e.plan, cur, p);
           if (p.enable_zero_cost_product_variables && !time_exceeded())
             rule_zero_cost_product_variables(e.plan, cur, p);
-        })) {
-    }
-    // Applies the batch when it changed the model, and in any case retires
-    // its plan: the reformulations below replace the working model, and the
-    // main loop's first rule then starts a fresh plan on the model they leave.
-    e.materialize("startup");
+        }))
+      e.materialize("startup");
     if (p.enable_structure_specific_rules && p.enable_piecewise_linear_reformulation_variable_pair && !e.terminal &&
         !time_exceeded())
       e.materialized_rule(true, "startup_piecewise_linear_reformulation_variable_pair",
