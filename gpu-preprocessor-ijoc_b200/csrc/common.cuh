@@ -290,6 +290,16 @@ std::vector<T> to_host(const T* d, size_t count) {
   }
   return h;
 }
+// Two arrays in one wait.
+template <class T, class U>
+std::pair<std::vector<T>, std::vector<U>> to_host2(const T* a, size_t na, const U* b, size_t nb) {
+  std::vector<T> ha(na);
+  std::vector<U> hb(nb);
+  if (na) check(cudaMemcpyAsync(ha.data(), a, na * sizeof(T), cudaMemcpyDeviceToHost, ctx().stream), "d2h");
+  if (nb) check(cudaMemcpyAsync(hb.data(), b, nb * sizeof(U), cudaMemcpyDeviceToHost, ctx().stream), "d2h");
+  if (na || nb) ctx().sync("d2h sync");
+  return {std::move(ha), std::move(hb)};
+}
 template <class T>
 T read_scalar(const T* d, const char* where = __builtin_FUNCTION()) {
   // Through the context's pinned block: a pageable destination would make

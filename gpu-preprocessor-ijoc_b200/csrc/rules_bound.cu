@@ -411,7 +411,7 @@ void rule_bound_strengthening(Plan& plan, const WorkingLp& lp, const Stats& stat
                seg.val.p, oc.p, ov.p);
     // append_compact_fixed_variable_tape_from_device (fixed_variable_tape.cu:286-315):
     // objective delta accumulated in long double in column order.
-    const std::vector<double> hc = to_host(oc.p, size_t(recs)), hv = to_host(ov.p, size_t(recs));
+    const auto [hc, hv] = to_host2(oc.p, size_t(recs), ov.p, size_t(recs));
     long double acc = 0.0L;
     for (size_t k = 0; k < hc.size(); ++k) acc += (long double)hc[k] * (long double)hv[k];
     obj_delta = double(acc);

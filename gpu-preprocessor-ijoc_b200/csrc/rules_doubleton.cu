@@ -926,8 +926,7 @@ void rule_doubleton_equations(Plan& plan, const WorkingLp& lp, const gpp_params&
   }
 
   // Objective: substitution terms, then fixed terms, each in batch order.
-  const std::vector<uint8_t> hk = to_host(kind.p, size_t(sel));
-  const std::vector<double> ho = to_host(obj_term.p, size_t(sel));
+  const auto [hk, ho] = to_host2(kind.p, size_t(sel), obj_term.p, size_t(sel));
   double obj = 0.0, fixed_obj = 0.0;
   for (int t = 0; t < sel; ++t) {
     if (hk[size_t(t)] == kPairSubst) obj += ho[size_t(t)];

@@ -704,8 +704,7 @@ void rule_singleton_columns(Plan& plan, const WorkingLp& lp, const Stats& stats,
   }
 
   if (nelim) {
-    std::vector<int64_t> ci = to_host(contrib_idx.p, size_t(nelim));
-    std::vector<double> cv = to_host(contrib_val.p, size_t(nelim));
+    auto [ci, cv] = to_host2(contrib_idx.p, size_t(nelim), contrib_val.p, size_t(nelim));
     std::vector<std::pair<int64_t, double>> entries(ci.size());
     for (size_t k = 0; k < ci.size(); ++k) entries[k] = {ci[k], cv[k]};
     plan.obj_delta += det_sum_sparse(std::move(entries));
