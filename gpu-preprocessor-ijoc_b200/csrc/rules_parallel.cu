@@ -171,10 +171,53 @@ row_hash_kernel(int rows, RowHashArgs g, const int32_t* __restrict__ medium, con
   for (int q = wid; q < counts[1]; q += nwarps) row_hash_warp(g, longq[q]);
 }
 
-__global__ void gather_live(int n, const uint8_t* __restrict__ keep, const int32_t* __restrict__ pos,
+__global__ void gather_live(int n, const int32_t* __restrict__ take, const int32_t* __restrict__ pos,
                             const uint64_t* __restrict__ hash, uint64_t* __restrict__ keys, int32_t* __restrict__ ids) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (keep[i]) { keys[pos[i]] = hash[i]; ids[pos[i]] = i; }
+    if (take[i]) { keys[pos[i]] = hash[i]; ids[pos[i]] = i; }
+}
+
+// Repeated-hash filter.  Only a hash that two or more live items share can
+// form a group, so only those items need sorting.  Every live item takes two
+// positions in a bitmap from its mixed hash (the SplitMix64 finaliser, so the
+// positions are spread whatever the row hash's low bits look like), sets them
+// in `seen`, and marks a position in `twice` when it finds it already set.
+// An item is a candidate when both of its positions are marked.  Items with
+// equal hashes have equal positions, so every group of two or more is kept
+// whole; a hash held once is kept only if both of its positions collide with
+// other items (with 32 bitmap positions per item, about 0.4% of them).  The
+// dropped items are groups of one, which the group kernels pass over, and the
+// kept ones stay in (hash, index) order, so the groups found, their order and
+// every record are those of the unfiltered sort.
+__device__ __forceinline__ uint64_t mix_hash(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+__global__ void mark_hash_bits(int n, const uint8_t* __restrict__ keep, const uint64_t* __restrict__ hash,
+                               uint32_t* __restrict__ seen, uint32_t* __restrict__ twice, uint64_t bit_mask) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!keep[i]) continue;
+    const uint64_t z = mix_hash(hash[i]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const uint64_t b = (k ? z >> 32 : z) & bit_mask;
+      const uint32_t bit = 1u << (b & 31u);
+      if (atomicOr(seen + (b >> 5), bit) & bit) atomicOr(twice + (b >> 5), bit);
+    }
+  }
+}
+__global__ void flag_repeated(int n, const uint8_t* __restrict__ keep, const uint64_t* __restrict__ hash,
+                              const uint32_t* __restrict__ twice, uint64_t bit_mask, int32_t* __restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int32_t f = 0;
+    if (keep[i]) {
+      const uint64_t z = mix_hash(hash[i]);
+      const uint64_t b0 = z & bit_mask, b1 = (z >> 32) & bit_mask;
+      f = (twice[b0 >> 5] >> (b0 & 31u) & 1u) && (twice[b1 >> 5] >> (b1 & 31u) & 1u);
+    }
+    flag[i] = f;
+  }
 }
 
 // --- parallel rows ------------------------------------------------------------
@@ -526,16 +569,33 @@ __global__ void fixed_pack(int n, const uint8_t* __restrict__ fx, const offset_t
   }
 }
 
-// Sorted (hash, index) pairs of the live rows (columns).
+// Sorted (hash, index) pairs of the live rows (columns) whose hash may be
+// shared: all live items up to kRepeatFilterMin, past it the candidates of
+// the repeated-hash filter.
+constexpr int32_t kRepeatFilterMin = 32768;
 int32_t sorted_live_hashes(const uint64_t* hash, const uint8_t* keep, int32_t n, DBuf<uint64_t>& keys,
                            DBuf<int32_t>& ids, cudaStream_t s) {
   DBuf<int32_t> flag(size_t(n) + 1, s), pos(size_t(n) + 1, s);
-  GPP_LAUNCH(flag_to_int, grid_stride_blocks(n), kThreads, 0, s, n, keep, flag.p);
+  if (n > kRepeatFilterMin) {
+    // 32 bitmap positions per item, a power of two between 2^20 and 2^29.
+    int lg = 20;
+    while (lg < 29 && (int64_t(1) << lg) < 32 * int64_t(n)) ++lg;
+    const size_t words = size_t(1) << (lg - 5);
+    DBuf<uint32_t> bits(2 * words, s);
+    bits.zero();
+    const uint64_t bit_mask = (uint64_t(1) << lg) - 1;
+    GPP_LAUNCH(mark_hash_bits, grid_stride_blocks(n), kThreads, 0, s, n, keep, hash, bits.p, bits.p + words,
+               bit_mask);
+    GPP_LAUNCH(flag_repeated, grid_stride_blocks(n), kThreads, 0, s, n, keep, hash, bits.p + words, bit_mask,
+               flag.p);
+  } else {
+    GPP_LAUNCH(flag_to_int, grid_stride_blocks(n), kThreads, 0, s, n, keep, flag.p);
+  }
   exclusive_scan_i32(flag.p, pos.p, n, s);
   const int32_t count = read_scalar(pos.p + n);
   keys.alloc(size_t(std::max(count, 1)), s);
   ids.alloc(size_t(std::max(count, 1)), s);
-  GPP_LAUNCH(gather_live, grid_stride_blocks(n), kThreads, 0, s, n, keep, pos.p, hash, keys.p, ids.p);
+  GPP_LAUNCH(gather_live, grid_stride_blocks(n), kThreads, 0, s, n, flag.p, pos.p, hash, keys.p, ids.p);
   radix_sort_pairs(keys.p, ids.p, count, s);
   return count;
 }
