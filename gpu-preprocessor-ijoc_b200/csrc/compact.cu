@@ -29,168 +29,247 @@ __global__ void prefix_to_map(const uint8_t* __restrict__ keep, const int32_t* _
     old_to_new[i] = keep[i] ? prefix[i] : -1;
 }
 
-// Copy roles.  Rows of up to kLongRow stored entries go four to a warp,
-// eight lanes per row, the warp's four rows consecutive (so its loads and
-// stores cover one contiguous stretch of the matrix); longer rows take a whole
-// block.  Entries are copied in stored order, so the schedule is free.
-// First of the four consecutive rows of this warp in the group role.
-__device__ __forceinline__ int warp_first_row(int block) {
-  return (block * (kThreads / 32) + int(threadIdx.x >> 5)) * 4;
+// ---- entry-tiled compaction -------------------------------------------------
+//
+// The stored entries are cut into tiles of kCompactTile consecutive positions,
+// one block per tile and kCompactPer consecutive positions per thread, so the
+// index and value streams are read with 128-bit loads whatever the row
+// lengths.  A tile learns the row of each of its entries without a search:
+// the rows whose pointer falls inside the tile mark their start positions in
+// shared memory, and a block scan of the marks counts the row starts at or
+// before every position.  The copy is a stream compaction in stored order, so
+// a kept entry's output position is the number of kept entries before it:
+// per-tile counts, one scan of the counts, then the copy, whose block scan
+// places each kept entry and each kept row's new pointer.
+constexpr int kCompactPer = 8;
+constexpr int kCompactTile = kThreads * kCompactPer;
+
+// first_row[t]: the first row whose pointer is at or past t * kCompactTile
+// (rows when there is none).  Row r takes the tiles whose start lies in
+// (ptr[r - 1], ptr[r]]; the virtual row `rows` takes the tiles past the last
+// row's pointer.
+__global__ void compact_tile_rows(int rows, const offset_t* __restrict__ ptr, int tiles,
+                                  int32_t* __restrict__ first_row) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= rows; r += gridDim.x * blockDim.x) {
+    const int64_t lo = r == 0 ? 0 : int64_t(ptr[r - 1]) / kCompactTile + 1;
+    int64_t hi = r == rows ? int64_t(tiles) - 1 : int64_t(ptr[r]) / kCompactTile;
+    if (hi > tiles - 1) hi = tiles - 1;
+    for (int64_t t = lo; t <= hi; ++t) first_row[t] = r;
+  }
 }
 
-// Count kept entries of kept rows: short rows by thread, medium by warp,
-// long by block (roles as in live.cu).
+// Exclusive scan of one value per thread over the block; the block total goes
+// to *total.  `warp_sums` holds kThreads / 32 ints of shared memory.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += y;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  int before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) {
+    const int sw = warp_sums[w];
+    before += w < warp ? sw : 0;
+    all += sw;
+  }
+  __syncthreads();
+  *total = all;
+  return before + incl - v;
+}
+
+template <bool kVec>
+__device__ __forceinline__ void load_tile_cols(const int32_t* __restrict__ p, int avail, int (&col)[kCompactPer]) {
+  if (kVec && avail >= kCompactPer) {
+    const int4 a = __ldcs(reinterpret_cast<const int4*>(p));
+    const int4 b = __ldcs(reinterpret_cast<const int4*>(p) + 1);
+    col[0] = a.x; col[1] = a.y; col[2] = a.z; col[3] = a.w;
+    col[4] = b.x; col[5] = b.y; col[6] = b.z; col[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) col[k] = k < avail ? __ldcs(p + k) : -1;
+  }
+}
+template <bool kVec>
+__device__ __forceinline__ void load_tile_vals(const double* __restrict__ p, int avail, double (&v)[kCompactPer]) {
+  if (kVec && avail >= kCompactPer) {
+#pragma unroll
+    for (int k = 0; k < kCompactPer / 2; ++k) {
+      const double2 d = __ldcs(reinterpret_cast<const double2*>(p) + k);
+      v[2 * k] = d.x;
+      v[2 * k + 1] = d.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) v[k] = k < avail ? __ldcs(p + k) : 0.0;
+  }
+}
+
+// Kept-entry mask of this thread's kCompactPer positions: the entry exists,
+// its row is kept and its (remapped) inner index is kept.  `col` holds the
+// inner indices already mapped (-1 for a dropped or missing entry).
+__device__ __forceinline__ unsigned tile_kept_mask(int r0, int64_t base, int len, const offset_t* __restrict__ ptr,
+                                                   int r1, const int32_t* __restrict__ outer_map,
+                                                   const int (&col)[kCompactPer], int* marker, int* warp_sums) {
+  const int p0 = int(threadIdx.x) * kCompactPer;
+  // Row starts inside the tile.
+#pragma unroll
+  for (int k = 0; k < kCompactPer; ++k) marker[p0 + k] = 0;
+  __syncthreads();
+  for (int r = r0 + int(threadIdx.x); r < r1; r += kThreads) {
+    const int64_t pos = int64_t(ptr[r]) - base;
+    if (pos < len) atomicAdd(marker + pos, 1);
+  }
+  __syncthreads();
+  int mk[kCompactPer], local = 0;
+#pragma unroll
+  for (int k = 0; k < kCompactPer; ++k) {
+    mk[k] = marker[p0 + k];
+    local += mk[k];
+  }
+  int total;
+  int row = r0 - 1 + block_exclusive_scan(local, warp_sums, &total);
+  unsigned mask = 0;
+  int cached_row = -1, cached_keep = -1;
+#pragma unroll
+  for (int k = 0; k < kCompactPer; ++k) {
+    row += mk[k];
+    if (p0 + k < len && col[k] >= 0) {
+      if (row != cached_row) {
+        cached_row = row;
+        cached_keep = outer_map[row];
+      }
+      if (cached_keep >= 0) mask |= 1u << k;
+    }
+  }
+  return mask;
+}
+
+// Both kernels are persistent: a block takes tiles blockIdx.x, + gridDim.x,
+// ... and loads the next tile's stored entries into registers before it works
+// on the current one, so the stream of the next tile is in flight while the
+// current tile runs its dependent chain (row starts, scans, gathers).
+template <bool kVec>
 __global__ void __launch_bounds__(kThreads)
-count_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-           const int32_t* __restrict__ outer_map, const int32_t* __restrict__ inner_map,
-           const int32_t* __restrict__ medium, const int32_t* __restrict__ longq,
-           const int32_t* __restrict__ counts, int short_blocks, int medium_blocks,
-           int32_t* __restrict__ out_counts) {
-  __shared__ int scount[8];
-  const int b = blockIdx.x;
-  if (b < short_blocks) {
-    const int stride_ = short_blocks * blockDim.x;
-    int r_next = b * blockDim.x + threadIdx.x;
-    offset_t first_next = r_next < rows ? ptr[r_next] : 0, last_next = r_next < rows ? ptr[r_next + 1] : 0;
-    for (int r = r_next; r < rows; r += stride_) {
-      const offset_t first = first_next, last = last_next;
-      r_next = r + stride_;   // the next row's pointers, one iteration ahead
-      first_next = r_next < rows ? ptr[r_next] : 0;
-      last_next = r_next < rows ? ptr[r_next + 1] : 0;
-      if (last - first > kShortRow) continue;
+compact_count(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+              const int32_t* __restrict__ outer_map, const int32_t* __restrict__ inner_map,
+              const int32_t* __restrict__ first_row, int rows, int tiles, int32_t* __restrict__ tile_counts) {
+  __shared__ __align__(16) int marker[kCompactTile];
+  __shared__ int warp_sums[kThreads / 32];
+  const int p0 = int(threadIdx.x) * kCompactPer;
+  int next[kCompactPer], next_r0 = 0, next_r1 = 0;
+  int t = blockIdx.x;
+  if (t < tiles) {
+    const int64_t base = int64_t(t) * kCompactTile;
+    load_tile_cols<kVec>(idx + base + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - base)) - p0, next);
+    next_r0 = first_row[t];
+    next_r1 = t + 1 < tiles ? first_row[t + 1] : rows;
+  }
+  for (; t < tiles; t += gridDim.x) {
+    const int64_t base = int64_t(t) * kCompactTile;
+    const int len = int(min(int64_t(kCompactTile), int64_t(nnz) - base));
+    int col[kCompactPer];
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) col[k] = next[k];
+    const int r0 = next_r0, r1 = next_r1;
+    const int tn = t + int(gridDim.x);
+    if (tn < tiles) {
+      const int64_t nbase = int64_t(tn) * kCompactTile;
+      load_tile_cols<kVec>(idx + nbase + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - nbase)) - p0, next);
+      next_r0 = first_row[tn];
+      next_r1 = tn + 1 < tiles ? first_row[tn + 1] : rows;
+    }
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) col[k] = col[k] >= 0 ? inner_map[col[k]] : -1;
+    const unsigned mask = tile_kept_mask(r0, base, len, ptr, r1, outer_map, col, marker, warp_sums);
+    int total;
+    block_exclusive_scan(__popc(mask), warp_sums, &total);
+    if (threadIdx.x == 0) tile_counts[t] = total;
+  }
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(kThreads)
+compact_copy(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+             const double* __restrict__ val, const int32_t* __restrict__ outer_map,
+             const int32_t* __restrict__ inner_map, const int32_t* __restrict__ first_row, int rows, int tiles,
+             const int32_t* __restrict__ tile_offsets, int32_t outer_new, offset_t* __restrict__ out_ptr,
+             int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
+  // `marker` is free once the rows are known and then stages the kept
+  // indices; `stage_val` the kept values.  The stores go out coalesced.
+  __shared__ __align__(16) int marker[kCompactTile];
+  __shared__ __align__(16) double stage_val[kCompactTile];
+  __shared__ int warp_sums[kThreads / 32];
+  __shared__ int thread_before[kThreads];
+  __shared__ unsigned thread_mask[kThreads];
+  const int p0 = int(threadIdx.x) * kCompactPer;
+  int next_col[kCompactPer], next_r0 = 0, next_r1 = 0;
+  int t = blockIdx.x;
+  if (t < tiles) {
+    const int64_t base = int64_t(t) * kCompactTile;
+    load_tile_cols<kVec>(idx + base + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - base)) - p0, next_col);
+    next_r0 = first_row[t];
+    next_r1 = t + 1 < tiles ? first_row[t + 1] : rows;
+  }
+  for (; t < tiles; t += gridDim.x) {
+    const int64_t base = int64_t(t) * kCompactTile;
+    const int len = int(min(int64_t(kCompactTile), int64_t(nnz) - base));
+    int col[kCompactPer];
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) col[k] = next_col[k];
+    // This tile's values are first needed by the stores at the end, the next
+    // tile's indices at the top of the next round: both loads run under this
+    // tile's chain.
+    double v[kCompactPer];
+    load_tile_vals<kVec>(val + base + p0, len - p0, v);
+    const int64_t tile_out = tile_offsets[t];
+    const int r0 = next_r0, r1 = next_r1;
+    const int tn = t + int(gridDim.x);
+    if (tn < tiles) {
+      const int64_t nbase = int64_t(tn) * kCompactTile;
+      load_tile_cols<kVec>(idx + nbase + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - nbase)) - p0, next_col);
+      next_r0 = first_row[tn];
+      next_r1 = tn + 1 < tiles ? first_row[tn + 1] : rows;
+    }
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k) col[k] = col[k] >= 0 ? inner_map[col[k]] : -1;
+    const unsigned mask = tile_kept_mask(r0, base, len, ptr, r1, outer_map, col, marker, warp_sums);
+    int total;
+    const int before = block_exclusive_scan(__popc(mask), warp_sums, &total);
+    int o = before;
+#pragma unroll
+    for (int k = 0; k < kCompactPer; ++k)
+      if (mask >> k & 1u) {
+        marker[o] = col[k];
+        stage_val[o] = v[k];
+        ++o;
+      }
+    thread_before[threadIdx.x] = before;
+    thread_mask[threadIdx.x] = mask;
+    __syncthreads();
+    for (int q = int(threadIdx.x); q < total; q += kThreads) {
+      out_idx[tile_out + q] = marker[q];
+      out_val[tile_out + q] = stage_val[q];
+    }
+    // New row pointers of the kept rows that start in this tile: the kept
+    // entries before the row's first position.
+    for (int r = r0 + int(threadIdx.x); r < r1; r += kThreads) {
       const int nr = outer_map[r];
       if (nr < 0) continue;
-      // All (at most 8) index loads, then all map gathers, in flight together.
-      int col[kShortRow];
-#pragma unroll
-      for (int k = 0; k < kShortRow; ++k) col[k] = first + k < last ? __ldcs(idx + first + k) : -1;
-      int c = 0;
-#pragma unroll
-      for (int k = 0; k < kShortRow; ++k) c += col[k] >= 0 && inner_map[col[k]] >= 0;
-      out_counts[nr] = c;
-    }
-    return;
-  }
-  if (b < short_blocks + medium_blocks) {
-    // Four medium rows per warp, eight lanes each.
-    const int g = threadIdx.x & 7;
-    const int nwarps = medium_blocks * (kThreads / 32);
-    for (int q0 = ((b - short_blocks) * (kThreads / 32) + (threadIdx.x >> 5)) * 4; q0 < counts[0]; q0 += nwarps * 4) {
-      const int q = q0 + ((threadIdx.x & 31) >> 3);
-      int nr = -1, c = 0;
-      if (q < counts[0]) {
-        const int r = medium[q];
-        nr = outer_map[r];
-        if (nr >= 0)
-          for (offset_t p = ptr[r] + g; p < ptr[r + 1]; p += 8) c += inner_map[__ldcs(idx + p)] >= 0;
+      const int64_t pos = int64_t(ptr[r]) - base;
+      int kept_before = total;
+      if (pos < len) {
+        const int q = int(pos) / kCompactPer, j = int(pos) % kCompactPer;
+        kept_before = thread_before[q] + __popc(thread_mask[q] & ((1u << j) - 1u));
       }
-      for (int off = 4; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off, 8);
-      if (g == 0 && nr >= 0) out_counts[nr] = c;
+      out_ptr[nr] = offset_t(tile_out + kept_before);
     }
-    return;
-  }
-  const int lb = b - short_blocks - medium_blocks, nlong = gridDim.x - short_blocks - medium_blocks;
-  for (int q = lb; q < counts[1]; q += nlong) {
-    const int r = longq[q];
-    const int nr = outer_map[r];
-    if (nr < 0) continue;  // block-uniform
-    int c = 0;
-    for (offset_t p = ptr[r] + threadIdx.x; p < ptr[r + 1]; p += kThreads) c += inner_map[__ldcs(idx + p)] >= 0;
-    for (int off = 16; off; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
-    if ((threadIdx.x & 31) == 0) scount[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 1; w < 8; ++w) c += scount[w];
-      out_counts[nr] = c;
-    }
-    __syncthreads();
-  }
-}
-
-// Stable copy of kept entries (order preserving), remapping inner indices.
-// In the group role a ballot over the group's eight lanes ranks the kept
-// entries of each round of eight stored entries; every lane runs the warp's
-// largest number of rounds, so the ballots stay warp-uniform.
-__global__ void __launch_bounds__(kThreads)
-copy_kept(int rows, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-          const double* __restrict__ val, const int32_t* __restrict__ outer_map,
-          const int32_t* __restrict__ inner_map, const int32_t* __restrict__ longq,
-          const int32_t* __restrict__ counts, int group_blocks, const offset_t* __restrict__ out_ptr,
-          int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
-  __shared__ int wcount[8];
-  const int b = blockIdx.x;
-  if (b < group_blocks) {
-    const int g = threadIdx.x & 7;
-    const unsigned shift = unsigned(threadIdx.x & 24);
-    const int stride = group_blocks * kThreads / 8;
-    for (int r0 = warp_first_row(b); r0 < rows; r0 += stride) {
-      const int r = r0 + int((threadIdx.x & 31) >> 3);
-      offset_t first = 0, end = 0, w = 0;
-      if (r < rows) {
-        const offset_t a = ptr[r], e = ptr[r + 1];
-        const int nr = e - a > kLongRow ? -1 : outer_map[r];
-        if (nr >= 0) {
-          first = a;
-          end = e;
-          w = out_ptr[nr];
-        }
-      }
-      const int rounds = __reduce_max_sync(0xffffffffu, int((end - first + 7) >> 3));
-      // Four rounds per step: their index loads, then their column-map
-      // gathers and value loads, are all in flight before the first ballot.
-      constexpr int kBatch = 4;
-      for (int k0 = 0; k0 < rounds; k0 += kBatch) {
-        int col[kBatch];
-        double v[kBatch];
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-          const offset_t p = first + offset_t(k0 + u) * 8 + g;
-          col[u] = k0 + u < rounds && p < end ? __ldcs(idx + p) : -1;
-        }
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-          const offset_t p = first + offset_t(k0 + u) * 8 + g;
-          col[u] = col[u] >= 0 ? inner_map[col[u]] : -1;
-          v[u] = col[u] >= 0 ? __ldcs(val + p) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-          if (k0 + u >= rounds) break;   // warp-uniform
-          const unsigned bits = (__ballot_sync(0xffffffffu, col[u] >= 0) >> shift) & 0xFFu;
-          if (col[u] >= 0) {
-            const offset_t o = w + __popc(bits & ((1u << g) - 1u));
-            out_idx[o] = col[u];
-            out_val[o] = v[u];
-          }
-          w += __popc(bits);
-        }
-      }
-    }
-    return;
-  }
-  const int lb = b - group_blocks, nlong = gridDim.x - group_blocks;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = lb; q < counts[1]; q += nlong) {
-    const int r = longq[q];
-    const int nr = outer_map[r];
-    if (nr < 0) continue;
-    offset_t w = out_ptr[nr];
-    for (offset_t chunk = ptr[r]; chunk < ptr[r + 1]; chunk += kThreads) {
-      const offset_t p = chunk + threadIdx.x;
-      const int c = p < ptr[r + 1] ? inner_map[__ldcs(idx + p)] : -1;
-      const unsigned mask = __ballot_sync(0xffffffffu, c >= 0);
-      if (lane == 0) wcount[warp] = __popc(mask);
-      __syncthreads();
-      int before = 0, total = 0;
-      for (int k = 0; k < 8; ++k) { before += k < warp ? wcount[k] : 0; total += wcount[k]; }
-      if (c >= 0) {
-        const offset_t o = w + before + __popc(mask & ((1u << lane) - 1u));
-        out_idx[o] = c;
-        out_val[o] = __ldcs(val + p);
-      }
-      w += total;
-      __syncthreads();
-    }
+    if (t == tiles - 1 && threadIdx.x == 0) out_ptr[outer_new] = offset_t(tile_out + total);
+    __syncthreads();   // the staging buffers are refilled by the next tile
   }
 }
 
@@ -268,6 +347,26 @@ __global__ void check_sorted(int rows, const offset_t* __restrict__ ptr, const i
       if (idx[p - 1] >= idx[p]) { atomicExch(bad, 1); break; }
 }
 
+// Structure of an uploaded CSR: pointers start at 0, end at nnz and never
+// decrease; every inner index lies in [0, cols).  Any violation sets *bad.
+__global__ void check_csr_structure(int rows, int cols, offset_t nnz, const offset_t* __restrict__ ptr,
+                                    const int32_t* __restrict__ idx, int32_t* bad) {
+  const int64_t top = int64_t(rows) + 1 > int64_t(nnz) ? int64_t(rows) + 1 : int64_t(nnz);
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < top; i += int64_t(gridDim.x) * blockDim.x) {
+    bool fail = false;
+    if (i <= rows) {
+      const offset_t p = ptr[i];
+      if (i == 0 ? p != 0 : p < ptr[i - 1]) fail = true;
+      if (i == rows && p != nnz) fail = true;
+    }
+    if (i < nnz) {
+      const int32_t c = idx[i];
+      if (c < 0 || c >= cols) fail = true;
+    }
+    if (fail) atomicExch(bad, 1);
+  }
+}
+
 __global__ void gather_kernel(double* __restrict__ dst, const double* __restrict__ src,
                               const int32_t* __restrict__ map, int32_t n) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
@@ -282,8 +381,6 @@ __global__ void compose_kernel(int32_t* __restrict__ next, const int32_t* __rest
     if (k >= 0) next[k] = prev[i];
   }
 }
-
-int roles_long(int rows) { return std::min<int>(kNumSMs * 4, rows); }
 
 // Old -> new maps of the row and the column masks together, straight from
 // the byte masks: one launch counts the kept items of every tile of
@@ -398,43 +495,61 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
     check(cudaMemsetAsync(out.ptr, 0, sizeof(offset_t) * (size_t(outer_new) + 1), s), "compact empty ptr");
     return out;
   }
-  const RowSchedule& sch = stored_schedule(M);
-  const int gb = std::max(1, std::min((M.rows + 31) / 32, kNumSMs * 16));
-  const int lb = roles_long(M.rows);
-  // Counting reads only: short rows one per thread (more rows in flight),
-  // medium rows four per warp, long rows one per block.
-  const int sb = grid_stride_blocks(M.rows, kThreads, 16), mb = std::min<int>(kNumSMs * 8, (M.rows + 7) / 8);
-  DBuf<int32_t> counts(size_t(outer_new) + 1, s);
-  const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * outer_new;
-  GPP_LAUNCH_BYTES(count_kept, count_bytes, sb + mb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, outer_map, inner_map,
-                   sch.medium.p, sch.long_rows.p, sch.counts.p, sb, mb, counts.p);
-  exclusive_scan_i32(counts.p, out.ptr, outer_new, s);
-  out.nnz = known_nnz >= 0 ? offset_t(known_nnz) : read_scalar(out.ptr + outer_new);
+  const int tiles = int((int64_t(M.nnz) + kCompactTile - 1) / kCompactTile);
+  DBuf<int32_t> first_row(size_t(tiles), s), tile_counts(size_t(tiles), s), tile_offsets(size_t(tiles) + 1, s);
+  GPP_LAUNCH(compact_tile_rows, grid_stride_blocks(int64_t(M.rows) + 1), kThreads, 0, s, M.rows, M.ptr, tiles,
+             first_row.p);
+  // 128-bit loads need 16-byte aligned index and value arrays (always so for
+  // the engine's own matrices; a caller's input may be offset).
+  const bool vec = reinterpret_cast<uintptr_t>(M.idx) % 16 == 0 && reinterpret_cast<uintptr_t>(M.val) % 16 == 0;
+  const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * tiles;
+  // One resident wave of persistent blocks (at most 6 per SM for the count,
+  // 4 for the copy: their register budgets).
+  const int count_grid = std::min(tiles, kNumSMs * 6), copy_grid = std::min(tiles, kNumSMs * 4);
+  if (vec)
+    GPP_LAUNCH_BYTES(compact_count<true>, count_bytes, count_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, tile_counts.p);
+  else
+    GPP_LAUNCH_BYTES(compact_count<false>, count_bytes, count_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, tile_counts.p);
+  exclusive_scan_i32(tile_counts.p, tile_offsets.p, tiles, s);
+  out.nnz = known_nnz >= 0 ? offset_t(known_nnz) : read_scalar(tile_offsets.p + tiles);
   out.idx = dalloc<int32_t>(size_t(out.nnz));
   out.val = dalloc<double>(size_t(out.nnz));
   const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +
                             4.0 * (outer_new + 1) + 12.0 * out.nnz;
-  GPP_LAUNCH_BYTES(copy_kept, copy_bytes, gb + lb, kThreads, 0, s, M.rows, M.ptr, M.idx, M.val, outer_map,
-                   inner_map, sch.long_rows.p, sch.counts.p, gb, out.ptr, out.idx, out.val);
+  if (vec)
+    GPP_LAUNCH_BYTES(compact_copy<true>, copy_bytes, copy_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, tile_offsets.p, outer_new, out.ptr, out.idx, out.val);
+  else
+    GPP_LAUNCH_BYTES(compact_copy<false>, copy_bytes, copy_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, tile_offsets.p, outer_new, out.ptr, out.idx, out.val);
   return out;
 }
 
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
-  // Entries ordered by column, each column in stored (row-major) order,
-  // i.e. ascending rows (duplicates in stored order): the row-sorted CSR of
-  // M^T.  Short columns (all at most kShortColumn long) use atomic slots and
-  // a per-column sort of the positions; otherwise a stable radix sort.
   DevCsr t;
   t.rows = M.cols;
   t.cols = M.rows;
   t.nnz = M.nnz;
   t.ptr = dalloc<offset_t>(size_t(t.rows) + 1);
+  if (M.nnz > 0) {
+    t.idx = dalloc<int32_t>(size_t(M.nnz));
+    t.val = dalloc<double>(size_t(M.nnz));
+  }
+  transpose_csr_into(M, t, s);
+  return t;
+}
+
+void transpose_csr_into(const DevCsr& M, const DevCsr& t, cudaStream_t s) {
+  // Entries ordered by column, each column in stored (row-major) order,
+  // i.e. ascending rows (duplicates in stored order): the row-sorted CSR of
+  // M^T.  Short columns (all at most kShortColumn long) use atomic slots and
+  // a per-column sort of the positions; otherwise a stable radix sort.
   if (M.nnz == 0) {
     check(cudaMemsetAsync(t.ptr, 0, sizeof(offset_t) * (size_t(t.rows) + 1), s), "transpose empty");
-    return t;
+    return;
   }
-  t.idx = dalloc<int32_t>(size_t(M.nnz));
-  t.val = dalloc<double>(size_t(M.nnz));
   DBuf<int32_t> cnt(size_t(t.rows) + 1, s);
   cnt.zero();
   const int g = grid_stride_blocks(M.nnz);
@@ -458,7 +573,15 @@ DevCsr transpose_csr(const DevCsr& M, cudaStream_t s) {
   GPP_LAUNCH(row_of_entry, std::max(1, std::min((M.rows + 7) / 8, kNumSMs * 16)), kThreads, 0, s, M.rows, M.ptr,
              row.p);
   GPP_LAUNCH(transpose_gather, g, kThreads, 0, s, M.nnz, pos.p, row.p, M.val, t.idx, t.val);
-  return t;
+}
+
+bool csr_structure_valid(const DevCsr& M, cudaStream_t s) {
+  if (M.rows < 0 || M.cols < 0 || M.nnz < 0) return false;
+  Status st;
+  st.clear(1);
+  GPP_LAUNCH(check_csr_structure, grid_stride_blocks(std::max<int64_t>(M.rows + 1, M.nnz)), kThreads, 0, s, M.rows,
+             M.cols, M.nnz, M.ptr, M.idx, st.d);
+  return st.read(1)[0] == 0;
 }
 
 bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s) {

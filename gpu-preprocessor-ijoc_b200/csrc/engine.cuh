@@ -206,6 +206,12 @@ DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
 // General transpose (histogram, scan, scatter, per-row sort): rows of the
 // result list source rows in ascending order.
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s);
+// The same transpose into preallocated arrays (t.ptr: M.cols + 1 offsets,
+// t.idx / t.val: M.nnz entries).
+void transpose_csr_into(const DevCsr& M, const DevCsr& t, cudaStream_t s);
+// Checks a CSR's structure on the device: ptr[0] = 0, ptr[rows] = nnz,
+// non-decreasing pointers and inner indices in [0, cols).  One readback.
+bool csr_structure_valid(const DevCsr& M, cudaStream_t s);
 bool rows_strictly_sorted(const DevCsr& M, cudaStream_t s);
 void gather_by_map(double* dst, const double* src, const int32_t* old_to_new, int32_t n_old,
                    cudaStream_t s);

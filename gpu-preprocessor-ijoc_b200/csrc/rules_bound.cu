@@ -112,10 +112,14 @@ candidates_entries(offset_t nnz, const int2* __restrict__ tile_rows, CandArgs g)
       const int jn = next ? ld_stream(g.idx + pn, hint.stream) : -1;
       const double an = next ? ld_stream(g.val + pn, hint.stream) : 0.0;
       const int i = staged ? r0 + row_of(sptr, 0, r1 - r0 + 1, p) : row_of(g.ptr, r0, r1 + 1, p);
-      if (g.keep_row[i] && g.row_nnz[i] > 1) {
-        const double2 b = ld_keep(g.lu + j, hint.keep);
-        if (!removed_column(b) && !(fabs(a) <= g.zero_tol)) candidate_update(g, row_ctx(g, i), j, a, b);
-      }
+      // Every load of the entry at once (the column's bounds do not depend on
+      // the row; the row's flags and summary come from one or two lines that
+      // the warp's neighbouring entries share), so an entry waits for one
+      // memory round trip instead of two.
+      const double2 b = ld_keep(g.lu + j, hint.keep);
+      const bool row_live = (g.keep_row[i] != 0) & (g.row_nnz[i] > 1);
+      const RowCtx rc = row_ctx(g, i);
+      if (row_live && !removed_column(b) && !(fabs(a) <= g.zero_tol)) candidate_update(g, rc, j, a, b);
       j = jn;
       a = an;
     }
