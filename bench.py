@@ -4,8 +4,9 @@ One step = gpu_preprocessor::preprocess (presolve) + postprocess (postsolve
 of a fixed reduced solution) of the single-GPU scale LP: the seeded random
 family at m = 2,000,000, n = 5,000,000 with 2,000 hub rows (~29.8M nnz).  The
 inputs stay resident in HBM for `value`; `e2e` repeats the step through the
-C ABI with the LP uploaded from pinned host memory and the solution read back
-every step.  The LP (~1 GB of arrays) is larger than the 126 MB L2, so no
+C ABI with the LP loaded from pinned host memory every step (A as CSR and the
+vectors cross PCIe; gpp_lp_from_host builds A^T on the GPU) and the solution
+read back into host memory.  The LP (~1 GB of arrays) is larger than the 126 MB L2, so no
 flush is needed between steps.
 
 --impl reference times the reference's own CPU implementation of the path,
@@ -483,8 +484,10 @@ def main():
                 for n, l, m, b in sorted(prof, key=lambda r: -r[2]):
                     f.write(f"{n},{l / args.steps:.1f},{m / args.steps:.4f},{b / args.steps:.0f}\n")
 
-    # End to end through the C ABI from pinned host memory.
-    host = {k: v.cpu().pin_memory() for k, v in dlp.t.items()}
+    # End to end through the C ABI from pinned host memory: gpp_lp_from_host
+    # loads A (CSR) and the vectors and builds A^T on the GPU, then presolve
+    # and a postsolve into host outputs.
+    host = {k: v.cpu().pin_memory() for k, v in dlp.t.items() if not k.startswith("AT_")}
     h2d = sum(v.numel() * v.element_size() for v in host.values())
     d2h = 8 * (lp.n + lp.m + lp.n)
     # Page-locked host outputs for the recovered solution (allocated once).
@@ -495,8 +498,7 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            for k, v in host.items():
-                dlp.t[k].copy_(v, non_blocking=True)
+            dlp.load_from_host(host)
             s = device.preprocess(dlp, params)
             device.postprocess(*red, s, dlp, out=host_out)
             device.free_summary(s)
@@ -654,7 +656,9 @@ def main():
             "gpu_launches": launches,
             "host_syncs_per_step": syncs,
             "e2e": None if e2e_ms is None else {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
-                                                "d2h_bytes_per_step": d2h},
+                                                "d2h_bytes_per_step": d2h,
+                                                "path": "gpp_lp_from_host (A as CSR + vectors; A^T built on "
+                                                        "the GPU) -> gpp_preprocess -> gpp_postprocess (host x, y, z)"},
             "roofline": roofline,
             "algorithmic": algorithmic,
             "reference_gpu": ref_gpu,

@@ -1101,6 +1101,69 @@ int gpp_mps_upload(const gpp_mps_model* model, gpp_lp* out) {
   });
 }
 
+int gpp_lp_from_host(const gpp_host_lp* host, gpp_lp* dev) {
+  return guarded([&] {
+    if (!host || !dev) throw std::invalid_argument("gpp_lp_from_host: null argument");
+    const int32_t m = host->rows, n = host->cols;
+    const gpp_offset nnz = host->nnz;
+    if (m < 0 || n < 0 || nnz < 0) throw std::invalid_argument("gpp_lp_from_host: negative LP dimensions");
+    if (!host->row_ptr || (nnz > 0 && (!host->col_idx || !host->val)) ||
+        (n > 0 && (!host->c || !host->l || !host->u)) || (m > 0 && (!host->AL || !host->AU)))
+      throw std::invalid_argument("gpp_lp_from_host: host array missing");
+    if (!dev->A.rowPtr || !dev->AT.rowPtr || (nnz > 0 && (!dev->A.colVal || !dev->A.nzVal || !dev->AT.colVal ||
+                                                          !dev->AT.nzVal)) ||
+        (n > 0 && (!dev->c || !dev->l || !dev->u)) || (m > 0 && (!dev->AL || !dev->AU)))
+      throw std::invalid_argument("gpp_lp_from_host: device array missing");
+    auto& c = gpp::ctx();
+    const cudaStream_t s = c.stream, side = c.side_stream();
+    auto up = [](void* d, const void* h, size_t bytes, cudaStream_t st) {
+      if (bytes) check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st), "gpp_lp_from_host: upload");
+    };
+    up(dev->A.rowPtr, host->row_ptr, sizeof(gpp_offset) * (size_t(m) + 1), s);
+    up(dev->A.colVal, host->col_idx, sizeof(int32_t) * size_t(nnz), s);
+    up(dev->A.nzVal, host->val, sizeof(double) * size_t(nnz), s);
+    // The vectors follow A on the side stream, so they cross the bus while
+    // the engine stream checks and transposes A.
+    cudaEvent_t a_done = nullptr, vec_done = nullptr;
+    check(cudaEventCreateWithFlags(&a_done, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&vec_done, cudaEventDisableTiming), "cudaEventCreate");
+    // On every exit, error paths included, the side stream's copies are
+    // finished before the caller gets its host arrays back.
+    struct Events {
+      cudaEvent_t a, b;
+      cudaStream_t side;
+      ~Events() {
+        cudaStreamSynchronize(side);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+      }
+    } events{a_done, vec_done, side};
+    check(cudaEventRecord(a_done, s), "cudaEventRecord");
+    check(cudaStreamWaitEvent(side, a_done, 0), "cudaStreamWaitEvent");
+    up(dev->c, host->c, sizeof(double) * size_t(n), side);
+    up(dev->l, host->l, sizeof(double) * size_t(n), side);
+    up(dev->u, host->u, sizeof(double) * size_t(n), side);
+    up(dev->AL, host->AL, sizeof(double) * size_t(m), side);
+    up(dev->AU, host->AU, sizeof(double) * size_t(m), side);
+    check(cudaEventRecord(vec_done, side), "cudaEventRecord");
+    const gpp::DevCsr A{m, n, nnz, dev->A.rowPtr, dev->A.colVal, dev->A.nzVal};
+    const gpp::DevCsr AT{n, m, nnz, dev->AT.rowPtr, dev->AT.colVal, dev->AT.nzVal};
+    const bool valid = gpp::csr_structure_valid(A, s);
+    if (valid) gpp::transpose_csr_into(A, AT, s);
+    check(cudaStreamWaitEvent(s, vec_done, 0), "cudaStreamWaitEvent");
+    c.sync("gpp_lp_from_host");
+    if (!valid)
+      throw std::invalid_argument("gpp_lp_from_host: A is not a valid CSR (row pointers or column indices)");
+    dev->A.rows = m;
+    dev->A.cols = n;
+    dev->A.nnz = nnz;
+    dev->AT.rows = n;
+    dev->AT.cols = m;
+    dev->AT.nnz = nnz;
+    dev->obj_constant = host->obj_constant;
+  });
+}
+
 void gpp_lp_free(gpp_lp* lp) {
   if (!lp) return;
   for (void* p : {static_cast<void*>(lp->A.rowPtr), static_cast<void*>(lp->A.colVal), static_cast<void*>(lp->A.nzVal),

@@ -54,7 +54,13 @@ void Context::sync(const char* label) {
 Context::~Context() {
   if (host_status) cudaFreeHost(host_status);
   if (host_scalar) cudaFreeHost(host_scalar);
+  if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
+}
+
+cudaStream_t Context::side_stream() {
+  if (!side) check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate side");
+  return side;
 }
 
 Context& ctx() {

@@ -206,7 +206,11 @@ struct Context {
   cudaMemPool_t pool = nullptr;   // this context's own stream-ordered pool
   int32_t* host_status = nullptr;   // pinned, kStatusWords ints
   unsigned char* host_scalar = nullptr;   // pinned, 16 bytes for scalar readbacks
+  cudaStream_t side = nullptr;
   static constexpr int kStatusWords = 64;
+  // A second stream for host-to-device copies that overlap the engine
+  // stream's kernels (created on first use; ordered by events).
+  cudaStream_t side_stream();
   Context();
   ~Context();
   Context(const Context&) = delete;

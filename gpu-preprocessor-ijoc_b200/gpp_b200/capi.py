@@ -126,6 +126,13 @@ class Summary(C.Structure):
                 ("folded_rows", i32), ("folded_cols", i32)]
 
 
+class HostLp(C.Structure):
+    """gpp_host_lp: A as a host CSR and the vectors (host pointers)."""
+    _fields_ = [("rows", i32), ("cols", i32), ("nnz", i32), ("row_ptr", C.c_void_p), ("col_idx", C.c_void_p),
+                ("val", C.c_void_p), ("c", C.c_void_p), ("AL", C.c_void_p), ("AU", C.c_void_p),
+                ("l", C.c_void_p), ("u", C.c_void_p), ("obj_constant", f64)]
+
+
 class AbsoluteValueRecovery(C.Structure):
     """gpp_absolute_value_recovery: one step as host arrays (pointers)."""
     _fields_ = [("pattern", i32), ("split_count", i32), ("split_t", C.c_void_p), ("split_e", C.c_void_p),
@@ -182,6 +189,7 @@ def load():
         "gpp_mps_free": (None, [vp]),
         "gpp_mps_upload": (C.c_int, [vp, P(Lp)]),
         "gpp_lp_free": (None, [P(Lp)]),
+        "gpp_lp_from_host": (C.c_int, [P(HostLp), P(Lp)]),
         "gpp_export_reduced": (C.c_int, [P(Summary), C.c_char_p, C.c_char_p]),
         "gpp_reduced_to_device": (C.c_int, [P(Summary), P(Lp)]),
         "gpp_reduced_to_host": (C.c_int, [P(Summary)] + [vp] * 9),
@@ -222,7 +230,7 @@ EXPORTED = [
     "gpp_last_error", "gpp_kernel_launches", "gpp_host_syncs",
     "gpp_preprocess_batch", "gpp_postprocess_batch", "gpp_batch_autotune",
     "gpp_mps_read", "gpp_mps_read_string", "gpp_mps_info", "gpp_mps_arrays", "gpp_mps_free", "gpp_mps_upload",
-    "gpp_lp_free", "gpp_export_reduced", "gpp_reduced_to_device", "gpp_reduced_to_host",
+    "gpp_lp_free", "gpp_lp_from_host", "gpp_export_reduced", "gpp_reduced_to_device", "gpp_reduced_to_host",
     "gpp_preprocess_traced", "gpp_schedule_model_create", "gpp_schedule_model_free",
     "gpp_schedule_model_create_per_rule", "gpp_preprocess_scheduled",
     "gpp_mlp_train", "gpp_mlp_forward", "gpp_mlp_gradients", "gpp_profile_enable", "gpp_profile_read",

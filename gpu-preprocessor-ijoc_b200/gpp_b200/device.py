@@ -72,6 +72,19 @@ class DeviceLp:
             self.t[k] = h.to("cuda", non_blocking=pinned)
         self.obj_constant = float(lp.obj_constant)
 
+    def load_from_host(self, host) -> None:
+        """gpp_lp_from_host: refill this LP's device arrays from host tensors
+        or arrays (keys A_ptr, A_idx, A_val, c, AL, AU, l, u, of this LP's
+        sizes); AT is rebuilt on the GPU.  Page-locked tensors copy
+        asynchronously."""
+        def hp(k):
+            a = host[k]
+            return C.c_void_p(a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+        h = capi.HostLp(self.m, self.n, self.nnz, hp("A_ptr"), hp("A_idx"), hp("A_val"), hp("c"), hp("AL"),
+                        hp("AU"), hp("l"), hp("u"), self.obj_constant)
+        dev = self.struct()
+        _raise(capi.load().gpp_lp_from_host(C.byref(h), C.byref(dev)))
+
     def struct(self) -> capi.Lp:
         t = self.t
         A = capi.Csr(self.m, self.n, self.nnz, ptr(t["A_ptr"]), ptr(t["A_idx"]), ptr(t["A_val"]))

@@ -433,6 +433,37 @@ GPP_API void gpp_mps_free(gpp_mps_model* model);
 GPP_API int gpp_mps_upload(const gpp_mps_model* model, gpp_lp* out);
 GPP_API void gpp_lp_free(gpp_lp* lp);
 
+/* An LP in host memory: A as CSR (row_ptr[rows+1], col_idx[nnz], val[nnz])
+ * and the vectors c/l/u[cols], AL/AU[rows].  No transpose. */
+typedef struct gpp_host_lp {
+  int32_t rows;
+  int32_t cols;
+  gpp_offset nnz;
+  const gpp_offset* row_ptr;
+  const int32_t* col_idx;
+  const double* val;
+  const double* c;
+  const double* AL;
+  const double* AU;
+  const double* l;
+  const double* u;
+  double obj_constant;
+} gpp_host_lp;
+/* Loads a host LP into device arrays the caller allocated on the current
+ * device (dev->A.rowPtr[rows+1], A.colVal/A.nzVal[nnz], AT.rowPtr[cols+1],
+ * AT.colVal/AT.nzVal[nnz], c/l/u[cols], AL/AU[rows]) and builds AT = A^T on
+ * the GPU, each column listing its rows in ascending order (the CSC that
+ * upload_lp copies from the host, cpp/tools/gpu_preprocessor_tool_common.hpp:
+ * 108-141).  Only A and the vectors cross PCIe: the transpose is built from
+ * the uploaded A while the vectors are still being copied.  Sets dev's sizes
+ * and obj_constant; the call returns when the device arrays are complete.
+ * Host arrays may be pageable or page-locked (page-locked copies run
+ * asynchronously at full bus speed).  GPP_ERR_INVALID for a structurally
+ * invalid A (row pointers not starting at 0, decreasing or not ending at nnz;
+ * a column index outside [0, cols)), checked on the device before the
+ * transpose reads it. */
+GPP_API int gpp_lp_from_host(const gpp_host_lp* host, gpp_lp* dev);
+
 /* Writes the reduced LP of a summary to `out_dir` in the reference's export
  * format (cpp/tools/gpu_preprocessor_export_reduced.cpp:17-64, format
  * gpu_preprocessor_reduced_lp_v1): meta.txt and the raw little-endian arrays
