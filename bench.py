@@ -49,7 +49,8 @@ KERNEL_SOURCES = {
     "activity_kernel<false>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
     "activity_kernel<true>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
     "candidates_entries": ["csrc/rules_bound.cu", "csrc/common.cuh"],
-    "copy_kept": ["csrc/compact.cu", "csrc/common.cuh"],
+    "compact_copy<true>": ["csrc/compact.cu", "csrc/common.cuh"],
+    "compact_count<true>": ["csrc/compact.cu", "csrc/common.cuh"],
 }
 
 
@@ -322,6 +323,32 @@ def optional(measure):
         return {"error": f"{type(e).__name__}: {e}"}
 
 
+def bind_to_gpu_cpus(device_index):
+    """Restrict this process to the host cores NVML reports as closest to
+    the GPU (its NUMA node), so page-locked host buffers are allocated next
+    to the GPU's PCIe root and launches come from a near core.  Changes only
+    this process's CPU affinity; returns the cores used or None."""
+    try:
+        import pynvml
+        import torch
+        props = torch.cuda.get_device_properties(device_index)
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+            words = (os.cpu_count() + 63) // 64
+            mask = pynvml.nvmlDeviceGetCpuAffinity(h, words)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * w + b for w, m in enumerate(mask) for b in range(64) if (int(m) >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        if not cpus:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return sorted(cpus)
+    except Exception:
+        return None
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -405,6 +432,7 @@ def main():
     from gpp_b200.capi import params_with_rules
 
     torch.cuda.set_device(local)
+    near_cpus = bind_to_gpu_cpus(local)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
@@ -652,6 +680,8 @@ def main():
                        "presolve_ms": round(statistics.mean(pre_ms), 3),
                        "postsolve_ms": round(post_ms, 3),
                        "l2": "inputs (~1 GB) larger than L2; no flush",
+                       "host_cpus": (f"{len(near_cpus)} cores of the GPU's NUMA node" if near_cpus
+                                     else "unbound (no NVML CPU affinity)"),
                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "gpu_launches": launches,
             "host_syncs_per_step": syncs,

@@ -200,15 +200,38 @@ __global__ void support_kernel(int n, const offset_t* __restrict__ at_ptr, const
     int sl = INT_MAX, su = INT_MAX;
     const bool nl = lch[j], nu = uch[j];
     if (nl || nu) {
-      for (offset_t p = at_ptr[j]; p < at_ptr[j + 1]; ++p) {
-        const int i = at_idx[p];
-        if (!keep_row[i] || row_nnz[i] <= 1) continue;
-        const double a = at_val[p];
-        if (fabs(a) <= zero_tol) continue;
-        double il, iu;
-        implied_bounds(a, l[j], u[j], AL[i], AU[i], rs.mn[i], rs.mx[i], rs.ni[i], rs.pi[i], il, iu);
-        if (nl && fl[j] > l[j] + tol && isfinite(il) && fabs(il - fl[j]) <= support_tol) sl = min(sl, i);
-        if (nu && fu[j] < u[j] - tol && isfinite(iu) && fabs(iu - fu[j]) <= support_tol) su = min(su, i);
+      const double lj = l[j], uj = u[j], flj = fl[j], fuj = fu[j];
+      const bool want_l = nl && flj > lj + tol, want_u = nu && fuj < uj - tol;
+      // Four entries per round with every load issued before the first use
+      // (one memory round trip per four entries); the support row is the
+      // smallest qualifying row, which does not depend on the visiting order.
+      constexpr int kBatch = 4;
+      const offset_t end = at_ptr[j + 1];
+      for (offset_t p0 = at_ptr[j]; p0 < end && (want_l || want_u); p0 += kBatch) {
+        int row[kBatch];
+        double a[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          row[k] = p0 + k < end ? at_idx[p0 + k] : -1;
+          a[k] = p0 + k < end ? at_val[p0 + k] : 0.0;
+        }
+        bool live[kBatch];
+        double al[kBatch], au[kBatch], mn[kBatch], mx[kBatch];
+        int ni[kBatch], pi[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          const int i = row[k] >= 0 ? row[k] : 0;
+          live[k] = row[k] >= 0 && (keep_row[i] != 0) & (row_nnz[i] > 1);
+          al[k] = AL[i]; au[k] = AU[i]; mn[k] = rs.mn[i]; mx[k] = rs.mx[i]; ni[k] = rs.ni[i]; pi[k] = rs.pi[i];
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          if (!live[k] || fabs(a[k]) <= zero_tol) continue;
+          double il, iu;
+          implied_bounds(a[k], lj, uj, al[k], au[k], mn[k], mx[k], ni[k], pi[k], il, iu);
+          if (want_l && isfinite(il) && fabs(il - flj) <= support_tol) sl = min(sl, row[k]);
+          if (want_u && isfinite(iu) && fabs(iu - fuj) <= support_tol) su = min(su, row[k]);
+        }
       }
     }
     sup_l[j] = sl;
