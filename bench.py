@@ -49,8 +49,7 @@ KERNEL_SOURCES = {
     "activity_kernel<false>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
     "activity_kernel<true>": ["csrc/live.cu", "csrc/live_visit.cuh", "csrc/common.cuh"],
     "candidates_entries": ["csrc/rules_bound.cu", "csrc/common.cuh"],
-    "compact_copy<true>": ["csrc/compact.cu", "csrc/common.cuh"],
-    "compact_count<true>": ["csrc/compact.cu", "csrc/common.cuh"],
+    "compact_tiles<true>": ["csrc/compact.cu", "csrc/common.cuh"],
 }
 
 

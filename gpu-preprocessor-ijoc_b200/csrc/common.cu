@@ -333,6 +333,14 @@ cudaEvent_t profile_event() {
 void profile_record(const char* name, double bytes, cudaEvent_t begin, cudaEvent_t end) {
   profile_state().records.push_back({name, bytes, begin, end, 0.0});
 }
+int64_t profile_last() {
+  auto& p = profile_state();
+  return p.on && !p.records.empty() ? int64_t(p.records.size()) - 1 : -1;
+}
+void profile_add_bytes(int64_t record, double bytes) {
+  auto& p = profile_state();
+  if (record >= 0 && size_t(record) < p.records.size()) p.records[size_t(record)].bytes += bytes;
+}
 void profile_sync(const char* label, double ms) {
   profile_state().records.push_back({std::string("sync: ") + label, 0.0, nullptr, nullptr, ms});
 }

@@ -46,6 +46,10 @@ uint64_t& sync_counter();   // host waits on the engine stream, calling thread
 bool profiling();
 void profile_record(const char* name, double bytes, cudaEvent_t begin, cudaEvent_t end);
 cudaEvent_t profile_event();
+// The last recorded launch (-1 when not profiling), and a way to add bytes
+// to it once they are known (a kernel whose output size is read back later).
+int64_t profile_last();
+void profile_add_bytes(int64_t record, double bytes);
 
 #define GPP_LAUNCH_BYTES(kernel, bytes, grid, block, smem, stream, ...)             \
   do {                                                                              \

@@ -38,9 +38,12 @@ __global__ void prefix_to_map(const uint8_t* __restrict__ keep, const int32_t* _
 // the rows whose pointer falls inside the tile mark their start positions in
 // shared memory, and a block scan of the marks counts the row starts at or
 // before every position.  The copy is a stream compaction in stored order, so
-// a kept entry's output position is the number of kept entries before it:
-// per-tile counts, one scan of the counts, then the copy, whose block scan
-// places each kept entry and each kept row's new pointer.
+// a kept entry's output position is the number of kept entries before it.
+// One pass does it: tiles are handed out in order by a ticket counter, each
+// tile publishes its kept count as soon as it knows it, and looks back over
+// its predecessors' published counts (a decoupled look-back) for its output
+// offset; its block scan then places each kept entry and each kept row's new
+// pointer.
 constexpr int kCompactPer = 8;
 constexpr int kCompactTile = kThreads * kCompactPer;
 
@@ -149,56 +152,65 @@ __device__ __forceinline__ unsigned tile_kept_mask(int r0, int64_t base, int len
   return mask;
 }
 
-// Both kernels are persistent: a block takes tiles blockIdx.x, + gridDim.x,
-// ... and loads the next tile's stored entries into registers before it works
-// on the current one, so the stream of the next tile is in flight while the
-// current tile runs its dependent chain (row starts, scans, gathers).
-template <bool kVec>
-__global__ void __launch_bounds__(kThreads)
-compact_count(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-              const int32_t* __restrict__ outer_map, const int32_t* __restrict__ inner_map,
-              const int32_t* __restrict__ first_row, int rows, int tiles, int32_t* __restrict__ tile_counts) {
-  __shared__ __align__(16) int marker[kCompactTile];
-  __shared__ int warp_sums[kThreads / 32];
-  const int p0 = int(threadIdx.x) * kCompactPer;
-  int next[kCompactPer], next_r0 = 0, next_r1 = 0;
-  int t = blockIdx.x;
-  if (t < tiles) {
-    const int64_t base = int64_t(t) * kCompactTile;
-    load_tile_cols<kVec>(idx + base + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - base)) - p0, next);
-    next_r0 = first_row[t];
-    next_r1 = t + 1 < tiles ? first_row[t + 1] : rows;
-  }
-  for (; t < tiles; t += gridDim.x) {
-    const int64_t base = int64_t(t) * kCompactTile;
-    const int len = int(min(int64_t(kCompactTile), int64_t(nnz) - base));
-    int col[kCompactPer];
-#pragma unroll
-    for (int k = 0; k < kCompactPer; ++k) col[k] = next[k];
-    const int r0 = next_r0, r1 = next_r1;
-    const int tn = t + int(gridDim.x);
-    if (tn < tiles) {
-      const int64_t nbase = int64_t(tn) * kCompactTile;
-      load_tile_cols<kVec>(idx + nbase + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - nbase)) - p0, next);
-      next_r0 = first_row[tn];
-      next_r1 = tn + 1 < tiles ? first_row[tn + 1] : rows;
+// Tile status words: the top two bits say what the low 62 hold (an aggregate:
+// the tile's own kept count; an inclusive count: the kept entries of every
+// tile up to and including it).  Zero means nothing published yet.
+constexpr unsigned long long kTileAggregate = 1ull << 62, kTileInclusive = 2ull << 62;
+constexpr unsigned long long kTileValue = (1ull << 62) - 1;
+// Polls of one predecessor before a look-back gives up (well over a second;
+// a predecessor that holds a ticket is running and publishes within
+// microseconds).  Giving up sets the error word, which the host checks.
+constexpr int kLookbackPolls = 1 << 22;
+
+__device__ __forceinline__ unsigned long long ld_tile_status(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_tile_status(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Kept entries before tile t, by warp 0: 32 predecessors per round, summing
+// aggregates back to the nearest inclusive count (before tile 0: zero).
+__device__ __forceinline__ int64_t tile_lookback(const unsigned long long* status, int t, int32_t* err) {
+  const int lane = threadIdx.x & 31;
+  int64_t before = 0;
+  for (int end = t - 1;; end -= 32) {
+    const int j = end - lane;
+    unsigned long long st = kTileInclusive;
+    if (j >= 0) {
+      st = ld_tile_status(status + j);
+      for (int polls = 1; (st >> 62) == 0; ++polls) {
+        if (polls == kLookbackPolls) {
+          atomicExch(err, 1);
+          st = kTileInclusive;
+          break;
+        }
+        __nanosleep(64);
+        st = ld_tile_status(status + j);
+      }
     }
+    const unsigned incl = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+    const int first = incl ? __ffs(incl) - 1 : 32;
+    unsigned long long v = lane <= first ? (st & kTileValue) : 0ull;
 #pragma unroll
-    for (int k = 0; k < kCompactPer; ++k) col[k] = col[k] >= 0 ? inner_map[col[k]] : -1;
-    const unsigned mask = tile_kept_mask(r0, base, len, ptr, r1, outer_map, col, marker, warp_sums);
-    int total;
-    block_exclusive_scan(__popc(mask), warp_sums, &total);
-    if (threadIdx.x == 0) tile_counts[t] = total;
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    before += int64_t(v);
+    if (incl) return before;
   }
 }
 
+// One pass: result[0] receives the kept total, result[1] is set if a
+// look-back gave up.  `status` holds tiles words and then the ticket counter,
+// all zero at launch.
 template <bool kVec>
 __global__ void __launch_bounds__(kThreads)
-compact_copy(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-             const double* __restrict__ val, const int32_t* __restrict__ outer_map,
-             const int32_t* __restrict__ inner_map, const int32_t* __restrict__ first_row, int rows, int tiles,
-             const int32_t* __restrict__ tile_offsets, int32_t outer_new, offset_t* __restrict__ out_ptr,
-             int32_t* __restrict__ out_idx, double* __restrict__ out_val) {
+compact_tiles(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+              const double* __restrict__ val, const int32_t* __restrict__ outer_map,
+              const int32_t* __restrict__ inner_map, const int32_t* __restrict__ first_row, int rows, int tiles,
+              unsigned long long* status, int32_t outer_new, offset_t* __restrict__ out_ptr,
+              int32_t* __restrict__ out_idx, double* __restrict__ out_val, int32_t* result) {
   // `marker` is free once the rows are known and then stages the kept
   // indices; `stage_val` the kept values.  The stores go out coalesced.
   __shared__ __align__(16) int marker[kCompactTile];
@@ -206,40 +218,35 @@ compact_copy(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __re
   __shared__ int warp_sums[kThreads / 32];
   __shared__ int thread_before[kThreads];
   __shared__ unsigned thread_mask[kThreads];
+  __shared__ int ticket;
+  __shared__ long long tile_before;
   const int p0 = int(threadIdx.x) * kCompactPer;
-  int next_col[kCompactPer], next_r0 = 0, next_r1 = 0;
-  int t = blockIdx.x;
-  if (t < tiles) {
-    const int64_t base = int64_t(t) * kCompactTile;
-    load_tile_cols<kVec>(idx + base + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - base)) - p0, next_col);
-    next_r0 = first_row[t];
-    next_r1 = t + 1 < tiles ? first_row[t + 1] : rows;
-  }
-  for (; t < tiles; t += gridDim.x) {
+  for (;;) {
+    if (threadIdx.x == 0) ticket = int(atomicAdd(status + tiles, 1ull));
+    __syncthreads();
+    const int t = ticket;
+    if (t >= tiles) return;   // block-uniform
     const int64_t base = int64_t(t) * kCompactTile;
     const int len = int(min(int64_t(kCompactTile), int64_t(nnz) - base));
     int col[kCompactPer];
-#pragma unroll
-    for (int k = 0; k < kCompactPer; ++k) col[k] = next_col[k];
-    // This tile's values are first needed by the stores at the end, the next
-    // tile's indices at the top of the next round: both loads run under this
-    // tile's chain.
     double v[kCompactPer];
+    load_tile_cols<kVec>(idx + base + p0, len - p0, col);
     load_tile_vals<kVec>(val + base + p0, len - p0, v);
-    const int64_t tile_out = tile_offsets[t];
-    const int r0 = next_r0, r1 = next_r1;
-    const int tn = t + int(gridDim.x);
-    if (tn < tiles) {
-      const int64_t nbase = int64_t(tn) * kCompactTile;
-      load_tile_cols<kVec>(idx + nbase + p0, int(min(int64_t(kCompactTile), int64_t(nnz) - nbase)) - p0, next_col);
-      next_r0 = first_row[tn];
-      next_r1 = tn + 1 < tiles ? first_row[tn + 1] : rows;
-    }
+    const int r0 = first_row[t], r1 = t + 1 < tiles ? first_row[t + 1] : rows;
 #pragma unroll
     for (int k = 0; k < kCompactPer; ++k) col[k] = col[k] >= 0 ? inner_map[col[k]] : -1;
     const unsigned mask = tile_kept_mask(r0, base, len, ptr, r1, outer_map, col, marker, warp_sums);
     int total;
     const int before = block_exclusive_scan(__popc(mask), warp_sums, &total);
+    if (threadIdx.x < 32) {
+      if (threadIdx.x == 0)
+        st_tile_status(status + t, (t == 0 ? kTileInclusive : kTileAggregate) | (unsigned long long)total);
+      const int64_t ahead = t == 0 ? 0 : tile_lookback(status, t, result + 1);
+      if (threadIdx.x == 0) {
+        if (t > 0) st_tile_status(status + t, kTileInclusive | (unsigned long long)(ahead + total));
+        tile_before = ahead;
+      }
+    }
     int o = before;
 #pragma unroll
     for (int k = 0; k < kCompactPer; ++k)
@@ -251,6 +258,7 @@ compact_copy(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __re
     thread_before[threadIdx.x] = before;
     thread_mask[threadIdx.x] = mask;
     __syncthreads();
+    const int64_t tile_out = tile_before;
     for (int q = int(threadIdx.x); q < total; q += kThreads) {
       out_idx[tile_out + q] = marker[q];
       out_val[tile_out + q] = stage_val[q];
@@ -268,8 +276,11 @@ compact_copy(offset_t nnz, const offset_t* __restrict__ ptr, const int32_t* __re
       }
       out_ptr[nr] = offset_t(tile_out + kept_before);
     }
-    if (t == tiles - 1 && threadIdx.x == 0) out_ptr[outer_new] = offset_t(tile_out + total);
-    __syncthreads();   // the staging buffers are refilled by the next tile
+    if (t == tiles - 1 && threadIdx.x == 0) {
+      out_ptr[outer_new] = offset_t(tile_out + total);
+      result[0] = int32_t(tile_out + total);
+    }
+    __syncthreads();   // the staging buffers and the ticket are reused by the next tile
   }
 }
 
@@ -485,45 +496,59 @@ std::pair<int32_t, int32_t> build_old_to_new_pair(const uint8_t* keep_row, int32
   return {t[0], t[1]};
 }
 
-DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
-                   int32_t inner_new, cudaStream_t s, int64_t known_nnz) {
+DevCsr compact_csr_queued(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
+                          int32_t inner_new, cudaStream_t s, int32_t* result, int64_t* profile_record) {
   DevCsr out;
   out.rows = outer_new;
   out.cols = inner_new;
+  out.nnz = -1;
   out.ptr = dalloc<offset_t>(size_t(outer_new) + 1);
+  *profile_record = -1;
   if (outer_new == 0 || inner_new == 0 || M.nnz == 0) {
     check(cudaMemsetAsync(out.ptr, 0, sizeof(offset_t) * (size_t(outer_new) + 1), s), "compact empty ptr");
+    check(cudaMemsetAsync(result, 0, 2 * sizeof(int32_t), s), "compact empty result");
     return out;
   }
+  // The kept entries are at most the stored ones: the outputs are sized for
+  // those, so nothing waits for the kept count before the copy.
+  out.idx = dalloc<int32_t>(size_t(M.nnz));
+  out.val = dalloc<double>(size_t(M.nnz));
   const int tiles = int((int64_t(M.nnz) + kCompactTile - 1) / kCompactTile);
-  DBuf<int32_t> first_row(size_t(tiles), s), tile_counts(size_t(tiles), s), tile_offsets(size_t(tiles) + 1, s);
+  DBuf<int32_t> first_row(size_t(tiles), s);
+  DBuf<unsigned long long> status(size_t(tiles) + 1, s);   // tile words, then the ticket counter
+  status.zero();
+  check(cudaMemsetAsync(result, 0, 2 * sizeof(int32_t), s), "compact result");
   GPP_LAUNCH(compact_tile_rows, grid_stride_blocks(int64_t(M.rows) + 1), kThreads, 0, s, M.rows, M.ptr, tiles,
              first_row.p);
   // 128-bit loads need 16-byte aligned index and value arrays (always so for
   // the engine's own matrices; a caller's input may be offset).
   const bool vec = reinterpret_cast<uintptr_t>(M.idx) % 16 == 0 && reinterpret_cast<uintptr_t>(M.val) % 16 == 0;
-  const double count_bytes = 4.0 * (M.rows + 1) + 4.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * tiles;
-  // One resident wave of persistent blocks (at most 6 per SM for the count,
-  // 4 for the copy: their register budgets).
-  const int count_grid = std::min(tiles, kNumSMs * 6), copy_grid = std::min(tiles, kNumSMs * 4);
+  // Reads; the writes (4 (outer_new + 1) + 12 nnz') are added to the launch's
+  // profile record once the kept count is known.
+  const double read_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * tiles;
+  const int grid = std::min(tiles, kNumSMs * 4);   // resident blocks at its register budget
   if (vec)
-    GPP_LAUNCH_BYTES(compact_count<true>, count_bytes, count_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, outer_map,
-                     inner_map, first_row.p, M.rows, tiles, tile_counts.p);
+    GPP_LAUNCH_BYTES(compact_tiles<true>, read_bytes, grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, status.p, outer_new, out.ptr, out.idx, out.val, result);
   else
-    GPP_LAUNCH_BYTES(compact_count<false>, count_bytes, count_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, outer_map,
-                     inner_map, first_row.p, M.rows, tiles, tile_counts.p);
-  exclusive_scan_i32(tile_counts.p, tile_offsets.p, tiles, s);
-  out.nnz = known_nnz >= 0 ? offset_t(known_nnz) : read_scalar(tile_offsets.p + tiles);
-  out.idx = dalloc<int32_t>(size_t(out.nnz));
-  out.val = dalloc<double>(size_t(out.nnz));
-  const double copy_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols +
-                            4.0 * (outer_new + 1) + 12.0 * out.nnz;
-  if (vec)
-    GPP_LAUNCH_BYTES(compact_copy<true>, copy_bytes, copy_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
-                     inner_map, first_row.p, M.rows, tiles, tile_offsets.p, outer_new, out.ptr, out.idx, out.val);
-  else
-    GPP_LAUNCH_BYTES(compact_copy<false>, copy_bytes, copy_grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
-                     inner_map, first_row.p, M.rows, tiles, tile_offsets.p, outer_new, out.ptr, out.idx, out.val);
+    GPP_LAUNCH_BYTES(compact_tiles<false>, read_bytes, grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
+                     inner_map, first_row.p, M.rows, tiles, status.p, outer_new, out.ptr, out.idx, out.val, result);
+  *profile_record = profile_last();
+  return out;
+}
+
+void compact_csr_finish(DevCsr& out, const int32_t* result_host, int64_t profile_record) {
+  if (result_host[1]) throw CudaError("compaction: a tile's look-back timed out waiting for its predecessors");
+  out.nnz = out.rows > 0 && out.cols > 0 ? offset_t(result_host[0]) : 0;
+  profile_add_bytes(profile_record, 4.0 * (out.rows + 1) + 12.0 * out.nnz);
+}
+
+DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
+                   int32_t inner_new, cudaStream_t s) {
+  Status st;
+  int64_t rec = -1;
+  DevCsr out = compact_csr_queued(M, outer_map, outer_new, inner_map, inner_new, s, st.d, &rec);
+  compact_csr_finish(out, st.read(2), rec);
   return out;
 }
 

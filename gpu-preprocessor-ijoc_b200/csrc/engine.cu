@@ -26,12 +26,6 @@ void WorkingLp::free_owned() {
 
 namespace {
 
-__global__ void any_removed(const uint8_t* __restrict__ rows, int m, const uint8_t* __restrict__ cols, int n,
-                            int32_t* flag) {
-  const int top = m > n ? m : n;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < top; i += gridDim.x * blockDim.x)
-    if ((i < m && !rows[i]) || (i < n && !cols[i])) { *flag = 1; return; }
-}
 __global__ void fill_u8(uint8_t* p, int n, uint8_t v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
@@ -49,7 +43,6 @@ struct Engine {
   DBuf<double> ref_bounds;
   uint32_t* inf_hist = nullptr;   // histogram features (scheduled runs only)
   uint64_t deletion_serial = 0;
-  Status status;
 
   Engine(const gpp_params& params, PresolveOutput& o) : p(params), out(o) {}
 
@@ -122,18 +115,15 @@ struct Engine {
     return changed;
   }
 
-  bool keeps_all(const Plan& pl) {
-    status.clear(1);
-    GPP_LAUNCH(any_removed, grid_stride_blocks(std::max(cur.m(), cur.n())), kThreads, 0, s(), pl.keep_row.p,
-               cur.m(), pl.keep_col.p, cur.n(), status.d);
-    return status.read(1)[0] == 0;
-  }
-
   // apply_plan_to_working_lp (gpu_presolve.cu:1953-2072).
   void apply(Plan& pl, bool cleanup_captured) {
     Record& r = out.record;
     const int m = cur.m(), n = cur.n();
-    if (cur.owns && !pl.has_new_A && keeps_all(pl)) {
+    // The old -> new maps' kept counts also tell whether the plan removes
+    // anything (one readback for both questions).
+    DBuf<int32_t> rmap(size_t(std::max(m, 1)), s()), cmap(size_t(std::max(n, 1)), s());
+    const auto [m_new, n_new] = build_old_to_new_pair(pl.keep_row.p, m, rmap.p, pl.keep_col.p, n, cmap.p, s());
+    if (cur.owns && !pl.has_new_A && m_new == m && n_new == n) {
       capture_tape(r, pl.tape);
       check(cudaMemcpyAsync(cur.c, pl.c.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s()), "commit c");
       check(cudaMemcpyAsync(cur.l, pl.l.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s()), "commit l");
@@ -143,16 +133,25 @@ struct Engine {
       cur.obj += pl.obj_delta;
       return;
     }
-    DBuf<int32_t> rmap(size_t(std::max(m, 1)), s()), cmap(size_t(std::max(n, 1)), s());
-    const auto [m_new, n_new] = build_old_to_new_pair(pl.keep_row.p, m, rmap.p, pl.keep_col.p, n, cmap.p, s());
     WorkingLp next;
     if (pl.has_new_A) {
       next.A = compact_csr(pl.new_A, rmap.p, m_new, cmap.p, n_new, s());
       next.AT = transpose_csr(next.A, s());
+    } else if (cur.AT_sorted()) {
+      // A and A^T are compacted back to back; one readback gives both kept
+      // counts (equal) and their look-back error words.
+      Status st;
+      int64_t rec_a = -1, rec_t = -1;
+      next.A = compact_csr_queued(cur.A, rmap.p, m_new, cmap.p, n_new, s(), st.d, &rec_a);
+      next.AT = compact_csr_queued(cur.AT, cmap.p, n_new, rmap.p, m_new, s(), st.d + 2, &rec_t);
+      const int32_t* r = st.read(4);
+      compact_csr_finish(next.A, r, rec_a);
+      compact_csr_finish(next.AT, r + 2, rec_t);
+      if (next.A.nnz != next.AT.nnz) throw std::logic_error("compaction: A and A^T kept different entry counts");
+      next.a_sorted = cur.a_sorted;
     } else {
       next.A = compact_csr(cur.A, rmap.p, m_new, cmap.p, n_new, s());
-      next.AT = cur.AT_sorted() ? compact_csr(cur.AT, cmap.p, n_new, rmap.p, m_new, s(), next.A.nnz)
-                                : transpose_csr(next.A, s());
+      next.AT = transpose_csr(next.A, s());
       next.a_sorted = cur.a_sorted;
     }
     next.at_sorted = 1;

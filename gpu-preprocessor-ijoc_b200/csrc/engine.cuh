@@ -197,12 +197,17 @@ int32_t build_old_to_new(const uint8_t* keep, int32_t n, int32_t* old_to_new, cu
 std::pair<int32_t, int32_t> build_old_to_new_pair(const uint8_t* keep_row, int32_t m, int32_t* row_map,
                                                   const uint8_t* keep_col, int32_t n, int32_t* col_map,
                                                   cudaStream_t s);
-// Stable compaction of M's kept rows (outer map) and kept entries (inner map).
-// `known_nnz` >= 0 is the compacted nnz when the caller knows it (the
-// transpose side of a materialisation keeps exactly the entries A keeps),
-// which saves the readback.
+// Stable compaction of M's kept rows (outer map) and kept entries (inner map),
+// in one pass.  The queued form only launches it: the result's nnz is -1 and
+// its index/value arrays hold M.nnz entries until compact_csr_finish applies
+// the two result words (kept total, look-back error) read back from
+// `result`; so several compactions can share one readback.
+DevCsr compact_csr_queued(const DevCsr& M, const int32_t* outer_map, int32_t outer_new, const int32_t* inner_map,
+                          int32_t inner_new, cudaStream_t s, int32_t* result, int64_t* profile_record);
+void compact_csr_finish(DevCsr& out, const int32_t* result_host, int64_t profile_record);
+// Queued and finished at once (one readback).
 DevCsr compact_csr(const DevCsr& M, const int32_t* outer_map, int32_t outer_new,
-                   const int32_t* inner_map, int32_t inner_new, cudaStream_t s, int64_t known_nnz = -1);
+                   const int32_t* inner_map, int32_t inner_new, cudaStream_t s);
 // General transpose (histogram, scan, scatter, per-row sort): rows of the
 // result list source rows in ascending order.
 DevCsr transpose_csr(const DevCsr& M, cudaStream_t s);
