@@ -526,7 +526,7 @@ DevCsr compact_csr_queued(const DevCsr& M, const int32_t* outer_map, int32_t out
   // Reads; the writes (4 (outer_new + 1) + 12 nnz') are added to the launch's
   // profile record once the kept count is known.
   const double read_bytes = 4.0 * (M.rows + 1) + 12.0 * M.nnz + 4.0 * M.rows + 4.0 * M.cols + 4.0 * tiles;
-  const int grid = std::min(tiles, kNumSMs * 4);   // resident blocks at its register budget
+  const int grid = std::min(tiles, kNumSMs * 5);   // resident blocks at its register budget
   if (vec)
     GPP_LAUNCH_BYTES(compact_tiles<true>, read_bytes, grid, kThreads, 0, s, M.nnz, M.ptr, M.idx, M.val, outer_map,
                      inner_map, first_row.p, M.rows, tiles, status.p, outer_new, out.ptr, out.idx, out.val, result);
