@@ -2,12 +2,14 @@
 #include "common.cuh"
 
 #include <atomic>
+#include <cstdlib>
 
 #include <algorithm>
 #include <chrono>
 #include <string>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 
 namespace gpp {
 
@@ -83,6 +85,42 @@ std::atomic<int64_t> g_alloc_countdown{-1};   // < 0: no failure armed
 
 void inject_alloc_failure(int64_t after) { g_alloc_countdown.store(after < 0 ? -1 : after); }
 
+// Host-side reuse of scratch blocks.  A presolve allocates and frees a few
+// thousand scratch buffers, each a cudaMallocFromPoolAsync / cudaFreeAsync
+// pair of driver calls on the host's critical path between launches.  Blocks
+// are rounded up to a size class (at most 25% over) and a block its own
+// context frees on that context's stream goes to the context's free list; the
+// next request of that class on that stream takes it back with no driver
+// call.  Reuse is safe without events: everything on one stream runs in issue
+// order, so a kernel that gets the block runs after every kernel that used it.
+// A block freed by another thread or on another stream goes back to the pool.
+// At most kCachedCap bytes are held this way across all contexts; past that a
+// freed block goes back to the pool.  GPP_ALLOC_CACHE=0 turns the reuse off.
+namespace {
+struct HandedOut {
+  size_t bytes;
+  const Context* owner;
+};
+std::mutex g_blocks_mu;
+std::unordered_map<void*, HandedOut>* g_blocks = new std::unordered_map<void*, HandedOut>();   // never destroyed
+std::atomic<int64_t> g_cached_bytes{0};
+constexpr int64_t kCachedCap = int64_t(8) << 30;
+
+bool alloc_cache_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("GPP_ALLOC_CACHE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+size_t size_class(size_t bytes) {
+  if (bytes <= 256) return 256;
+  const int high = 63 - __builtin_clzll(uint64_t(bytes));
+  const size_t grain = size_t(1) << std::max(8, high - 2);
+  return (bytes + grain - 1) / grain * grain;
+}
+}  // namespace
+
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
   if (g_alloc_countdown.load(std::memory_order_relaxed) >= 0) {
     int64_t left = g_alloc_countdown.load();
@@ -93,14 +131,56 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
       return cudaErrorMemoryAllocation;
     }
   }
-  return cudaMallocFromPoolAsync(p, bytes, ctx().pool, s);
+  Context& c = ctx();
+  if (!alloc_cache_on()) return cudaMallocFromPoolAsync(p, bytes, c.pool, s);
+  const size_t cls = size_class(bytes);
+  if (s == c.stream) {
+    auto it = c.free_blocks.find(cls);
+    if (it != c.free_blocks.end() && !it->second.empty()) {
+      *p = it->second.back();
+      it->second.pop_back();
+      g_cached_bytes.fetch_sub(int64_t(cls), std::memory_order_relaxed);
+      std::lock_guard<std::mutex> lock(g_blocks_mu);
+      (*g_blocks)[*p] = HandedOut{cls, &c};
+      return cudaSuccess;
+    }
+  }
+  const cudaError_t e = cudaMallocFromPoolAsync(p, cls, c.pool, s);
+  if (e == cudaSuccess) {
+    std::lock_guard<std::mutex> lock(g_blocks_mu);
+    (*g_blocks)[*p] = HandedOut{cls, &c};
+  }
+  return e;
+}
+
+void pool_free(void* p, cudaStream_t s) {
+  if (!p) return;
+  if (alloc_cache_on()) {
+    HandedOut b{0, nullptr};
+    {
+      std::lock_guard<std::mutex> lock(g_blocks_mu);
+      auto it = g_blocks->find(p);
+      if (it != g_blocks->end()) {
+        b = it->second;
+        g_blocks->erase(it);
+      }
+    }
+    Context& c = ctx();
+    if (b.owner == &c && s == c.stream &&
+        g_cached_bytes.fetch_add(int64_t(b.bytes), std::memory_order_relaxed) + int64_t(b.bytes) <= kCachedCap) {
+      c.free_blocks[b.bytes].push_back(p);
+      return;
+    }
+    if (b.owner == &c && s == c.stream) g_cached_bytes.fetch_sub(int64_t(b.bytes), std::memory_order_relaxed);
+  }
+  cudaFreeAsync(p, s);
 }
 
 Status::Status() {
   check(pool_alloc(reinterpret_cast<void**>(&d), sizeof(int32_t) * Context::kStatusWords, ctx().stream),
         "status alloc");
 }
-Status::~Status() { if (d) cudaFreeAsync(d, ctx().stream); }
+Status::~Status() { if (d) pool_free(d, ctx().stream); }
 void Status::clear(int words) {
   check(cudaMemsetAsync(d, 0, sizeof(int32_t) * size_t(words), ctx().stream), "status clear");
 }

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -211,6 +212,9 @@ struct Context {
   int32_t* host_status = nullptr;   // pinned, kStatusWords ints
   unsigned char* host_scalar = nullptr;   // pinned, 16 bytes for scalar readbacks
   cudaStream_t side = nullptr;
+  // Scratch blocks this context freed on its own stream, by size class,
+  // ready to be handed out again without a driver call (pool_alloc/free).
+  std::unordered_map<size_t, std::vector<void*>> free_blocks;
   static constexpr int kStatusWords = 64;
   // A second stream for host-to-device copies that overlap the engine
   // stream's kernels (created on first use; ordered by events).
@@ -230,6 +234,8 @@ Context& ctx();
 // it was armed return cudaErrorMemoryAllocation instead, a host-side fake of
 // an out-of-memory failure that touches no device state.
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
+// Every engine device release (buffers of pool_alloc only).
+void pool_free(void* p, cudaStream_t s);
 void inject_alloc_failure(int64_t after);
 
 template <class T>
@@ -246,7 +252,7 @@ struct DBuf {
     if (count) check(pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), s), "cudaMallocFromPoolAsync");
   }
   void release() {
-    if (p) cudaFreeAsync(p, s);
+    if (p) pool_free(p, s);
     p = nullptr;
     n = 0;
   }
@@ -286,7 +292,7 @@ T* dalloc(size_t count) {
   return p;
 }
 inline void dfree(void* p) {
-  if (p) cudaFreeAsync(p, ctx().stream);
+  if (p) pool_free(p, ctx().stream);
 }
 
 template <class T>
