@@ -40,6 +40,7 @@ Context::Context() {
   check(cudaMallocHost(reinterpret_cast<void**>(&host_status), sizeof(int32_t) * kStatusWords),
         "cudaMallocHost status");
   check(cudaMallocHost(reinterpret_cast<void**>(&host_scalar), 16), "cudaMallocHost scalar");
+  check(cudaMallocHost(reinterpret_cast<void**>(&host_later), sizeof(unsigned long long)), "cudaMallocHost later");
 }
 
 void Context::sync(const char* label) {
@@ -56,6 +57,7 @@ void Context::sync(const char* label) {
 Context::~Context() {
   if (host_status) cudaFreeHost(host_status);
   if (host_scalar) cudaFreeHost(host_scalar);
+  if (host_later) cudaFreeHost(host_later);
   if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
 }

@@ -211,6 +211,7 @@ struct Context {
   cudaMemPool_t pool = nullptr;   // this context's own stream-ordered pool
   int32_t* host_status = nullptr;   // pinned, kStatusWords ints
   unsigned char* host_scalar = nullptr;   // pinned, 16 bytes for scalar readbacks
+  unsigned long long* host_later = nullptr;   // pinned, one word read after a later wait
   cudaStream_t side = nullptr;
   // Scratch blocks this context freed on its own stream, by size class,
   // ready to be handed out again without a driver call (pool_alloc/free).

@@ -82,6 +82,37 @@ struct Engine {
     refresh();
     return int64_t(read_scalar(stats.live_nnz.p));
   }
+  // The live nnz before a phase is used only once the phase is over (its
+  // progress test), after the phase's own waits: it is copied to page-locked
+  // host memory with no wait of its own, and read when needed (waiting only
+  // if no wait has happened since the copy was queued).
+  struct LaterCount {
+    int64_t value = 0;
+    bool pending = false;
+    uint64_t queued_at = 0;
+  };
+  LaterCount live_nnz_later() {
+    LaterCount c;
+    if (!active) {
+      c.value = cur.A.nnz;
+      return c;
+    }
+    refresh();
+    check(cudaMemcpyAsync(ctx().host_later, stats.live_nnz.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          s()),
+          "live nnz (later)");
+    c.pending = true;
+    c.queued_at = sync_counter();
+    return c;
+  }
+  int64_t value(LaterCount& c) {
+    if (c.pending) {
+      if (sync_counter() == c.queued_at) ctx().sync("live_nnz");
+      c.value = int64_t(*ctx().host_later);
+      c.pending = false;
+    }
+    return c.value;
+  }
 
   template <class F>
   bool deferred_rule(bool enabled, const char* name, F rule) {
@@ -113,6 +144,17 @@ struct Engine {
     plan.obj_delta = 0.0;
     out.trace.push_back(std::string("rule=") + name + " changed=" + (changed ? "1" : "0"));
     return changed;
+  }
+
+  // A rule that a probe of the unchanged plan showed would change nothing:
+  // the bookkeeping deferred_rule does for an unchanged rule, without
+  // running it.
+  bool skipped_rule(bool enabled, const char* name) {
+    if (!enabled || terminal) return false;
+    prepare();
+    refresh();
+    out.trace.push_back(std::string("rule=") + name + " changed=0");
+    return false;
   }
 
   // apply_plan_to_working_lp (gpu_presolve.cu:1953-2072).
@@ -301,11 +343,36 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
   };
   auto cleanup = [&]() {
     out.trace.push_back("phase=cleanup");
-    bool ch = deferred(p.enable_infeasible_and_fixed_variables, "infeasible_and_fixed_variables",
-                       [&] { rule_fixed_variables(e.plan, cur, p); });
-    ch = deferred(p.enable_empty_columns, "empty_columns", [&] { rule_empty_columns(e.plan, cur, e.stats, p); }) || ch;
-    ch = deferred(p.enable_empty_rows, "empty_rows", [&] { rule_empty_rows(e.plan, cur, e.stats, p); }) || ch;
-    ch = deferred(p.enable_singleton_rows, "singleton_rows", [&] { rule_singleton_rows(e.plan, cur, e.stats, p); }) || ch;
+    // The first four rules' first checks run at once on the plan as it stands
+    // (one readback instead of four).  While every rule so far has changed
+    // nothing the plan is still the probed one, so a rule whose check found
+    // nothing is passed over; from the first rule that changes the plan on,
+    // the rules run as usual.
+    uint32_t may = ~0u;
+    const uint32_t probed = (p.enable_infeasible_and_fixed_variables ? kProbeFixed : 0u) |
+                            (p.enable_empty_columns ? kProbeEmptyColumns : 0u) |
+                            (p.enable_empty_rows ? kProbeEmptyRows : 0u) |
+                            (p.enable_singleton_rows ? kProbeSingletonRows : 0u);
+    if (probed && !e.terminal && !time_exceeded()) {
+      e.prepare();
+      e.refresh();
+      may = cleanup_probe(e.plan, cur, e.stats, p, probed);
+    }
+    bool quiet = true;
+    auto step = [&](uint32_t bit, bool enabled, const char* name, auto rule) {
+      if (quiet && !(may & bit)) return !time_exceeded() && e.skipped_rule(enabled, name);
+      const bool changed = deferred(enabled, name, rule);
+      quiet = quiet && !changed;
+      return changed;
+    };
+    bool ch = step(kProbeFixed, p.enable_infeasible_and_fixed_variables, "infeasible_and_fixed_variables",
+                   [&] { rule_fixed_variables(e.plan, cur, p); });
+    ch = step(kProbeEmptyColumns, p.enable_empty_columns, "empty_columns",
+              [&] { rule_empty_columns(e.plan, cur, e.stats, p); }) || ch;
+    ch = step(kProbeEmptyRows, p.enable_empty_rows, "empty_rows", [&] { rule_empty_rows(e.plan, cur, e.stats, p); }) ||
+         ch;
+    ch = step(kProbeSingletonRows, p.enable_singleton_rows, "singleton_rows",
+              [&] { rule_singleton_rows(e.plan, cur, e.stats, p); }) || ch;
     ch = note(kGateSingletonColumns,
               deferred(gate(kGateSingletonColumns, p.enable_singleton_columns), "singleton_columns",
                        [&] { rule_singleton_columns(e.plan, cur, e.stats, p); })) || ch;
@@ -369,14 +436,19 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       if (out.iterations >= p.max_iters) { out.stopped_at_iteration_limit = true; break; }
       ++out.iterations;
     }
-    const int64_t before = e.live_nnz();
+    // Cleanup does not use the nnz before it (outside traced runs); the other
+    // phases read it after their own waits.
+    Engine::LaterCount before_count;
+    if (scheduled) before_count.value = e.live_nnz();
+    else if (phase != Cleanup) before_count = e.live_nnz_later();
+    const auto before_nnz = [&]() { return e.value(before_count); };
     RoundRecord rec;
     skip = ran = changed_rules = 0;
     if (scheduled) {
       float* f = rec.features;
       f[int(phase)] = 1.0f;
       f[4] = float(round) / 32.0f;
-      f[5] = float(double(before) / double(initial_nnz_all));
+      f[5] = float(double(before_count.value) / double(initial_nnz_all));
       f[6] = float(double(removed_prev) / double(initial_nnz_all));
       f[7] = float(double(removed_prev2) / double(initial_nnz_all));
       for (int g = 0; g < kGatedRules; ++g) {
@@ -385,7 +457,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       }
       f[20] = float(bound_only_rounds) / 8.0f;
       f[21] = float(std::log10(double(initial_nnz_all)) / 8.0);
-      f[22] = float(1.0 - double(before) / double(initial_nnz_all));
+      f[22] = float(1.0 - double(before_count.value) / double(initial_nnz_all));
       f[23] = float(double(cur.m()) / double(initial_rows));
       const std::vector<uint32_t> h = to_host(inf_hist.p, 8);
       for (int side = 0; side < 2; ++side) {
@@ -394,7 +466,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       }
       rec.phase = int32_t(phase);
       rec.iteration = out.iterations;
-      rec.nnz_before = before;
+      rec.nnz_before = before_count.value;
       if (policy) {
         bool stop = false;
         skip = policy->decide(f, &stop);
@@ -412,7 +484,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       bound_only_rounds = e.deletion_serial != ser ? 0 : bound_only_rounds + 1;
       e.materialize("1");
       const int64_t after = e.live_nnz();
-      const bool nnz_progress = good_progress(before, after, min_dec);
+      const bool nnz_progress = good_progress(before_nnz(), after, min_dec);
       const bool bound_progress = bounds_changed && bound_only_rounds < limit;
       phase = nnz_progress || bound_progress ? Cleanup : Aggregation;
       if (phase == Aggregation) bound_only_rounds = 0;
@@ -421,6 +493,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       if (!time_exceeded() && gate(kGateDoubleton, p.enable_doubleton_equations))
         e.materialized_rule(true, "doubleton_equations", [&](Plan& pl) { rule_doubleton_equations(pl, cur, p); });
       const int64_t after = e.live_nnz();
+      const int64_t before = before_nnz();
       note(kGateDoubleton, after < before);
       phase = good_progress(before, after, min_dec) ? Cleanup : Parallel;
     } else {
@@ -433,6 +506,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
                               [&] { rule_parallel_columns(e.plan, cur, e.stats, p); })) || changed;
       e.materialize("2");
       const int64_t after = e.live_nnz();
+      const int64_t before = before_nnz();
       const bool stop_loop = !(changed && good_progress(before, after, min_dec));
       if (scheduled) {
         rec.ran = ran; rec.changed = changed_rules; rec.nnz_after = after;
@@ -454,7 +528,7 @@ void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out,
       rec.ran = ran; rec.changed = changed_rules; rec.nnz_after = after;
       if (trace) trace->push_back(rec);
       removed_prev2 = removed_prev;
-      removed_prev = before - after;
+      removed_prev = before_count.value - after;
       for (int g = 0; g < kGatedRules; ++g)
         if (ran >> g & 1u) { last_ran[g] = round; last_changed[g] = (changed_rules >> g & 1u) != 0; }
       ++round;

@@ -239,6 +239,12 @@ void capture_absolute_value(Record& r, AbsValueRecovery&& step);
 void capture_variable_pair(Record& r, VarPairRecovery&& step);
 
 // rules_*.cu
+// The first-stage detections of the first four Cleanup rules at once, with
+// one readback: returns the kProbe* bits of `rules` whose rule may change the
+// plan.  A rule whose bit comes back clear would return at its first check
+// without changing anything, as long as the plan is the probed one.
+constexpr uint32_t kProbeFixed = 1, kProbeEmptyColumns = 2, kProbeEmptyRows = 4, kProbeSingletonRows = 8;
+uint32_t cleanup_probe(const Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p, uint32_t rules);
 void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p);
 void rule_empty_columns(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);
 void rule_empty_rows(Plan& plan, const WorkingLp& lp, const Stats& s, const gpp_params& p);

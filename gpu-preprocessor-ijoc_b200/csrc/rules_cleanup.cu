@@ -228,6 +228,48 @@ double domain_objective(const double* contrib, const uint8_t* entry_keep, int32_
   return det_sum(masked.p, n, s);
 }
 
+uint32_t cleanup_probe(const Plan& plan, const WorkingLp& lp, const Stats& stats, const gpp_params& p, uint32_t rules) {
+  // The first-stage detections of the four rules below, on the current plan,
+  // with one readback.  Each is the kernel its rule launches first and writes
+  // only scratch and status words; a rule whose detection finds nothing
+  // (no candidate, no infeasibility) returns without touching the plan.
+  if (plan.has_infeasible || plan.has_unbounded) return rules;
+  const int n = lp.n(), m = lp.m();
+  auto s = ctx().stream;
+  Status st;
+  st.clear(16);
+  DBuf<uint8_t> fixed(size_t(std::max(n, 1)), s), remove(size_t(std::max(m, 1)), s);
+  DBuf<double> fval(size_t(std::max(n, 1)), s), contrib(size_t(std::max(n, 1)), s), radius(size_t(std::max(n, 1)), s);
+  DBuf<double> cl, cu;
+  if ((rules & kProbeFixed) && n > 0)
+    GPP_LAUNCH(fixed_candidates, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, plan.l.p, plan.u.p,
+               plan.c.p, p.bound_tol, fixed.p, fval.p, contrib.p, radius.p, st.d + 1);
+  if ((rules & kProbeEmptyColumns) && n > 0)
+    GPP_LAUNCH(empty_columns_classify, grid_stride_blocks(n), kThreads, 0, s, n, plan.keep_col.p, stats.empty_col.p,
+               plan.c.p, plan.l.p, plan.u.p, p.bound_tol, p.zero_tol, fixed.p, fval.p, contrib.p, st.d + 4);
+  if ((rules & kProbeEmptyRows) && m > 0)
+    GPP_LAUNCH(empty_rows_kernel, grid_stride_blocks(m), kThreads, 0, s, m, plan.keep_row.p, stats.row_nnz.p,
+               plan.AL.p, plan.AU.p, p.feasibility_tol, st.d + 8, 0);
+  if ((rules & kProbeSingletonRows) && m > 0) {
+    cl.alloc(size_t(std::max(n, 1)), s);
+    cu.alloc(size_t(std::max(n, 1)), s);
+    cl.copy_from(plan.l.p, size_t(n));
+    cu.copy_from(plan.u.p, size_t(n));
+    GPP_LAUNCH(singleton_row_bounds, grid_stride_blocks(m), kThreads, 0, s, m, n, plan.keep_row.p,
+               stats.singleton_row.p, stats.srow_col.p, stats.srow_val.p, plan.AL.p, plan.AU.p, p.zero_tol, cl.p,
+               cu.p, remove.p);
+    GPP_LAUNCH(singleton_rows_check, grid_stride_blocks(std::max(m, n)), kThreads, 0, s, m, n, cl.p, cu.p, plan.l.p,
+               plan.u.p, remove.p, p.bound_tol, st.d + 12);
+  }
+  const int32_t* f = st.read(16);
+  uint32_t act = 0;
+  if ((rules & kProbeFixed) && n > 0 && f[1] != 0) act |= kProbeFixed;
+  if ((rules & kProbeEmptyColumns) && n > 0 && (f[4] | f[5] | f[6]) != 0) act |= kProbeEmptyColumns;
+  if ((rules & kProbeEmptyRows) && m > 0 && (f[8] | f[9]) != 0) act |= kProbeEmptyRows;
+  if ((rules & kProbeSingletonRows) && m > 0 && (f[12] | f[13] | f[14]) != 0) act |= kProbeSingletonRows;
+  return act;
+}
+
 void rule_fixed_variables(Plan& plan, const WorkingLp& lp, const gpp_params& p) {
   if (plan.has_infeasible || plan.has_unbounded) return;
   const int n = lp.n(), m = lp.m();
