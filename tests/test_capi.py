@@ -59,3 +59,6 @@ def test_no_device_fails_loudly():
     st = lib.gpp_preprocess(C.byref(lp), C.byref(p), C.byref(s))
     assert st == 5
     assert b"no CUDA device" in lib.gpp_last_error()
+    # Loading a host LP (A^T is built on the device) has no host fallback either.
+    host = capi.HostLp()
+    assert lib.gpp_lp_from_host(C.byref(host), C.byref(lp)) == 5
