@@ -405,6 +405,7 @@ def main():
                     help="LPs in the batched-form measurement (0 skips it); sharded over the ranks when N > 1")
     ap.add_argument("--batch-max-workers", type=int, default=32)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule measurement")
+    ap.add_argument("--no-qap", action="store_true", help="skip the QAP N=30 measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference GPU library on the same LP")
     ap.add_argument("--kernel-table-out", default=None,
@@ -661,6 +662,39 @@ def main():
         learned_pool.close()
         learned_pool.join()
 
+    # QAP N = 30 (Adams-Johnson linearisation, 1,674,960 rows x 810,900
+    # columns): the structured workload of the parallel row / column rules and
+    # of folding.  Presolve time, whether folding applies and the sizes, with
+    # the reference GPU library on the same LP beside it.
+    def qap_measurement():
+        qlp = lpgen.workload("qap30", seed=0)
+        qd = device.DeviceLp(qlp)
+        reps = max(3, min(args.steps, 5))
+        times = []
+        for it in range(2 + reps):
+            s = device.preprocess(qd, params)
+            if it >= 2:
+                times.append(1e3 * s.elapsed_seconds)
+            if it == 0:
+                res = device.Result(s, copy_lp=True, copy_tape=False)
+                point = [np.clip(np.zeros(s.reduced_cols), res.l, res.u), np.zeros(s.reduced_rows),
+                         np.zeros(s.reduced_cols)]
+                info = {"folding_applied": bool(s.folding_applied), "folded": [s.folded_rows, s.folded_cols],
+                        "reduced": {"rows": s.reduced_rows, "cols": s.reduced_cols, "nnz": s.reduced_nnz,
+                                    "iterations": s.iterations}}
+            device.free_summary(s)
+        pre = statistics.mean(times)
+        out = {"workload": "QAP N=30, Adams-Johnson linearisation (lpgen.qap_lp), seed 0", "rows": qlp.m,
+               "cols": qlp.n, "nnz": qlp.nnz, "presolve_ms": round(pre, 3), **info,
+               "timing": f"presolve elapsed_seconds, mean of {reps} runs after 2 warm-up"}
+        if not args.no_reference_gpu:
+            ref = reference_gpu(qlp, point, reps, 2, pre, 1.0)
+            out["reference_gpu"] = {k: ref[k] for k in ("presolve_ms", "reduced", "presolve_speedup", "unavailable")
+                                    if k in ref}
+        return out
+
+    qap = optional(qap_measurement) if rank == 0 and not args.no_qap else None
+
     batched = None
     if batch_result is not None:
         gloo = dist.new_group(backend="gloo") if world > 1 else None
@@ -696,6 +730,7 @@ def main():
             "cpu_baseline": cpu,
             "batched": batched,
             "learned_schedule": learned,
+            "qap30": qap,
             "clocks": clk,
         }))
     if world > 1:
