@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <cstring>
@@ -37,6 +38,16 @@ struct LengthError : std::length_error {
 inline void check(cudaError_t e, const char* ctx) {
   if (e != cudaSuccess) throw CudaError(std::string(ctx) + ": " + cudaGetErrorString(e));
 }
+
+// An NVTX range over a scope (a presolve, a rule, a materialisation, a
+// postsolve), for profilers that show them (ncu --nvtx); without a profiler
+// attached the calls return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Kernel launch counter (per host thread) for the benchmark's launch report.
 uint64_t& launch_counter();

@@ -117,6 +117,7 @@ struct Engine {
   template <class F>
   bool deferred_rule(bool enabled, const char* name, F rule) {
     if (!enabled || terminal) return false;
+    const NvtxRange range(name);
     prepare();
     refresh();
     entry_cols.copy_from(plan.keep_col.p, size_t(cur.n()));
@@ -159,6 +160,7 @@ struct Engine {
 
   // apply_plan_to_working_lp (gpu_presolve.cu:1953-2072).
   void apply(Plan& pl, bool cleanup_captured) {
+    const NvtxRange range("materialize");
     Record& r = out.record;
     const int m = cur.m(), n = cur.n();
     // The old -> new maps' kept counts also tell whether the plan removes
@@ -245,6 +247,7 @@ struct Engine {
   template <class F>
   bool materialized_rule(bool enabled, const char* name, F rule) {
     if (!enabled || terminal) return false;
+    const NvtxRange range(name);
     Plan pl;
     init_plan(pl);
     rule(pl);
@@ -276,6 +279,7 @@ bool good_progress(int64_t before, int64_t after, int64_t d) { return before >= 
 
 void run_presolve(const gpp_lp& input, const gpp_params& p, PresolveOutput& out, SchedulePolicy* policy,
                   std::vector<RoundRecord>* trace) {
+  const NvtxRange range("presolve");
   Engine e(p, out);
   WorkingLp& cur = e.cur;
   cur.A = DevCsr{input.A.rows, input.A.cols, input.A.nnz, input.A.rowPtr, input.A.colVal, input.A.nzVal};

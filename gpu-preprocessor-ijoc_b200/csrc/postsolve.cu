@@ -707,6 +707,7 @@ void restore_absolute_value(double* x, const AbsValueRecovery& r, const double* 
 
 void run_postsolve(const PresolveOutput& out, const double* x_red, const double* y_red, const double* z_red,
                    const gpp_lp* original, double* x, double* y, double* z, const double* lower) {
+  const NvtxRange range("postsolve");
   if (!lower && original) lower = original->l;
   auto st = ctx().stream;
   const Record& r = out.record;
